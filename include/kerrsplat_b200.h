@@ -1,0 +1,119 @@
+/*
+ * kerrsplat_b200.h -- C ABI of libkerrsplat_b200.so, the B200 (sm_100a) render hot path of
+ * KerrSplat: per-pixel geodesic constants sorted by radial root case, the fused Recurrence(M)
+ * geodesic march (Jacobi addition-theorem recurrence for r and theta, anchored Mino-time
+ * quadrature for t~ and phi) and the transport consumers folded over it.
+ *
+ * Conventions (all entry points):
+ *   - every call returns an int status (KS_OK = 0); nothing throws across the ABI, and
+ *     ks_last_error(ctx) holds a one-line message for the last failure;
+ *   - calls are synchronous: they return after the device work is complete;
+ *   - array arguments may be host or device pointers (the library asks the CUDA runtime which);
+ *     host arrays are staged through the library's own device buffers;
+ *   - the library owns the per-ray constants, the anchor table and its scratch buffers; the
+ *     caller owns inputs and outputs;
+ *   - a context is not thread-safe: one context per host thread, or external locking.
+ *
+ * Each declaration cites the reference (KerrSplat.jl) entry point it replaces, by file:line
+ * within the reference project.
+ */
+#ifndef KERRSPLAT_B200_H
+#define KERRSPLAT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define KS_OK 0
+#define KS_ERR_ARGUMENT 1         /* bad size or argument (reference: ArgumentError / DimensionMismatch) */
+#define KS_ERR_NOT_REGENERATED 2  /* render before ks_regenerate (reference: cache.jl:203) */
+#define KS_ERR_OUT_OF_MEMORY 3
+#define KS_ERR_NONFINITE 4        /* NaN/Inf in an input */
+#define KS_ERR_DEVICE 5           /* CUDA error */
+#define KS_ERR_TIMEOUT 6          /* a bounded device wait gave up */
+
+/* precision of a render */
+#define KS_FP64 0   /* the plain FP64 path: one re-march per (frame, frequency), like the reference */
+#define KS_MIXED 1  /* FP32 march and transport re-anchored to the FP64 anchor table */
+
+/* output order */
+#define KS_ORDER_SORTED 0   /* root-case-sorted slots (the reference's fused_march! output) */
+#define KS_ORDER_SCREEN 1   /* camera order (the reference's to_screen/unsort, cache.jl:271-296) */
+
+/* splat parameter layouts (column-major nrows x nsplat) */
+#define KS_THIN14 0       /* Splats.jl:54 */
+#define KS_THERMAL21 1    /* polarized.jl:17-19 */
+#define KS_POWERLAW22 2   /* populations.jl:13-15 */
+#define KS_KAPPA22 3      /* populations.jl:24-26 */
+#define KS_KNOT21 4       /* trajectories.jl:80-88: THERMAL21 rows with centres from knots */
+
+typedef struct ks_context ks_context;
+
+/* One splat set of a scene (a Transfer model; several sets form a CompositeModel,
+ * transport.jl:348-358). */
+typedef struct ks_splat_set {
+    int32_t kind;              /* KS_THERMAL21, KS_POWERLAW22, KS_KAPPA22, KS_KNOT21 */
+    int32_t nsplat;
+    const double* params;      /* nrows(kind) x nsplat, column-major */
+    const double* hyp;         /* KS_KAPPA22: per-splat 2F1 factor (kappa.jl:97-100); else NULL */
+    const double* knots;       /* KS_KNOT21: 3 x nknots x nsplat knot centres; else NULL */
+    const double* knot_times;  /* KS_KNOT21: nknots increasing coordinate times */
+    int32_t nknots;
+    double gamma_max;          /* KS_POWERLAW22: gamma_max of the set (populations.jl:40) */
+} ks_splat_set;
+
+/* Context (the device-side GeodesicCache, cache.jl:85-125, without the Julia object). */
+int ks_context_create(int device, int flags, ks_context** out);
+int ks_context_destroy(ks_context* ctx);
+const char* ks_last_error(const ks_context* ctx);
+
+/* Camera (camera.jl:19-46 / GeodesicCache(backend, camera, Val(N)), cache.jl:106-125):
+ * npix screen points, screen shape (nalpha, nbeta) with nalpha * nbeta == npix. */
+int ks_camera_set(ks_context* ctx, const double* alpha, const double* beta, int64_t npix,
+                  int32_t nalpha, int32_t nbeta);
+
+/* regenerate!(cache, a, theta_o; marcher = Fused(M)) (cache.jl:153-180): root cases, the stable
+ * case sort (4, 2, 0 real roots), the FP64 per-ray constants and the FP64 anchor table of every
+ * ray for `nsamples` samples and anchor interval `anchor_M` (Recurrence(M)/Fused(M)). */
+int ks_regenerate(ks_context* ctx, double a, double theta_o, int32_t nsamples, int32_t anchor_M);
+
+/* cache.perm / cache.ranges (cache.jl:73-76, pixel_constants.jl:167-176): perm[j] is the screen
+ * index (0-based) of sorted slot j; ranges = {case2_begin, case2_end, case3_begin, case3_end,
+ * case4_begin, case4_end} as half-open 0-based slot ranges. */
+int ks_get_perm(ks_context* ctx, int64_t* perm);
+int ks_get_ranges(ks_context* ctx, int64_t ranges[6]);
+
+/* cache.residual_t / residual_phi (cache.jl:78-79): the largest |quadrature - anchor| of each ray
+ * in the last FP64 march (sorted order). */
+int ks_get_residuals(ks_context* ctx, double* resid_t, double* resid_phi);
+
+/* Per-ray constants in sorted order, npix x 24 rows (PixelConstants, pixel_constants.jl:29-54,
+ * with the march constants): eta, lambda, numreals, k, c, fo (I0_inf), tau_total, tau_valid,
+ * G_theta^o, r1..r4 (re, im), mu_theta, scale_theta, tempfac, offset_theta, M_anchor, 2K, scattering. */
+int ks_get_ray_constants(ks_context* ctx, double* out);
+
+/* Recurrence(M) stored mode (quadrature_march!, quadrature.jl:336-348): every sample of every ray,
+ * npix x nsamples arrays in sorted order; flags bit 0 ok, bit 1 nu_r, bit 2 nu_theta
+ * (direct_march.jl:14-17). */
+int ks_march_samples(ks_context* ctx, double* t, double* r, double* theta, double* phi, uint8_t* flags);
+
+/* thin_image!(out, cache, params, t_obs) (Splats.jl:137-140): optically-thin Stokes I of
+ * KS_THIN14 splats at one observation time; out[npix] in `order`. */
+int ks_thin_image(ks_context* ctx, const double* params, int32_t nsplat, double t_obs, int32_t precision,
+                  double* out, int32_t order);
+
+/* polarized_image! / polarized_cube (polarized.jl:160-198) over frames x frequencies:
+ * out has npix x 4 x nframes x nfreq doubles, index ((f_nu * nframes + f_t) * npix + pixel) * 4 + stokes,
+ * Stokes (I, Q, U, V) in cgs (observed_stokes, transport.jl:337), pixels in `order`.
+ * nmax >= 0 truncates rays after their nmax-th passage through |z| < slab (transport.jl:182-188). */
+int ks_render(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes,
+              const double* nus, int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab,
+              double* out, int32_t order);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KERRSPLAT_B200_H */

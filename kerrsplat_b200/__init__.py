@@ -1,0 +1,385 @@
+"""kerrsplat_b200 -- the B200 render hot path of KerrSplat behind the reference's interface.
+
+Python mirror of the reference's Geodesics/Splats API for this path (names follow the Julia
+functions without the `!`):
+
+    cam = Camera((-15, 15), (-15, 15), 128)             # camera.jl:19-46
+    cache = GeodesicCache(cam, 512)                      # cache.jl:106-125 (fused mode: no samples)
+    regenerate(cache, 0.94, np.deg2rad(17), marcher=Fused(64))   # cache.jl:153-180
+    img = thin_image(cache, params14, t_obs)             # Splats.jl:137-147
+    stokes = polarized_image(cache, PolarizedSplats(p21), t_obs, 230e9, L)   # polarized.jl:174-179
+    cube = polarized_cube(cache, PolarizedSplats(p21), times, nus, L)         # polarized.jl:187-198
+
+Every call runs on the GPU through libkerrsplat_b200.so (ctypes, include/kerrsplat_b200.h); there
+is no CPU fallback. Parameter matrices are (NROWS, nsplat) like the reference's column-major
+`p[row, i]`; numpy arrays, CPU tensors and CUDA tensors are accepted.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import KS_FP64, KS_MIXED, KsError
+
+__all__ = [
+    "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
+    "polarized_image", "polarized_cube", "render", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
+    "KS_FP64", "KS_MIXED", "KsError", "NU0",
+]
+
+# constants.jl:3-12 and coefficients.jl:299
+GNEWT, MSUN, CL, JY = 6.6742e-8, 1.989e33, 2.99792458e10, 1e-23
+NU0 = 1e11
+
+
+def gravitational_radius(M_solar):
+    """L = GM/c^2 in cm (transport.jl:58)."""
+    return GNEWT * M_solar * MSUN / (CL * CL)
+
+
+def pixel_solid_angle(dalpha, L, D):
+    """Solid angle of a square pixel of side `dalpha` M (transport.jl:125)."""
+    return (dalpha * L / D) ** 2
+
+
+def flux_density(img, dalpha, L, D):
+    """Flux density per pixel in Jy (polarized.jl:201)."""
+    return np.asarray(img) * (pixel_solid_angle(dalpha, L, D) / JY)
+
+
+class Camera:
+    """Bardeen screen (camera.jl:19-46): `Camera((amin, amax), (bmin, bmax), res)` builds Krang's
+    endpoint-inclusive grid in column-major order (alpha fastest); `Camera(alphas, betas)` is an
+    arbitrary point set of shape (npix, 1)."""
+
+    def __init__(self, a, b, res=None):
+        if res is None:
+            self.alpha = np.ascontiguousarray(a, dtype=np.float64).ravel()
+            self.beta = np.ascontiguousarray(b, dtype=np.float64).ravel()
+            if self.alpha.size != self.beta.size:
+                raise ValueError("camera pixel vectors do not match the screen size")
+            self.size = (self.alpha.size, 1)
+            return
+        na, nb = (res, res) if np.isscalar(res) else res
+        av = self.grid_axis(float(a[0]), float(a[1]), int(na))
+        bv = self.grid_axis(float(b[0]), float(b[1]), int(nb))
+        self.alpha = np.tile(av, nb)
+        self.beta = np.repeat(bv, na)
+        self.size = (int(na), int(nb))
+
+    @staticmethod
+    def grid_axis(lo, hi, n):
+        """camera.jl:123-124, evaluated the same way so that pixels agree bit for bit."""
+        if n == 1:
+            return np.array([lo])
+        return np.array([lo + (hi - lo) * (float(i) - 1.0) / (n - 1) for i in range(1, n + 1)])
+
+    @property
+    def npix(self):
+        return self.alpha.size
+
+
+class Fused:
+    """Fused(M): the march runs inside the consumer, re-anchored every M samples (cache.jl:57-61)."""
+
+    def __init__(self, M=64):
+        self.M = int(M)
+
+
+class Recurrence(Fused):
+    """Recurrence(M): the same march; stored samples are produced on demand by `cache.samples()`."""
+
+
+def _ptr(x):
+    """Device or host address of a contiguous float64 buffer (numpy array or torch tensor)."""
+    if hasattr(x, "data_ptr"):
+        return ctypes.c_void_p(x.data_ptr())
+    return ctypes.c_void_p(x.ctypes.data)
+
+
+def _as_f64(x):
+    if hasattr(x, "data_ptr"):
+        import torch
+        return x.to(torch.float64).contiguous()
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def _colmajor(p, nrows):
+    """(nrows, nsplat) parameter matrix -> contiguous buffer in column-major order."""
+    if hasattr(p, "data_ptr"):
+        import torch
+        if p.dim() != 2 or p.shape[0] != nrows:
+            raise ValueError(f"parameter matrix must be {nrows} x nsplat, got {tuple(p.shape)}")
+        return p.to(torch.float64).t().contiguous(), int(p.shape[1])
+    p = np.asarray(p, dtype=np.float64)
+    if p.ndim != 2 or p.shape[0] != nrows:
+        raise ValueError(f"parameter matrix must be {nrows} x nsplat, got {p.shape}")
+    return np.ascontiguousarray(p.T), int(p.shape[1])
+
+
+class GeodesicCache:
+    """Device-resident geodesic data for one camera and `nsamples` samples per ray (cache.jl:85-125):
+    the per-ray FP64 constants in root-case-sorted order, the permutation and case ranges, the FP64
+    anchor table, and the anchor residuals of the last FP64 march."""
+
+    def __init__(self, camera, nsamples, device=0):
+        if nsamples < 1:
+            raise ValueError("need at least one sample per ray")
+        self._lib = _lib.load()
+        ctx = ctypes.c_void_p()
+        st = self._lib.ks_context_create(int(device), 0, ctypes.byref(ctx))
+        if st != _lib.KS_OK:
+            raise KsError(st, f"cannot create a context on CUDA device {device} (status {st})")
+        self._ctx = ctx
+        self.nsamples = int(nsamples)
+        self.camera = None
+        self.spin = float("nan")
+        self.theta_o = float("nan")
+        self.generation = 0
+        self.marcher = None
+        self.set_camera(camera)
+
+    def _check(self, status):
+        _lib.check(status, self._ctx)
+
+    def set_camera(self, camera):
+        self.camera = camera
+        na, nb = camera.size
+        self._check(self._lib.ks_camera_set(self._ctx, _ptr(camera.alpha), _ptr(camera.beta), camera.npix, na, nb))
+        self.generation = 0
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.ks_context_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def npix(self):
+        return self.camera.npix
+
+    @property
+    def size(self):
+        return self.camera.size
+
+    @property
+    def perm(self):
+        """perm[j] = screen index (0-based) of sorted slot j."""
+        out = np.empty(self.npix, dtype=np.int64)
+        self._check(self._lib.ks_get_perm(self._ctx, _ptr(out)))
+        return out
+
+    @property
+    def ranges(self):
+        """Half-open sorted-slot ranges of the three root cases (4, 2, 0 real roots)."""
+        r = np.empty(6, dtype=np.int64)
+        self._check(self._lib.ks_get_ranges(self._ctx, _ptr(r)))
+        return {"case2": range(r[0], r[1]), "case3": range(r[2], r[3]), "case4": range(r[4], r[5])}
+
+    def residuals(self):
+        rt = np.empty(self.npix)
+        rp = np.empty(self.npix)
+        self._check(self._lib.ks_get_residuals(self._ctx, _ptr(rt), _ptr(rp)))
+        return rt, rp
+
+    def ray_constants(self):
+        """npix x 24 FP64 per-ray constants in sorted order (see ks_get_ray_constants)."""
+        out = np.empty((self.npix, 24))
+        self._check(self._lib.ks_get_ray_constants(self._ctx, _ptr(out)))
+        return out
+
+    def samples(self):
+        """Recurrence(M) stored mode (quadrature.jl:336-348): dict of (N, npix) arrays t, r, theta,
+        phi, flags in sorted order (the reference's (npix, N) column-major matrices)."""
+        N, n = self.nsamples, self.npix
+        t, r, th, ph = (np.empty((N, n)) for _ in range(4))
+        fl = np.empty((N, n), dtype=np.uint8)
+        self._check(self._lib.ks_march_samples(self._ctx, _ptr(t), _ptr(r), _ptr(th), _ptr(ph), _ptr(fl)))
+        return {"t": t, "r": r, "theta": th, "phi": ph, "flags": fl}
+
+    def kernel_stats(self, reset=False):
+        ms = ctypes.c_double()
+        kl = ctypes.c_longlong()
+        al = ctypes.c_longlong()
+        self._check(self._lib.ks_kernel_stats(self._ctx, ctypes.byref(ms), ctypes.byref(kl), ctypes.byref(al), int(reset)))
+        return ms.value, kl.value, al.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(self._lib.ks_context_stream(self._ctx, ctypes.byref(s)))
+        return s.value
+
+
+def regenerate(cache, a, theta_o, camera=None, marcher=None):
+    """regenerate!(cache, a, theta_o[, camera]; marcher) (cache.jl:153-180, 248-255)."""
+    if camera is not None:
+        if camera.npix != cache.npix:
+            raise ValueError(f"camera has {camera.npix} pixels, cache was built for {cache.npix}")
+        cache.set_camera(camera)
+    marcher = marcher or Fused(64)
+    cache._check(cache._lib.ks_regenerate(cache._ctx, float(a), float(theta_o), cache.nsamples, marcher.M))
+    cache.spin, cache.theta_o, cache.marcher = float(a), float(theta_o), marcher
+    cache.generation += 1
+    return cache
+
+
+def _precision(p):
+    if p in (KS_FP64, "fp64", "float64"):
+        return KS_FP64
+    if p in (KS_MIXED, "mixed", "fp32"):
+        return KS_MIXED
+    raise ValueError(f"unknown precision {p!r}")
+
+
+def _out_like(x, shape):
+    if hasattr(x, "data_ptr") and x.is_cuda:
+        import torch
+        return torch.empty(shape, dtype=torch.float64, device=x.device)
+    return np.empty(shape)
+
+
+def thin_image_sorted(cache, params, t_obs, precision=KS_FP64, out=None):
+    """thin_image!(out, cache, params, t_obs) (Splats.jl:137-140): sorted-order Stokes I."""
+    buf, ns = _colmajor(params, 14)
+    out = _out_like(buf, cache.npix) if out is None else out
+    cache._check(cache._lib.ks_thin_image(cache._ctx, _ptr(buf), ns, float(t_obs), _precision(precision), _ptr(out), _lib.KS_ORDER_SORTED))
+    return out
+
+
+def thin_image(cache, params, t_obs, precision=KS_FP64):
+    """Screen-shaped optically-thin image (Splats.jl:143-147): shape (nalpha, nbeta) in the
+    reference's column-major sense, i.e. img[i, j] is pixel i + j * nalpha."""
+    buf, ns = _colmajor(params, 14)
+    out = _out_like(buf, cache.npix)
+    cache._check(cache._lib.ks_thin_image(cache._ctx, _ptr(buf), ns, float(t_obs), _precision(precision), _ptr(out), _lib.KS_ORDER_SCREEN))
+    na, nb = cache.size
+    return out.reshape(nb, na).T if isinstance(out, np.ndarray) else out.reshape(nb, na).t()
+
+
+class _Model:
+    kind = None
+
+    def sets(self):
+        return [self]
+
+
+class PolarizedSplats(_Model):
+    """Thermal splats, 21 rows (polarized.jl:17-19, 41-49)."""
+    kind = _lib.KS_THERMAL21
+
+    def __init__(self, params):
+        self.params, self.nsplat = _colmajor(params, 21)
+
+
+class PowerLawSplats(_Model):
+    """Power-law splats, 22 rows, common gamma_max (populations.jl:34-41)."""
+    kind = _lib.KS_POWERLAW22
+
+    def __init__(self, params, gamma_max=1e5):
+        self.params, self.nsplat = _colmajor(params, 22)
+        self.gamma_max = float(gamma_max)
+
+
+def kappa_hypergeometric(kappa, w):
+    """2F1(kappa - 1/3, kappa + 1, kappa + 2/3, -kappa w), host side (kappa.jl:97-100)."""
+    import mpmath
+    return float(mpmath.hyp2f1(kappa - 1.0 / 3, kappa + 1.0, kappa + 2.0 / 3, -kappa * w))
+
+
+class KappaSplats(_Model):
+    """kappa splats, 22 rows; the hypergeometric factors are computed on the host
+    (populations.jl:50-60)."""
+    kind = _lib.KS_KAPPA22
+
+    def __init__(self, params, hyp=None):
+        self.params, self.nsplat = _colmajor(params, 22)
+        if hyp is None:
+            hp = np.asarray(params if not hasattr(params, "cpu") else params.cpu().numpy(), dtype=np.float64)
+            hyp = [kappa_hypergeometric(hp[13, i], np.exp(hp[14, i])) for i in range(hp.shape[1])]
+        self.hyp = np.ascontiguousarray(hyp, dtype=np.float64)
+
+
+class CompositeModel(_Model):
+    """Union of models (transport.jl:348-358): the elements of `a` followed by those of `b`."""
+
+    def __init__(self, *models):
+        self.models = models
+
+    def sets(self):
+        out = []
+        for m in self.models:
+            out.extend(m.sets())
+        return out
+
+
+def _set_array(model):
+    sets = model.sets()
+    arr = (_lib.SplatSetC * max(1, len(sets)))()
+    keep = []
+    for i, m in enumerate(sets):
+        arr[i].kind = m.kind
+        arr[i].nsplat = m.nsplat
+        arr[i].params = _ptr(m.params).value
+        hyp = getattr(m, "hyp", None)
+        arr[i].hyp = _ptr(hyp).value if hyp is not None else None
+        arr[i].knots = None
+        arr[i].knot_times = None
+        arr[i].nknots = 0
+        arr[i].gamma_max = getattr(m, "gamma_max", 1e5)
+        keep.append(m)
+    return arr, len(sets), keep
+
+
+def render(cache, model, times, nus, L, nmax=-1, slab=0.0, precision=KS_FP64, order="screen", out=None):
+    """Stokes (I, Q, U, V) in cgs for every (frame, frequency): array (nfreq, nframes, npix, 4) in
+    screen (camera) or sorted order. One GPU call (ks_render)."""
+    times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+    nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+    nt, nf = int(times.shape[0]), int(nus.shape[0])
+    arr, nsets, _keep = _set_array(model)
+    if out is None:
+        out = _out_like(model.sets()[0].params if nsets else times, (nf, nt, cache.npix, 4))
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_render(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision),
+                                      int(nmax), float(slab), _ptr(out), o))
+    return out
+
+
+def polarized_image(cache, model, t_obs, nu, L, nmax=-1, slab=0.0, precision=KS_FP64):
+    """Screen-shaped Stokes image (polarized.jl:174-179): shape (nalpha, nbeta, 4) in cgs."""
+    if not isinstance(model, _Model):
+        model = PolarizedSplats(model)
+    out = render(cache, model, [t_obs], [nu], L, nmax=nmax, slab=slab, precision=precision)
+    na, nb = cache.size
+    return np.asarray(out).reshape(nb, na, 4).transpose(1, 0, 2)
+
+
+def polarized_cube(cache, model, times, nus, L, nmax=-1, slab=0.0, precision=KS_FP64):
+    """Stokes movie cube (polarized.jl:187-198): shape (nalpha, nbeta, ntimes, nfreq, 4)."""
+    if not isinstance(model, _Model):
+        model = PolarizedSplats(model)
+    out = np.asarray(render(cache, model, times, nus, L, nmax=nmax, slab=slab, precision=precision))
+    nf, nt = out.shape[0], out.shape[1]
+    na, nb = cache.size
+    return out.reshape(nf, nt, nb, na, 4).transpose(3, 2, 1, 0, 4)
+
+
+def unsort(cache, x):
+    """Sorted-order rows -> screen order (cache.jl:271-286)."""
+    x = np.asarray(x)
+    y = np.empty_like(x)
+    y[cache.perm] = x
+    return y
+
+
+def to_screen(cache, x):
+    """unsort followed by the screen reshape (cache.jl:293-296)."""
+    y = unsort(cache, x)
+    na, nb = cache.size
+    return y.reshape((nb, na) + y.shape[1:]).swapaxes(0, 1)

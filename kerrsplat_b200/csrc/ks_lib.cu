@@ -1,0 +1,1043 @@
+// ks_lib.cu -- libkerrsplat_b200.so: the kernels of the render hot path and the C ABI of
+// include/kerrsplat_b200.h.
+//
+// Pipeline of one context (the device-side GeodesicCache of cache.jl:85-125):
+//   ks_regenerate: k_root_case (K0, screen order) -> stable radix sort by root case (4, 2, 0 real
+//     roots; cub, deterministic) -> k_build_plan (K1: FP64 per-ray constants, sorted order) ->
+//     exclusive scan of anchor counts -> k_anchor_segments (one thread per (ray, anchor): Jacobi
+//     states, validity, closed-form parts and the Gauss-Legendre integral of the smooth part since
+//     the previous anchor) -> k_anchor_prefix (per-ray running sums).
+//   ks_thin_image / ks_render: k_splat_table (per-splat FP64 constants) -> k_thin / k_polarized
+//     (one thread per ray, the fused march with the consumer folded over the samples) -> k_unsort.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/kerrsplat_b200.h"
+#include "ks_transfer.cuh"
+
+using namespace ks;
+
+__constant__ MomentCoeffs c_moments;
+
+namespace {
+
+constexpr int kBlock = 128;
+
+// ---- kernels: regenerate ---------------------------------------------------------------------------
+
+__global__ void k_root_case(Spacetime st, const double* __restrict__ alpha, const double* __restrict__ beta, long long npix,
+                            unsigned char* __restrict__ key, long long* __restrict__ idx) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    RayC R = build_ray(st, alpha[i], beta[i]);
+    key[i] = (unsigned char)(4 - R.numreals);   // 4 real roots first (pixel_constants.jl:167-176)
+    idx[i] = i;
+}
+
+__device__ __forceinline__ MarchRay<double> march_ray_of(const RayC& R, const Spacetime& st, double dtau) {
+    MarchRay<double> M;
+    M.rcase = R.rcase; M.k = R.k; M.c = R.c; M.fo = R.fo; M.fo_d = R.fo;
+    M.m0 = R.map[0]; M.m1 = R.map[1]; M.m2 = R.map[2]; M.m3 = R.map[3];
+    M.tau_valid = R.tau_valid; M.dtau = dtau;
+    M.pmu = R.pmu; M.pscale = R.pscale; M.tempfac = R.tempfac; M.poffset = R.poffset; M.sqrt_up = R.sqrt_up;
+    M.um = R.um; M.up_m_um = R.up_m_um; M.psign = R.psign; M.vortical = R.vortical; M.scattering = R.scattering;
+    M.a = st.a; M.lam = R.lam; M.eta = R.eta; M.rp = st.rp; M.rmn = st.rmn; M.sp = R.sp; M.sm = R.sm;
+    M.Qt = R.Qt; M.Qtm = R.Qtm; M.Qphi = R.Qphi; M.Qphim = R.Qphim; M.r4 = R.r4; M.qC = R.qC; M.qn = R.qn;
+    M.sqrt_eps = R.sqrt_eps; M.gc = R.gc; M.mp = R.mp; M.K2 = R.K2;
+    M.vabsalpha = R.vabsalpha; M.valpha2 = R.valpha2; M.vabsbeta = R.vabsbeta; M.vabscos = st.abscos; M.vcos2 = st.cos2;
+    return M;
+}
+
+__device__ __forceinline__ JS<double> xr_at(const RayC& R, double tau) { return jstate(R.c * (R.fo - tau), R.k); }
+__device__ __forceinline__ JS<double> xt_at(const RayC& R, double tau) { return jstate(R.pscale * (tau + R.poffset) / R.tempfac, R.pmu); }
+
+__global__ void k_build_plan(Spacetime st, const double* __restrict__ alpha, const double* __restrict__ beta,
+                             const long long* __restrict__ perm, long long npix, long long npad, double* __restrict__ f,
+                             long long* __restrict__ nanch_out) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    long long i = perm[j];
+    RayC R = build_ray(st, alpha[i], beta[i]);
+    auto put = [&](int field, double v) { f[field * npad + j] = v; };
+    double dtau = R.tau_total / (st.N + 1);
+    double h = dtau / 2.0;
+    int Man = anchor_interval(st.M, 1.0 - R.k);
+    int nanch = (st.N - 1) / Man + 1;
+    put(PF_ALPHA, R.alpha); put(PF_BETA, R.beta); put(PF_ETA, R.eta); put(PF_LAM, R.lam);
+    put(PF_NUMREALS, R.numreals); put(PF_CASE, R.rcase);
+    put(PF_K, R.k); put(PF_C, R.c); put(PF_FO, R.fo);
+    put(PF_MAP0, R.map[0]); put(PF_MAP1, R.map[1]); put(PF_MAP2, R.map[2]); put(PF_MAP3, R.map[3]);
+    put(PF_TAU_VALID, R.tau_valid); put(PF_TAU_TOTAL, R.tau_total); put(PF_DTAU, dtau);
+    put(PF_PMU, R.pmu); put(PF_PSCALE, R.pscale); put(PF_TEMPFAC, R.tempfac); put(PF_POFFSET, R.poffset);
+    put(PF_SQRTUP, R.sqrt_up); put(PF_UM, R.um); put(PF_UPMUM, R.up_m_um); put(PF_PSIGN, R.psign);
+    put(PF_VORTICAL, R.vortical ? 1.0 : 0.0); put(PF_GTHO, R.gtho);
+    put(PF_SP, R.sp); put(PF_SM, R.sm); put(PF_QT, R.Qt); put(PF_QTM, R.Qtm); put(PF_QPHI, R.Qphi); put(PF_QPHIM, R.Qphim);
+    put(PF_R4, R.r4); put(PF_SCATTER, R.scattering ? 1.0 : 0.0);
+    put(PF_QC, R.qC); put(PF_QN, R.qn); put(PF_SQRTEPS, R.sqrt_eps); put(PF_GC, R.gc); put(PF_MP, R.mp); put(PF_K2, R.K2);
+    put(PF_VABSALPHA, R.vabsalpha); put(PF_VALPHA2, R.valpha2); put(PF_VABSBETA, R.vabsbeta);
+    JS<double> dr = jstep_constants(-R.c * h, R.k);
+    JS<double> dth = jstep_constants(R.pscale * h / R.tempfac, R.pmu);
+    put(PF_DR_SN, dr.sn); put(PF_DR_CN, dr.cn); put(PF_DR_DN, dr.dn);
+    put(PF_DTH_SN, dth.sn); put(PF_DTH_CN, dth.cn); put(PF_DTH_DN, dth.dn);
+    // the interval that holds the radial turning point of a scattering ray (quadrature.jl:269)
+    int turn_k = -1;
+    if (R.scattering) {
+        for (int k = 2; k <= st.N; ++k) {
+            double ta = (k - 1) * dtau, tb = k * dtau;
+            if (ta < R.fo && R.fo < tb) { turn_k = k; break; }
+        }
+    }
+    put(PF_TURN_K, turn_k);
+    if (turn_k > 0) {
+        double ta = (turn_k - 1) * dtau, tb = turn_k * dtau;
+        JS<double> a1 = xr_at(R, (ta + R.fo) / 2.0), b1 = xt_at(R, (ta + R.fo) / 2.0);
+        JS<double> a2 = xr_at(R, (R.fo + tb) / 2.0), b2 = xt_at(R, (R.fo + tb) / 2.0);
+        JS<double> pt = xt_at(R, R.fo);
+        put(PF_P1R_SN, a1.sn); put(PF_P1R_CN, a1.cn); put(PF_P1R_DN, a1.dn);
+        put(PF_P1T_SN, b1.sn); put(PF_P1T_CN, b1.cn); put(PF_P1T_DN, b1.dn);
+        put(PF_P2R_SN, a2.sn); put(PF_P2R_CN, a2.cn); put(PF_P2R_DN, a2.dn);
+        put(PF_P2T_SN, b2.sn); put(PF_P2T_CN, b2.cn); put(PF_P2T_DN, b2.dn);
+        put(PF_PTT_SN, pt.sn); put(PF_PTT_CN, pt.cn); put(PF_PTT_DN, pt.dn);
+    } else {
+        for (int q = PF_P1R_SN; q <= PF_PTT_DN; ++q) put(q, 0.0);
+    }
+    put(PF_MANCHOR, Man); put(PF_NANCH, nanch);
+    put(PF_R1RE, R.rre[0]); put(PF_R1IM, R.rim[0]); put(PF_R2RE, R.rre[1]); put(PF_R2IM, R.rim[1]);
+    put(PF_R3RE, R.rre[2]); put(PF_R3IM, R.rim[2]); put(PF_R4RE, R.rre[3]); put(PF_R4IM, R.rim[3]);
+    nanch_out[j] = nanch;
+}
+
+// The smooth integrands at tau from direct Jacobi states, the t part in its large-r form past r = 64.
+__device__ __forceinline__ void anchor_integrand(const RayC& R, const MarchRay<double>& M, double tau, double& gt, double& gp) {
+    JS<double> xr = xr_at(R, tau), xt = xt_at(R, tau);
+    Point<double> p = ray_point(M, xr, xt, tau);
+    gt = p.gt; gp = p.gphi;
+    double r = p.r, a = M.a, lam = M.lam;
+    double P = r * r + a * a - a * lam;
+    if (r > 64.0 && P > 0.0) {
+        double D = r * r - 2.0 * r + a * a;
+        double Qv = M.eta + (lam - a) * (lam - a);
+        double as = fabs(p.s);
+        double diff = D * Qv / (P + as) * (1.0 + 2.0 / r) + 2.0 * (2.0 * r - a * a) * P / (r * D);
+        double s2 = 1.0 - p.cth * p.cth;
+        double wp = p.s * M.rp / (r * (r - M.rp)) / M.sp;
+        double wm = p.s * M.rmn / (r * (r - M.rmn)) / M.sm;
+        gt = diff + a * (lam - a * s2) - M.Qt * wp - M.Qtm * wm;
+    }
+}
+
+__constant__ double c_gl_x[16];
+__constant__ double c_gl_w[16];
+
+__device__ void gl_panel(const RayC& R, const MarchRay<double>& M, double ta, double tb, double& It, double& Ip) {
+    double mid = 0.5 * (ta + tb), half = 0.5 * (tb - ta);
+    double st = 0.0, sp = 0.0;
+    for (int i = 0; i < 16; ++i) {
+        double gt, gp;
+        anchor_integrand(R, M, mid + half * c_gl_x[i], gt, gp);
+        st += c_gl_w[i] * gt; sp += c_gl_w[i] * gp;
+    }
+    It = half * st; Ip = half * sp;
+}
+
+constexpr int kAnchorPanelSamples = 4;
+
+__global__ void k_anchor_segments(Spacetime st, const double* __restrict__ alpha, const double* __restrict__ beta,
+                                  const long long* __restrict__ perm, long long npix, long long npad, const double* __restrict__ f,
+                                  const long long* __restrict__ aoff, double* __restrict__ anchors) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int m = blockIdx.y;
+    if (j >= npix) return;
+    int nanch = int(f[PF_NANCH * npad + j]);
+    if (m >= nanch) return;
+    long long i = perm[j];
+    RayC R = build_ray(st, alpha[i], beta[i]);
+    int Man = int(f[PF_MANCHOR * npad + j]);
+    double dtau = f[PF_DTAU * npad + j];
+    MarchRay<double> M = march_ray_of(R, st, dtau);
+    int k = 1 + m * Man;
+    double tau = k * dtau;
+    double* A = anchors + (aoff[j] + m) * AF_COUNT;
+    JS<double> xr = xr_at(R, tau), xt = xt_at(R, tau);
+    A[AF_XR_SN] = xr.sn; A[AF_XR_CN] = xr.cn; A[AF_XR_DN] = xr.dn;
+    A[AF_XT_SN] = xt.sn; A[AF_XT_CN] = xt.cn; A[AF_XT_DN] = xt.dn;
+    double th, cth; bool nu;
+    polar_cos(M, xt, th, cth, nu);
+    bool ok = (tau <= R.tau_valid) && visible(M, cth);
+    A[AF_OK] = ok ? 1.0 : 0.0;
+    A[AF_PAD] = 0.0;
+    if (!(tau <= R.tau_valid)) {
+        A[AF_T] = 0.0; A[AF_PHI] = 0.0; A[AF_SEG_T] = 0.0; A[AF_SEG_PHI] = 0.0;
+        return;
+    }
+    // closed-form parts at tau, accumulated from the observer
+    Point<double> p = ray_point(M, xr, xt, tau);
+    double r = p.r;
+    double F = r + 2.0 * log(r);
+    double L = (R.scattering && tau > R.fo) ? F - 2.0 * (R.r4 + 2.0 * log(R.r4)) : -F;
+    double lp = log((r - st.rp) / r) / R.sp;
+    double lm = log((r - st.rmn) / r) / R.sm;
+    JS<double> x0 = xt_at(R, 0.0);
+    double sn0 = x0.sn / (R.pscale * x0.dn), cn0 = x0.cn / x0.dn;
+    A[AF_T] = L + R.Qt * lp + R.Qtm * lm;
+    A[AF_PHI] = R.Qphi * lp + R.Qphim * lm + polar_closed(M, tau, p.sn, p.cn) - polar_closed(M, 0.0, sn0, cn0);
+    // smooth part over (previous anchor, tau]
+    double ta = (m == 0) ? 0.0 : (1 + (m - 1) * Man) * dtau;
+    int nsamp = (m == 0) ? 1 : Man;
+    int np = (m == 0) ? 1 : (nsamp + kAnchorPanelSamples - 1) / kAnchorPanelSamples;
+    double hp = (tau - ta) / np;
+    double It = 0.0, Ip = 0.0;
+    for (int q = 0; q < np; ++q) {
+        double a0 = ta + q * hp, b0 = (q == np - 1) ? tau : ta + (q + 1) * hp;
+        double t1, p1;
+        if (R.scattering && a0 < R.fo && R.fo < b0) {
+            gl_panel(R, M, a0, R.fo, t1, p1); It += t1; Ip += p1;
+            gl_panel(R, M, R.fo, b0, t1, p1); It += t1; Ip += p1;
+        } else {
+            gl_panel(R, M, a0, b0, t1, p1); It += t1; Ip += p1;
+        }
+    }
+    A[AF_SEG_T] = It; A[AF_SEG_PHI] = Ip;
+}
+
+__global__ void k_anchor_prefix(long long npix, long long npad, const double* __restrict__ f, const long long* __restrict__ aoff,
+                                double* __restrict__ anchors) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    int nanch = int(f[PF_NANCH * npad + j]);
+    double st = 0.0, sp = 0.0;
+    for (int m = 0; m < nanch; ++m) {
+        double* A = anchors + (aoff[j] + m) * AF_COUNT;
+        st += A[AF_SEG_T]; sp += A[AF_SEG_PHI];
+        A[AF_T] += st; A[AF_PHI] += sp;
+    }
+}
+
+// ---- kernels: splat tables ---------------------------------------------------------------------------
+
+// K0 and K1 from K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt by the trapezoidal rule.
+__host__ __device__ void besselk01(double x, double& k0, double& k1) {
+    const double h = 0.125;
+    double s0 = 0.5 * exp(-x), s1 = 0.5 * exp(-x);
+    for (int j = 1; j < 4000; ++j) {
+        double t = j * h;
+        double e = exp(-x * cosh(t));
+        if (e == 0.0) break;
+        s0 += e; s1 += e * cosh(t);
+        if (e < 1e-300) break;
+    }
+    k0 = h * s0; k1 = h * s1;
+}
+
+struct SetDesc {
+    int kind, nrows, nsplat, first;   // first = index of its first splat in the concatenated table
+    const double* params;
+    const double* hyp;
+    double gmax;
+};
+
+__global__ void k_splat_table(SetDesc d, double* __restrict__ tab) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d.nsplat) return;
+    const double* p = d.params + (long long)d.nrows * i;
+    double* o = tab + (long long)(d.first + i) * ST_COUNT;
+    for (int q = 0; q < ST_COUNT; ++q) o[q] = 0.0;
+    o[ST_KIND] = d.kind;
+    o[ST_CX] = p[0]; o[ST_CY] = p[1]; o[ST_CZ] = p[2];
+    o[ST_T0] = p[10]; o[ST_OMEGA] = p[d.nrows - 1];
+    o[ST_ES1] = exp(-p[3]); o[ST_ES2] = exp(-p[4]); o[ST_ES3] = exp(-p[5]);
+    double q1 = p[6], q2 = p[7], q3 = p[8], q4 = p[9];
+    double n = sqrt(q1 * q1 + q2 * q2 + q3 * q3 + q4 * q4);
+    double w = q1 / n, x = q2 / n, y = q3 / n, z = q4 / n;
+    o[ST_R0] = 1 - 2 * (y * y + z * z); o[ST_R1] = 2 * (x * y - w * z); o[ST_R2] = 2 * (x * z + w * y);
+    o[ST_R3] = 2 * (x * y + w * z); o[ST_R4] = 1 - 2 * (x * x + z * z); o[ST_R5] = 2 * (y * z - w * x);
+    o[ST_R6] = 2 * (x * z - w * y); o[ST_R7] = 2 * (y * z + w * x); o[ST_R8] = 1 - 2 * (x * x + y * y);
+    o[ST_INVW] = exp(-p[11]);
+    double smax = fmax(p[3], fmax(p[4], p[5]));
+    o[ST_SUPP] = (-2.0 * log(kWEIGHT_CUTOFF)) * exp(2 * smax);
+    if (d.kind == KS_THIN14) { o[ST_LOGA] = p[12]; return; }
+    o[ST_NE] = exp(p[12]);
+    double Bmag, thB, phB, u1, u2, u3;
+    if (d.kind == KS_THERMAL21 || d.kind == KS_KNOT21) {
+        double Te = exp(p[13]);
+        o[ST_TE] = Te;
+        double k0, k1;
+        besselk01(1.0 / Te, k0, k1);
+        double xb = 1.0 / Te;
+        double k2 = k0 + 2.0 * k1 / xb;
+        o[ST_F0] = k2 > 0 ? k0 / k2 : 1.0;
+        o[ST_KR] = k2 > 0 ? k1 / k2 : 1.0;
+        Bmag = exp(p[14]); thB = p[15]; phB = p[16]; u1 = p[17]; u2 = p[18]; u3 = p[19];
+    } else {
+        Bmag = exp(p[15]); thB = p[16]; phB = p[17]; u1 = p[18]; u2 = p[19]; u3 = p[20];
+        if (d.kind == KS_POWERLAW22) {
+            double pp = p[13], gmin = exp(p[14]);
+            o[ST_P] = pp; o[ST_GMIN] = gmin; o[ST_GMAX] = d.gmax;
+            o[ST_GSPAN] = pow(gmin, 1 - pp) - pow(d.gmax, 1 - pp);
+            o[ST_GAMJ] = tgamma((3 * pp - 1) / 12) * tgamma((3 * pp + 19) / 12);
+            o[ST_GAMA] = tgamma((3 * pp + 2) / 12) * tgamma((3 * pp + 22) / 12);
+        } else {
+            double kap = p[13], wk = exp(p[14]);
+            o[ST_KAP] = kap; o[ST_W] = wk; o[ST_HYP] = d.hyp ? d.hyp[i] : 0.0;
+            o[ST_G43] = tgamma(kap - 4.0 / 3); o[ST_G2] = tgamma(kap - 2);
+            o[ST_GQ] = tgamma(kap / 4 - 1.0 / 3); o[ST_GP] = tgamma(kap / 4 + 4.0 / 3);
+            o[ST_GK2] = tgamma(2 + kap / 2);
+            double k0, k1;
+            besselk01(1.0 / wk, k0, k1);
+            double xb = 1.0 / wk;
+            double k2 = k0 + 2.0 * k1 / xb;
+            o[ST_KB] = k0 / (k2 + 1e-40);
+        }
+    }
+    double B[3] = {Bmag * sin(thB) * cos(phB), Bmag * sin(thB) * sin(phB), Bmag * cos(thB)};
+    double Bn = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    o[ST_BMAG] = Bmag;
+    if (Bn > 0) { o[ST_BHX] = B[0] / Bn; o[ST_BHY] = B[1] / Bn; o[ST_BHZ] = B[2] / Bn; o[ST_BZERO] = 0.0; }
+    else { o[ST_BHX] = 0; o[ST_BHY] = 0; o[ST_BHZ] = 1; o[ST_BZERO] = 1.0; }
+    o[ST_U1] = u1; o[ST_U2] = u2; o[ST_U3] = u3;
+}
+
+// ---- kernels: the fused march with its consumers -----------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ void ks_coords(T a, T r, T th, T ph, T& x, T& y, T& z, T& sth, T& cth) {
+    T temp = sqrt(T(1) - a * a);
+    T rp = T(1) + temp, rm = T(1) - temp;
+    T phks = ph + a / (T(2) * temp) * log(fabs((r - rp + keps<T>()) / (r - rm + keps<T>()))) - atan2(a, r);
+    sth = sin(th); cth = cos(th);
+    T sp = sin(phks), cp = cos(phks);
+    x = r * sth * cp; y = r * sth * sp; z = r * cth;
+}
+
+struct StoreSink {
+    double *t, *r, *th, *ph; unsigned char* fl;
+    long long npix, j;
+    __device__ void operator()(int k, const Sample<double>& s) {
+        long long q = (long long)(k - 1) * npix + j;
+        t[q] = s.t; r[q] = s.r; th[q] = s.theta; ph[q] = s.phi;
+        fl[q] = (s.ok ? 1 : 0) | (s.nur ? 2 : 0) | (s.nutheta ? 4 : 0);
+    }
+};
+
+__global__ void k_march_store(PlanView P, Spacetime st, long long npix, double* t, double* r, double* th, double* ph,
+                              unsigned char* fl, double* resid_t, double* resid_phi) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    MarchRay<double> R = load_ray<double>(P, st, j);
+    StoreSink sink{t, r, th, ph, fl, npix, j};
+    double rt, rp;
+    march(P, st, j, R, sink, rt, rp);
+    resid_t[j] = rt; resid_phi[j] = rp;
+}
+
+// ThinRenderer (Splats.jl:113-128)
+template <class T>
+struct ThinSink {
+    const T* tab; int nsplat; T t_obs; T a, rh_lo; T dtau; T acc;
+    T eta, lam;
+    __device__ void operator()(int, const Sample<T>& s) {
+        if (!(s.ok && rh_lo < s.r && s.r < T(1e3))) return;
+        T x, y, z, sth, cth;
+        ks_coords(a, s.r, s.theta, s.phi, x, y, z, sth, cth);
+        T t = t_obs - s.t;
+        T jt = T(0);
+        for (int i = 0; i < nsplat; ++i) {
+            const T* p = tab + i * ST_COUNT;
+            T q;
+            splat_exponent(p, t, x, y, z, false, q);
+            jt += exp(p[ST_LOGA] - q);
+        }
+        SampleFrame<T> F = sample_frame(a, s.r, s.theta, sth, cth, eta, lam, s.nur, s.nutheta);
+        T g = T(1) / F.pz[0];
+        T Sg = s.r * s.r + a * a * cth * cth;
+        acc += g * g * jt * Sg * dtau;
+    }
+};
+
+template <class T>
+__global__ void k_thin(PlanView P, Spacetime st, long long npix, const double* __restrict__ tab64, int nsplat, double t_obs,
+                       double* __restrict__ out, double* __restrict__ resid_t, double* __restrict__ resid_phi) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* tab = reinterpret_cast<T*>(smem);
+    for (int q = threadIdx.x; q < nsplat * ST_COUNT; q += blockDim.x) tab[q] = T(tab64[q]);
+    __syncthreads();
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    MarchRay<T> R = load_ray<T>(P, st, j);
+    ThinSink<T> sink{tab, nsplat, T(t_obs), T(st.a), T(st.rh * (1 + 1e-3)), T(R.dtau), T(0), R.eta, R.lam};
+    double rt, rp;
+    march(P, st, j, R, sink, rt, rp);
+    out[j] = double(sink.acc);
+    if (resid_t) { resid_t[j] = rt; resid_phi[j] = rp; }
+}
+
+// RadiativeTransport over a concatenated splat table (transport.jl:171-198, polarized.jl:121-150,
+// populations.jl:70-104), CH (t_obs, nu) combinations per thread sharing the march.
+template <class T, int CH>
+struct PolSink {
+    const T* tab; int ntot;
+    T t_obs[CH], nu[CH], nuh[CH], Lnu[CH];
+    int nc;
+    T a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
+    int nmax;
+    T P[CH][16], S[CH][4];
+    T zprev; int wn; bool inside, crossed, zset;
+
+    __device__ void init() {
+        for (int c = 0; c < CH; ++c) {
+            for (int q = 0; q < 16; ++q) P[c][q] = (q % 5 == 0) ? T(1) : T(0);
+            for (int q = 0; q < 4; ++q) S[c][q] = T(0);
+        }
+        wn = 0; inside = false; crossed = false; zset = false; zprev = T(0);
+    }
+
+    __device__ void wind(T z) {   // step.jl:379-398
+        if (!zset) { zprev = z; zset = true; inside = fabs(z) < slab; crossed = false; return; }
+        bool inside_now = fabs(z) < slab;
+        bool crossing = zprev * z < T(0);
+        if (inside || inside_now) {
+            crossed = crossed || crossing;
+            if (inside && !inside_now) { if (crossed) wn += 1; crossed = false; }
+            else if (!inside && inside_now) { crossed = crossing; }
+            inside = inside_now;
+        } else if (crossing) {
+            wn += 1;
+        }
+        zprev = z;
+    }
+
+    __device__ void operator()(int, const Sample<T>& s) {
+        if (!(s.ok && s.r > rh_lo)) return;
+        if (nmax >= 0) {
+            wind(s.r * cos(s.theta));
+            if (wn > nmax) return;
+        }
+        T x, y, z, sth, cth;
+        ks_coords(a, s.r, s.theta, s.phi, x, y, z, sth, cth);
+        T j4[CH][4], a4[CH][4], r3[CH][3];
+        bool active[CH];
+        for (int c = 0; c < CH; ++c) {
+            active[c] = false;
+            for (int q = 0; q < 4; ++q) { j4[c][q] = T(0); a4[c][q] = T(0); }
+            for (int q = 0; q < 3; ++q) r3[c][q] = T(0);
+        }
+        bool have_frame = false;
+        SampleFrame<T> F;
+        for (int i = 0; i < ntot; ++i) {
+            const T* p = tab + i * ST_COUNT;
+            const int kind = int(p[ST_KIND]);
+            bool fr_done = false;
+            LFrame<T> lf;
+            for (int c = 0; c < CH; ++c) {
+                if (c >= nc) break;
+                T t = t_obs[c] - s.t;
+                T q;
+                if (!splat_exponent(p, t, x, y, z, kind != KS_KNOT21, q)) continue;
+                T G = exp(-q);
+                if (!(G > T(kWEIGHT_CUTOFF))) continue;
+                if (!have_frame) { F = sample_frame(a, s.r, s.theta, sth, cth, eta, lam, s.nur, s.nutheta); have_frame = true; }
+                if (!fr_done) {
+                    lf = local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != T(0),
+                                     alpha, beta, a_sin_tho);
+                    fr_done = true;
+                }
+                T nuf = nu[c] / lf.g;
+                T thb = acos(fmin(T(1), fmax(T(-1), lf.cosB)));
+                T ne = p[ST_NE] * G;
+                Coef<T> cf;
+                if (kind == KS_POWERLAW22)
+                    cf = powerlaw(ne, p[ST_P], p[ST_GMIN], p[ST_GSPAN], p[ST_GAMJ], p[ST_GAMA], p[ST_BMAG], nuf, thb);
+                else if (kind == KS_KAPPA22)
+                    cf = kappa(ne, p[ST_KAP], p[ST_W], p[ST_HYP], p[ST_G43], p[ST_G2], p[ST_GQ], p[ST_GP], p[ST_GK2], p[ST_KB], p[ST_BMAG], nuf, thb);
+                else
+                    cf = thermal(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
+                // screen_coefficients (transport.jl:265-270): cap, invariants at nu/g, rotate by 2 chi
+                if (!(cf.jI > T(0) || cf.aI > T(0) || cf.rQ != T(0) || cf.rV != T(0))) continue;
+                T fe = cap_factor(cf.jI, cf.jQ, cf.jV, T(0.99));
+                T fa = cap_factor(cf.aI, cf.aQ, cf.aV, T(0.99));
+                T nh = nuf / T(kNU0);
+                T i2 = T(1) / (nh * nh);
+                T s2c = sin(T(2) * lf.chi), c2c = cos(T(2) * lf.chi);
+                T jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+                j4[c][0] += cf.jI * i2; j4[c][1] += jQ * c2c; j4[c][2] += jQ * s2c; j4[c][3] += cf.jV * fe * i2;
+                a4[c][0] += nh * cf.aI; a4[c][1] += aQ * c2c; a4[c][2] += aQ * s2c; a4[c][3] += cf.aV * fa * nh;
+                r3[c][0] += rQ * c2c; r3[c][1] += rQ * s2c; r3[c][2] += nh * cf.rV;
+                active[c] = true;
+            }
+        }
+        T Sg = s.r * s.r + a * a * cos(s.theta) * cos(s.theta);
+        for (int c = 0; c < CH; ++c) {
+            if (c >= nc || !active[c]) continue;
+            T Dl = Lnu[c] * Sg * dtau;
+            T O[16], E[4];
+            transfer_step(c_moments, j4[c], a4[c], r3[c], Dl, O, E);
+            // advance (step.jl:347): S += P E, P = P O
+            T Pn[16];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                S[c][r] += P[c][4 * r] * E[0] + P[c][4 * r + 1] * E[1] + P[c][4 * r + 2] * E[2] + P[c][4 * r + 3] * E[3];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    Pn[4 * r + q] = P[c][4 * r] * O[q] + P[c][4 * r + 1] * O[4 + q] + P[c][4 * r + 2] * O[8 + q] + P[c][4 * r + 3] * O[12 + q];
+            }
+#pragma unroll
+            for (int q = 0; q < 16; ++q) P[c][q] = Pn[q];
+        }
+    }
+};
+
+template <class T, int CH>
+__global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, long long npix, const double* __restrict__ tab64, int ntot,
+                                                      const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L,
+                                                      int nmax, double slab, double* __restrict__ out, double* __restrict__ resid_t,
+                                                      double* __restrict__ resid_phi) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* tab = reinterpret_cast<T*>(smem);
+    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = T(tab64[q]);
+    __syncthreads();
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    const int c0 = blockIdx.y * CH;
+    MarchRay<T> R = load_ray<T>(P, st, j);
+    PolSink<T, CH> sink;
+    sink.tab = tab; sink.ntot = ntot;
+    sink.nc = min(CH, ncombo - c0);
+    for (int c = 0; c < CH; ++c) {
+        int cc = min(c0 + c, ncombo - 1);
+        sink.t_obs[c] = T(ct[cc]); sink.nu[c] = T(cnu[cc]);
+        double nh = cnu[cc] / kNU0;
+        sink.nuh[c] = T(nh);
+        sink.Lnu[c] = T(L / nh);
+    }
+    sink.a = T(st.a); sink.rh_lo = T(st.rh * (1 + 1e-3)); sink.dtau = T(R.dtau);
+    sink.alpha = T(P.get(PF_ALPHA, j)); sink.beta = T(P.get(PF_BETA, j)); sink.eta = R.eta; sink.lam = R.lam;
+    sink.a_sin_tho = T(st.a * sin(st.thetao)); sink.slab = T(slab); sink.nmax = nmax;
+    sink.init();
+    double rt, rp;
+    march(P, st, j, R, sink, rt, rp);
+    for (int c = 0; c < CH; ++c) {
+        if (c >= sink.nc) break;
+        double n3 = double(sink.nuh[c]) * double(sink.nuh[c]) * double(sink.nuh[c]);
+        double* o = out + ((long long)(c0 + c) * npix + j) * 4;
+        o[0] = double(sink.S[c][0]) * n3; o[1] = double(sink.S[c][1]) * n3;
+        o[2] = double(sink.S[c][2]) * n3; o[3] = double(sink.S[c][3]) * n3;
+    }
+    if (blockIdx.y == 0 && resid_t) { resid_t[j] = rt; resid_phi[j] = rp; }
+}
+
+// sorted slot -> output order, for `nvec` blocks of npix rows of `width` doubles
+__global__ void k_unsort(const double* __restrict__ src, const long long* __restrict__ perm, long long npix, int width, int nvec,
+                         int to_screen, double* __restrict__ dst) {
+    long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long total = npix * nvec;
+    if (q >= total) return;
+    long long v = q / npix, j = q % npix;
+    long long dj = to_screen ? perm[j] : j;
+    for (int w = 0; w < width; ++w) dst[(v * npix + dj) * width + w] = src[(v * npix + j) * width + w];
+}
+
+}  // namespace
+
+// ---- the context ----------------------------------------------------------------------------------------
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr; n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) n = bytes;
+        return e;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    template <class U> U* as() const { return reinterpret_cast<U*>(p); }
+};
+
+struct ks_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long npix = 0, npad = 0;
+    int nalpha = 0, nbeta = 0;
+    bool regenerated = false;
+    Spacetime st{};
+    DevBuf alpha, beta, key, key2, idx, perm, plan, nanch, aoff, anchors, resid_t, resid_phi, scratch;
+    DevBuf tab, combos, out_sorted, stage_in, stage_out;
+    long long total_anchors = 0;
+    int max_nanch = 0;
+    long long ranges[6] = {0, 0, 0, 0, 0, 0};
+    // timing of the render kernels (CUDA events on the context stream)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double kernel_ms = 0.0;
+    long long kernel_launches = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+int fail(ks_context* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+int cuda_fail(ks_context* c, cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) return fail(c, KS_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    return fail(c, KS_ERR_DEVICE, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define KS_CUDA(ctx, call)                                            \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);    \
+    } while (0)
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Make `src` (host or device, `bytes`) available on the device: returns the device pointer.
+int stage_in(ks_context* c, DevBuf& buf, const void* src, size_t bytes, const void** dev) {
+    if (is_device_ptr(src)) { *dev = src; return KS_OK; }
+    KS_CUDA(c, buf.ensure(bytes));
+    KS_CUDA(c, cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    *dev = buf.p;
+    return KS_OK;
+}
+
+void init_constants() {
+    MomentCoeffs mc;
+    for (int n = 0; n < 10; ++n) {
+        double fact = 1.0;
+        for (int m = 0; m < 24; ++m) {
+            if (m > 0) fact *= m;
+            mc.c[n][m] = ((m % 2) ? -1.0 : 1.0) / (fact * (n + m + 1));
+            mc.cf[n][m] = float(mc.c[n][m]);
+        }
+    }
+    cudaMemcpyToSymbol(c_moments, &mc, sizeof mc);
+    // 16-point Gauss-Legendre nodes on [-1, 1] (Newton on P_16)
+    double x[16], w[16];
+    const int n = 16;
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(kPi * (i + 0.75) / (n + 0.5)), dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p1 = 1.0, p2 = 0.0;
+            for (int jj = 1; jj <= n; ++jj) { double p3 = p2; p2 = p1; p1 = ((2.0 * jj - 1.0) * z * p2 - (jj - 1.0) * p3) / jj; }
+            dp = n * (z * p1 - p2) / (z * z - 1.0);
+            double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-17) break;
+        }
+        double p1 = 1.0, p2 = 0.0;
+        for (int jj = 1; jj <= n; ++jj) { double p3 = p2; p2 = p1; p1 = ((2.0 * jj - 1.0) * z * p2 - (jj - 1.0) * p3) / jj; }
+        dp = n * (z * p1 - p2) / (z * z - 1.0);
+        x[i] = z; w[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+    }
+    cudaMemcpyToSymbol(c_gl_x, x, sizeof x);
+    cudaMemcpyToSymbol(c_gl_w, w, sizeof w);
+}
+
+unsigned nblocks(long long n, int b = kBlock) { return unsigned((n + b - 1) / b); }
+
+PlanView plan_view(ks_context* c) {
+    PlanView P;
+    P.f = c->plan.as<double>(); P.npad = c->npad; P.anchors = c->anchors.as<double>(); P.anchor_off = c->aoff.as<long long>();
+    return P;
+}
+
+int nrows_of(int kind) {
+    switch (kind) {
+        case KS_THIN14: return 14;
+        case KS_THERMAL21: case KS_KNOT21: return 21;
+        case KS_POWERLAW22: case KS_KAPPA22: return 22;
+        default: return -1;
+    }
+}
+
+// Write `nvec` x npix x width doubles from the sorted device buffer to `out` (host or device) in `order`.
+int emit(ks_context* c, const double* sorted, int width, int nvec, int order, double* out) {
+    size_t bytes = size_t(c->npix) * width * nvec * sizeof(double);
+    bool dev = is_device_ptr(out);
+    double* dst = out;
+    if (!dev) { KS_CUDA(c, c->stage_out.ensure(bytes)); dst = c->stage_out.as<double>(); }
+    long long total = c->npix * nvec;
+    k_unsort<<<nblocks(total), kBlock, 0, c->stream>>>(sorted, c->perm.as<long long>(), c->npix, width, nvec,
+                                                       order == KS_ORDER_SCREEN ? 1 : 0, dst);
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    if (!dev) KS_CUDA(c, cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return KS_OK;
+}
+
+}  // namespace
+
+// ---- C ABI -------------------------------------------------------------------------------------------
+
+extern "C" {
+
+int ks_context_create(int device, int flags, ks_context** out) {
+    (void)flags;
+    if (!out) return KS_ERR_ARGUMENT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) { cudaGetLastError(); return KS_ERR_DEVICE; }
+    if (cudaSetDevice(device) != cudaSuccess) return KS_ERR_DEVICE;
+    ks_context* c = new ks_context();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return KS_ERR_DEVICE; }
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+    init_constants();
+    if (cudaGetLastError() != cudaSuccess) { delete c; return KS_ERR_DEVICE; }
+    *out = c;
+    return KS_OK;
+}
+
+int ks_context_destroy(ks_context* c) {
+    if (!c) return KS_OK;
+    cudaSetDevice(c->device);
+    for (DevBuf* b : {&c->alpha, &c->beta, &c->key, &c->key2, &c->idx, &c->perm, &c->plan, &c->nanch, &c->aoff, &c->anchors,
+                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out})
+        b->release();
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return KS_OK;
+}
+
+const char* ks_last_error(const ks_context* c) { return c ? c->err.c_str() : "null context"; }
+
+int ks_context_stream(ks_context* c, void** stream) {
+    if (!c || !stream) return KS_ERR_ARGUMENT;
+    *stream = (void*)c->stream;
+    return KS_OK;
+}
+
+// Accumulated device time of the render kernels (k_thin / k_polarized) since the last reset, and
+// the number of launches of this library's kernels.
+int ks_kernel_stats(ks_context* c, double* render_ms, long long* render_launches, long long* all_launches, int reset) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (render_ms) *render_ms = c->kernel_ms;
+    if (render_launches) *render_launches = c->kernel_launches;
+    if (all_launches) *all_launches = c->launches;
+    if (reset) { c->kernel_ms = 0.0; c->kernel_launches = 0; c->launches = 0; }
+    return KS_OK;
+}
+
+int ks_camera_set(ks_context* c, const double* alpha, const double* beta, int64_t npix, int32_t nalpha, int32_t nbeta) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (!alpha || !beta || npix <= 0) return fail(c, KS_ERR_ARGUMENT, "camera needs at least one pixel");
+    if ((long long)nalpha * nbeta != npix) return fail(c, KS_ERR_ARGUMENT, "camera pixel vectors do not match the screen size");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    std::vector<double> ha(npix), hb(npix);
+    KS_CUDA(c, cudaMemcpy(ha.data(), alpha, npix * sizeof(double), cudaMemcpyDefault));
+    KS_CUDA(c, cudaMemcpy(hb.data(), beta, npix * sizeof(double), cudaMemcpyDefault));
+    for (long long i = 0; i < npix; ++i)
+        if (!std::isfinite(ha[i]) || !std::isfinite(hb[i])) return fail(c, KS_ERR_NONFINITE, "non-finite screen coordinate at pixel %lld", i);
+    c->npix = npix;
+    c->npad = (npix + 31) / 32 * 32;
+    c->nalpha = nalpha; c->nbeta = nbeta;
+    KS_CUDA(c, c->alpha.ensure(npix * sizeof(double)));
+    KS_CUDA(c, c->beta.ensure(npix * sizeof(double)));
+    KS_CUDA(c, cudaMemcpy(c->alpha.p, ha.data(), npix * sizeof(double), cudaMemcpyHostToDevice));
+    KS_CUDA(c, cudaMemcpy(c->beta.p, hb.data(), npix * sizeof(double), cudaMemcpyHostToDevice));
+    c->regenerated = false;
+    return KS_OK;
+}
+
+int ks_regenerate(ks_context* c, double a, double theta_o, int32_t nsamples, int32_t anchor_M) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (c->npix <= 0) return fail(c, KS_ERR_ARGUMENT, "set a camera before regenerate");
+    if (!std::isfinite(a) || !std::isfinite(theta_o)) return fail(c, KS_ERR_NONFINITE, "non-finite spin or inclination");
+    if (!(a > 0.0 && a < 1.0)) return fail(c, KS_ERR_ARGUMENT, "spin must lie in (0, 1) (the analytic polar solution divides by a)");
+    if (nsamples < 1) return fail(c, KS_ERR_ARGUMENT, "need at least one sample per ray");
+    if (anchor_M < 1) return fail(c, KS_ERR_ARGUMENT, "re-anchoring interval must be positive");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const long long n = c->npix, npad = c->npad;
+    Spacetime& st = c->st;
+    st.a = a; st.thetao = theta_o;
+    st.rp = 1.0 + std::sqrt(1.0 - a * a); st.rmn = 1.0 - std::sqrt(1.0 - a * a); st.rh = st.rp;
+    st.abscos = std::fabs(std::cos(theta_o)); st.cos2 = std::cos(theta_o) * std::cos(theta_o);
+    st.N = nsamples; st.M = anchor_M;
+    KS_CUDA(c, c->key.ensure(n)); KS_CUDA(c, c->key2.ensure(n));
+    KS_CUDA(c, c->idx.ensure(n * sizeof(long long))); KS_CUDA(c, c->perm.ensure(n * sizeof(long long)));
+    k_root_case<<<nblocks(n), kBlock, 0, c->stream>>>(st, c->alpha.as<double>(), c->beta.as<double>(), n, c->key.as<unsigned char>(),
+                                                        c->idx.as<long long>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    size_t tmp = 0;
+    KS_CUDA(c, cub::DeviceRadixSort::SortPairs(nullptr, tmp, c->key.as<unsigned char>(), c->key2.as<unsigned char>(),
+                                               c->idx.as<long long>(), c->perm.as<long long>(), (int)n, 0, 3, c->stream));
+    KS_CUDA(c, c->scratch.ensure(tmp));
+    KS_CUDA(c, cub::DeviceRadixSort::SortPairs(c->scratch.p, tmp, c->key.as<unsigned char>(), c->key2.as<unsigned char>(),
+                                               c->idx.as<long long>(), c->perm.as<long long>(), (int)n, 0, 3, c->stream));
+    KS_CUDA(c, c->plan.ensure(size_t(PF_COUNT) * npad * sizeof(double)));
+    KS_CUDA(c, c->nanch.ensure(n * sizeof(long long)));
+    KS_CUDA(c, c->aoff.ensure((n + 1) * sizeof(long long)));
+    k_build_plan<<<nblocks(n), kBlock, 0, c->stream>>>(st, c->alpha.as<double>(), c->beta.as<double>(), c->perm.as<long long>(), n, npad,
+                                                         c->plan.as<double>(), c->nanch.as<long long>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    tmp = 0;
+    KS_CUDA(c, cub::DeviceScan::ExclusiveSum(nullptr, tmp, c->nanch.as<long long>(), c->aoff.as<long long>(), (int)n, c->stream));
+    KS_CUDA(c, c->scratch.ensure(tmp));
+    KS_CUDA(c, cub::DeviceScan::ExclusiveSum(c->scratch.p, tmp, c->nanch.as<long long>(), c->aoff.as<long long>(), (int)n, c->stream));
+    // totals and case ranges
+    std::vector<long long> hn(n), ho(n);
+    std::vector<unsigned char> hk(n);
+    KS_CUDA(c, cudaMemcpyAsync(hn.data(), c->nanch.p, n * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    KS_CUDA(c, cudaMemcpyAsync(ho.data(), c->aoff.p, n * sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+    KS_CUDA(c, cudaMemcpyAsync(hk.data(), c->key2.p, n, cudaMemcpyDeviceToHost, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->total_anchors = ho[n - 1] + hn[n - 1];
+    c->max_nanch = 0;
+    for (long long j = 0; j < n; ++j) c->max_nanch = std::max<int>(c->max_nanch, (int)hn[j]);
+    long long cnt[3] = {0, 0, 0};
+    for (long long j = 0; j < n; ++j) cnt[hk[j] / 2]++;
+    c->ranges[0] = 0; c->ranges[1] = cnt[0];
+    c->ranges[2] = cnt[0]; c->ranges[3] = cnt[0] + cnt[1];
+    c->ranges[4] = cnt[0] + cnt[1]; c->ranges[5] = n;
+    KS_CUDA(c, c->anchors.ensure(size_t(c->total_anchors) * AF_COUNT * sizeof(double)));
+    dim3 grid(nblocks(n), c->max_nanch);
+    k_anchor_segments<<<grid, kBlock, 0, c->stream>>>(st, c->alpha.as<double>(), c->beta.as<double>(), c->perm.as<long long>(), n, npad,
+                                                       c->plan.as<double>(), c->aoff.as<long long>(), c->anchors.as<double>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    k_anchor_prefix<<<nblocks(n), kBlock, 0, c->stream>>>(n, npad, c->plan.as<double>(), c->aoff.as<long long>(), c->anchors.as<double>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, c->resid_t.ensure(n * sizeof(double)));
+    KS_CUDA(c, c->resid_phi.ensure(n * sizeof(double)));
+    KS_CUDA(c, cudaMemsetAsync(c->resid_t.p, 0, n * sizeof(double), c->stream));
+    KS_CUDA(c, cudaMemsetAsync(c->resid_phi.p, 0, n * sizeof(double), c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->regenerated = true;
+    return KS_OK;
+}
+
+int ks_get_perm(ks_context* c, int64_t* perm) {
+    if (!c || !perm) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    KS_CUDA(c, cudaMemcpy(perm, c->perm.p, c->npix * sizeof(long long), cudaMemcpyDefault));
+    return KS_OK;
+}
+
+int ks_get_ranges(ks_context* c, int64_t ranges[6]) {
+    if (!c || !ranges) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    for (int q = 0; q < 6; ++q) ranges[q] = c->ranges[q];
+    return KS_OK;
+}
+
+int ks_get_residuals(ks_context* c, double* rt, double* rp) {
+    if (!c || !rt || !rp) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    KS_CUDA(c, cudaMemcpy(rt, c->resid_t.p, c->npix * sizeof(double), cudaMemcpyDefault));
+    KS_CUDA(c, cudaMemcpy(rp, c->resid_phi.p, c->npix * sizeof(double), cudaMemcpyDefault));
+    return KS_OK;
+}
+
+int ks_get_ray_constants(ks_context* c, double* out) {
+    if (!c || !out) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    const long long n = c->npix, np = c->npad;
+    std::vector<double> f(size_t(PF_COUNT) * np);
+    KS_CUDA(c, cudaMemcpy(f.data(), c->plan.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<double> o(size_t(n) * 24);
+    const int fields[24] = {PF_ETA, PF_LAM, PF_NUMREALS, PF_K, PF_C, PF_FO, PF_TAU_TOTAL, PF_TAU_VALID, PF_GTHO,
+                            PF_R1RE, PF_R1IM, PF_R2RE, PF_R2IM, PF_R3RE, PF_R3IM, PF_R4RE, PF_R4IM,
+                            PF_PMU, PF_PSCALE, PF_TEMPFAC, PF_POFFSET, PF_MANCHOR, PF_K2, PF_SCATTER};
+    for (long long j = 0; j < n; ++j)
+        for (int q = 0; q < 24; ++q) o[size_t(j) * 24 + q] = f[size_t(fields[q]) * np + j];
+    KS_CUDA(c, cudaMemcpy(out, o.data(), o.size() * sizeof(double), cudaMemcpyDefault));
+    return KS_OK;
+}
+
+int ks_march_samples(ks_context* c, double* t, double* r, double* theta, double* phi, uint8_t* flags) {
+    if (!c || !t || !r || !theta || !phi || !flags) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const long long n = c->npix;
+    const size_t ns = size_t(n) * c->st.N;
+    KS_CUDA(c, c->stage_out.ensure(ns * (4 * sizeof(double) + 1)));
+    double* d = c->stage_out.as<double>();
+    unsigned char* fl = reinterpret_cast<unsigned char*>(d + 4 * ns);
+    k_march_store<<<nblocks(n), kBlock, 0, c->stream>>>(plan_view(c), c->st, n, d, d + ns, d + 2 * ns, d + 3 * ns, fl,
+                                                          c->resid_t.as<double>(), c->resid_phi.as<double>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, cudaMemcpyAsync(t, d, ns * sizeof(double), cudaMemcpyDefault, c->stream));
+    KS_CUDA(c, cudaMemcpyAsync(r, d + ns, ns * sizeof(double), cudaMemcpyDefault, c->stream));
+    KS_CUDA(c, cudaMemcpyAsync(theta, d + 2 * ns, ns * sizeof(double), cudaMemcpyDefault, c->stream));
+    KS_CUDA(c, cudaMemcpyAsync(phi, d + 3 * ns, ns * sizeof(double), cudaMemcpyDefault, c->stream));
+    KS_CUDA(c, cudaMemcpyAsync(flags, fl, ns, cudaMemcpyDefault, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KS_OK;
+}
+
+int ks_thin_image(ks_context* c, const double* params, int32_t nsplat, double t_obs, int32_t precision, double* out, int32_t order) {
+    if (!c || !out) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    if (nsplat < 0 || (nsplat > 0 && !params)) return fail(c, KS_ERR_ARGUMENT, "bad splat count or parameters");
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    if (!std::isfinite(t_obs)) return fail(c, KS_ERR_NONFINITE, "non-finite observation time");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const long long n = c->npix;
+    const void* dparams = nullptr;
+    if (nsplat > 0) {
+        int s = stage_in(c, c->stage_in, params, size_t(14) * nsplat * sizeof(double), &dparams);
+        if (s) return s;
+    }
+    KS_CUDA(c, c->tab.ensure(size_t(std::max(nsplat, 1)) * ST_COUNT * sizeof(double)));
+    if (nsplat > 0) {
+        SetDesc d{KS_THIN14, 14, nsplat, 0, (const double*)dparams, nullptr, 0.0};
+        k_splat_table<<<nblocks(nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
+    KS_CUDA(c, c->out_sorted.ensure(n * sizeof(double)));
+    size_t smem = size_t(nsplat) * ST_COUNT * (precision == KS_FP64 ? sizeof(double) : sizeof(float));
+    if (smem > 200 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", nsplat);
+    cudaEventRecord(c->ev0, c->stream);
+    if (precision == KS_FP64) {
+        KS_CUDA(c, cudaFuncSetAttribute(k_thin<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_thin<double><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, c->tab.as<double>(), nsplat, t_obs,
+                                                                 c->out_sorted.as<double>(), c->resid_t.as<double>(), c->resid_phi.as<double>());
+    } else {
+        KS_CUDA(c, cudaFuncSetAttribute(k_thin<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_thin<float><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, c->tab.as<double>(), nsplat, t_obs,
+                                                                c->out_sorted.as<double>(), nullptr, nullptr);
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    int s = emit(c, c->out_sorted.as<double>(), 1, 1, order, out);
+    if (s) return s;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->kernel_ms += ms; c->kernel_launches++;
+    return KS_OK;
+}
+
+int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+              int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, double* out, int32_t order) {
+    if (!c || !out) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    if (nsets < 0 || (nsets > 0 && !sets)) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
+    if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
+    if (!std::isfinite(slab)) return fail(c, KS_ERR_NONFINITE, "non-finite slab");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    std::vector<double> ht(nframes), hnu(nfreq);
+    KS_CUDA(c, cudaMemcpy(ht.data(), times, nframes * sizeof(double), cudaMemcpyDefault));
+    KS_CUDA(c, cudaMemcpy(hnu.data(), nus, nfreq * sizeof(double), cudaMemcpyDefault));
+    for (double v : ht) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite observation time");
+    for (double v : hnu) if (!(std::isfinite(v) && v > 0)) return fail(c, KS_ERR_NONFINITE, "frequencies must be finite and positive");
+    int ntot = 0;
+    for (int s = 0; s < nsets; ++s) {
+        int nr = nrows_of(sets[s].kind);
+        if (nr < 0 || sets[s].kind == KS_THIN14) return fail(c, KS_ERR_ARGUMENT, "set %d: unsupported kind %d", s, sets[s].kind);
+        if (sets[s].kind == KS_KNOT21) return fail(c, KS_ERR_ARGUMENT, "set %d: knot splats are not supported by ks_render yet", s);
+        if (sets[s].nsplat < 0 || (sets[s].nsplat > 0 && !sets[s].params)) return fail(c, KS_ERR_ARGUMENT, "set %d: bad parameters", s);
+        if (sets[s].kind == KS_KAPPA22 && sets[s].nsplat > 0 && !sets[s].hyp) return fail(c, KS_ERR_ARGUMENT, "set %d: kappa sets need hyp", s);
+        ntot += sets[s].nsplat;
+    }
+    const long long n = c->npix;
+    KS_CUDA(c, c->tab.ensure(size_t(std::max(ntot, 1)) * ST_COUNT * sizeof(double)));
+    int first = 0;
+    for (int s = 0; s < nsets; ++s) {
+        const ks_splat_set& S = sets[s];
+        if (S.nsplat == 0) continue;
+        int nr = nrows_of(S.kind);
+        const void* dp = nullptr;
+        const void* dh = nullptr;
+        // each set is staged into its own slice of the staging buffer
+        std::vector<double> hp(size_t(nr) * S.nsplat);
+        KS_CUDA(c, cudaMemcpy(hp.data(), S.params, hp.size() * sizeof(double), cudaMemcpyDefault));
+        for (double v : hp) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "set %d: non-finite parameter", s);
+        DevBuf tmp;
+        KS_CUDA(c, tmp.ensure(hp.size() * sizeof(double) + size_t(S.nsplat) * sizeof(double)));
+        KS_CUDA(c, cudaMemcpyAsync(tmp.p, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        dp = tmp.p;
+        if (S.kind == KS_KAPPA22) {
+            double* hd = tmp.as<double>() + hp.size();
+            KS_CUDA(c, cudaMemcpyAsync(hd, S.hyp, S.nsplat * sizeof(double), cudaMemcpyDefault, c->stream));
+            dh = hd;
+        }
+        SetDesc d{S.kind, nr, S.nsplat, first, (const double*)dp, (const double*)dh, S.gamma_max > 0 ? S.gamma_max : 1e5};
+        k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+        KS_CUDA(c, cudaStreamSynchronize(c->stream));
+        tmp.release();
+        first += S.nsplat;
+    }
+    const int ncombo = nframes * nfreq;
+    std::vector<double> hc(2 * size_t(ncombo));
+    for (int fv = 0; fv < nfreq; ++fv)
+        for (int ft = 0; ft < nframes; ++ft) {
+            hc[size_t(fv) * nframes + ft] = ht[ft];
+            hc[ncombo + size_t(fv) * nframes + ft] = hnu[fv];
+        }
+    KS_CUDA(c, c->combos.ensure(hc.size() * sizeof(double)));
+    KS_CUDA(c, cudaMemcpyAsync(c->combos.p, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    KS_CUDA(c, c->out_sorted.ensure(size_t(n) * 4 * ncombo * sizeof(double)));
+    const double* dct = c->combos.as<double>();
+    const double* dcn = dct + ncombo;
+    cudaEventRecord(c->ev0, c->stream);
+    if (precision == KS_FP64) {
+        // the plain path: one march per (frame, frequency), as the reference's polarized_cube does
+        size_t smem = size_t(ntot) * ST_COUNT * sizeof(double);
+        if (smem > 220 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
+        KS_CUDA(c, cudaFuncSetAttribute(k_polarized<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        for (int cc = 0; cc < ncombo; ++cc) {
+            k_polarized<double, 1><<<dim3(nblocks(n), 1), kBlock, smem, c->stream>>>(
+                plan_view(c), c->st, n, c->tab.as<double>(), ntot, dct + cc, dcn + cc, 1, L, nmax, slab,
+                c->out_sorted.as<double>() + size_t(cc) * n * 4, c->resid_t.as<double>(), c->resid_phi.as<double>());
+            c->launches++;
+            c->kernel_launches++;
+        }
+    } else {
+        size_t smem = size_t(ntot) * ST_COUNT * sizeof(float);
+        if (smem > 220 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
+        constexpr int CH = 4;
+        KS_CUDA(c, cudaFuncSetAttribute(k_polarized<float, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_polarized<float, CH><<<dim3(nblocks(n), (ncombo + CH - 1) / CH), kBlock, smem, c->stream>>>(
+            plan_view(c), c->st, n, c->tab.as<double>(), ntot, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), nullptr, nullptr);
+        c->launches++;
+        c->kernel_launches++;
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    KS_CUDA(c, cudaGetLastError());
+    int s = emit(c, c->out_sorted.as<double>(), 4, ncombo, order, out);
+    if (s) return s;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->kernel_ms += ms;
+    return KS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,288 @@
+// ks_march.cuh -- the fused Recurrence(M) march of one ray (quadrature.jl:231-296) in precision T,
+// reading the FP64 plan and anchor table built by regenerate.
+//
+// T = double is the plain FP64 port of the reference's march_ray, sample for sample. T = float is
+// the mixed path: the recurrence and the quadrature run in FP32 and are reset to the FP64 anchors
+// every M samples; the smooth t-integrand uses the cancellation-free large-r form there (its
+// r^2 terms would otherwise lose everything in FP32 at r ~ 1e4).
+#pragma once
+#include "ks_plan.cuh"
+
+namespace ks {
+
+template <class T>
+struct Sample {
+    T t, r, theta, cos_theta, phi;
+    bool nur, nutheta, ok;
+};
+
+template <class T>
+struct MarchRay {
+    int rcase;
+    T k, c, fo, m0, m1, m2, m3;
+    double tau_valid, dtau, fo_d;  // compared against sample times in FP64
+    T pmu, pscale, tempfac, poffset, sqrt_up, um, up_m_um, psign;
+    bool vortical, scattering;
+    T a, lam, eta, rp, rmn, sp, sm, Qt, Qtm, Qphi, Qphim, r4, qC, qn, sqrt_eps, gc, mp, K2;
+    T vabsalpha, valpha2, vabsbeta, vabscos, vcos2;
+    JS<T> dr, dth;
+    int turn_k, Manchor, nanch;
+    long long anchor_off;
+};
+
+struct PlanView {
+    const double* f;       // PF_COUNT arrays of stride npad
+    long long npad;
+    const double* anchors; // AF_COUNT doubles per anchor
+    const long long* anchor_off;
+    __device__ __forceinline__ double get(int field, long long j) const { return f[field * npad + j]; }
+};
+
+template <class T>
+__device__ __forceinline__ MarchRay<T> load_ray(const PlanView& P, const Spacetime& st, long long j) {
+    MarchRay<T> R;
+    R.rcase = int(P.get(PF_CASE, j));
+    R.k = T(P.get(PF_K, j)); R.c = T(P.get(PF_C, j)); R.fo = T(P.get(PF_FO, j));
+    R.m0 = T(P.get(PF_MAP0, j)); R.m1 = T(P.get(PF_MAP1, j)); R.m2 = T(P.get(PF_MAP2, j)); R.m3 = T(P.get(PF_MAP3, j));
+    R.tau_valid = P.get(PF_TAU_VALID, j); R.dtau = P.get(PF_DTAU, j); R.fo_d = P.get(PF_FO, j);
+    R.pmu = T(P.get(PF_PMU, j)); R.pscale = T(P.get(PF_PSCALE, j)); R.tempfac = T(P.get(PF_TEMPFAC, j));
+    R.poffset = T(P.get(PF_POFFSET, j)); R.sqrt_up = T(P.get(PF_SQRTUP, j)); R.um = T(P.get(PF_UM, j));
+    R.up_m_um = T(P.get(PF_UPMUM, j)); R.psign = T(P.get(PF_PSIGN, j));
+    R.vortical = P.get(PF_VORTICAL, j) != 0.0; R.scattering = P.get(PF_SCATTER, j) != 0.0;
+    R.a = T(st.a); R.lam = T(P.get(PF_LAM, j)); R.eta = T(P.get(PF_ETA, j)); R.rp = T(st.rp); R.rmn = T(st.rmn);
+    R.sp = T(P.get(PF_SP, j)); R.sm = T(P.get(PF_SM, j)); R.Qt = T(P.get(PF_QT, j)); R.Qtm = T(P.get(PF_QTM, j));
+    R.Qphi = T(P.get(PF_QPHI, j)); R.Qphim = T(P.get(PF_QPHIM, j)); R.r4 = T(P.get(PF_R4, j));
+    R.qC = T(P.get(PF_QC, j)); R.qn = T(P.get(PF_QN, j)); R.sqrt_eps = T(P.get(PF_SQRTEPS, j));
+    R.gc = T(P.get(PF_GC, j)); R.mp = T(P.get(PF_MP, j)); R.K2 = T(P.get(PF_K2, j));
+    R.vabsalpha = T(P.get(PF_VABSALPHA, j)); R.valpha2 = T(P.get(PF_VALPHA2, j)); R.vabsbeta = T(P.get(PF_VABSBETA, j));
+    R.vabscos = T(st.abscos); R.vcos2 = T(st.cos2);
+    R.dr = {T(P.get(PF_DR_SN, j)), T(P.get(PF_DR_CN, j)), T(P.get(PF_DR_DN, j))};
+    R.dth = {T(P.get(PF_DTH_SN, j)), T(P.get(PF_DTH_CN, j)), T(P.get(PF_DTH_DN, j))};
+    R.turn_k = int(P.get(PF_TURN_K, j));
+    R.Manchor = int(P.get(PF_MANCHOR, j));
+    R.nanch = int(P.get(PF_NANCH, j));
+    R.anchor_off = P.anchor_off[j];
+    return R;
+}
+
+// ---- per-sample geometry (recurrence.jl:169-308, quadrature.jl:110-215) ---------------------------
+
+template <class T> __device__ __forceinline__ T kpi();
+template <> __device__ __forceinline__ double kpi<double>() { return kPi; }
+template <> __device__ __forceinline__ float kpi<float>() { return 3.14159265358979323846f; }
+template <class T> __device__ __forceinline__ T keps();
+template <> __device__ __forceinline__ double keps<double>() { return kEps; }
+template <> __device__ __forceinline__ float keps<float>() { return 1.1920929e-7f; }
+
+template <class T>
+__device__ __forceinline__ T radius(const MarchRay<T>& R, const JS<T>& x) {
+    if (R.rcase == 2) {
+        T cn2 = R.m2 * x.cn * x.cn;
+        return (R.m1 * cn2 - R.m0 * R.m3) / (cn2 - R.m3);
+    } else if (R.rcase == 3) {
+        return (R.m0 + R.m1 * x.cn) / (R.m2 + R.m3 * x.cn);
+    }
+    T sc = x.sn / x.cn;
+    return -(R.m0 * (R.m2 - sc) / (T(1) + R.m2 * sc) + R.m1);
+}
+
+template <class T>
+__device__ __forceinline__ void polar_cos(const MarchRay<T>& R, const JS<T>& x, T& theta, T& cth, bool& nu) {
+    T snX = x.sn / (R.pscale * x.dn);
+    T c;
+    if (R.vortical) {
+        c = R.psign * sqrt(fmax(R.um + R.up_m_um * snX * snX, T(0)));
+        nu = R.psign * x.sn * x.cn > T(0);
+    } else {
+        c = R.psign * R.sqrt_up * snX;
+        nu = R.psign * x.cn > T(0);
+    }
+    c = fmin(T(1), fmax(T(-1), c));
+    cth = c;
+    theta = acos(c);
+}
+
+template <class T>
+__device__ __forceinline__ bool visible(const MarchRay<T>& R, T cths) {
+    if (!(cths > R.vabscos)) return true;
+    T c2 = cths * cths;
+    T s2 = T(1) - c2;
+    T amin = R.a * sqrt(s2);
+    if (!(R.vabsalpha >= amin + keps<T>())) return true;
+    T temp = (R.vcos2 - c2) * (R.valpha2 - R.a * R.a * s2) / (c2 - T(1));
+    T bb = sqrt(fmax(temp, T(0)));
+    return !(R.vabsbeta < bb);
+}
+
+template <class T>
+struct Point {
+    T r, theta, cth, s, sn, cn, gt, gphi;
+    bool nur, nuth;
+};
+
+template <class T>
+__device__ __forceinline__ void smooth(const MarchRay<T>& R, Point<T>& p, T dn) {
+    const T a = R.a, lam = R.lam, r = p.r, s = p.s;
+    T D = r * r - T(2) * r + a * a;
+    T s2 = T(1) - p.cth * p.cth;
+    T wp = s * R.rp / (r * (r - R.rp)) / R.sp;
+    T wm = s * R.rmn / (r * (r - R.rmn)) / R.sm;
+    T P = r * r + a * a - a * lam;
+    if constexpr (sizeof(T) == 4) {
+        if (r > T(64) && P > T(0)) {
+            // dt/dtau - |s|(1 + 2/r) without cancellation (see the anchor integrand)
+            T Qv = R.eta + (lam - a) * (lam - a);
+            T as = fabs(s);
+            T diff = D * Qv / (P + as) * (T(1) + T(2) / r) + T(2) * (T(2) * r - a * a) * P / (r * D);
+            p.gt = diff + a * (lam - a * s2) - R.Qt * wp - R.Qtm * wm;
+        } else {
+            T ft = (r * r + a * a) * P / D + a * (lam - a * s2);
+            p.gt = ft - fabs(s) * (T(1) + T(2) / r) - R.Qt * wp - R.Qtm * wm;
+        }
+    } else {
+        T ft = (r * r + a * a) * (r * r + a * a - a * lam) / D + a * (lam - a * s2);
+        p.gt = ft - fabs(s) * (T(1) + T(2) / r) - R.Qt * wp - R.Qtm * wm;
+    }
+    T fphi = a * (T(2) * r - a * lam) / D;
+    T gpol = lam * R.qC * (T(1) - R.gc * dn * (T(1) - R.mp * p.cn * p.cn / T(2))) / (T(1) - R.qn * p.sn * p.sn);
+    p.gphi = fphi - R.Qphi * wp - R.Qphim * wm + gpol;
+}
+
+template <class T>
+__device__ __forceinline__ T r_pot(const MarchRay<T>& R, T r) {
+    T P = r * r + R.a * R.a - R.a * R.lam;
+    T D = r * r - T(2) * r + R.a * R.a;
+    return P * P - D * (R.eta + (R.lam - R.a) * (R.lam - R.a));
+}
+
+template <class T>
+__device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<T>& xr, const JS<T>& xt, double tau) {
+    Point<T> p;
+    p.r = radius(R, xr);
+    polar_cos(R, xt, p.theta, p.cth, p.nuth);
+    p.nur = tau < R.fo_d;
+    p.s = (p.nur ? T(-1) : T(1)) * sqrt(fmax(r_pot(R, p.r), T(0)));
+    p.sn = xt.sn / (R.pscale * xt.dn);
+    p.cn = xt.cn / xt.dn;
+    smooth(R, p, T(1) / xt.dn);
+    return p;
+}
+
+template <class T>
+__device__ __forceinline__ Point<T> turning_point(const MarchRay<T>& R, const JS<T>& xt) {
+    Point<T> p;
+    p.r = R.r4;
+    polar_cos(R, xt, p.theta, p.cth, p.nuth);
+    p.nur = true;
+    p.s = T(0);
+    p.sn = xt.sn / (R.pscale * xt.dn);
+    p.cn = xt.cn / xt.dn;
+    smooth(R, p, T(1) / xt.dn);
+    return p;
+}
+
+template <class T>
+__device__ __forceinline__ T polar_closed(const MarchRay<T>& R, double tau, T sn, T cn) {
+    T X = (T(tau) + R.poffset) / R.tempfac;
+    T nw = floor((X + R.K2 / T(2)) / R.K2);
+    T A = (atan(R.sqrt_eps * sn / cn) + nw * kpi<T>()) / R.sqrt_eps;
+    T ph = atan(sn / cn) + nw * kpi<T>();
+    T e = R.sqrt_eps * R.sqrt_eps;
+    return R.lam * R.qC * R.tempfac * R.gc * ((T(1) + R.mp * e / (T(2) * R.qn)) * A - R.mp / (T(2) * R.qn) * ph);
+}
+
+// Interval increment (quadrature.jl:205-215); pca = polar_closed at the interval's start, carried
+// from the previous interval (the same inputs, hence the same value).
+template <class T>
+__device__ __forceinline__ void increment(const MarchRay<T>& R, const Point<T>& pa, const Point<T>& pm, const Point<T>& pb,
+                                          double ta, double tb, T pca, T pcb, T& It, T& Iphi) {
+    T h = T(tb - ta);
+    T ra = pa.r, rb = pb.r;
+    T dFr = (rb - ra) + T(2) * log(rb / ra);
+    T dFp = log((rb - R.rp) * ra / ((ra - R.rp) * rb)) / R.sp;
+    T dFm = log((rb - R.rmn) * ra / ((ra - R.rmn) * rb)) / R.sm;
+    It = h / T(6) * (pa.gt + T(4) * pm.gt + pb.gt) + fabs(dFr) + R.Qt * dFp + R.Qtm * dFm;
+    Iphi = h / T(6) * (pa.gphi + T(4) * pm.gphi + pb.gphi) + R.Qphi * dFp + R.Qphim * dFm + pcb - pca;
+}
+
+template <class T>
+__device__ __forceinline__ JS<T> load_js(const double* rec, int off) {
+    return {T(rec[off]), T(rec[off + 1]), T(rec[off + 2])};
+}
+
+// March ray j with N samples and call f(k, sample) for k = 1..N; returns the largest anchor residuals.
+template <class T, class F>
+__device__ __forceinline__ void march(const PlanView& P, const Spacetime& st, long long j, const MarchRay<T>& R,
+                                      F& f, double& resid_t, double& resid_phi) {
+    const int N = st.N;
+    const double dtau = R.dtau;
+    const double h = dtau / 2.0;
+    const double* A0 = P.anchors + R.anchor_off * AF_COUNT;
+    JS<T> xr = load_js<T>(A0, AF_XR_SN), xt = load_js<T>(A0, AF_XT_SN);
+    Point<T> pa = ray_point(R, xr, xt, dtau);
+    T pca = polar_closed(R, dtau, pa.sn, pa.cn);
+    T t = T(A0[AF_T]), phi = T(A0[AF_PHI]);
+    double rt = 0.0, rphi = 0.0;
+    {
+        Sample<T> s{t, pa.r, pa.theta, pa.cth, phi, pa.nur, pa.nuth, (dtau <= R.tau_valid) && visible(R, pa.cth)};
+        f(1, s);
+    }
+    int next_anchor = 1 + R.Manchor;   // sample index of the next anchor
+    int m = 1;
+    for (int k = 2; k <= N; ++k) {
+        double ta = (k - 1) * dtau, tb = k * dtau;
+        xr = jstep(xr, R.dr, R.k);
+        xt = jstep(xt, R.dth, R.pmu);
+        Point<T> pm = ray_point(R, xr, xt, ta + h);
+        const bool anchor = (k == next_anchor);
+        const double* Am = P.anchors + (R.anchor_off + m) * AF_COUNT;
+        if (anchor) {
+            xr = load_js<T>(Am, AF_XR_SN); xt = load_js<T>(Am, AF_XT_SN);
+        } else {
+            xr = jstep(xr, R.dr, R.k);
+            xt = jstep(xt, R.dth, R.pmu);
+        }
+        Point<T> pb = ray_point(R, xr, xt, tb);
+        T pcb = polar_closed(R, tb, pb.sn, pb.cn);
+        if (k == R.turn_k) {
+            const double* pf = P.f;
+            const long long np = P.npad;
+            JS<T> p1r = {T(pf[PF_P1R_SN * np + j]), T(pf[PF_P1R_CN * np + j]), T(pf[PF_P1R_DN * np + j])};
+            JS<T> p1t = {T(pf[PF_P1T_SN * np + j]), T(pf[PF_P1T_CN * np + j]), T(pf[PF_P1T_DN * np + j])};
+            JS<T> p2r = {T(pf[PF_P2R_SN * np + j]), T(pf[PF_P2R_CN * np + j]), T(pf[PF_P2R_DN * np + j])};
+            JS<T> p2t = {T(pf[PF_P2T_SN * np + j]), T(pf[PF_P2T_CN * np + j]), T(pf[PF_P2T_DN * np + j])};
+            JS<T> ptt = {T(pf[PF_PTT_SN * np + j]), T(pf[PF_PTT_CN * np + j]), T(pf[PF_PTT_DN * np + j])};
+            double fo = R.fo_d;
+            Point<T> pt = turning_point(R, ptt);
+            Point<T> p1 = ray_point(R, p1r, p1t, (ta + fo) / 2.0);
+            Point<T> p2 = ray_point(R, p2r, p2t, (fo + tb) / 2.0);
+            T pct = polar_closed(R, fo, pt.sn, pt.cn);
+            T It1, Ip1, It2, Ip2;
+            increment(R, pa, p1, pt, ta, fo, pca, pct, It1, Ip1);
+            increment(R, pt, p2, pb, fo, tb, pct, pcb, It2, Ip2);
+            t += It1 + It2; phi += Ip1 + Ip2;
+        } else {
+            T It, Ip;
+            increment(R, pa, pm, pb, ta, tb, pca, pcb, It, Ip);
+            t += It; phi += Ip;
+        }
+        if (anchor) {
+            if (Am[AF_OK] != 0.0) {
+                double at = Am[AF_T], ap = Am[AF_PHI];
+                rt = fmax(rt, fabs(double(t) - at));
+                rphi = fmax(rphi, fabs(double(phi) - ap));
+                t = T(at); phi = T(ap);
+            }
+            ++m;
+            next_anchor += R.Manchor;
+        }
+        Sample<T> s{t, pb.r, pb.theta, pb.cth, phi, pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cth)};
+        f(k, s);
+        pa = pb;
+        pca = pcb;
+    }
+    resid_t = rt;
+    resid_phi = rphi;
+}
+
+}  // namespace ks

@@ -1,0 +1,158 @@
+"""ctypes binding of the CPU oracle (oracle/_build/libks_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+leg, never by the kerrsplat_b200 package. `build()` compiles it with the Makefile beside this file.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libks_oracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = ctypes.CDLL(LIB)
+        _lib.kso_num_threads.restype = ctypes.c_int
+    return _lib
+
+
+def _p(x):
+    return ctypes.c_void_p(x.ctypes.data)
+
+
+def _d(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def set_threads(n):
+    load().kso_set_num_threads(int(n))
+
+
+def num_threads():
+    return load().kso_num_threads()
+
+
+def ray_constants(a, theta_o, alpha, beta):
+    alpha, beta = _d(alpha), _d(beta)
+    out = np.empty((alpha.size, 24))
+    load().kso_ray_constants(ctypes.c_double(a), ctypes.c_double(theta_o), _p(alpha), _p(beta), ctypes.c_long(alpha.size), _p(out))
+    return out
+
+
+def march_samples(a, theta_o, alpha, beta, N, M=64):
+    """Sample stream of the recurrence march: dict of (npix, N) arrays, screen order."""
+    alpha, beta = _d(alpha), _d(beta)
+    n = alpha.size
+    t, r, th, ph = (np.empty((n, N)) for _ in range(4))
+    fl = np.empty((n, N), dtype=np.uint8)
+    rt, rp = np.empty(n), np.empty(n)
+    load().kso_march_samples(ctypes.c_double(a), ctypes.c_double(theta_o), _p(alpha), _p(beta), ctypes.c_long(n), int(N), int(M),
+                             _p(t), _p(r), _p(th), _p(ph), _p(fl), _p(rt), _p(rp))
+    return {"t": t, "r": r, "theta": th, "phi": ph, "flags": fl, "resid_t": rt, "resid_phi": rp}
+
+
+def anchor_values(a, theta_o, alpha, beta, N):
+    """t~ and phi of the anchor evaluator at every sample (no recurrence): (npix, N) arrays."""
+    alpha, beta = _d(alpha), _d(beta)
+    n = alpha.size
+    t, ph = np.empty((n, N)), np.empty((n, N))
+    ok = np.empty((n, N), dtype=np.uint8)
+    load().kso_anchor_values(ctypes.c_double(a), ctypes.c_double(theta_o), _p(alpha), _p(beta), ctypes.c_long(n), int(N), _p(t), _p(ph), _p(ok))
+    return t, ph, ok
+
+
+def thin_image(a, theta_o, alpha, beta, N, M, params, t_obs):
+    alpha, beta = _d(alpha), _d(beta)
+    p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).T)
+    n = alpha.size
+    out, rt, rp = np.empty(n), np.empty(n), np.empty(n)
+    load().kso_thin_image(ctypes.c_double(a), ctypes.c_double(theta_o), _p(alpha), _p(beta), ctypes.c_long(n), int(N), int(M),
+                          _p(p), int(p.shape[0]), ctypes.c_double(t_obs), _p(out), _p(rt), _p(rp))
+    return out
+
+
+KIND = {"thermal": 1, "powerlaw": 2, "kappa": 3, "knot": 4}
+NROWS = {1: 21, 2: 22, 3: 22, 4: 21}
+
+
+def polarized_image(a, theta_o, alpha, beta, N, M, sets, t_obs, nu, L, nmax=-1, slab=0.0, gmax=1e5):
+    """sets: list of (kind, params (nrows, nsplat), hyp or None). Returns (npix, 4) cgs, screen order."""
+    alpha, beta = _d(alpha), _d(beta)
+    n = alpha.size
+    ns = len(sets)
+    kinds = (ctypes.c_int * ns)(*[KIND[k] if isinstance(k, str) else k for k, _, _ in sets])
+    nrows = (ctypes.c_int * ns)(*[NROWS[kinds[i]] for i in range(ns)])
+    keep = [np.ascontiguousarray(np.asarray(p, dtype=np.float64).T) for _, p, _ in sets]
+    nsplat = (ctypes.c_int * ns)(*[k.shape[0] for k in keep])
+    params = (ctypes.c_void_p * ns)(*[k.ctypes.data for k in keep])
+    hyps = [None if h is None else _d(h) for _, _, h in sets]
+    hyp = (ctypes.c_void_p * ns)(*[None if h is None else h.ctypes.data for h in hyps])
+    out = np.empty((n, 4))
+    load().kso_polarized_image(ctypes.c_double(a), ctypes.c_double(theta_o), _p(alpha), _p(beta), ctypes.c_long(n), int(N), int(M),
+                               ns, kinds, nrows, nsplat, params, hyp, None, None, None, ctypes.c_double(gmax),
+                               ctypes.c_double(t_obs), ctypes.c_double(nu), ctypes.c_double(L), int(nmax), ctypes.c_double(slab), _p(out))
+    return out
+
+
+def transfer_step(j, alpha, rho, D):
+    O, E = np.empty(16), np.empty(4)
+    load().kso_transfer_step(_p(_d(j)), _p(_d(alpha)), _p(_d(rho)), ctypes.c_double(D), _p(O), _p(E))
+    return O.reshape(4, 4), E
+
+
+def thermal(ne, Te, B, nu, th, dexter_rhoV=False):
+    args = [_d(np.atleast_1d(x)) for x in (ne, Te, B, nu, th)]
+    n = args[0].size
+    out = np.empty((n, 8))
+    load().kso_thermal(ctypes.c_long(n), *[_p(x) for x in args], int(dexter_rhoV), _p(out))
+    return out
+
+
+def powerlaw(ne, p, gmin, gmax, B, nu, th):
+    args = [_d(np.atleast_1d(x)) for x in (ne, p, gmin, gmax, B, nu, th)]
+    n = args[0].size
+    out = np.empty((n, 8))
+    load().kso_powerlaw(ctypes.c_long(n), *[_p(x) for x in args], _p(out))
+    return out
+
+
+def kappa(ne, kap, w, B, nu, th, hyp):
+    args = [_d(np.atleast_1d(x)) for x in (ne, kap, w, B, nu, th, hyp)]
+    n = args[0].size
+    out = np.empty((n, 8))
+    load().kso_kappa(ctypes.c_long(n), *[_p(x) for x in args], _p(out))
+    return out
+
+
+def besselk01(x):
+    x = _d(np.atleast_1d(x))
+    k0, k1 = np.empty_like(x), np.empty_like(x)
+    load().kso_besselk01(ctypes.c_long(x.size), _p(x), _p(k0), _p(k1))
+    return k0, k1
+
+
+def jacobi_state(u, m):
+    u, m = _d(np.atleast_1d(u)), _d(np.atleast_1d(m))
+    sn, cn, dn = np.empty_like(u), np.empty_like(u), np.empty_like(u)
+    load().kso_jacobi_state(ctypes.c_long(u.size), _p(u), _p(m), _p(sn), _p(cn), _p(dn))
+    return sn, cn, dn
+
+
+def ellipf(phi, m):
+    phi, m = _d(np.atleast_1d(phi)), _d(np.atleast_1d(m))
+    out = np.empty_like(phi)
+    load().kso_ellipf(ctypes.c_long(phi.size), _p(phi), _p(m), _p(out))
+    return out
