@@ -1,0 +1,290 @@
+"""Benchmark of the render hot path: Stokes ray-samples/s of the full-Stokes polarized image
+workload (256 x 256 screen over +-20 M, a = 0.5, theta_o = 60 deg, 1024 samples per ray, 64
+thermal splats, 3 frequencies), one GPU per process.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64]
+
+One step = one render of every ray at every frequency (ks_render). `value` is device-resident
+throughput (inputs and the FP64 plan/anchor table resident in HBM; the table, about 150 MB, is
+larger than L2, so nothing is flushed between steps); `e2e` is the same metric through the public
+Python API with host buffers (parameters uploaded, Stokes images read back every step). Under
+torchrun every rank renders its own parameter set (weak scaling, no data-path collective) and the
+step time is the max over ranks. `--impl reference` times the CPU oracle (the C++ FP64
+restatement of the reference's path; the reference itself is Julia and cannot run here) on a
+bounded sample of the same workload with every host thread.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Stokes ray-samples/s (full-Stokes polarized transport)"
+UNIT = "ray-samples/s"
+
+# Algorithmic FP32-pipe work per event of the polarized consumer and the march (flops: add, mul =
+# 1, fma = 2, div = 1) and special-function-unit operations (sqrt, exp, log, sin, cos, atan, acos,
+# pow count 1 each), counted from the kernel source (kerrsplat_b200/csrc/ks_march.cuh,
+# ks_transfer.cuh, ks_lib.cu PolSink): see DESIGN.md "Roofline".
+FLOPS = {"samples": 330, "valid_samples": 95, "splat_tests": 22, "weights": 32, "coefficients": 170,
+         "frames": 115, "steps": 1150}
+SFU = {"samples": 12, "valid_samples": 9, "splat_tests": 2, "weights": 1, "coefficients": 22, "frames": 4, "steps": 12}
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            v = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(v[0]))
+                smax = float(v[1])
+            except (ValueError, IndexError):
+                continue
+            for n, x in zip(names, v[3:7]):
+                if x.lower() in ("active", "1"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(seed_offset=0):
+    from kerrsplat_b200 import scenes
+    c = scenes.config2()
+    if seed_offset:
+        rng = np.random.Generator(np.random.PCG64(1 + 1000 * seed_offset))
+        c["params"] = scenes.thermal_params(rng, 64, c["a"])
+    return c
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import kerrsplat_b200 as ks
+    from kerrsplat_b200 import build
+    rank, world, local = rank_info()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    build.build(verbose=False)
+    c = workload(seed_offset=rank)
+    prec = ks.KS_MIXED if args.precision == "mixed" else ks.KS_FP64
+    cache = ks.GeodesicCache(c["camera"], c["N"], device=local)
+    ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
+    dev = torch.device("cuda", local)
+    model_dev = ks.PolarizedSplats(torch.tensor(c["params"], device=dev))
+    times_dev = torch.tensor([c["t_obs"]], dtype=torch.float64, device=dev)
+    nus_dev = torch.tensor(c["nus"], dtype=torch.float64, device=dev)
+    nf = len(c["nus"])
+    out_dev = torch.empty((nf, 1, cache.npix, 4), dtype=torch.float64, device=dev)
+    units_per_step = cache.npix * c["N"] * 1 * nf
+    stream = torch.cuda.ExternalStream(cache.stream(), device=dev)
+
+    def step():
+        ks.render(cache, model_dev, times_dev, nus_dev, c["L"], precision=prec, out=out_dev, order="sorted")
+
+    for _ in range(args.warmup):
+        step()
+    # work-event counts of one render (the algorithmic-work model of the roofline)
+    cache.count_events(True)
+    step()
+    counts = cache.event_counts()
+    cache.count_events(False)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    cache.kernel_stats(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms_total = e0.elapsed_time(e1)
+    render_ms, render_launches, all_launches = cache.kernel_stats(reset=True)
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = units_per_step * world / (ms_step / 1e3)
+
+    # e2e: the public API with host buffers (parameters uploaded, images read back every step)
+    model_host = ks.PolarizedSplats(c["params"])
+    out_host = np.empty((nf, 1, cache.npix, 4))
+    h2d = c["params"].nbytes + 8 * (1 + nf)
+    d2h = out_host.nbytes
+    ks.render(cache, model_host, [c["t_obs"]], c["nus"], c["L"], precision=prec, out=out_host)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(e2e_steps):
+        ks.render(cache, ks.PolarizedSplats(c["params"]), [c["t_obs"]], c["nus"], c["L"], precision=prec, out=out_host)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = units_per_step * world / (e2e_ms / 1e3)
+
+    # roofline of the dominant kernel (k_polarized): algorithmic FP32 work per launch / its time
+    flops = sum(FLOPS[k] * counts[k] for k in FLOPS)
+    sfu = sum(SFU[k] * counts[k] for k in SFU)
+    launch_ms = render_ms / max(render_launches, 1)
+    launches_per_step = render_launches / args.steps
+    flops_per_launch = flops / max(launches_per_step, 1)
+    achieved = flops_per_launch / (launch_ms / 1e3) / 1e12
+    pk = peaks()
+    clocks = clk.summary()
+    smax = pk.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * smax * 1e6 / 1e12   # nominal FP32 (non-tensor) FMA peak at max clock
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if prec == ks.KS_MIXED else "f64", "data": "synthetic (seeded PCG64 scene, cfg 2 distributions)",
+        "config": {"workload": "polarized image 256x256 +-20M, a=0.5, theta_o=60deg, N=1024, M=64, 64 thermal splats, 86/230/345 GHz",
+                   "precision": args.precision, "rays": cache.npix, "samples_per_ray": c["N"], "frequencies": nf,
+                   "l2": "no flush: the per-ray FP64 plan + anchor table (~150 MB) exceeds the 126 MB L2"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": None, "peak_source": "nominal FP32 pipe (148 SMs x 128 lanes x 2 x max SM clock); MEASURED_PEAKS.json has no FP32 figure",
+                     "kernel": "k_polarized", "flops_per_launch": flops_per_launch, "sfu_ops_per_launch": sfu / max(launches_per_step, 1),
+                     "events": counts},
+        "gpu_launches": int(all_launches),
+        "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(c, args.cpu_rays)
+    if args.fp64_steps > 0 and prec == ks.KS_MIXED:
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(args.fp64_steps):
+            ks.render(cache, model_dev, times_dev, nus_dev, c["L"], precision=ks.KS_FP64, out=out_dev, order="sorted")
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms64 = e0.elapsed_time(e1) / args.fp64_steps
+        line["fp64_plain"] = {"value": units_per_step / (ms64 / 1e3), "ms_per_step": ms64, "speedup_mixed_over_fp64": ms64 / ms_step}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    cache.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_sample(c, nrays, seed=7):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    idx = np.sort(rng.choice(c["camera"].npix, size=min(nrays, c["camera"].npix), replace=False))
+    return idx
+
+
+def cpu_baseline(c, nrays):
+    """The CPU oracle (C++ FP64 restatement, OpenMP over rays, every host thread) on a bounded
+    random sample of the workload's rays at all frequencies."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    oracle.set_threads(os.cpu_count() or 1)
+    idx = cpu_sample(c, nrays)
+    cam = c["camera"]
+    t0 = time.perf_counter()
+    for nu in c["nus"]:
+        oracle.polarized_image(c["a"], c["theta_o"], cam.alpha[idx], cam.beta[idx], c["N"], c["M"], [("thermal", c["params"], None)],
+                               c["t_obs"], nu, c["L"])
+    dt = time.perf_counter() - t0
+    units = idx.size * c["N"] * len(c["nus"])
+    return {"value": units / dt, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{idx.size} random rays of the 256x256 workload x {c['N']} samples x {len(c['nus'])} frequencies ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    rank, world, local = rank_info()
+    if rank != 0:
+        return
+    c = workload()
+    samples = []
+    for k in range(args.warmup + args.steps):
+        b = cpu_baseline(c, args.cpu_rays)
+        if k >= args.warmup:
+            samples.append(b["value"])
+    v = float(np.mean(samples))
+    units_per_step = c["camera"].npix * c["N"] * len(c["nus"])
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": units_per_step / v * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64 scene, cfg 2 distributions)",
+            "config": {"workload": "polarized image 256x256 +-20M, a=0.5, theta_o=60deg, N=1024, M=64, 64 thermal splats, 86/230/345 GHz",
+                       "note": "each step renders a bounded random sample of the rays; ms_per_step extrapolates to the full screen"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": b["cores"], "kind": "port", "sample": b["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cpu-rays", type=int, default=1024)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -113,6 +113,21 @@ int ks_render(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const do
               const double* nus, int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab,
               double* out, int32_t order);
 
+/* ---- library extensions with no counterpart in the reference (measurement and streams) ---- */
+
+/* The CUDA stream every call of this context runs on (a cudaStream_t). */
+int ks_context_stream(ks_context* ctx, void** stream);
+
+/* Device time (CUDA events on the context stream) of the render kernels since the last reset,
+ * their launch count, and the launch count of every kernel of this library. */
+int ks_kernel_stats(ks_context* ctx, double* render_ms, long long* render_launches, long long* all_launches, int reset);
+
+/* Count work events during ks_render (samples, valid samples, splat tests, weights evaluated,
+ * coefficient evaluations, local frames, transfer steps); ks_event_counts reads the 7 counters of
+ * the last counted render. */
+int ks_set_event_counting(ks_context* ctx, int on);
+int ks_event_counts(ks_context* ctx, unsigned long long out[7]);
+
 #ifdef __cplusplus
 }
 #endif

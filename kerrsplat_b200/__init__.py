@@ -210,6 +210,17 @@ class GeodesicCache:
         self._check(self._lib.ks_kernel_stats(self._ctx, ctypes.byref(ms), ctypes.byref(kl), ctypes.byref(al), int(reset)))
         return ms.value, kl.value, al.value
 
+    def count_events(self, on=True):
+        self._check(self._lib.ks_set_event_counting(self._ctx, int(on)))
+
+    def event_counts(self):
+        """Work events of the last counted ks_render: samples (per combination), valid samples,
+        splat tests, weights evaluated, coefficient evaluations, frames, transfer steps."""
+        out = np.zeros(7, dtype=np.uint64)
+        self._check(self._lib.ks_event_counts(self._ctx, _ptr(out)))
+        keys = ("samples", "valid_samples", "splat_tests", "weights", "coefficients", "frames", "steps")
+        return dict(zip(keys, (int(v) for v in out)))
+
     def stream(self):
         s = ctypes.c_void_p()
         self._check(self._lib.ks_context_stream(self._ctx, ctypes.byref(s)))

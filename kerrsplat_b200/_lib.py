@@ -59,6 +59,8 @@ SIGNATURES = [
 EXTRA_SIGNATURES = [
     ("ks_context_stream", ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     ("ks_kernel_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+    ("ks_set_event_counting", ctypes.c_int, [_VP, ctypes.c_int]),
+    ("ks_event_counts", ctypes.c_int, [_VP, _VP]),
 ]
 
 _lib = None

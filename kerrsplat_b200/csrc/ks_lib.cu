@@ -389,8 +389,12 @@ struct PolSink {
     int nmax;
     T P[CH][16], S[CH][4];
     T zprev; int wn; bool inside, crossed, zset;
+    // event counts of this thread (the algorithmic-work model of the roofline): samples, valid
+    // samples, splat tests, weights evaluated, coefficient evaluations, frames, steps
+    unsigned int ev[7];
 
     __device__ void init() {
+        for (int q = 0; q < 7; ++q) ev[q] = 0;
         for (int c = 0; c < CH; ++c) {
             for (int q = 0; q < 16; ++q) P[c][q] = (q % 5 == 0) ? T(1) : T(0);
             for (int q = 0; q < 4; ++q) S[c][q] = T(0);
@@ -414,7 +418,9 @@ struct PolSink {
     }
 
     __device__ void operator()(int, const Sample<T>& s) {
+        ev[0]++;
         if (!(s.ok && s.r > rh_lo)) return;
+        ev[1]++;
         if (nmax >= 0) {
             wind(s.r * cos(s.theta));
             if (wn > nmax) return;
@@ -439,11 +445,15 @@ struct PolSink {
                 if (c >= nc) break;
                 T t = t_obs[c] - s.t;
                 T q;
+                ev[2]++;
                 if (!splat_exponent(p, t, x, y, z, kind != KS_KNOT21, q)) continue;
+                ev[3]++;
                 T G = exp(-q);
                 if (!(G > T(kWEIGHT_CUTOFF))) continue;
                 if (!have_frame) { F = sample_frame(a, s.r, s.theta, sth, cth, eta, lam, s.nur, s.nutheta); have_frame = true; }
+                ev[4]++;
                 if (!fr_done) {
+                    ev[5]++;
                     lf = local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != T(0),
                                      alpha, beta, a_sin_tho);
                     fr_done = true;
@@ -476,6 +486,7 @@ struct PolSink {
         for (int c = 0; c < CH; ++c) {
             if (c >= nc || !active[c]) continue;
             T Dl = Lnu[c] * Sg * dtau;
+            ev[6]++;
             T O[16], E[4];
             transfer_step(c_moments, j4[c], a4[c], r3[c], Dl, O, E);
             // advance (step.jl:347): S += P E, P = P O
@@ -497,7 +508,7 @@ template <class T, int CH>
 __global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, long long npix, const double* __restrict__ tab64, int ntot,
                                                       const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L,
                                                       int nmax, double slab, double* __restrict__ out, double* __restrict__ resid_t,
-                                                      double* __restrict__ resid_phi) {
+                                                      double* __restrict__ resid_phi, unsigned long long* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char smem[];
     T* tab = reinterpret_cast<T*>(smem);
     for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = T(tab64[q]);
@@ -530,6 +541,11 @@ __global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, 
         o[2] = double(sink.S[c][2]) * n3; o[3] = double(sink.S[c][3]) * n3;
     }
     if (blockIdx.y == 0 && resid_t) { resid_t[j] = rt; resid_phi[j] = rp; }
+    if (counters) {
+        // samples are counted once per (ray, combo) as the metric counts them
+        atomicAdd(&counters[0], (unsigned long long)sink.ev[0] * sink.nc);
+        for (int q = 1; q < 7; ++q) atomicAdd(&counters[q], (unsigned long long)sink.ev[q]);
+    }
 }
 
 // sorted slot -> output order, for `nvec` blocks of npix rows of `width` doubles
@@ -571,7 +587,8 @@ struct ks_context {
     bool regenerated = false;
     Spacetime st{};
     DevBuf alpha, beta, key, key2, idx, perm, plan, nanch, aoff, anchors, resid_t, resid_phi, scratch;
-    DevBuf tab, combos, out_sorted, stage_in, stage_out;
+    DevBuf tab, combos, out_sorted, stage_in, stage_out, counters;
+    bool count_events = false;
     long long total_anchors = 0;
     int max_nanch = 0;
     long long ranges[6] = {0, 0, 0, 0, 0, 0};
@@ -714,7 +731,7 @@ int ks_context_destroy(ks_context* c) {
     if (!c) return KS_OK;
     cudaSetDevice(c->device);
     for (DevBuf* b : {&c->alpha, &c->beta, &c->key, &c->key2, &c->idx, &c->perm, &c->plan, &c->nanch, &c->aoff, &c->anchors,
-                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out})
+                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out, &c->counters})
         b->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -739,6 +756,21 @@ int ks_kernel_stats(ks_context* c, double* render_ms, long long* render_launches
     if (render_launches) *render_launches = c->kernel_launches;
     if (all_launches) *all_launches = c->launches;
     if (reset) { c->kernel_ms = 0.0; c->kernel_launches = 0; c->launches = 0; }
+    return KS_OK;
+}
+
+// Count the work events of the following ks_render calls (samples, valid samples, splat tests,
+// weights, coefficient evaluations, frames, steps) into a device counter; ks_event_counts reads them.
+int ks_set_event_counting(ks_context* c, int on) {
+    if (!c) return KS_ERR_ARGUMENT;
+    c->count_events = on != 0;
+    return KS_OK;
+}
+
+int ks_event_counts(ks_context* c, unsigned long long out[7]) {
+    if (!c || !out) return KS_ERR_ARGUMENT;
+    if (!c->counters.p) { for (int q = 0; q < 7; ++q) out[q] = 0; return KS_OK; }
+    KS_CUDA(c, cudaMemcpy(out, c->counters.p, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     return KS_OK;
 }
 
@@ -1006,6 +1038,10 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     KS_CUDA(c, c->out_sorted.ensure(size_t(n) * 4 * ncombo * sizeof(double)));
     const double* dct = c->combos.as<double>();
     const double* dcn = dct + ncombo;
+    if (c->count_events) {
+        KS_CUDA(c, c->counters.ensure(8 * sizeof(unsigned long long)));
+        KS_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(unsigned long long), c->stream));
+    }
     cudaEventRecord(c->ev0, c->stream);
     if (precision == KS_FP64) {
         // the plain path: one march per (frame, frequency), as the reference's polarized_cube does
@@ -1015,7 +1051,8 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
         for (int cc = 0; cc < ncombo; ++cc) {
             k_polarized<double, 1><<<dim3(nblocks(n), 1), kBlock, smem, c->stream>>>(
                 plan_view(c), c->st, n, c->tab.as<double>(), ntot, dct + cc, dcn + cc, 1, L, nmax, slab,
-                c->out_sorted.as<double>() + size_t(cc) * n * 4, c->resid_t.as<double>(), c->resid_phi.as<double>());
+                c->out_sorted.as<double>() + size_t(cc) * n * 4, c->resid_t.as<double>(), c->resid_phi.as<double>(),
+                c->count_events ? c->counters.as<unsigned long long>() : nullptr);
             c->launches++;
             c->kernel_launches++;
         }
@@ -1025,7 +1062,8 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
         constexpr int CH = 4;
         KS_CUDA(c, cudaFuncSetAttribute(k_polarized<float, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_polarized<float, CH><<<dim3(nblocks(n), (ncombo + CH - 1) / CH), kBlock, smem, c->stream>>>(
-            plan_view(c), c->st, n, c->tab.as<double>(), ntot, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), nullptr, nullptr);
+            plan_view(c), c->st, n, c->tab.as<double>(), ntot, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), nullptr, nullptr,
+            c->count_events ? c->counters.as<unsigned long long>() : nullptr);
         c->launches++;
         c->kernel_launches++;
     }

@@ -65,7 +65,9 @@ def test_samples_match_oracle(cfg1_cache, oracle):
     assert np.max(np.abs(t_got - t_ref) / np.maximum(np.abs(t_ref), 1.0)) < 1e-10
     assert np.array_equal(s["flags"].T, ref["flags"][perm])
     rt, rp = cache.residuals()
-    assert np.max(rt) < 1e-8 and np.max(rp) < 1e-8
+    assert np.max(np.abs(rt - ref["resid_t"][perm])) < 1e-10
+    assert np.max(np.abs(rp - ref["resid_phi"][perm])) < 1e-10
+    assert np.max(rt) < 1e-6 and np.max(rp) < 1e-6
 
 
 def test_thin_image_fp64_and_mixed(cfg1_cache, oracle):
