@@ -94,9 +94,9 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload(seed_offset=0):
+def workload(seed_offset=0, res=256, nsamples=1024):
     from kerrsplat_b200 import scenes
-    c = scenes.config2()
+    c = scenes.config2(res=res, N=nsamples)
     if seed_offset:
         rng = np.random.Generator(np.random.PCG64(1 + 1000 * seed_offset))
         c["params"] = scenes.thermal_params(rng, 64, c["a"])
@@ -113,7 +113,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
     build.build(verbose=False)
-    c = workload(seed_offset=rank)
+    c = workload(seed_offset=rank, res=args.res, nsamples=args.nsamples)
     prec = ks.KS_MIXED if args.precision == "mixed" else ks.KS_FP64
     cache = ks.GeodesicCache(c["camera"], c["N"], device=local)
     ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
@@ -192,7 +192,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if prec == ks.KS_MIXED else "f64", "data": "synthetic (seeded PCG64 scene, cfg 2 distributions)",
-        "config": {"workload": "polarized image 256x256 +-20M, a=0.5, theta_o=60deg, N=1024, M=64, 64 thermal splats, 86/230/345 GHz",
+        "config": {"workload": f"polarized image {args.res}x{args.res} +-20M, a=0.5, theta_o=60deg, N={args.nsamples}, M=64, 64 thermal splats, 86/230/345 GHz",
                    "precision": args.precision, "rays": cache.npix, "samples_per_ray": c["N"], "frequencies": nf,
                    "l2": "no flush: the per-ray FP64 plan + anchor table (~150 MB) exceeds the 126 MB L2"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -279,6 +279,8 @@ def main():
     ap.add_argument("--cpu-rays", type=int, default=1024)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--res", type=int, default=256, help="screen resolution (smaller cases for profiling)")
+    ap.add_argument("--nsamples", type=int, default=1024)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -262,6 +262,7 @@ __global__ void k_splat_table(SetDesc d, double* __restrict__ tab) {
     o[ST_INVW] = exp(-p[11]);
     double smax = fmax(p[3], fmax(p[4], p[5]));
     o[ST_SUPP] = (-2.0 * log(kWEIGHT_CUTOFF)) * exp(2 * smax);
+    o[ST_RHO] = sqrt(p[0] * p[0] + p[1] * p[1]);
     if (d.kind == KS_THIN14) { o[ST_LOGA] = p[12]; return; }
     o[ST_NE] = exp(p[12]);
     double Bmag, thB, phB, u1, u2, u3;
@@ -315,6 +316,12 @@ __device__ __forceinline__ void ks_coords(T a, T r, T th, T ph, T& x, T& y, T& z
     T sp = sin(phks), cp = cos(phks);
     x = r * sth * cp; y = r * sth * sp; z = r * cth;
 }
+
+}  // namespace
+
+#include "ks_mixed.cuh"
+
+namespace {
 
 struct StoreSink {
     double *t, *r, *th, *ph; unsigned char* fl;
@@ -587,7 +594,7 @@ struct ks_context {
     bool regenerated = false;
     Spacetime st{};
     DevBuf alpha, beta, key, key2, idx, perm, plan, nanch, aoff, anchors, resid_t, resid_phi, scratch;
-    DevBuf tab, combos, out_sorted, stage_in, stage_out, counters;
+    DevBuf tab, combos, out_sorted, stage_in, stage_out, counters, seg_out, work;
     bool count_events = false;
     long long total_anchors = 0;
     int max_nanch = 0;
@@ -688,6 +695,59 @@ int nrows_of(int kind) {
     }
 }
 
+template <int CH>
+int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, int nmax, double slab) {
+    size_t smem = MixedSmem<CH>::bytes(ntot);
+    if (smem > 227 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
+    KS_CUDA(c, cudaFuncSetAttribute(k_mixed<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    KS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mixed<CH>, kMixedBlock, smem));
+    int nsm = 0;
+    KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    per_sm = std::max(per_sm, 1);
+    MixedJob job;
+    job.npix = c->npix; job.nframes = nframes; job.nfreq = nfreq;
+    job.nvc = (nfreq + CH - 1) / CH;
+    job.nchunks = (c->npix + 31) / 32;
+    // split the sample range into segments (at multiples of the anchor interval) until there are
+    // about eight work units per resident warp, so that the most expensive unit is short
+    const long long resident = (long long)nsm * per_sm * kWarps;
+    const long long base_units = job.nchunks * nframes * job.nvc;
+    int nseg = 1;
+    const int M = c->st.M, N = c->st.N;
+    while (nmax < 0 && base_units * nseg < 8 * resident && (nseg * 2) * M <= N) nseg *= 2;
+    job.seg_len = ((N + nseg - 1) / nseg + M - 1) / M * M;
+    job.nseg = (N + job.seg_len - 1) / job.seg_len;
+    job.total = base_units * job.nseg;
+    job.nmax = nmax; job.slab = float(slab); job.L = L;
+    const double* dt = c->combos.as<double>();
+    const double* dn = dt + nframes;
+    const size_t seg_bytes = size_t(nframes) * nfreq * job.nseg * c->npix * 20 * sizeof(float);
+    KS_CUDA(c, c->seg_out.ensure(seg_bytes));
+    KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
+    KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
+    const long long grid = std::min<long long>(job.total / kWarps + 1, (long long)nsm * per_sm);
+    k_mixed<CH><<<unsigned(grid), kMixedBlock, smem, c->stream>>>(
+        plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->work.as<unsigned long long>(), c->seg_out.as<float>(),
+        c->count_events ? c->counters.as<unsigned long long>() : nullptr);
+    c->launches++;
+    c->kernel_launches++;
+    KS_CUDA(c, cudaGetLastError());
+    const long long nq = c->npix * (long long)nframes * nfreq;
+    k_combine<<<nblocks(nq, 256), 256, 0, c->stream>>>(job, dn, c->seg_out.as<float>(), c->out_sorted.as<double>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
+int launch_mixed(ks_context* c, int ntot, const double* ht, int nframes, int nfreq, double L, int nmax, double slab) {
+    (void)ht;
+    if (nfreq >= 4) return launch_mixed_ch<4>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (nfreq == 3) return launch_mixed_ch<3>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (nfreq == 2) return launch_mixed_ch<2>(c, ntot, nframes, nfreq, L, nmax, slab);
+    return launch_mixed_ch<1>(c, ntot, nframes, nfreq, L, nmax, slab);
+}
+
 // Write `nvec` x npix x width doubles from the sorted device buffer to `out` (host or device) in `order`.
 int emit(ks_context* c, const double* sorted, int width, int nvec, int order, double* out) {
     size_t bytes = size_t(c->npix) * width * nvec * sizeof(double);
@@ -731,7 +791,7 @@ int ks_context_destroy(ks_context* c) {
     if (!c) return KS_OK;
     cudaSetDevice(c->device);
     for (DevBuf* b : {&c->alpha, &c->beta, &c->key, &c->key2, &c->idx, &c->perm, &c->plan, &c->nanch, &c->aoff, &c->anchors,
-                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out, &c->counters})
+                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out, &c->counters, &c->seg_out, &c->work})
         b->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1033,6 +1093,11 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
             hc[size_t(fv) * nframes + ft] = ht[ft];
             hc[ncombo + size_t(fv) * nframes + ft] = hnu[fv];
         }
+    if (precision == KS_MIXED) {
+        // times then frequencies
+        hc.assign(ht.begin(), ht.end());
+        hc.insert(hc.end(), hnu.begin(), hnu.end());
+    }
     KS_CUDA(c, c->combos.ensure(hc.size() * sizeof(double)));
     KS_CUDA(c, cudaMemcpyAsync(c->combos.p, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     KS_CUDA(c, c->out_sorted.ensure(size_t(n) * 4 * ncombo * sizeof(double)));
@@ -1057,15 +1122,9 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
             c->kernel_launches++;
         }
     } else {
-        size_t smem = size_t(ntot) * ST_COUNT * sizeof(float);
-        if (smem > 220 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
-        constexpr int CH = 4;
-        KS_CUDA(c, cudaFuncSetAttribute(k_polarized<float, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_polarized<float, CH><<<dim3(nblocks(n), (ncombo + CH - 1) / CH), kBlock, smem, c->stream>>>(
-            plan_view(c), c->st, n, c->tab.as<double>(), ntot, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), nullptr, nullptr,
-            c->count_events ? c->counters.as<unsigned long long>() : nullptr);
-        c->launches++;
-        c->kernel_launches++;
+        // the mixed path: one launch over rays x (frame, frequency chunk)
+        int s = launch_mixed(c, ntot, ht.data(), nframes, nfreq, L, nmax, slab);
+        if (s) return s;
     }
     cudaEventRecord(c->ev1, c->stream);
     KS_CUDA(c, cudaGetLastError());

@@ -1,0 +1,432 @@
+// ks_mixed.cuh -- the mixed-precision march-and-transfer kernel with warp-cooperative compaction.
+//
+// One thread owns one ray (sorted slot) and marches it in FP32 (the recurrence and the quadrature,
+// re-anchored to the FP64 table every M samples). What the reference does per sample
+// (transport.jl:190-198: every element's coefficients, their sum, one exact step, compositing)
+// is split across the 32 lanes of the warp so that the expensive parts run on full warps:
+//   1. every lane with a valid sample tests a chunk of 32 splats against the support sphere and the
+//      weight cutoff (cheap, uniform work) and records the passing (lane, splat) pairs in a per-warp
+//      list in shared memory, in lane order and splat order;
+//   2. the warp evaluates the listed pairs 32 at a time (weight, local frame, synchrotron
+//      coefficients at every frequency, cap, invariants, rotation into the screen basis), each lane
+//      taking one pair whatever ray it belongs to; the owner lane then adds the results of its own
+//      pairs in splat order (the same order as the reference's sum over elements, so the result is
+//      deterministic);
+//   3. the (lane, frequency) pairs with an active sample are again spread over the warp for the
+//      exact 4x4 step (O, E), and each owner composes its own steps front to back (S += P E,
+//      P = P O; step.jl:347).
+// The per-lane Stokes states live in shared memory, the splat table too.
+#pragma once
+#include "ks_transfer.cuh"
+
+namespace ks {
+
+constexpr int kMixedBlock = 128;
+constexpr int kWarps = kMixedBlock / 32;
+constexpr float kQCUT = 13.815510557964274f;   // -ln(WEIGHT_CUTOFF): G > 1e-6 <=> q < QCUT
+constexpr int kSF = 24;                         // floats per lane of sample data
+
+// per-lane sample data (shared memory)
+enum SampleField { SF_X, SF_Y, SF_Z, SF_T, SF_PU0, SF_PU1, SF_PU2, SF_PU3, SF_PZ0, SF_PZ1, SF_PZ2, SF_PZ3,
+                   SF_LI, SF_OL, SF_SDS, SF_MIS, SF_IVP, SF_R, SF_STH, SF_CTH, SF_SG, SF_ALPHA, SF_BETA, SF_PAD2 };
+
+template <int CH>
+struct MixedSmem {
+    // bytes of the per-warp and per-thread regions (the splat table comes first)
+    static constexpr int kSampleBytes = 32 * kSF * 4;
+    static constexpr int kItemBytes = 32 * 32 * 2 > 32 * 20 * 4 ? 32 * 32 * 2 : 32 * 20 * 4;   // item list | step results
+    static constexpr int kResBytes = 32 * CH * 12 * 4;                                          // pair results | step inputs
+    static constexpr int kMetaBytes = 32 * 4 * 2;
+    static constexpr int kWarpBytes = kSampleBytes + kItemBytes + kResBytes + kMetaBytes;
+    static constexpr int kStateBytes = kMixedBlock * CH * 20 * 4;                               // P (16) and S (4) per lane and frequency
+    static size_t bytes(int ntot) { return size_t(ntot) * ST_COUNT * 4 + size_t(kWarps) * kWarpBytes + kStateBytes; }
+};
+
+template <int CH>
+struct MixedSink {
+    const float* tab; int ntot;
+    float t_obs;
+    float nu[CH], Lnu[CH];
+    int nc;
+    float a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
+    int nmax;
+    int lane;
+    bool live;        // false for the padding lanes past the last ray
+    float* sf;        // this warp's sample data [kSF][32]
+    uint16_t* items;  // this warp's pair list [1024]
+    float* sres;      // step results [20][32] (aliases the pair list)
+    float* res;       // pair results [CH * 12][32] | step inputs
+    float* state;     // this thread's P/S column of the block's [CH * 20][kMixedBlock] array
+    int* meta_off;    // this warp's first step item per lane [32]
+    unsigned* meta_bits;   // and active-frequency bits [32]
+    float zprev; int wn; bool inside, crossed, zset;
+    unsigned int ev[7];
+
+    __device__ void init() {
+        for (int c = 0; c < CH; ++c) {
+            float* st = state + c * 20 * kMixedBlock;
+            for (int q = 0; q < 16; ++q) st[q * kMixedBlock] = (q % 5 == 0) ? 1.f : 0.f;
+            for (int q = 16; q < 20; ++q) st[q * kMixedBlock] = 0.f;
+        }
+        for (int q = 0; q < 7; ++q) ev[q] = 0;
+        wn = 0; inside = false; crossed = false; zset = false; zprev = 0.f;
+    }
+
+    __device__ bool wind_ok(float z) {   // step.jl:379-398; returns whether the sample is kept
+        if (!zset) { zprev = z; zset = true; inside = fabsf(z) < slab; crossed = false; return wn <= nmax; }
+        bool inside_now = fabsf(z) < slab;
+        bool crossing = zprev * z < 0.f;
+        if (inside || inside_now) {
+            crossed = crossed || crossing;
+            if (inside && !inside_now) { if (crossed) wn += 1; crossed = false; }
+            else if (!inside && inside_now) { crossed = crossing; }
+            inside = inside_now;
+        } else if (crossing) {
+            wn += 1;
+        }
+        zprev = z;
+        return wn <= nmax;
+    }
+
+    // pair (owner lane o, splat i): weight, frame, coefficients at every frequency -> res slot
+    __device__ void evaluate(int o, int i, float* out) {
+        // this warp's sample data is stored field-major ([field][lane]) so that lanes hit distinct banks
+        const float* s = sf + o;
+        const float* p = tab + i * ST_COUNT;
+        const int kind = int(p[ST_KIND]);
+        float q;
+        splat_exponent(p, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], false, q);
+        float G = __expf(-q);
+        SampleFrame<float> F;
+        F.pu[0] = s[SF_PU0 * 32]; F.pu[1] = s[SF_PU1 * 32]; F.pu[2] = s[SF_PU2 * 32]; F.pu[3] = s[SF_PU3 * 32];
+        F.pz[0] = s[SF_PZ0 * 32]; F.pz[1] = s[SF_PZ1 * 32]; F.pz[2] = s[SF_PZ2 * 32]; F.pz[3] = s[SF_PZ3 * 32];
+        F.lapse_inv = s[SF_LI * 32]; F.om_lapse = s[SF_OL * 32]; F.sDS = s[SF_SDS * 32]; F.misS = s[SF_MIS * 32]; F.ivarpi = s[SF_IVP * 32];
+        F.r = s[SF_R * 32]; F.sth = s[SF_STH * 32]; F.cth = s[SF_CTH * 32]; F.a = a;
+        // the owner's screen coordinates (the pair may belong to another lane's ray)
+        LFrame<float> lf = local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != 0.f,
+                                       s[SF_ALPHA * 32], s[SF_BETA * 32], a_sin_tho);
+        float thb = acosf(fminf(1.f, fmaxf(-1.f, lf.cosB)));
+        float ne = p[ST_NE] * G;
+        float s2c, c2c;
+        sincosf(2.f * lf.chi, &s2c, &c2c);
+        int act = 0;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            float* r = out + c * 12 * 32;   // out = res + slot; fields are 32 apart
+            if (c >= nc) { r[11 * 32] = 0.f; continue; }
+            float nuf = nu[c] / lf.g;
+            Coef<float> cf;
+            if (kind == KS_POWERLAW22)
+                cf = powerlaw(ne, p[ST_P], p[ST_GMIN], p[ST_GSPAN], p[ST_GAMJ], p[ST_GAMA], p[ST_BMAG], nuf, thb);
+            else if (kind == KS_KAPPA22)
+                cf = kappa(ne, p[ST_KAP], p[ST_W], p[ST_HYP], p[ST_G43], p[ST_G2], p[ST_GQ], p[ST_GP], p[ST_GK2], p[ST_KB], p[ST_BMAG], nuf, thb);
+            else
+                cf = thermal(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
+            bool on = cf.jI > 0.f || cf.aI > 0.f || cf.rQ != 0.f || cf.rV != 0.f;
+            if (!on) { r[11 * 32] = 0.f; continue; }
+            float fe = cap_factor(cf.jI, cf.jQ, cf.jV, 0.99f);
+            float fa = cap_factor(cf.aI, cf.aQ, cf.aV, 0.99f);
+            float nh = nuf / float(kNU0);
+            float i2 = 1.f / (nh * nh);
+            float jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+            r[0] = cf.jI * i2; r[32] = jQ * c2c; r[64] = jQ * s2c; r[96] = cf.jV * fe * i2;
+            r[128] = nh * cf.aI; r[160] = aQ * c2c; r[192] = aQ * s2c; r[224] = cf.aV * fa * nh;
+            r[256] = rQ * c2c; r[288] = rQ * s2c; r[320] = nh * cf.rV;
+            r[352] = 1.f;
+            act++;
+        }
+        ev[4] += act ? 1 : 0;
+    }
+
+    // The consumer for one sample of every lane of the warp (all 32 lanes call it together).
+    __device__ void operator()(int, const Sample<float>& s) {
+        const unsigned full = 0xffffffffu;
+        ev[0]++;
+        bool valid = live && s.ok && s.r > rh_lo;
+        if (valid) ev[1]++;
+        if (valid && nmax >= 0) valid = wind_ok(s.r * cosf(s.theta));
+        unsigned vmask = __ballot_sync(full, valid);
+        if (vmask == 0u) return;
+        float* mys = sf + lane;
+        float x = 0.f, y = 0.f, z = 0.f, t = 0.f, rho = 0.f;
+        if (valid) {
+            float sth, cth;
+            ks_coords(a, s.r, s.theta, s.phi, x, y, z, sth, cth);
+            rho = sqrtf(x * x + y * y);
+            t = t_obs - s.t;
+            SampleFrame<float> F = sample_frame(a, s.r, s.theta, sth, cth, eta, lam, s.nur, s.nutheta);
+            mys[SF_X * 32] = x; mys[SF_Y * 32] = y; mys[SF_Z * 32] = z; mys[SF_T * 32] = s.t;
+            mys[SF_PU0 * 32] = F.pu[0]; mys[SF_PU1 * 32] = F.pu[1]; mys[SF_PU2 * 32] = F.pu[2]; mys[SF_PU3 * 32] = F.pu[3];
+            mys[SF_PZ0 * 32] = F.pz[0]; mys[SF_PZ1 * 32] = F.pz[1]; mys[SF_PZ2 * 32] = F.pz[2]; mys[SF_PZ3 * 32] = F.pz[3];
+            mys[SF_LI * 32] = F.lapse_inv; mys[SF_OL * 32] = F.om_lapse; mys[SF_SDS * 32] = F.sDS; mys[SF_MIS * 32] = F.misS; mys[SF_IVP * 32] = F.ivarpi;
+            mys[SF_R * 32] = s.r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
+            mys[SF_SG * 32] = (s.r * s.r + a * a * cth * cth) * dtau;   // Sigma dtau of this lane's ray
+            mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
+        }
+        float acc[CH][11];
+        unsigned actbits = 0u;
+#pragma unroll
+        for (int c = 0; c < CH; ++c)
+#pragma unroll
+            for (int q = 0; q < 11; ++q) acc[c][q] = 0.f;
+        __syncwarp();
+        for (int s0 = 0; s0 < ntot; s0 += 32) {
+            // 1. tests: support sphere, then the weight cutoff
+            unsigned mask = 0u;
+            if (valid) {
+                const int nb = min(32, ntot - s0);
+                for (int b = 0; b < nb; ++b) {
+                    const float* p = tab + (s0 + b) * ST_COUNT;
+                    float q;
+                    ev[2]++;
+                    // the pattern rotation keeps the centre on a circle about the spin axis: a point
+                    // farther than the support radius from that circle is outside the support sphere
+                    // at every time (no trigonometry needed)
+                    const float dr = rho - p[ST_RHO], dz = z - p[ST_CZ];
+                    if (dr * dr + dz * dz > p[ST_SUPP] && int(p[ST_KIND]) != KS_KNOT21) continue;
+                    if (!splat_exponent(p, t, x, y, z, int(p[ST_KIND]) != KS_KNOT21, q)) continue;
+                    ev[3]++;
+                    if (q < kQCUT) mask |= 1u << b;
+                }
+            }
+            int n = __popc(mask);
+            int incl = n;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                int v = __shfl_up_sync(full, incl, d);
+                if (lane >= d) incl += v;
+            }
+            const int off = incl - n;
+            const int total = __shfl_sync(full, incl, 31);
+            if (total == 0) continue;
+            {
+                unsigned m = mask;
+                int k = off;
+                while (m) {
+                    int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    items[k++] = uint16_t((lane << 5) | b);
+                }
+            }
+            __syncwarp();
+            // 2. evaluation rounds over the warp, then owner accumulation in list order
+            for (int base = 0; base < total; base += 32) {
+                const int k = base + lane;
+                if (k < total) {
+                    const int it = items[k];
+                    evaluate(it >> 5, s0 + (it & 31), res + lane);
+                }
+                __syncwarp();
+                const int lo = max(off, base), hi = min(off + n, base + 32);
+                for (int kk = lo; kk < hi; ++kk) {
+                    const float* r = res + (kk - base);
+#pragma unroll
+                    for (int c = 0; c < CH; ++c) {
+                        if (r[(c * 12 + 11) * 32] != 0.f) {
+#pragma unroll
+                            for (int q = 0; q < 11; ++q) acc[c][q] += r[(c * 12 + q) * 32];
+                            actbits |= 1u << c;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        // 3. steps: (lane, frequency) pairs with active coefficients, spread over the warp
+        const int n2 = __popc(actbits);
+        int incl2 = n2;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int v = __shfl_up_sync(full, incl2, d);
+            if (lane >= d) incl2 += v;
+        }
+        const int off2 = incl2 - n2;
+        const int total2 = __shfl_sync(full, incl2, 31);
+        if (total2 == 0) return;
+        // publish this lane's sums (step inputs) in the results buffer: [lane][c][12]
+        {
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+#pragma unroll
+                for (int q = 0; q < 11; ++q) res[(c * 12 + q) * 32 + lane] = acc[c][q];
+        }
+        meta_off[lane] = off2;
+        meta_bits[lane] = actbits;
+        __syncwarp();
+        for (int base = 0; base < total2; base += 32) {
+            const int g = base + lane;
+            if (g < total2) {
+                // owner: the last lane whose first item is <= g (offsets are non-decreasing)
+                int o = 0;
+#pragma unroll
+                for (int d = 16; d >= 1; d >>= 1)
+                    if (o + d < 32 && meta_off[o + d] <= g) o += d;
+                // its (g - off)-th active frequency
+                unsigned bits = meta_bits[o];
+                int j = g - meta_off[o];
+                for (int q = 0; q < j; ++q) bits &= bits - 1;
+                const int c = __ffs(bits) - 1;
+                float in[11];
+#pragma unroll
+                for (int q = 0; q < 11; ++q) in[q] = res[(c * 12 + q) * 32 + o];
+                float Lc = Lnu[0];
+#pragma unroll
+                for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;   // no dynamic register indexing
+                float Dl = Lc * sf[SF_SG * 32 + o];   // the owner's Sigma dtau
+                float O[16], E[4];
+                transfer_step(c_moments, in, in + 4, in + 8, Dl, O, E);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) sres[q * 32 + lane] = O[q];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) sres[(16 + q) * 32 + lane] = E[q];
+            }
+            __syncwarp();
+            // owners compose their steps front to back (frequency order)
+            const int lo = max(off2, base), hi = min(off2 + n2, base + 32);
+            if (lo < hi) {
+                unsigned bits = actbits;
+                for (int q = off2; q < lo; ++q) bits &= bits - 1;
+                for (int g2 = lo; g2 < hi; ++g2) {
+                    const int c = __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    float OE[20];
+#pragma unroll
+                    for (int q = 0; q < 20; ++q) OE[q] = sres[q * 32 + (g2 - base)];
+                    float* st = state + c * 20 * kMixedBlock;   // this thread's column, fields kMixedBlock apart
+                    float P[16], S4[4];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) P[q] = st[q * kMixedBlock];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) S4[q] = st[(16 + q) * kMixedBlock];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        S4[r] += P[4 * r] * OE[16] + P[4 * r + 1] * OE[17] + P[4 * r + 2] * OE[18] + P[4 * r + 3] * OE[19];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            st[(4 * r + q) * kMixedBlock] = P[4 * r] * OE[q] + P[4 * r + 1] * OE[4 + q] + P[4 * r + 2] * OE[8 + q] + P[4 * r + 3] * OE[12 + q];
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) st[(16 + q) * kMixedBlock] = S4[q];
+                    ev[6]++;
+                }
+            }
+            __syncwarp();
+        }
+    }
+};
+
+// ks_coords is defined in ks_lib.cu before this header is included.
+
+// Persistent launch: every warp takes work units (32 consecutive sorted rays x one segment of the
+// sample range x one frame and up to CH frequencies) from a device counter until none is left, the
+// last rays first (the plunging rays near the centre of the screen, sorted last, carry most of the
+// transport work). A segment [k0, k1) composes its own (P, S) from the identity; k_combine
+// composes the segments of a ray front to back (S = S_0 + P_0 (S_1 + P_1 (...))).
+struct MixedJob {
+    long long npix;
+    int nframes, nfreq, nseg, seg_len, nvc;
+    long long nchunks, total;
+    int nmax;
+    float slab;
+    double L;
+};
+
+template <int CH>
+__global__ void __launch_bounds__(kMixedBlock, 2)
+k_mixed(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64, int ntot, const double* __restrict__ ct,
+        const double* __restrict__ cnu, unsigned long long* __restrict__ work, float* __restrict__ seg_out,
+        unsigned long long* __restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* tab = reinterpret_cast<float*>(smem);
+    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
+    unsigned char* wbase = smem + size_t(ntot) * ST_COUNT * 4;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wb = wbase + size_t(warp) * MixedSmem<CH>::kWarpBytes;
+    float* state_base = reinterpret_cast<float*>(wbase + size_t(kWarps) * MixedSmem<CH>::kWarpBytes);
+    __syncthreads();
+    unsigned int ev[7] = {0, 0, 0, 0, 0, 0, 0};
+    unsigned int samples_c = 0;
+    const int N = st.N;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(work, 1ull);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= (unsigned long long)job.total) break;
+        const long long ur = job.total - 1 - (long long)u;          // last rays first
+        const long long w = ur / (job.nseg * (long long)job.nframes * job.nvc);
+        const long long rem = ur % (job.nseg * (long long)job.nframes * job.nvc);
+        const int seg = int(rem / (job.nframes * job.nvc));
+        const int y = int(rem % (job.nframes * job.nvc));
+        const int f = y / job.nvc, v0 = (y % job.nvc) * CH;
+        const long long j0 = w * 32 + lane;
+        const bool live = j0 < job.npix;
+        const long long j = live ? j0 : job.npix - 1;
+        const int k0 = 1 + seg * job.seg_len;
+        const int k1 = min(N + 1, k0 + job.seg_len);
+        MarchRay<float> R = load_ray<float>(P, st, j);
+        MixedSink<CH> sink;
+        sink.tab = tab; sink.ntot = ntot;
+        sink.t_obs = float(ct[f]);
+        sink.nc = min(CH, job.nfreq - v0);
+        for (int c = 0; c < CH; ++c) {
+            int v = min(v0 + c, job.nfreq - 1);
+            double nh = cnu[v] / kNU0;
+            sink.nu[c] = float(cnu[v]);
+            sink.Lnu[c] = float(job.L / nh);
+        }
+        sink.a = float(st.a); sink.rh_lo = float(st.rh * (1 + 1e-3)); sink.dtau = float(R.dtau);
+        sink.alpha = float(P.get(PF_ALPHA, j)); sink.beta = float(P.get(PF_BETA, j)); sink.eta = R.eta; sink.lam = R.lam;
+        sink.a_sin_tho = float(st.a * sin(st.thetao)); sink.slab = job.slab; sink.nmax = job.nmax;
+        sink.lane = lane; sink.live = live;
+        sink.sf = reinterpret_cast<float*>(wb);
+        sink.items = reinterpret_cast<uint16_t*>(wb + MixedSmem<CH>::kSampleBytes);
+        sink.sres = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes);
+        sink.res = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes);
+        sink.meta_off = reinterpret_cast<int*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes + MixedSmem<CH>::kResBytes);
+        sink.meta_bits = reinterpret_cast<unsigned*>(sink.meta_off + 32);
+        sink.state = state_base + threadIdx.x;
+        sink.init();
+        march_range(P, j, R, sink, k0, k1);
+        __syncwarp();
+        if (live) {
+            for (int c = 0; c < sink.nc; ++c) {
+                const float* S = sink.state + c * 20 * kMixedBlock;
+                float* o = seg_out + (((long long)((v0 + c) * job.nframes + f) * job.nseg + seg) * job.npix + j) * 20;
+#pragma unroll
+                for (int q = 0; q < 20; ++q) o[q] = S[q * kMixedBlock];
+            }
+            for (int q = 0; q < 7; ++q) ev[q] += sink.ev[q];
+            samples_c += sink.ev[0] * sink.nc;
+        }
+        __syncwarp();
+    }
+    if (counters) {
+        atomicAdd(&counters[0], (unsigned long long)samples_c);
+        for (int q = 1; q < 7; ++q) atomicAdd(&counters[q], (unsigned long long)ev[q]);
+    }
+}
+
+// Front-to-back composition of a ray's segments and the observed Stokes vector (x nuhat^3).
+__global__ void k_combine(MixedJob job, const double* __restrict__ cnu, const float* __restrict__ seg_out, double* __restrict__ out) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ncombo = (long long)job.nframes * job.nfreq;
+    if (q >= job.npix * ncombo) return;
+    const long long combo = q / job.npix, j = q % job.npix;
+    const float* base = seg_out + ((combo * job.nseg) * job.npix + j) * 20;
+    double S[4];
+    const float* last = base + (long long)(job.nseg - 1) * job.npix * 20;
+    for (int r = 0; r < 4; ++r) S[r] = last[16 + r];
+    for (int s = job.nseg - 2; s >= 0; --s) {
+        const float* PS = base + (long long)s * job.npix * 20;
+        double Sn[4];
+        for (int r = 0; r < 4; ++r)
+            Sn[r] = PS[16 + r] + PS[4 * r] * S[0] + PS[4 * r + 1] * S[1] + PS[4 * r + 2] * S[2] + PS[4 * r + 3] * S[3];
+        for (int r = 0; r < 4; ++r) S[r] = Sn[r];
+    }
+    const int v = int(combo / job.nframes);
+    const double nh = cnu[v] / kNU0, n3 = nh * nh * nh;
+    double* o = out + (combo * job.npix + j) * 4;
+    for (int r = 0; r < 4; ++r) o[r] = S[r] * n3;
+}
+
+}  // namespace ks

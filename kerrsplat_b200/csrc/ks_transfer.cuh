@@ -28,7 +28,7 @@ enum SplatTab {
     ST_BMAG, ST_BHX, ST_BHY, ST_BHZ, ST_U1, ST_U2, ST_U3, ST_BZERO,
     ST_P, ST_GMIN, ST_GMAX, ST_GSPAN, ST_GAMJ, ST_GAMA,
     ST_KAP, ST_W, ST_HYP, ST_G43, ST_G2, ST_GQ, ST_GP, ST_GK2, ST_KB,
-    ST_KIND,
+    ST_KIND, ST_RHO,
     ST_COUNT
 };
 
@@ -47,6 +47,16 @@ __device__ __forceinline__ float pow2_below(float v) {
     return ldexpf(1.0f, e - 1);
 }
 
+// Transcendentals of the coefficient fits: the hardware approximations in FP32 (relative errors of a
+// few 1e-6 at the arguments these fits take, inside the mixed path's 1e-4 budget), the correctly
+// rounded library functions in FP64.
+__device__ __forceinline__ float fpow(float x, float y) { return __powf(x, y); }
+__device__ __forceinline__ double fpow(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float fexp(float x) { return __expf(x); }
+__device__ __forceinline__ double fexp(double x) { return exp(x); }
+__device__ __forceinline__ float flog(float x) { return __logf(x); }
+__device__ __forceinline__ double flog(double x) { return log(x); }
+
 // ---- coefficients.jl ------------------------------------------------------------------------------
 template <class T>
 struct Coef { T jI, jQ, jV, aI, aQ, aV, rQ, rV; };
@@ -57,6 +67,7 @@ __device__ __forceinline__ T planck(T nu, T Te) {
     T nh = nu / T(kNU0);
     T pref = T(kPLANCK0) * nh * nh * nh;
     if (x < T(2e-3)) return pref / (x / T(24) * (T(24) + x * (T(12) + x * (T(4) + x))));
+    if constexpr (sizeof(T) == 4) return pref / expm1f(x);   // no cancellation in FP32
     return pref / (exp(x) - T(1));
 }
 
@@ -75,22 +86,22 @@ __device__ __forceinline__ Coef<T> thermal(T ne, T Te, T f0, T kr, T B, T nu, T 
         return {T(0), T(0), T(0), T(0), T(0), T(0), T(0), rV0};
     }
     T x = Te * sqrt(T(1.4142135623730951) * st * (T(1e3) * w0w));
-    T extraterm = (T(0.011) * exp(-x / T(47.2)) - T(7.9370052598409974e-01 /* 2^(-1/3) */) / T(67.44733739010397 /* 3^(23/6) */) * PI * T(1e4) * pow(x + T(1e-16), T(-8.0 / 3))) *
-                  (T(0.5) + T(0.5) * tanh((log(x) - T(4.787491742782046 /* ln 120 */)) / T(0.1)));
-    T jffunc = T(2.011) * exp(-pow(x, T(1.035)) / T(4.7)) - cos(x / T(2)) * exp(-pow(x, T(1.2)) / T(2.73)) - T(0.011) * exp(-x / T(47.2)) + extraterm;
+    T extraterm = (T(0.011) * fexp(-x / T(47.2)) - T(7.9370052598409974e-01 /* 2^(-1/3) */) / T(67.44733739010397 /* 3^(23/6) */) * PI * T(1e4) * fpow(x + T(1e-16), T(-8.0 / 3))) *
+                  (T(0.5) + T(0.5) * tanh((flog(x) - T(4.787491742782046 /* ln 120 */)) / T(0.1)));
+    T jffunc = T(2.011) * fexp(-fpow(x, T(1.035)) / T(4.7)) - cos(x / T(2)) * fexp(-fpow(x, T(1.2)) / T(2.73)) - T(0.011) * fexp(-x / T(47.2)) + extraterm;
     T eps11m22 = jffunc * wp2w2 * w0w * w0w * (kr + T(6) * Te) * st * st;
     T rQ = w / (T(2) * T(kCL)) * eps11m22;
-    T ff = f0 * (T(1) - T(0.11) * log(T(1) + T(0.035) * x));
+    T ff = f0 * (T(1) - T(0.11) * flog(T(1) + T(0.035) * x));
     T rV = w / T(kCL) * (wp2w2 * w0w * ff * ct);
     T nus = T(3) * T(kEE) * B * st / (T(4) * PI * T(kME) * T(kCL)) * Te * Te + T(1);
     T xs = nu / nus;
-    T c13 = pow(xs, T(-1.0 / 3)), c23 = c13 * c13;
-    T e13 = exp(T(-1.8899) / c13);     // exp(-1.8899 x^(1/3))
+    T c13 = fpow(xs, T(-1.0 / 3)), c23 = c13 * c13;
+    T e13 = fexp(T(-1.8899) / c13);     // fexp(-1.8899 x^(1/3))
     T pref = ne * T(kEE) * T(kEE) * nu / (T(2) * T(1.7320508075688772) * T(kCL) * Te * Te);
     T jI = pref * T(2.5651) * (T(1) + T(1.92) * c13 + T(0.9977) * c23) * e13;
     T jQ = pref * T(2.5651) * (T(1) + T(0.93193) * c13 + T(0.499873) * c23) * e13;
     T jV = T(2) * ne * T(kEE) * T(kEE) * nu * ct / st / (T(3) * T(1.7320508075688772) * T(kCL) * Te * Te * Te) *
-           ((T(1.81384) / xs + T(3.42319) * c23 + T(0.0292545) * pow(xs, T(-0.5)) + T(2.03773) * c13) * e13);
+           ((T(1.81384) / xs + T(3.42319) * c23 + T(0.0292545) * fpow(xs, T(-0.5)) + T(2.03773) * c13) * e13);
     T Bn = planck(nu, Te);
     T invB = Bn > T(0) ? T(1) / Bn : T(0);
     return {jI, jQ, jV, jI * invB, jQ * invB, jV * invB, rQ, rV};
@@ -105,40 +116,40 @@ __device__ __forceinline__ Coef<T> powerlaw(T ne, T p, T gmin, T gspan, T gamj, 
     T nc = T(kEE) * B / (T(2) * PI * T(kME) * T(kCL));
     T pref = ne * T(kEE) * T(kEE) * nc / T(kCL);
     T xx = nu / (nc * st);
-    T jI = pref * (pow(T(3), p / T(2)) * (p - T(1)) * st) / (T(2) * (p + T(1)) * gspan) * gamj * pow(xx, -(p - T(1)) / T(2));
+    T jI = pref * (fpow(T(3), p / T(2)) * (p - T(1)) * st) / (T(2) * (p + T(1)) * gspan) * gamj * fpow(xx, -(p - T(1)) / T(2));
     T jQ = (p + T(1)) / (p + T(7.0 / 3)) * jI;
-    T jV = T(171.0 / 250) * pow(p, T(49.0 / 100)) * ct / st * pow(nu / (T(3) * nc * st), T(-0.5)) * jI;
+    T jV = T(171.0 / 250) * fpow(p, T(49.0 / 100)) * ct / st * fpow(nu / (T(3) * nc * st), T(-0.5)) * jI;
     T apref = ne * T(kEE) * T(kEE) / (nu * T(kME) * T(kCL));
-    T aI = apref * pow(T(3), (p + T(1)) / T(2)) * (p - T(1)) / (T(4) * gspan) * gama * pow(xx, -(p + T(2)) / T(2));
-    T aQ = aI * pow(T(17.0 / 500) * p - T(43.0 / 1250), T(43.0 / 500));
-    T term6 = pow(T(31.0 / 10) * pow(st, T(-48.0 / 25)) - T(31.0 / 10), T(64.0 / 125));
+    T aI = apref * fpow(T(3), (p + T(1)) / T(2)) * (p - T(1)) / (T(4) * gspan) * gama * fpow(xx, -(p + T(2)) / T(2));
+    T aQ = aI * fpow(T(17.0 / 500) * p - T(43.0 / 1250), T(43.0 / 500));
+    T term6 = fpow(T(31.0 / 10) * fpow(st, T(-48.0 / 25)) - T(31.0 / 10), T(64.0 / 125));
     T sg = ct > T(0) ? T(1) : (ct < T(0) ? T(-1) : T(0));
-    T aV = aI * pow(T(71.0 / 100) * p + T(22.0 / 625), T(197.0 / 500)) * term6 * pow(xx, T(-0.5)) * sg;
+    T aV = aI * fpow(T(71.0 / 100) * p + T(22.0 / 625), T(197.0 / 500)) * term6 * fpow(xx, T(-0.5)) * sg;
     // rotativities
     T nB = T(kEE) * B * st / (T(2) * PI * T(kME) * T(kCL));
     T rperp = ne * T(kEE) * T(kEE) * (p - T(1)) / (T(kME) * T(kCL) * nB * gspan);
     T nmin = gmin * gmin * nB;
-    T rQ = -rperp * pow(nB / nu, T(3)) * pow(gmin, T(2) - p) * (T(1) - pow(nmin / nu, p / T(2) - T(1))) / (p / T(2) - T(1));
-    T rV = T(2) * (p + T(2)) / (p + T(1)) * rperp * sq(nB / nu) * pow(gmin, -(p + T(1))) * log(gmin) * ct / st;
+    T rQ = -rperp * fpow(nB / nu, T(3)) * fpow(gmin, T(2) - p) * (T(1) - fpow(nmin / nu, p / T(2) - T(1))) / (p / T(2) - T(1));
+    T rV = T(2) * (p + T(2)) / (p + T(1)) * rperp * sq(nB / nu) * fpow(gmin, -(p + T(1))) * flog(gmin) * ct / st;
     return {jI, jQ, jV, aI, aQ, aV, rQ, rV};
 }
 
 // kappa.jl:158-203 (Marszewski+ 2021 rotativity fits)
 template <class T>
 __device__ __forceinline__ T kappa_rhoQ_fit(int i, T w, T X) {
-    T sw = sqrt(w), e5 = exp(T(-5) * w), x84 = pow(X, T(0.84));
-    if (i == 1) return (T(17) * w - T(3) * sw + T(7) * sw * e5) * (T(1) - exp(-x84 / T(30)) - sin(X / T(10)) * exp(T(-3) * pow(X, T(0.471)) / T(2)));
-    if (i == 2) return (T(46) * w / T(3) - T(5) * sw / T(3) + T(17) * sw / T(3) * e5) * (T(1) - exp(-x84 / T(18)) - sin(X / T(6)) * exp(T(-7) * pow(X, T(0.5)) / T(4)));
-    if (i == 3) return (T(14) * w - T(13) * sw / T(8) + T(9) * sw / T(2) * e5) * (T(1) - exp(-x84 / T(12)) - sin(X / T(4)) * exp(T(-2) * pow(X, T(0.525))));
-    return (T(25) * w / T(2) - sw + T(5) * sw * e5) * (T(1) - exp(-x84 / T(8)) - sin(T(3) * X / T(8)) * exp(T(-9) * pow(X, T(0.541)) / T(4)));
+    T sw = sqrt(w), e5 = fexp(T(-5) * w), x84 = fpow(X, T(0.84));
+    if (i == 1) return (T(17) * w - T(3) * sw + T(7) * sw * e5) * (T(1) - fexp(-x84 / T(30)) - sin(X / T(10)) * fexp(T(-3) * fpow(X, T(0.471)) / T(2)));
+    if (i == 2) return (T(46) * w / T(3) - T(5) * sw / T(3) + T(17) * sw / T(3) * e5) * (T(1) - fexp(-x84 / T(18)) - sin(X / T(6)) * fexp(T(-7) * fpow(X, T(0.5)) / T(4)));
+    if (i == 3) return (T(14) * w - T(13) * sw / T(8) + T(9) * sw / T(2) * e5) * (T(1) - fexp(-x84 / T(12)) - sin(X / T(4)) * fexp(T(-2) * fpow(X, T(0.525))));
+    return (T(25) * w / T(2) - sw + T(5) * sw * e5) * (T(1) - fexp(-x84 / T(8)) - sin(T(3) * X / T(8)) * fexp(T(-9) * fpow(X, T(0.541)) / T(4)));
 }
 template <class T>
 __device__ __forceinline__ T kappa_rhoV_fit(int i, T w, T X) {
-    T xm = pow(X, T(-0.5));
-    if (i == 1) return (w * w + T(2) * w + T(1)) / (T(25) * w * w / T(8) + T(4) * w + T(1)) * (T(1) - T(0.17) * log(T(1) + T(0.447) * xm));
-    if (i == 2) return (w * w + T(54) * w + T(50)) / (T(30) * w * w / T(11) + T(134) * w + T(50)) * (T(1) - T(0.17) * log(T(1) + T(0.391) * xm));
-    if (i == 3) return (w * w + T(43) * w + T(38)) / (T(7) * w * w / T(3) + T(185) * w / T(2) + T(38)) * (T(1) - T(0.17) * log(T(1) + T(0.348) * xm));
-    return (w + T(13.0 / 14)) / (T(2) * w + T(13.0 / 14)) * (T(1) - T(0.17) * log(T(1) + T(0.313) * xm));
+    T xm = fpow(X, T(-0.5));
+    if (i == 1) return (w * w + T(2) * w + T(1)) / (T(25) * w * w / T(8) + T(4) * w + T(1)) * (T(1) - T(0.17) * flog(T(1) + T(0.447) * xm));
+    if (i == 2) return (w * w + T(54) * w + T(50)) / (T(30) * w * w / T(11) + T(134) * w + T(50)) * (T(1) - T(0.17) * flog(T(1) + T(0.391) * xm));
+    if (i == 3) return (w * w + T(43) * w + T(38)) / (T(7) * w * w / T(3) + T(185) * w / T(2) + T(38)) * (T(1) - T(0.17) * flog(T(1) + T(0.348) * xm));
+    return (w + T(13.0 / 14)) / (T(2) * w + T(13.0 / 14)) * (T(1) - T(0.17) * flog(T(1) + T(0.313) * xm));
 }
 
 // kappa.jl:109-155; g43 = Gamma(k - 4/3), g2 = Gamma(k - 2), gq = Gamma(k/4 - 1/3), gp = Gamma(k/4 + 4/3),
@@ -154,42 +165,42 @@ __device__ __forceinline__ Coef<T> kappa(T ne, T kap, T w, T hyp, T g43, T g2, T
     T pref = ne * T(kEE) * T(kEE) * nc * st / T(kCL);
     T c373 = T(12.980246132766677);  // 3^(7/3)
     T NlowI = T(4) * PI * g43 / (c373 * g2);
-    T hk = T(0.25) * pow(T(3), (kap - T(1)) / T(2)) * (kap - T(2)) * (kap - T(1)) * gq * gp;
+    T hk = T(0.25) * fpow(T(3), (kap - T(1)) / T(2)) * (kap - T(2)) * (kap - T(1)) * gq * gp;
     T NhighI = hk + small;
-    T xI = T(3) * pow(kap, T(-1.5));
-    T X13 = pow(X, T(1.0 / 3));
-    T jI = pref * NlowI * X13 * pow(T(1) + pow(X, xI * (T(3) * kap - T(4)) / T(6)) * pow(NlowI / NhighI, xI), T(-1) / xI);
+    T xI = T(3) * fpow(kap, T(-1.5));
+    T X13 = fpow(X, T(1.0 / 3));
+    T jI = pref * NlowI * X13 * fpow(T(1) + fpow(X, xI * (T(3) * kap - T(4)) / T(6)) * fpow(NlowI / NhighI, xI), T(-1) / xI);
     T NlowQ = T(-0.5) * T(4) * PI * g43 / (c373 * g2);
     T NhighQ = -(T(0.64) + kap / T(50)) * hk + small;
-    T xQ = T(3.7) * pow(kap, T(-1.6));
-    T jQ = -(pref * NlowQ * X13 * pow(T(1) + pow(X, xQ * (T(3) * kap - T(4)) / T(6)) * pow(NlowQ / NhighQ, xQ), T(-1) / xQ));
-    T NlowV = -T(0.5625) * pow(pow(st, T(-12.0 / 5)) - T(1), T(12.0 / 25)) * (pow(kap, T(-66.0 / 125)) / w) * pow(X, T(-7.0 / 20)) * T(4) * PI * g43 / (c373 * g2);
-    T NhighV = -T(0.765625) * pow(pow(st, T(-2.5)) - T(1), T(11.0 / 25)) * (pow(kap, T(-11.0 / 25)) / w) * pow(X, T(-0.5)) * hk - small;
-    T xV = T(3) * pow(kap, T(-1.5));
+    T xQ = T(3.7) * fpow(kap, T(-1.6));
+    T jQ = -(pref * NlowQ * X13 * fpow(T(1) + fpow(X, xQ * (T(3) * kap - T(4)) / T(6)) * fpow(NlowQ / NhighQ, xQ), T(-1) / xQ));
+    T NlowV = -T(0.5625) * fpow(fpow(st, T(-12.0 / 5)) - T(1), T(12.0 / 25)) * (fpow(kap, T(-66.0 / 125)) / w) * fpow(X, T(-7.0 / 20)) * T(4) * PI * g43 / (c373 * g2);
+    T NhighV = -T(0.765625) * fpow(fpow(st, T(-2.5)) - T(1), T(11.0 / 25)) * (fpow(kap, T(-11.0 / 25)) / w) * fpow(X, T(-0.5)) * hk - small;
+    T xV = T(3) * fpow(kap, T(-1.5));
     T sg = ct > T(0) ? T(1) : (ct < T(0) ? T(-1) : T(0));
     const T small2 = sizeof(T) == 8 ? T(1e-80) : T(0);   // small^2 (zero in FP32)
     T jV = fabs(NhighV) < small2 ? T(0)
-         : -(pref * NlowV * X13 * pow(T(1) + pow(X, xV * (T(3) * kap - T(4)) / T(6)) * pow(NlowV / NhighV, xV), T(-1) / xV)) * sg;
+         : -(pref * NlowV * X13 * fpow(T(1) + fpow(X, xV * (T(3) * kap - T(4)) / T(6)) * fpow(NlowV / NhighV, xV), T(-1) / xV)) * sg;
     T apref = ne * T(kEE) / (B * st);
     T g53 = T(0.9027452929509336);  // Gamma(5/3)
     T ck = (kap - T(2)) * (kap - T(1)) * kap;
     T c16 = T(1.2009369551760027);  // 3^(1/6)
-    T base = c16 * T(10.0 / 41) * T(4) * PI * PI / pow(w * kap, T(16.0 / 3) - kap) * ck / (T(3) * kap - T(1)) * g53 * hyp;
-    T hiA = T(2) * pow(PI, T(2.5)) / T(3) * ck / pow(w * kap, T(5)) * (T(2) * gk2 / (T(2) + kap) - T(1));
+    T base = c16 * T(10.0 / 41) * T(4) * PI * PI / fpow(w * kap, T(16.0 / 3) - kap) * ck / (T(3) * kap - T(1)) * g53 * hyp;
+    T hiA = T(2) * fpow(PI, T(2.5)) / T(3) * ck / fpow(w * kap, T(5)) * (T(2) * gk2 / (T(2) + kap) - T(1));
     T NlowA = base;
-    T NhighA = hiA * (pow(T(3) / kap, T(19.0 / 4)) + T(3.0 / 5)) + small;
-    T xA = pow(T(-7.0 / 4) + T(8) * kap / T(5), T(-43.0 / 50));
-    T X53 = pow(X, T(-5.0 / 3));
-    T aI = apref * NlowA * X53 * pow(T(1) + pow(X, xA * (T(3) * kap - T(1)) / T(6)) * pow(NlowA / NhighA, xA), T(-1) / xA);
+    T NhighA = hiA * (fpow(T(3) / kap, T(19.0 / 4)) + T(3.0 / 5)) + small;
+    T xA = fpow(T(-7.0 / 4) + T(8) * kap / T(5), T(-43.0 / 50));
+    T X53 = fpow(X, T(-5.0 / 3));
+    T aI = apref * NlowA * X53 * fpow(T(1) + fpow(X, xA * (T(3) * kap - T(1)) / T(6)) * fpow(NlowA / NhighA, xA), T(-1) / xA);
     T NlowQA = -T(25.0 / 48) * base;
-    T NhighQA = -(T(441) * pow(kap, T(-144.0 / 25)) + T(11.0 / 20)) * hiA + small;
-    T xQA = T(1.4) * pow(kap, T(-23.0 / 20));
-    T aQ = -(apref * NlowQA * X53 * pow(T(1) + pow(X, xQA * (T(3) * kap - T(1)) / T(6)) * pow(NlowQA / NhighQA, xQA), T(-1) / xQA));
-    T NlowVA = -(T(77) / (T(100) * w)) * pow(pow(st, T(-114.0 / 50)) - T(1), T(223.0 / 500)) * pow(X, T(-7.0 / 20)) * pow(kap, T(-0.7)) * base;
-    T NhighVA = -(T(14.3) * pow(w, T(-116.0 / 125))) * pow(pow(st, T(-41.0 / 20)) - T(1), T(0.5)) *
-                (T(169) * pow(kap, T(-8)) + T(13.0 / 2500) * kap - T(263.0 / 5000) + T(47) / (T(200) * kap)) * pow(X, T(-0.5)) * hiA + small;
-    T xVA = T(1.22) * pow(kap, T(-142.0 / 125)) + T(7.0 / 1000);
-    T aV = -(apref * NlowVA * X53 * pow(T(1) + pow(X, xVA * (T(3) * kap - T(1)) / T(6)) * pow(NlowVA / NhighVA, xVA), T(-1) / xVA)) * sg;
+    T NhighQA = -(T(441) * fpow(kap, T(-144.0 / 25)) + T(11.0 / 20)) * hiA + small;
+    T xQA = T(1.4) * fpow(kap, T(-23.0 / 20));
+    T aQ = -(apref * NlowQA * X53 * fpow(T(1) + fpow(X, xQA * (T(3) * kap - T(1)) / T(6)) * fpow(NlowQA / NhighQA, xQA), T(-1) / xQA));
+    T NlowVA = -(T(77) / (T(100) * w)) * fpow(fpow(st, T(-114.0 / 50)) - T(1), T(223.0 / 500)) * fpow(X, T(-7.0 / 20)) * fpow(kap, T(-0.7)) * base;
+    T NhighVA = -(T(14.3) * fpow(w, T(-116.0 / 125))) * fpow(fpow(st, T(-41.0 / 20)) - T(1), T(0.5)) *
+                (T(169) * fpow(kap, T(-8)) + T(13.0 / 2500) * kap - T(263.0 / 5000) + T(47) / (T(200) * kap)) * fpow(X, T(-0.5)) * hiA + small;
+    T xVA = T(1.22) * fpow(kap, T(-142.0 / 125)) + T(7.0 / 1000);
+    T aV = -(apref * NlowVA * X53 * fpow(T(1) + fpow(X, xVA * (T(3) * kap - T(1)) / T(6)) * fpow(NlowVA / NhighVA, xVA), T(-1) / xVA)) * sg;
     // rotativities (kappa.jl:188-203)
     T Xr = nu / ((w * kap) * (w * kap) * nc * st);
     T kc = fmin(T(5), fmax(T(3.5), kap));
