@@ -594,7 +594,7 @@ struct ks_context {
     bool regenerated = false;
     Spacetime st{};
     DevBuf alpha, beta, key, key2, idx, perm, plan, nanch, aoff, anchors, resid_t, resid_phi, scratch;
-    DevBuf tab, combos, out_sorted, stage_in, stage_out, counters, seg_out, work;
+    DevBuf tab, combos, out_sorted, stage_in, stage_out, counters, seg_out, work, stream_buf;
     bool count_events = false;
     long long total_anchors = 0;
     int max_nanch = 0;
@@ -699,24 +699,32 @@ template <int CH>
 int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, int nmax, double slab) {
     size_t smem = MixedSmem<CH>::bytes(ntot);
     if (smem > 227 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
-    KS_CUDA(c, cudaFuncSetAttribute(k_mixed<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    KS_CUDA(c, cudaFuncSetAttribute(k_consume<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    KS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mixed<CH>, kMixedBlock, smem));
+    KS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_consume<CH>, kMixedBlock, smem));
     int nsm = 0;
     KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     per_sm = std::max(per_sm, 1);
+    const int M = c->st.M, N = c->st.N;
+    // 1. the FP32 sample stream (one march per ray, shared by every frame and frequency)
+    const int sseg = std::max(M, (N / 4 + M - 1) / M * M);
+    const int nsseg = (N + sseg - 1) / sseg;
+    KS_CUDA(c, c->stream_buf.ensure(size_t(N) * SM_COUNT * c->npad * sizeof(float)));
+    k_stream<<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    // 2. the persistent consumer
     MixedJob job;
-    job.npix = c->npix; job.nframes = nframes; job.nfreq = nfreq;
+    job.npix = c->npix; job.npad = c->npad; job.nframes = nframes; job.nfreq = nfreq;
     job.nvc = (nfreq + CH - 1) / CH;
     job.nchunks = (c->npix + 31) / 32;
-    // split the sample range into segments (at multiples of the anchor interval) until there are
-    // about eight work units per resident warp, so that the most expensive unit is short
+    // split the sample range into segments until there are about eight work units per resident
+    // warp, so that the most expensive unit is short
     const long long resident = (long long)nsm * per_sm * kWarps;
     const long long base_units = job.nchunks * nframes * job.nvc;
     int nseg = 1;
-    const int M = c->st.M, N = c->st.N;
-    while (nmax < 0 && base_units * nseg < 8 * resident && (nseg * 2) * M <= N) nseg *= 2;
-    job.seg_len = ((N + nseg - 1) / nseg + M - 1) / M * M;
+    while (nmax < 0 && base_units * nseg < 8 * resident && (nseg * 2) * 16 <= N) nseg *= 2;
+    job.seg_len = (N + nseg - 1) / nseg;
     job.nseg = (N + job.seg_len - 1) / job.seg_len;
     job.total = base_units * job.nseg;
     job.nmax = nmax; job.slab = float(slab); job.L = L;
@@ -727,9 +735,9 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
     KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
     const long long grid = std::min<long long>(job.total / kWarps + 1, (long long)nsm * per_sm);
-    k_mixed<CH><<<unsigned(grid), kMixedBlock, smem, c->stream>>>(
-        plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->work.as<unsigned long long>(), c->seg_out.as<float>(),
-        c->count_events ? c->counters.as<unsigned long long>() : nullptr);
+    k_consume<CH><<<unsigned(grid), kMixedBlock, smem, c->stream>>>(
+        plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
+        c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr);
     c->launches++;
     c->kernel_launches++;
     KS_CUDA(c, cudaGetLastError());
@@ -791,7 +799,7 @@ int ks_context_destroy(ks_context* c) {
     if (!c) return KS_OK;
     cudaSetDevice(c->device);
     for (DevBuf* b : {&c->alpha, &c->beta, &c->key, &c->key2, &c->idx, &c->perm, &c->plan, &c->nanch, &c->aoff, &c->anchors,
-                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out, &c->counters, &c->seg_out, &c->work})
+                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out, &c->counters, &c->seg_out, &c->work, &c->stream_buf})
         b->release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);

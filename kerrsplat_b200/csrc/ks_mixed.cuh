@@ -42,6 +42,52 @@ struct MixedSmem {
     static size_t bytes(int ntot) { return size_t(ntot) * ST_COUNT * 4 + size_t(kWarps) * kWarpBytes + kStateBytes; }
 };
 
+// Out-of-line pieces of the consumer: one copy of each in the instruction cache (inlined into the
+// per-frequency loop and the three populations they overflowed it; ncu: "no instruction" stalls).
+// s: the owner lane's column of the warp's sample data ([field][32] layout)
+__device__ __noinline__ LFrame<float> local_frame_ool(const float* s, const float* p, float a, float a_sin_tho) {
+    SampleFrame<float> F;
+    F.pu[0] = s[SF_PU0 * 32]; F.pu[1] = s[SF_PU1 * 32]; F.pu[2] = s[SF_PU2 * 32]; F.pu[3] = s[SF_PU3 * 32];
+    F.pz[0] = s[SF_PZ0 * 32]; F.pz[1] = s[SF_PZ1 * 32]; F.pz[2] = s[SF_PZ2 * 32]; F.pz[3] = s[SF_PZ3 * 32];
+    F.lapse_inv = s[SF_LI * 32]; F.om_lapse = s[SF_OL * 32]; F.sDS = s[SF_SDS * 32]; F.misS = s[SF_MIS * 32]; F.ivarpi = s[SF_IVP * 32];
+    F.r = s[SF_R * 32]; F.sth = s[SF_STH * 32]; F.cth = s[SF_CTH * 32]; F.a = a;
+    return local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != 0.f,
+                       s[SF_ALPHA * 32], s[SF_BETA * 32], a_sin_tho);
+}
+
+// Screen-basis coefficients of one splat at one frequency (transport.jl:265-270), written with a
+// stride of 32 floats: j (4), alpha (4), rho (3), active flag.
+__device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, float ne, float nuf, float thb, float s2c, float c2c,
+                                                     float* r) {
+    Coef<float> cf;
+    if (kind == KS_POWERLAW22)
+        cf = powerlaw(ne, p[ST_P], p[ST_GMIN], p[ST_GSPAN], p[ST_GAMJ], p[ST_GAMA], p[ST_BMAG], nuf, thb);
+    else if (kind == KS_KAPPA22)
+        cf = kappa(ne, p[ST_KAP], p[ST_W], p[ST_HYP], p[ST_G43], p[ST_G2], p[ST_GQ], p[ST_GP], p[ST_GK2], p[ST_KB], p[ST_BMAG], nuf, thb);
+    else
+        cf = thermal(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
+    bool on = cf.jI > 0.f || cf.aI > 0.f || cf.rQ != 0.f || cf.rV != 0.f;
+    if (!on) { r[352] = 0.f; return; }
+    float fe = cap_factor(cf.jI, cf.jQ, cf.jV, 0.99f);
+    float fa = cap_factor(cf.aI, cf.aQ, cf.aV, 0.99f);
+    float nh = nuf / float(kNU0);
+    float i2 = 1.f / (nh * nh);
+    float jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+    r[0] = cf.jI * i2; r[32] = jQ * c2c; r[64] = jQ * s2c; r[96] = cf.jV * fe * i2;
+    r[128] = nh * cf.aI; r[160] = aQ * c2c; r[192] = aQ * s2c; r[224] = cf.aV * fa * nh;
+    r[256] = rQ * c2c; r[288] = rQ * s2c; r[320] = nh * cf.rV;
+    r[352] = 1.f;
+}
+
+__device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float* O, float* E) {
+    float o[16], e[4];
+    transfer_step(c_moments, in, in + 4, in + 8, Dl, o, e);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) O[q] = o[q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) E[q] = e[q];
+}
+
 template <int CH>
 struct MixedSink {
     const float* tab; int ntot;
@@ -97,70 +143,48 @@ struct MixedSink {
         float q;
         splat_exponent(p, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], false, q);
         float G = __expf(-q);
-        SampleFrame<float> F;
-        F.pu[0] = s[SF_PU0 * 32]; F.pu[1] = s[SF_PU1 * 32]; F.pu[2] = s[SF_PU2 * 32]; F.pu[3] = s[SF_PU3 * 32];
-        F.pz[0] = s[SF_PZ0 * 32]; F.pz[1] = s[SF_PZ1 * 32]; F.pz[2] = s[SF_PZ2 * 32]; F.pz[3] = s[SF_PZ3 * 32];
-        F.lapse_inv = s[SF_LI * 32]; F.om_lapse = s[SF_OL * 32]; F.sDS = s[SF_SDS * 32]; F.misS = s[SF_MIS * 32]; F.ivarpi = s[SF_IVP * 32];
-        F.r = s[SF_R * 32]; F.sth = s[SF_STH * 32]; F.cth = s[SF_CTH * 32]; F.a = a;
-        // the owner's screen coordinates (the pair may belong to another lane's ray)
-        LFrame<float> lf = local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != 0.f,
-                                       s[SF_ALPHA * 32], s[SF_BETA * 32], a_sin_tho);
+        LFrame<float> lf = local_frame_ool(s, p, a, a_sin_tho);
         float thb = acosf(fminf(1.f, fmaxf(-1.f, lf.cosB)));
         float ne = p[ST_NE] * G;
         float s2c, c2c;
         sincosf(2.f * lf.chi, &s2c, &c2c);
         int act = 0;
-#pragma unroll
+#pragma unroll 1
         for (int c = 0; c < CH; ++c) {
             float* r = out + c * 12 * 32;   // out = res + slot; fields are 32 apart
-            if (c >= nc) { r[11 * 32] = 0.f; continue; }
-            float nuf = nu[c] / lf.g;
-            Coef<float> cf;
-            if (kind == KS_POWERLAW22)
-                cf = powerlaw(ne, p[ST_P], p[ST_GMIN], p[ST_GSPAN], p[ST_GAMJ], p[ST_GAMA], p[ST_BMAG], nuf, thb);
-            else if (kind == KS_KAPPA22)
-                cf = kappa(ne, p[ST_KAP], p[ST_W], p[ST_HYP], p[ST_G43], p[ST_G2], p[ST_GQ], p[ST_GP], p[ST_GK2], p[ST_KB], p[ST_BMAG], nuf, thb);
-            else
-                cf = thermal(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
-            bool on = cf.jI > 0.f || cf.aI > 0.f || cf.rQ != 0.f || cf.rV != 0.f;
-            if (!on) { r[11 * 32] = 0.f; continue; }
-            float fe = cap_factor(cf.jI, cf.jQ, cf.jV, 0.99f);
-            float fa = cap_factor(cf.aI, cf.aQ, cf.aV, 0.99f);
-            float nh = nuf / float(kNU0);
-            float i2 = 1.f / (nh * nh);
-            float jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
-            r[0] = cf.jI * i2; r[32] = jQ * c2c; r[64] = jQ * s2c; r[96] = cf.jV * fe * i2;
-            r[128] = nh * cf.aI; r[160] = aQ * c2c; r[192] = aQ * s2c; r[224] = cf.aV * fa * nh;
-            r[256] = rQ * c2c; r[288] = rQ * s2c; r[320] = nh * cf.rV;
-            r[352] = 1.f;
-            act++;
+            if (c >= nc) { r[352] = 0.f; continue; }
+            float nuc = nu[0];
+#pragma unroll
+            for (int cc = 1; cc < CH; ++cc) nuc = (cc == c) ? nu[cc] : nuc;
+            screen_coefficients_ool(kind, p, ne, nuc / lf.g, thb, s2c, c2c, r);
+            act |= r[352] != 0.f;
         }
         ev[4] += act ? 1 : 0;
     }
 
-    // The consumer for one sample of every lane of the warp (all 32 lanes call it together).
-    __device__ void operator()(int, const Sample<float>& s) {
+    // The consumer for one sample of every lane of the warp (all 32 lanes call it together):
+    // `usable` = Krang's validity and outside r_h (1 + 1e-3) (transport.jl:171-173); x, y, z the
+    // quasi-Cartesian Kerr-Schild position, ts the regularized lookback time t~.
+    __device__ void consume(bool usable, float x, float y, float z, float ts, float r, float sth, float cth, bool nur, bool nuth) {
         const unsigned full = 0xffffffffu;
         ev[0]++;
-        bool valid = live && s.ok && s.r > rh_lo;
+        bool valid = live && usable;
         if (valid) ev[1]++;
-        if (valid && nmax >= 0) valid = wind_ok(s.r * cosf(s.theta));
+        if (valid && nmax >= 0) valid = wind_ok(r * cth);
         unsigned vmask = __ballot_sync(full, valid);
         if (vmask == 0u) return;
         float* mys = sf + lane;
-        float x = 0.f, y = 0.f, z = 0.f, t = 0.f, rho = 0.f;
+        float t = 0.f, rho = 0.f;
         if (valid) {
-            float sth, cth;
-            ks_coords(a, s.r, s.theta, s.phi, x, y, z, sth, cth);
             rho = sqrtf(x * x + y * y);
-            t = t_obs - s.t;
-            SampleFrame<float> F = sample_frame(a, s.r, s.theta, sth, cth, eta, lam, s.nur, s.nutheta);
-            mys[SF_X * 32] = x; mys[SF_Y * 32] = y; mys[SF_Z * 32] = z; mys[SF_T * 32] = s.t;
+            t = t_obs - ts;
+            SampleFrame<float> F = sample_frame(a, r, 0.f, sth, cth, eta, lam, nur, nuth);
+            mys[SF_X * 32] = x; mys[SF_Y * 32] = y; mys[SF_Z * 32] = z; mys[SF_T * 32] = ts;
             mys[SF_PU0 * 32] = F.pu[0]; mys[SF_PU1 * 32] = F.pu[1]; mys[SF_PU2 * 32] = F.pu[2]; mys[SF_PU3 * 32] = F.pu[3];
             mys[SF_PZ0 * 32] = F.pz[0]; mys[SF_PZ1 * 32] = F.pz[1]; mys[SF_PZ2 * 32] = F.pz[2]; mys[SF_PZ3 * 32] = F.pz[3];
             mys[SF_LI * 32] = F.lapse_inv; mys[SF_OL * 32] = F.om_lapse; mys[SF_SDS * 32] = F.sDS; mys[SF_MIS * 32] = F.misS; mys[SF_IVP * 32] = F.ivarpi;
-            mys[SF_R * 32] = s.r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
-            mys[SF_SG * 32] = (s.r * s.r + a * a * cth * cth) * dtau;   // Sigma dtau of this lane's ray
+            mys[SF_R * 32] = r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
+            mys[SF_SG * 32] = (r * r + a * a * cth * cth) * dtau;   // Sigma dtau of this lane's ray
             mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
         }
         float acc[CH][11];
@@ -274,7 +298,7 @@ struct MixedSink {
                 for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;   // no dynamic register indexing
                 float Dl = Lc * sf[SF_SG * 32 + o];   // the owner's Sigma dtau
                 float O[16], E[4];
-                transfer_step(c_moments, in, in + 4, in + 8, Dl, O, E);
+                transfer_step_ool(in, Dl, O, E);
 #pragma unroll
                 for (int q = 0; q < 16; ++q) sres[q * 32 + lane] = O[q];
 #pragma unroll
@@ -317,13 +341,46 @@ struct MixedSink {
 
 // ks_coords is defined in ks_lib.cu before this header is included.
 
-// Persistent launch: every warp takes work units (32 consecutive sorted rays x one segment of the
+// The FP32 sample stream: every sample of every ray, marched once per render (the recurrence and the
+// quadrature re-anchored to the FP64 table) and shared by every frame, frequency and parameter set.
+// Layout [k][field][npad] (k = sample - 1): the lanes of a warp (consecutive sorted rays) read and
+// write consecutive addresses.
+enum StreamField { SM_X, SM_Y, SM_Z, SM_T, SM_R, SM_STH, SM_CTH, SM_FLAGS, SM_COUNT };
+
+struct StreamSink {
+    float* out;
+    long long npad, j;
+    float a, rh_lo;
+    __device__ void operator()(int k, const Sample<float>& s) {
+        float* o = out + (long long)(k - 1) * SM_COUNT * npad + j;
+        const bool usable = s.ok && s.r > rh_lo;
+        unsigned flags = (s.ok ? 1u : 0u) | (s.nur ? 2u : 0u) | (s.nutheta ? 4u : 0u) | (usable ? 8u : 0u);
+        float x = 0.f, y = 0.f, z = 0.f, sth = 0.f, cth = 0.f;
+        if (usable) ks_coords(a, s.r, s.theta, s.phi, x, y, z, sth, cth);
+        o[SM_X * npad] = x; o[SM_Y * npad] = y; o[SM_Z * npad] = z; o[SM_T * npad] = s.t;
+        o[SM_R * npad] = s.r; o[SM_STH * npad] = sth; o[SM_CTH * npad] = cth; o[SM_FLAGS * npad] = __uint_as_float(flags);
+    }
+};
+
+// One thread per (ray, segment of seg_len samples starting at an anchor multiple).
+__global__ void __launch_bounds__(128) k_stream(PlanView P, Spacetime st, long long npix, int seg_len, int nseg, float* __restrict__ out) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= npix * nseg) return;
+    const long long j = q % npix;
+    const int seg = int(q / npix);
+    const int k0 = 1 + seg * seg_len, k1 = min(st.N + 1, k0 + seg_len);
+    MarchRay<float> R = load_ray<float>(P, st, j);
+    StreamSink sink{out, P.npad, j, float(st.a), float(st.rh * (1 + 1e-3))};
+    march_range(P, j, R, sink, k0, k1);
+}
+
+// Persistent consumer: every warp takes work units (32 consecutive sorted rays x one segment of the
 // sample range x one frame and up to CH frequencies) from a device counter until none is left, the
 // last rays first (the plunging rays near the centre of the screen, sorted last, carry most of the
 // transport work). A segment [k0, k1) composes its own (P, S) from the identity; k_combine
 // composes the segments of a ray front to back (S = S_0 + P_0 (S_1 + P_1 (...))).
 struct MixedJob {
-    long long npix;
+    long long npix, npad;
     int nframes, nfreq, nseg, seg_len, nvc;
     long long nchunks, total;
     int nmax;
@@ -332,10 +389,10 @@ struct MixedJob {
 };
 
 template <int CH>
-__global__ void __launch_bounds__(kMixedBlock, 2)
-k_mixed(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64, int ntot, const double* __restrict__ ct,
-        const double* __restrict__ cnu, unsigned long long* __restrict__ work, float* __restrict__ seg_out,
-        unsigned long long* __restrict__ counters) {
+__global__ void __launch_bounds__(kMixedBlock, 3)
+k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64, int ntot, const double* __restrict__ ct,
+          const double* __restrict__ cnu, const float* __restrict__ stream, unsigned long long* __restrict__ work,
+          float* __restrict__ seg_out, unsigned long long* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* tab = reinterpret_cast<float*>(smem);
     for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
@@ -347,14 +404,16 @@ k_mixed(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64
     unsigned int ev[7] = {0, 0, 0, 0, 0, 0, 0};
     unsigned int samples_c = 0;
     const int N = st.N;
+    const long long npad = job.npad;
     for (;;) {
         unsigned long long u = 0;
         if (lane == 0) u = atomicAdd(work, 1ull);
         u = __shfl_sync(0xffffffffu, u, 0);
         if (u >= (unsigned long long)job.total) break;
         const long long ur = job.total - 1 - (long long)u;          // last rays first
-        const long long w = ur / (job.nseg * (long long)job.nframes * job.nvc);
-        const long long rem = ur % (job.nseg * (long long)job.nframes * job.nvc);
+        const long long per_chunk = (long long)job.nseg * job.nframes * job.nvc;
+        const long long w = ur / per_chunk;
+        const long long rem = ur % per_chunk;
         const int seg = int(rem / (job.nframes * job.nvc));
         const int y = int(rem % (job.nframes * job.nvc));
         const int f = y / job.nvc, v0 = (y % job.nvc) * CH;
@@ -363,7 +422,6 @@ k_mixed(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64
         const long long j = live ? j0 : job.npix - 1;
         const int k0 = 1 + seg * job.seg_len;
         const int k1 = min(N + 1, k0 + job.seg_len);
-        MarchRay<float> R = load_ray<float>(P, st, j);
         MixedSink<CH> sink;
         sink.tab = tab; sink.ntot = ntot;
         sink.t_obs = float(ct[f]);
@@ -374,8 +432,9 @@ k_mixed(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64
             sink.nu[c] = float(cnu[v]);
             sink.Lnu[c] = float(job.L / nh);
         }
-        sink.a = float(st.a); sink.rh_lo = float(st.rh * (1 + 1e-3)); sink.dtau = float(R.dtau);
-        sink.alpha = float(P.get(PF_ALPHA, j)); sink.beta = float(P.get(PF_BETA, j)); sink.eta = R.eta; sink.lam = R.lam;
+        sink.a = float(st.a); sink.rh_lo = float(st.rh * (1 + 1e-3)); sink.dtau = float(P.get(PF_DTAU, j));
+        sink.alpha = float(P.get(PF_ALPHA, j)); sink.beta = float(P.get(PF_BETA, j));
+        sink.eta = float(P.get(PF_ETA, j)); sink.lam = float(P.get(PF_LAM, j));
         sink.a_sin_tho = float(st.a * sin(st.thetao)); sink.slab = job.slab; sink.nmax = job.nmax;
         sink.lane = lane; sink.live = live;
         sink.sf = reinterpret_cast<float*>(wb);
@@ -386,7 +445,12 @@ k_mixed(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64
         sink.meta_bits = reinterpret_cast<unsigned*>(sink.meta_off + 32);
         sink.state = state_base + threadIdx.x;
         sink.init();
-        march_range(P, j, R, sink, k0, k1);
+        const float* sp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
+        for (int k = k0; k < k1; ++k, sp += SM_COUNT * npad) {
+            const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
+            sink.consume((flags & 8u) != 0u, sp[SM_X * npad], sp[SM_Y * npad], sp[SM_Z * npad], sp[SM_T * npad], sp[SM_R * npad],
+                         sp[SM_STH * npad], sp[SM_CTH * npad], (flags & 2u) != 0u, (flags & 4u) != 0u);
+        }
         __syncwarp();
         if (live) {
             for (int c = 0; c < sink.nc; ++c) {
