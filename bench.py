@@ -42,6 +42,17 @@ def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(value, device=None):
+    """The largest `value` over the ranks of the default process group (a step time, in ms)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -150,10 +161,7 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
     ms_total = e0.elapsed_time(e1)
     render_ms, render_launches, all_launches = cache.kernel_stats(reset=True)
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(ms_total, dev)
     ms_step = ms_total / args.steps
     value = units_per_step * world / (ms_step / 1e3)
 
@@ -171,10 +179,7 @@ def run_ours(args):
     for _ in range(e2e_steps):
         ks.render(cache, ks.PolarizedSplats(c["params"]), [c["t_obs"]], c["nus"], c["L"], precision=prec, out=out_host)
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dev)
     e2e_value = units_per_step * world / (e2e_ms / 1e3)
 
     # roofline of the dominant kernel (k_polarized): algorithmic FP32 work per launch / its time

@@ -224,16 +224,20 @@ __global__ void k_anchor_prefix(long long npix, long long npad, const double* __
 
 // K0 and K1 from K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt by the trapezoidal rule.
 __host__ __device__ void besselk01(double x, double& k0, double& k1) {
-    const double h = 0.125;
-    double s0 = 0.5 * exp(-x), s1 = 0.5 * exp(-x);
-    for (int j = 1; j < 4000; ++j) {
+    // trapezoid in t on exp(-x (cosh t - 1)) (the factor exp(-x) applied at the end); the step
+    // resolves the Gaussian core of width 1/sqrt(x) (error ~ exp(-2 pi^2 / (x h^2)) < 1e-17)
+    const double h = fmin(0.125, 0.6 / sqrt(x));
+    double s0 = 0.5, s1 = 0.5;
+    for (int j = 1; j < 20000; ++j) {
         double t = j * h;
-        double e = exp(-x * cosh(t));
-        if (e == 0.0) break;
-        s0 += e; s1 += e * cosh(t);
-        if (e < 1e-300) break;
+        double ch = cosh(t);
+        double e = exp(-x * (ch - 1.0));
+        s0 += e;
+        s1 += e * ch;
+        if (e < 1e-18 * s0) break;
     }
-    k0 = h * s0; k1 = h * s1;
+    double ex = exp(-x);
+    k0 = h * s0 * ex; k1 = h * s1 * ex;
 }
 
 struct SetDesc {
@@ -695,16 +699,59 @@ int nrows_of(int kind) {
     }
 }
 
+template <int CH, int NT>
+int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int per_sm) {
+    MixedJob job = job0;
+    const int N = c->st.N;
+    constexpr int W = NT / 32;
+    const size_t smem = MixedSmem<CH>::bytes(ntot, W);
+    // split the sample range into segments until there are about eight work units per resident
+    // warp, so that the most expensive unit is short
+    const long long resident = (long long)nsm * per_sm * W;
+    const long long base_units = job.nchunks * job.nframes * job.nvc;
+    int nseg = 1;
+    while (job.nmax < 0 && base_units * nseg < 8 * resident && (nseg * 2) * 16 <= N) nseg *= 2;
+    job.seg_len = (N + nseg - 1) / nseg;
+    job.nseg = (N + job.seg_len - 1) / job.seg_len;
+    job.total = base_units * job.nseg;
+    const double* dt = c->combos.as<double>();
+    const double* dn = dt + job.nframes;
+    const size_t seg_bytes = size_t(job.nframes) * job.nfreq * job.nseg * c->npix * 20 * sizeof(float);
+    KS_CUDA(c, c->seg_out.ensure(seg_bytes));
+    KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
+    KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
+    const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
+    k_consume<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(
+        plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
+        c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr);
+    c->launches++;
+    c->kernel_launches++;
+    KS_CUDA(c, cudaGetLastError());
+    const long long nq = c->npix * (long long)job.nframes * job.nfreq;
+    k_combine<<<nblocks(nq, 256), 256, 0, c->stream>>>(job, dn, c->seg_out.as<float>(), c->out_sorted.as<double>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
+// Occupancy of k_consume<CH, NT> with its shared memory for `ntot` splats (0 if it does not fit).
+template <int CH, int NT>
+int consume_blocks(ks_context* c, int ntot) {
+    const size_t smem = MixedSmem<CH>::bytes(ntot, NT / 32);
+    if (smem > 227 * 1024) return 0;
+    if (cudaFuncSetAttribute(k_consume<CH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_consume<CH, NT>, NT, smem) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return per_sm;
+}
+
 template <int CH>
 int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, int nmax, double slab) {
-    size_t smem = MixedSmem<CH>::bytes(ntot);
-    if (smem > 227 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
-    KS_CUDA(c, cudaFuncSetAttribute(k_consume<CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    KS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_consume<CH>, kMixedBlock, smem));
     int nsm = 0;
     KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    per_sm = std::max(per_sm, 1);
     const int M = c->st.M, N = c->st.N;
     // 1. the FP32 sample stream (one march per ray, shared by every frame and frequency)
     const int sseg = std::max(M, (N / 4 + M - 1) / M * M);
@@ -713,46 +760,28 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     k_stream<<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
     c->launches++;
     KS_CUDA(c, cudaGetLastError());
-    // 2. the persistent consumer
     MixedJob job;
     job.npix = c->npix; job.npad = c->npad; job.nframes = nframes; job.nfreq = nfreq;
     job.nvc = (nfreq + CH - 1) / CH;
     job.nchunks = (c->npix + 31) / 32;
-    // split the sample range into segments until there are about eight work units per resident
-    // warp, so that the most expensive unit is short
-    const long long resident = (long long)nsm * per_sm * kWarps;
-    const long long base_units = job.nchunks * nframes * job.nvc;
-    int nseg = 1;
-    while (nmax < 0 && base_units * nseg < 8 * resident && (nseg * 2) * 16 <= N) nseg *= 2;
-    job.seg_len = (N + nseg - 1) / nseg;
-    job.nseg = (N + job.seg_len - 1) / job.seg_len;
-    job.total = base_units * job.nseg;
     job.nmax = nmax; job.slab = float(slab); job.L = L;
-    const double* dt = c->combos.as<double>();
-    const double* dn = dt + nframes;
-    const size_t seg_bytes = size_t(nframes) * nfreq * job.nseg * c->npix * 20 * sizeof(float);
-    KS_CUDA(c, c->seg_out.ensure(seg_bytes));
-    KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
-    KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
-    const long long grid = std::min<long long>(job.total / kWarps + 1, (long long)nsm * per_sm);
-    k_consume<CH><<<unsigned(grid), kMixedBlock, smem, c->stream>>>(
-        plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
-        c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr);
-    c->launches++;
-    c->kernel_launches++;
-    KS_CUDA(c, cudaGetLastError());
-    const long long nq = c->npix * (long long)nframes * nfreq;
-    k_combine<<<nblocks(nq, 256), 256, 0, c->stream>>>(job, dn, c->seg_out.as<float>(), c->out_sorted.as<double>());
-    c->launches++;
-    KS_CUDA(c, cudaGetLastError());
-    return KS_OK;
+    // the block size with the most resident warps (the per-warp shared memory sets the limit)
+    const int w384 = consume_blocks<CH, 384>(c, ntot) * 12, w352 = consume_blocks<CH, 352>(c, ntot) * 11,
+              w256 = consume_blocks<CH, 256>(c, ntot) * 8, w128 = consume_blocks<CH, 128>(c, ntot) * 4;
+    const int best = std::max(std::max(w384, w352), std::max(w256, w128));
+    if (best <= 0) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
+    if (w384 == best) return launch_consume<CH, 384>(c, job, ntot, nsm, w384 / 12);
+    if (w352 == best) return launch_consume<CH, 352>(c, job, ntot, nsm, w352 / 11);
+    if (w256 == best) return launch_consume<CH, 256>(c, job, ntot, nsm, w256 / 8);
+    if (w128 > 0) return launch_consume<CH, 128>(c, job, ntot, nsm, w128 / 4);
+    return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
+    (void)M;
 }
 
 int launch_mixed(ks_context* c, int ntot, const double* ht, int nframes, int nfreq, double L, int nmax, double slab) {
     (void)ht;
     if (nfreq >= 4) return launch_mixed_ch<4>(c, ntot, nframes, nfreq, L, nmax, slab);
     if (nfreq == 3) return launch_mixed_ch<3>(c, ntot, nframes, nfreq, L, nmax, slab);
-    if (nfreq == 2) return launch_mixed_ch<2>(c, ntot, nframes, nfreq, L, nmax, slab);
     return launch_mixed_ch<1>(c, ntot, nframes, nfreq, L, nmax, slab);
 }
 

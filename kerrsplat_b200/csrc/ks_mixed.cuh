@@ -21,25 +21,23 @@
 
 namespace ks {
 
-constexpr int kMixedBlock = 128;
-constexpr int kWarps = kMixedBlock / 32;
 constexpr float kQCUT = 13.815510557964274f;   // -ln(WEIGHT_CUTOFF): G > 1e-6 <=> q < QCUT
-constexpr int kSF = 24;                         // floats per lane of sample data
 
 // per-lane sample data (shared memory)
 enum SampleField { SF_X, SF_Y, SF_Z, SF_T, SF_PU0, SF_PU1, SF_PU2, SF_PU3, SF_PZ0, SF_PZ1, SF_PZ2, SF_PZ3,
-                   SF_LI, SF_OL, SF_SDS, SF_MIS, SF_IVP, SF_R, SF_STH, SF_CTH, SF_SG, SF_ALPHA, SF_BETA, SF_PAD2 };
+                   SF_LI, SF_OL, SF_SDS, SF_MIS, SF_IVP, SF_R, SF_STH, SF_CTH, SF_SG, SF_ALPHA, SF_BETA, SF_COUNT };
+constexpr int kSF = SF_COUNT;                   // floats per lane of sample data
 
 template <int CH>
 struct MixedSmem {
-    // bytes of the per-warp and per-thread regions (the splat table comes first)
+    // bytes of the per-warp regions (the splat table comes first), all [field][32 lanes]
     static constexpr int kSampleBytes = 32 * kSF * 4;
     static constexpr int kItemBytes = 32 * 32 * 2 > 32 * 20 * 4 ? 32 * 32 * 2 : 32 * 20 * 4;   // item list | step results
     static constexpr int kResBytes = 32 * CH * 12 * 4;                                          // pair results | step inputs
     static constexpr int kMetaBytes = 32 * 4 * 2;
-    static constexpr int kWarpBytes = kSampleBytes + kItemBytes + kResBytes + kMetaBytes;
-    static constexpr int kStateBytes = kMixedBlock * CH * 20 * 4;                               // P (16) and S (4) per lane and frequency
-    static size_t bytes(int ntot) { return size_t(ntot) * ST_COUNT * 4 + size_t(kWarps) * kWarpBytes + kStateBytes; }
+    static constexpr int kStateBytes = 32 * CH * 20 * 4;                                        // P (16) and S (4) per lane and frequency
+    static constexpr int kWarpBytes = kSampleBytes + kItemBytes + kResBytes + kMetaBytes + kStateBytes;
+    static size_t bytes(int ntot, int warps) { return size_t(ntot) * ST_COUNT * 4 + size_t(warps) * kWarpBytes; }
 };
 
 // Out-of-line pieces of the consumer: one copy of each in the instruction cache (inlined into the
@@ -102,7 +100,7 @@ struct MixedSink {
     uint16_t* items;  // this warp's pair list [1024]
     float* sres;      // step results [20][32] (aliases the pair list)
     float* res;       // pair results [CH * 12][32] | step inputs
-    float* state;     // this thread's P/S column of the block's [CH * 20][kMixedBlock] array
+    float* state;     // this lane's P/S column of the warp's [CH * 20][32] array
     int* meta_off;    // this warp's first step item per lane [32]
     unsigned* meta_bits;   // and active-frequency bits [32]
     float zprev; int wn; bool inside, crossed, zset;
@@ -110,9 +108,9 @@ struct MixedSink {
 
     __device__ void init() {
         for (int c = 0; c < CH; ++c) {
-            float* st = state + c * 20 * kMixedBlock;
-            for (int q = 0; q < 16; ++q) st[q * kMixedBlock] = (q % 5 == 0) ? 1.f : 0.f;
-            for (int q = 16; q < 20; ++q) st[q * kMixedBlock] = 0.f;
+            float* st = state + c * 20 * 32;
+            for (int q = 0; q < 16; ++q) st[q * 32] = (q % 5 == 0) ? 1.f : 0.f;
+            for (int q = 16; q < 20; ++q) st[q * 32] = 0.f;
         }
         for (int q = 0; q < 7; ++q) ev[q] = 0;
         wn = 0; inside = false; crossed = false; zset = false; zprev = 0.f;
@@ -316,21 +314,21 @@ struct MixedSink {
                     float OE[20];
 #pragma unroll
                     for (int q = 0; q < 20; ++q) OE[q] = sres[q * 32 + (g2 - base)];
-                    float* st = state + c * 20 * kMixedBlock;   // this thread's column, fields kMixedBlock apart
+                    float* st = state + c * 20 * 32;   // this lane's column, fields 32 apart
                     float P[16], S4[4];
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) P[q] = st[q * kMixedBlock];
+                    for (int q = 0; q < 16; ++q) P[q] = st[q * 32];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) S4[q] = st[(16 + q) * kMixedBlock];
+                    for (int q = 0; q < 4; ++q) S4[q] = st[(16 + q) * 32];
 #pragma unroll
                     for (int r = 0; r < 4; ++r) {
                         S4[r] += P[4 * r] * OE[16] + P[4 * r + 1] * OE[17] + P[4 * r + 2] * OE[18] + P[4 * r + 3] * OE[19];
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
-                            st[(4 * r + q) * kMixedBlock] = P[4 * r] * OE[q] + P[4 * r + 1] * OE[4 + q] + P[4 * r + 2] * OE[8 + q] + P[4 * r + 3] * OE[12 + q];
+                            st[(4 * r + q) * 32] = P[4 * r] * OE[q] + P[4 * r + 1] * OE[4 + q] + P[4 * r + 2] * OE[8 + q] + P[4 * r + 3] * OE[12 + q];
                     }
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) st[(16 + q) * kMixedBlock] = S4[q];
+                    for (int q = 0; q < 4; ++q) st[(16 + q) * 32] = S4[q];
                     ev[6]++;
                 }
             }
@@ -388,8 +386,8 @@ struct MixedJob {
     double L;
 };
 
-template <int CH>
-__global__ void __launch_bounds__(kMixedBlock, 3)
+template <int CH, int NT>
+__global__ void __launch_bounds__(NT, 1)
 k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64, int ntot, const double* __restrict__ ct,
           const double* __restrict__ cnu, const float* __restrict__ stream, unsigned long long* __restrict__ work,
           float* __restrict__ seg_out, unsigned long long* __restrict__ counters) {
@@ -399,7 +397,6 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
     unsigned char* wbase = smem + size_t(ntot) * ST_COUNT * 4;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* wb = wbase + size_t(warp) * MixedSmem<CH>::kWarpBytes;
-    float* state_base = reinterpret_cast<float*>(wbase + size_t(kWarps) * MixedSmem<CH>::kWarpBytes);
     __syncthreads();
     unsigned int ev[7] = {0, 0, 0, 0, 0, 0, 0};
     unsigned int samples_c = 0;
@@ -443,7 +440,8 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         sink.res = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes);
         sink.meta_off = reinterpret_cast<int*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes + MixedSmem<CH>::kResBytes);
         sink.meta_bits = reinterpret_cast<unsigned*>(sink.meta_off + 32);
-        sink.state = state_base + threadIdx.x;
+        sink.state = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes + MixedSmem<CH>::kResBytes +
+                                              MixedSmem<CH>::kMetaBytes) + lane;
         sink.init();
         const float* sp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
         for (int k = k0; k < k1; ++k, sp += SM_COUNT * npad) {
@@ -454,10 +452,10 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         __syncwarp();
         if (live) {
             for (int c = 0; c < sink.nc; ++c) {
-                const float* S = sink.state + c * 20 * kMixedBlock;
+                const float* S = sink.state + c * 20 * 32;
                 float* o = seg_out + (((long long)((v0 + c) * job.nframes + f) * job.nseg + seg) * job.npix + j) * 20;
 #pragma unroll
-                for (int q = 0; q < 20; ++q) o[q] = S[q * kMixedBlock];
+                for (int q = 0; q < 20; ++q) o[q] = S[q * 32];
             }
             for (int q = 0; q < 7; ++q) ev[q] += sink.ev[q];
             samples_c += sink.ev[0] * sink.nc;

@@ -28,18 +28,20 @@ inline double gravitational_radius(double Msun) { return GNEWT * Msun * MSUN / (
 
 // ---- Bessel K0, K1 ------------------------------------------------------------------------------
 inline void besselk01(double x, double& k0, double& k1) {
-    // trapezoid in t with step h; terms until x cosh t exceeds 745 + |ln x| headroom
-    const double h = 0.125;
-    double s0 = 0.5 * std::exp(-x), s1 = 0.5 * std::exp(-x);
-    for (int j = 1; j < 4000; ++j) {
+    // trapezoid in t on exp(-x (cosh t - 1)) (the factor exp(-x) applied at the end); the step
+    // resolves the Gaussian core of width 1/std::sqrt(x) (error ~ exp(-2 pi^2 / (x h^2)) < 1e-17)
+    const double h = std::fmin(0.125, 0.6 / std::sqrt(x));
+    double s0 = 0.5, s1 = 0.5;
+    for (int j = 1; j < 20000; ++j) {
         double t = j * h;
-        double e = std::exp(-x * std::cosh(t));
-        if (e == 0.0) break;
+        double ch = std::cosh(t);
+        double e = std::exp(-x * (ch - 1.0));
         s0 += e;
-        s1 += e * std::cosh(t);
-        if (e < 1e-300) break;
+        s1 += e * ch;
+        if (e < 1e-18 * s0) break;
     }
-    k0 = h * s0; k1 = h * s1;
+    double ex = std::exp(-x);
+    k0 = h * s0 * ex; k1 = h * s1 * ex;
 }
 // coefficients.jl:79-84
 inline void besselk012(double x, double& k0, double& k1, double& k2) {

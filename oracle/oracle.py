@@ -109,7 +109,8 @@ def polarized_image(a, theta_o, alpha, beta, N, M, sets, t_obs, nu, L, nmax=-1, 
 
 def transfer_step(j, alpha, rho, D):
     O, E = np.empty(16), np.empty(4)
-    load().kso_transfer_step(_p(_d(j)), _p(_d(alpha)), _p(_d(rho)), ctypes.c_double(D), _p(O), _p(E))
+    j, alpha, rho = _d(j), _d(alpha), _d(rho)   # keep the buffers alive across the call
+    load().kso_transfer_step(_p(j), _p(alpha), _p(rho), ctypes.c_double(D), _p(O), _p(E))
     return O.reshape(4, 4), E
 
 
