@@ -128,6 +128,23 @@ int ks_kernel_stats(ks_context* ctx, double* render_ms, long long* render_launch
 int ks_set_event_counting(ks_context* ctx, int on);
 int ks_event_counts(ks_context* ctx, unsigned long long out[7]);
 
+/* ---- the allocation-free thin image (no counterpart in the reference) ----
+ *
+ * ks_thin_image_noalloc is ks_thin_image for callers that cannot let a library call cudaMalloc:
+ * callers whose device memory is handed out by their own pool (for example a CUDA.jl process, whose
+ * allocator must see every byte it owns), and loops where an allocation's implicit device
+ * synchronisation would stall the other streams. It allocates nothing: `params` (14 x nsplat,
+ * column-major) and `out` (npix doubles, in `order`) must be device pointers the caller owns, the
+ * context must have been regenerated (the plan and anchors were allocated then), and the splat table
+ * lives in a file-scope device array of KS_NOALLOC_MAX_SPLATS rows (about 100 KB, held by every GPU that
+ * loads the library until the process exits). The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress, once per device); make that first call before any stream capture.
+ * Every call shares the array: calls that overlap on the GPU race. More than KS_NOALLOC_MAX_SPLATS
+ * splats, or host pointers, return KS_ERR_ARGUMENT. */
+#define KS_NOALLOC_MAX_SPLATS 256
+int ks_thin_image_noalloc(ks_context* ctx, const double* params, int32_t nsplat, double t_obs, int32_t precision,
+                          double* out, int32_t order);
+
 #ifdef __cplusplus
 }
 #endif

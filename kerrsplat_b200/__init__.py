@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "thin_image_noalloc", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KsError", "NU0",
 ]
@@ -271,6 +271,17 @@ def thin_image(cache, params, t_obs, precision=KS_FP64):
     cache._check(cache._lib.ks_thin_image(cache._ctx, _ptr(buf), ns, float(t_obs), _precision(precision), _ptr(out), _lib.KS_ORDER_SCREEN))
     na, nb = cache.size
     return out.reshape(nb, na).T if isinstance(out, np.ndarray) else out.reshape(nb, na).t()
+
+
+def thin_image_noalloc(cache, params, t_obs, out, precision=KS_FP64, order="sorted"):
+    """ks_thin_image_noalloc: the thin image with no device allocation inside the call, for callers
+    whose device memory is owned by their own allocator. `params` (14, nsplat) and `out` (npix) must
+    be CUDA tensors (params in column-major order: pass `p.t().contiguous()` of a (nsplat, 14) view or
+    use `_colmajor`); at most KS_NOALLOC_MAX_SPLATS splats; see include/kerrsplat_b200.h."""
+    buf, ns = _colmajor(params, 14)
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_thin_image_noalloc(cache._ctx, _ptr(buf), ns, float(t_obs), _precision(precision), _ptr(out), o))
+    return out
 
 
 class _Model:

@@ -28,6 +28,8 @@ KS_POWERLAW22 = 2
 KS_KAPPA22 = 3
 KS_KNOT21 = 4
 
+KS_NOALLOC_MAX_SPLATS = 256
+
 NROWS = {KS_THIN14: 14, KS_THERMAL21: 21, KS_POWERLAW22: 22, KS_KAPPA22: 22, KS_KNOT21: 21}
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -61,6 +63,7 @@ EXTRA_SIGNATURES = [
     ("ks_kernel_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     ("ks_set_event_counting", ctypes.c_int, [_VP, ctypes.c_int]),
     ("ks_event_counts", ctypes.c_int, [_VP, _VP]),
+    ("ks_thin_image_noalloc", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _VP, ctypes.c_int32]),
 ]
 
 _lib = None

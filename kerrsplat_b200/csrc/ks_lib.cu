@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -387,6 +388,31 @@ __global__ void k_thin(PlanView P, Spacetime st, long long npix, const double* _
     march(P, st, j, R, sink, rt, rp);
     out[j] = double(sink.acc);
     if (resid_t) { resid_t[j] = rt; resid_phi[j] = rp; }
+}
+
+// The allocation-free thin-image variant (ks_thin_image_noalloc) keeps its splat table in this
+// file-scope device array instead of a context buffer. Every GPU that loads the library holds it until
+// the process exits; every call overwrites the first nsplat rows before reading them; calls that
+// overlap on the GPU (two streams, two host threads) share it and race.
+constexpr int kNoAllocMaxSplats = 256;
+static __device__ __align__(256) double g_noalloc_tab[kNoAllocMaxSplats * ST_COUNT];
+
+// k_thin, with the image written straight into the caller's buffer (in sorted or screen order
+// through the permutation) so that no intermediate device buffer is needed.
+template <class T>
+__global__ void k_thin_noalloc(PlanView P, Spacetime st, long long npix, const double* __restrict__ tab64, int nsplat, double t_obs,
+                               const long long* __restrict__ perm, double* __restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    T* tab = reinterpret_cast<T*>(smem);
+    for (int q = threadIdx.x; q < nsplat * ST_COUNT; q += blockDim.x) tab[q] = T(tab64[q]);
+    __syncthreads();
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    MarchRay<T> R = load_ray<T>(P, st, j);
+    ThinSink<T> sink{tab, nsplat, T(t_obs), T(st.a), T(st.rh * (1 + 1e-3)), T(R.dtau), T(0), R.eta, R.lam};
+    double rt, rp;
+    march(P, st, j, R, sink, rt, rp);
+    out[perm ? perm[j] : j] = double(sink.acc);
 }
 
 // RadiativeTransport over a concatenated splat table (transport.jl:171-198, polarized.jl:121-150,
@@ -1171,6 +1197,63 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->kernel_ms += ms;
+    return KS_OK;
+}
+
+// ---- the allocation-free thin image -------------------------------------------------------------
+
+// Device address of g_noalloc_tab, looked up once per device (with that device current) by the first
+// ks_thin_image_noalloc call on it. cudaGetSymbolAddress does not allocate.
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[64] = {nullptr};
+
+static int noalloc_table(ks_context* c, double** tab) {
+    if (c->device < 0 || c->device >= 64) return fail(c, KS_ERR_DEVICE, "device index %d out of range", c->device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[c->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_tab);
+        if (e != cudaSuccess || !p) return cuda_fail(c, e == cudaSuccess ? cudaErrorInvalidSymbol : e, "cudaGetSymbolAddress(g_noalloc_tab)");
+        g_noalloc_addr[c->device] = p;
+    }
+    *tab = static_cast<double*>(g_noalloc_addr[c->device]);
+    return KS_OK;
+}
+
+int ks_thin_image_noalloc(ks_context* c, const double* params, int32_t nsplat, double t_obs, int32_t precision, double* out,
+                          int32_t order) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    if (nsplat < 0 || nsplat > kNoAllocMaxSplats)
+        return fail(c, KS_ERR_ARGUMENT, "ks_thin_image_noalloc takes at most %d splats (got %d)", kNoAllocMaxSplats, nsplat);
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    if (!std::isfinite(t_obs)) return fail(c, KS_ERR_NONFINITE, "non-finite observation time");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    if (!is_device_ptr(out) || (nsplat > 0 && !is_device_ptr(params)))
+        return fail(c, KS_ERR_ARGUMENT, "ks_thin_image_noalloc needs device pointers for params and out");
+    double* tab = nullptr;
+    int s = noalloc_table(c, &tab);
+    if (s) return s;
+    const long long n = c->npix;
+    if (nsplat > 0) {
+        SetDesc d{KS_THIN14, 14, nsplat, 0, params, nullptr, 0.0};
+        k_splat_table<<<nblocks(nsplat, 64), 64, 0, c->stream>>>(d, tab);
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
+    const long long* perm = order == KS_ORDER_SCREEN ? c->perm.as<long long>() : nullptr;
+    const size_t smem = size_t(nsplat) * ST_COUNT * (precision == KS_FP64 ? sizeof(double) : sizeof(float));
+    if (precision == KS_FP64) {
+        KS_CUDA(c, cudaFuncSetAttribute(k_thin_noalloc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_thin_noalloc<double><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, tab, nsplat, t_obs, perm, out);
+    } else {
+        KS_CUDA(c, cudaFuncSetAttribute(k_thin_noalloc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_thin_noalloc<float><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, tab, nsplat, t_obs, perm, out);
+    }
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
     return KS_OK;
 }
 
