@@ -125,7 +125,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     build.build(verbose=False)
     c = workload(seed_offset=rank, res=args.res, nsamples=args.nsamples)
-    prec = ks.KS_MIXED if args.precision == "mixed" else ks.KS_FP64
+    prec = {"mixed": ks.KS_MIXED, "mixed_fp32": ks.KS_MIXED_FP32, "fp64": ks.KS_FP64}[args.precision]
     cache = ks.GeodesicCache(c["camera"], c["N"], device=local)
     ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
     dev = torch.device("cuda", local)
@@ -196,7 +196,7 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if prec == ks.KS_MIXED else "f64", "data": "synthetic (seeded PCG64 scene, cfg 2 distributions)",
+        "dtype": "f64" if prec == ks.KS_FP64 else "f32", "data": "synthetic (seeded PCG64 scene, cfg 2 distributions)",
         "config": {"workload": f"polarized image {args.res}x{args.res} +-20M, a=0.5, theta_o=60deg, N={args.nsamples}, M=64, 64 thermal splats, 86/230/345 GHz",
                    "precision": args.precision, "rays": cache.npix, "samples_per_ray": c["N"], "frequencies": nf,
                    "l2": "no flush: the per-ray FP64 plan + anchor table (~150 MB) exceeds the 126 MB L2"},
@@ -210,7 +210,7 @@ def run_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(c, args.cpu_rays)
-    if args.fp64_steps > 0 and prec == ks.KS_MIXED:
+    if args.fp64_steps > 0 and prec != ks.KS_FP64:
         torch.cuda.synchronize(dev)
         e0.record(stream)
         for _ in range(args.fp64_steps):
@@ -280,7 +280,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed_fp32", "fp64"])
     ap.add_argument("--cpu-rays", type=int, default=1024)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")

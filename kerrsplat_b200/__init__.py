@@ -19,13 +19,13 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import KS_FP64, KS_MIXED, KsError
+from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
     "polarized_image", "polarized_cube", "render", "thin_image_noalloc", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
-    "KS_FP64", "KS_MIXED", "KsError", "NU0",
+    "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
 
 # constants.jl:3-12 and coefficients.jl:299
@@ -245,6 +245,8 @@ def _precision(p):
         return KS_FP64
     if p in (KS_MIXED, "mixed", "fp32"):
         return KS_MIXED
+    if p in (KS_MIXED_FP32, "mixed_fp32"):
+        return KS_MIXED_FP32
     raise ValueError(f"unknown precision {p!r}")
 
 

@@ -626,6 +626,7 @@ struct ks_context {
     DevBuf alpha, beta, key, key2, idx, perm, plan, nanch, aoff, anchors, resid_t, resid_phi, scratch;
     DevBuf tab, combos, out_sorted, stage_in, stage_out, counters, seg_out, work, stream_buf;
     bool count_events = false;
+    bool geo64 = true;    // mixed path: FP64 march feeding the FP32 transport (false: KS_MIXED_FP32 march)
     long long total_anchors = 0;
     int max_nanch = 0;
     long long ranges[6] = {0, 0, 0, 0, 0, 0};
@@ -725,7 +726,7 @@ int nrows_of(int kind) {
     }
 }
 
-template <int CH, int NT>
+template <int CH, int NT, int KM>
 int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int per_sm) {
     MixedJob job = job0;
     const int N = c->st.N;
@@ -747,7 +748,7 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
     KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
     const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
-    k_consume<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(
+    k_consume<CH, NT, KM><<<unsigned(grid), NT, smem, c->stream>>>(
         plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
         c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr);
     c->launches++;
@@ -760,21 +761,21 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     return KS_OK;
 }
 
-// Occupancy of k_consume<CH, NT> with its shared memory for `ntot` splats (0 if it does not fit).
-template <int CH, int NT>
+// Occupancy of k_consume<CH, NT, KM> with its shared memory for `ntot` splats (0 if it does not fit).
+template <int CH, int NT, int KM>
 int consume_blocks(ks_context* c, int ntot) {
     const size_t smem = MixedSmem<CH>::bytes(ntot, NT / 32);
     if (smem > 227 * 1024) return 0;
-    if (cudaFuncSetAttribute(k_consume<CH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_consume<CH, NT, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_consume<CH, NT>, NT, smem) != cudaSuccess) { cudaGetLastError(); return 0; }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_consume<CH, NT, KM>, NT, smem) != cudaSuccess) { cudaGetLastError(); return 0; }
     return per_sm;
 }
 
-template <int CH>
+template <int CH, int KM>
 int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, int nmax, double slab) {
     int nsm = 0;
     KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
@@ -783,7 +784,10 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     const int sseg = std::max(M, (N / 4 + M - 1) / M * M);
     const int nsseg = (N + sseg - 1) / sseg;
     KS_CUDA(c, c->stream_buf.ensure(size_t(N) * SM_COUNT * c->npad * sizeof(float)));
-    k_stream<<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
+    if (c->geo64)
+        k_stream<double><<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
+    else
+        k_stream<float><<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
     c->launches++;
     KS_CUDA(c, cudaGetLastError());
     MixedJob job;
@@ -792,23 +796,27 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     job.nchunks = (c->npix + 31) / 32;
     job.nmax = nmax; job.slab = float(slab); job.L = L;
     // the block size with the most resident warps (the per-warp shared memory sets the limit)
-    const int w384 = consume_blocks<CH, 384>(c, ntot) * 12, w352 = consume_blocks<CH, 352>(c, ntot) * 11,
-              w256 = consume_blocks<CH, 256>(c, ntot) * 8, w128 = consume_blocks<CH, 128>(c, ntot) * 4;
-    const int best = std::max(std::max(w384, w352), std::max(w256, w128));
+    const int w384 = consume_blocks<CH, 384, KM>(c, ntot) * 12, w256 = consume_blocks<CH, 256, KM>(c, ntot) * 8,
+              w128 = consume_blocks<CH, 128, KM>(c, ntot) * 4;
+    const int best = std::max(w384, std::max(w256, w128));
     if (best <= 0) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
-    if (w384 == best) return launch_consume<CH, 384>(c, job, ntot, nsm, w384 / 12);
-    if (w352 == best) return launch_consume<CH, 352>(c, job, ntot, nsm, w352 / 11);
-    if (w256 == best) return launch_consume<CH, 256>(c, job, ntot, nsm, w256 / 8);
-    if (w128 > 0) return launch_consume<CH, 128>(c, job, ntot, nsm, w128 / 4);
+    if (w384 == best) return launch_consume<CH, 384, KM>(c, job, ntot, nsm, w384 / 12);
+    if (w256 == best) return launch_consume<CH, 256, KM>(c, job, ntot, nsm, w256 / 8);
+    if (w128 > 0) return launch_consume<CH, 128, KM>(c, job, ntot, nsm, w128 / 4);
     return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
     (void)M;
 }
 
-int launch_mixed(ks_context* c, int ntot, const double* ht, int nframes, int nfreq, double L, int nmax, double slab) {
+int launch_mixed(ks_context* c, int ntot, const double* ht, int nframes, int nfreq, double L, int nmax, double slab, bool thermal_only) {
     (void)ht;
-    if (nfreq >= 4) return launch_mixed_ch<4>(c, ntot, nframes, nfreq, L, nmax, slab);
-    if (nfreq == 3) return launch_mixed_ch<3>(c, ntot, nframes, nfreq, L, nmax, slab);
-    return launch_mixed_ch<1>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (thermal_only) {
+        if (nfreq >= 4) return launch_mixed_ch<4, 1>(c, ntot, nframes, nfreq, L, nmax, slab);
+        if (nfreq == 3) return launch_mixed_ch<3, 1>(c, ntot, nframes, nfreq, L, nmax, slab);
+        return launch_mixed_ch<1, 1>(c, ntot, nframes, nfreq, L, nmax, slab);
+    }
+    if (nfreq >= 4) return launch_mixed_ch<4, 7>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (nfreq == 3) return launch_mixed_ch<3, 7>(c, ntot, nframes, nfreq, L, nmax, slab);
+    return launch_mixed_ch<1, 7>(c, ntot, nframes, nfreq, L, nmax, slab);
 }
 
 // Write `nvec` x npix x width doubles from the sorted device buffer to `out` (host or device) in `order`.
@@ -1100,9 +1108,12 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
     if (nsets < 0 || (nsets > 0 && !sets)) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
     if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
-    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    if (precision != KS_FP64 && precision != KS_MIXED && precision != KS_MIXED_FP32)
+        return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
     if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
     if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
+    c->geo64 = precision != KS_MIXED_FP32;
+    if (precision == KS_MIXED_FP32) precision = KS_MIXED;
     if (!std::isfinite(slab)) return fail(c, KS_ERR_NONFINITE, "non-finite slab");
     KS_CUDA(c, cudaSetDevice(c->device));
     std::vector<double> ht(nframes), hnu(nfreq);
@@ -1186,7 +1197,9 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
         }
     } else {
         // the mixed path: one launch over rays x (frame, frequency chunk)
-        int s = launch_mixed(c, ntot, ht.data(), nframes, nfreq, L, nmax, slab);
+        bool thermal_only = true;
+        for (int q = 0; q < nsets; ++q) thermal_only = thermal_only && (sets[q].kind == KS_THERMAL21 || sets[q].nsplat == 0);
+        int s = launch_mixed(c, ntot, ht.data(), nframes, nfreq, L, nmax, slab, thermal_only);
         if (s) return s;
     }
     cudaEventRecord(c->ev1, c->stream);

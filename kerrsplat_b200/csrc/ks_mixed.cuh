@@ -55,12 +55,15 @@ __device__ __noinline__ LFrame<float> local_frame_ool(const float* s, const floa
 
 // Screen-basis coefficients of one splat at one frequency (transport.jl:265-270), written with a
 // stride of 32 floats: j (4), alpha (4), rho (3), active flag.
+// KM: the populations the scene contains (bit 0 thermal, 1 power law, 2 kappa); the kernel for a
+// thermal-only scene carries none of the other fits' code.
+template <int KM>
 __device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, float ne, float nuf, float thb, float s2c, float c2c,
                                                      float* r) {
     Coef<float> cf;
-    if (kind == KS_POWERLAW22)
+    if ((KM & 2) && kind == KS_POWERLAW22)
         cf = powerlaw(ne, p[ST_P], p[ST_GMIN], p[ST_GSPAN], p[ST_GAMJ], p[ST_GAMA], p[ST_BMAG], nuf, thb);
-    else if (kind == KS_KAPPA22)
+    else if ((KM & 4) && kind == KS_KAPPA22)
         cf = kappa(ne, p[ST_KAP], p[ST_W], p[ST_HYP], p[ST_G43], p[ST_G2], p[ST_GQ], p[ST_GP], p[ST_GK2], p[ST_KB], p[ST_BMAG], nuf, thb);
     else
         cf = thermal(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
@@ -86,7 +89,7 @@ __device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float*
     for (int q = 0; q < 4; ++q) E[q] = e[q];
 }
 
-template <int CH>
+template <int CH, int KM>
 struct MixedSink {
     const float* tab; int ntot;
     float t_obs;
@@ -154,7 +157,7 @@ struct MixedSink {
             float nuc = nu[0];
 #pragma unroll
             for (int cc = 1; cc < CH; ++cc) nuc = (cc == c) ? nu[cc] : nuc;
-            screen_coefficients_ool(kind, p, ne, nuc / lf.g, thb, s2c, c2c, r);
+            screen_coefficients_ool<KM>(kind, p, ne, nuc / lf.g, thb, s2c, c2c, r);
             act |= r[352] != 0.f;
         }
         ev[4] += act ? 1 : 0;
@@ -345,30 +348,35 @@ struct MixedSink {
 // write consecutive addresses.
 enum StreamField { SM_X, SM_Y, SM_Z, SM_T, SM_R, SM_STH, SM_CTH, SM_FLAGS, SM_COUNT };
 
+// T: the precision of the march (float: the mixed path; double: FP64 geodesics with the transport in
+// FP32, the reference's `precision(cache, Float32)` arrangement, cache.jl:212-232). The stream is FP32.
+template <class T>
 struct StreamSink {
     float* out;
     long long npad, j;
-    float a, rh_lo;
-    __device__ void operator()(int k, const Sample<float>& s) {
+    T a, rh_lo;
+    __device__ void operator()(int k, const Sample<T>& s) {
         float* o = out + (long long)(k - 1) * SM_COUNT * npad + j;
         const bool usable = s.ok && s.r > rh_lo;
         unsigned flags = (s.ok ? 1u : 0u) | (s.nur ? 2u : 0u) | (s.nutheta ? 4u : 0u) | (usable ? 8u : 0u);
-        float x = 0.f, y = 0.f, z = 0.f, sth = 0.f, cth = 0.f;
+        T x = 0, y = 0, z = 0, sth = 0, cth = 0;
         if (usable) ks_coords(a, s.r, s.theta, s.phi, x, y, z, sth, cth);
-        o[SM_X * npad] = x; o[SM_Y * npad] = y; o[SM_Z * npad] = z; o[SM_T * npad] = s.t;
-        o[SM_R * npad] = s.r; o[SM_STH * npad] = sth; o[SM_CTH * npad] = cth; o[SM_FLAGS * npad] = __uint_as_float(flags);
+        o[SM_X * npad] = float(x); o[SM_Y * npad] = float(y); o[SM_Z * npad] = float(z); o[SM_T * npad] = float(s.t);
+        o[SM_R * npad] = float(s.r); o[SM_STH * npad] = float(sth); o[SM_CTH * npad] = float(cth);
+        o[SM_FLAGS * npad] = __uint_as_float(flags);
     }
 };
 
 // One thread per (ray, segment of seg_len samples starting at an anchor multiple).
+template <class T>
 __global__ void __launch_bounds__(128) k_stream(PlanView P, Spacetime st, long long npix, int seg_len, int nseg, float* __restrict__ out) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= npix * nseg) return;
     const long long j = q % npix;
     const int seg = int(q / npix);
     const int k0 = 1 + seg * seg_len, k1 = min(st.N + 1, k0 + seg_len);
-    MarchRay<float> R = load_ray<float>(P, st, j);
-    StreamSink sink{out, P.npad, j, float(st.a), float(st.rh * (1 + 1e-3))};
+    MarchRay<T> R = load_ray<T>(P, st, j);
+    StreamSink<T> sink{out, P.npad, j, T(st.a), T(st.rh * (1 + 1e-3))};
     march_range(P, j, R, sink, k0, k1);
 }
 
@@ -386,7 +394,7 @@ struct MixedJob {
     double L;
 };
 
-template <int CH, int NT>
+template <int CH, int NT, int KM>
 __global__ void __launch_bounds__(NT, 1)
 k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64, int ntot, const double* __restrict__ ct,
           const double* __restrict__ cnu, const float* __restrict__ stream, unsigned long long* __restrict__ work,
@@ -419,7 +427,7 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         const long long j = live ? j0 : job.npix - 1;
         const int k0 = 1 + seg * job.seg_len;
         const int k1 = min(N + 1, k0 + job.seg_len);
-        MixedSink<CH> sink;
+        MixedSink<CH, KM> sink;
         sink.tab = tab; sink.ntot = ntot;
         sink.t_obs = float(ct[f]);
         sink.nc = min(CH, job.nfreq - v0);

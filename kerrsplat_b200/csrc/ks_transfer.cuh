@@ -345,6 +345,25 @@ __device__ __forceinline__ void moments(const MomentCoeffs& MC, T a, T M[10]) {
         for (int n = 1; n < 10; ++n) M[n] = (T(n) * M[n - 1] - e) / a;
     }
 }
+// FP32: one out-of-line copy of the series (it would otherwise be unrolled at every call site)
+__device__ __noinline__ void moments_f32(const MomentCoeffs& MC, float a, float* M) {
+    if (fabsf(a) < 1.f) {
+#pragma unroll 1
+        for (int n = 0; n < 10; ++n) {
+            float s = MC.cf[n][23];
+#pragma unroll
+            for (int m = 22; m >= 0; --m) s = fmaf(a, s, MC.cf[n][m]);
+            M[n] = s;
+        }
+    } else {
+        float e = expf(-a);
+        M[0] = (1.f - e) / a;
+#pragma unroll
+        for (int n = 1; n < 10; ++n) M[n] = (float(n) * M[n - 1] - e) / a;
+    }
+}
+template <> __device__ __forceinline__ void moments<float>(const MomentCoeffs& MC, float a, float M[10]) { moments_f32(MC, a, M); }
+
 template <class T> __device__ __forceinline__ T phi_fn(const MomentCoeffs& MC, T a) {
     if (fabs(a) < T(1)) return moment_n(MC, a, 0);
     return -expm1(-a) / a;

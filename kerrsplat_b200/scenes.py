@@ -80,3 +80,37 @@ def config2(res=256, N=1024):
     p = thermal_params(rng, 64, a)
     return dict(a=a, theta_o=tho, camera=Camera((-20.0, 20.0), (-20.0, 20.0), res), N=N, M=64, params=p,
                 t_obs=0.0, nus=np.array([86e9, 230e9, 345e9]), L=gravitational_radius(4.0e6))
+
+
+def _population_rows(rng, n, a, rlo=2.5, rhi=12.0):
+    """The 22-row layout shared by power-law and kappa splats (populations.jl:13-26) with the
+    geometry, field and velocity rows of thermal_params; rows 13-14 are set by the caller."""
+    r, th, xyz, s, q, om = _geometry(rng, n, rlo, rhi, a)
+    p = np.zeros((22, n))
+    p[0:3] = xyz; p[3:6] = s; p[6:10] = q
+    p[10] = 0.0; p[11] = np.log(1e9)
+    p[12] = np.log(np.exp(rng.uniform(np.log(1e4), np.log(1e6), n)))
+    p[15] = np.log(rng.uniform(1.0, 30.0, n))
+    p[16] = np.arccos(rng.uniform(-1.0, 1.0, n))
+    p[17] = rng.uniform(0.0, 2 * np.pi, n)
+    uk = keplerian_zamo_velocity(a, r, th)
+    nrm = np.linalg.norm(uk, axis=0)
+    p[18:21] = uk + 0.1 * nrm * rng.standard_normal((3, n))
+    p[21] = om
+    return p
+
+
+def powerlaw_params(rng, n, a):
+    """Power-law splats: p ~ U[2.5, 3.5], gamma_min = 10 (populations.jl:13-15)."""
+    p = _population_rows(rng, n, a)
+    p[13] = rng.uniform(2.5, 3.5, n)
+    p[14] = np.log(10.0)
+    return p
+
+
+def kappa_params(rng, n, a):
+    """kappa splats: kappa ~ U[3, 6], w = log-uniform in [1, 50] (populations.jl:24-26)."""
+    p = _population_rows(rng, n, a)
+    p[13] = rng.uniform(3.0, 6.0, n)
+    p[14] = np.log(np.exp(rng.uniform(np.log(1.0), np.log(50.0), n)))
+    return p
