@@ -117,6 +117,26 @@ int ks_render(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const do
               const double* nus, int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab,
               double* out, int32_t order);
 
+/* Visibilities of an image (vis_kernel!, src/Fit/device_visibilities.jl:61-73): `image` npix x 4
+ * (Stokes I, Q, U, V per pixel, in `order`), V nuv x 4 complex as (re, im) doubles,
+ * V_k = tap_k scale sum_j I_j exp(2 pi i (u_k l_j + v_k m_j)) with l = -(i - (nalpha + 1)/2) psize
+ * (east is -alpha), m = (j - (nbeta + 1)/2) psize; tap may be NULL (ones). KS_FP64: the direct
+ * transform; KS_MIXED: the separable transform as 3xTF32 tensor-core GEMMs. */
+int ks_visibilities(ks_context* ctx, const double* image, int32_t order, int64_t nuv, const double* u, const double* v,
+                    const double* tap, double psize, double scale, int32_t precision, double* V);
+
+/* The adjoint transform (seed_kernel!, device_visibilities.jl:76-88): seed_j = sum_k Re[w_k conj(dV_k/dI_j)]
+ * for weights w (nuv x 4 complex); seed npix x 4 in `order`. */
+int ks_vis_seed(ks_context* ctx, const double* w, int64_t nuv, const double* u, const double* v, const double* tap,
+                double psize, double scale, int32_t precision, double* seed, int32_t order);
+
+/* frame_chi2_seed! (device_visibilities.jl:97-111): chi^2 = sum |(g V - d)/sigma|^2 over baselines and
+ * Stokes, and the seed of the weights 2 conj(g) r / sigma; g (nuv complex) may be NULL (no gains),
+ * vis nuv x 4 complex, sigma nuv x 4. */
+int ks_frame_chi2_seed(ks_context* ctx, const double* image, int32_t order, int64_t nuv, const double* u, const double* v,
+                       const double* tap, const double* g, const double* vis, const double* sigma, double psize, double scale,
+                       int32_t precision, double* chi2, double* seed);
+
 /* ---- library extensions with no counterpart in the reference (measurement and streams) ---- */
 
 /* The CUDA stream every call of this context runs on (a cudaStream_t). */

@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "thin_image_noalloc", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -392,6 +392,56 @@ def polarized_cube(cache, model, times, nus, L, nmax=-1, slab=0.0, precision=KS_
     nf, nt = out.shape[0], out.shape[1]
     na, nb = cache.size
     return out.reshape(nf, nt, nb, na, 4).transpose(3, 2, 1, 0, 4)
+
+
+def _complex_pairs(z):
+    z = np.ascontiguousarray(z, dtype=np.complex128)
+    return z.view(np.float64)
+
+
+def visibilities(cache, image, u, v, psize, scale, tap=None, precision=KS_MIXED, order="screen"):
+    """Stokes visibilities V (nuv, 4) complex of an (npix, 4) image (device_visibilities.jl:61-73):
+    V_k = tap_k scale sum_j I_j exp(2 pi i (u_k l_j + v_k m_j)), l toward the east (-alpha). The mixed
+    path runs the separable transform as 3xTF32 tensor-core GEMMs; KS_FP64 is the direct transform."""
+    img = np.ascontiguousarray(image, dtype=np.float64).reshape(cache.npix, 4)
+    u = np.ascontiguousarray(u, dtype=np.float64); v = np.ascontiguousarray(v, dtype=np.float64)
+    tp = None if tap is None else np.ascontiguousarray(tap, dtype=np.float64)
+    out = np.empty((u.size, 4), dtype=np.complex128)
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_visibilities(cache._ctx, _ptr(img), o, u.size, _ptr(u), _ptr(v), None if tp is None else _ptr(tp),
+                                            float(psize), float(scale), _precision(precision), _ptr(out.view(np.float64))))
+    return out
+
+
+def vis_seed(cache, w, u, v, psize, scale, tap=None, precision=KS_MIXED, order="screen"):
+    """The adjoint of `visibilities` applied to weights w (nuv, 4) complex: seed (npix, 4)
+    (seed_kernel!, device_visibilities.jl:76-88)."""
+    wp = _complex_pairs(w)
+    u = np.ascontiguousarray(u, dtype=np.float64); v = np.ascontiguousarray(v, dtype=np.float64)
+    tp = None if tap is None else np.ascontiguousarray(tap, dtype=np.float64)
+    out = np.empty((cache.npix, 4))
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_vis_seed(cache._ctx, _ptr(wp), u.size, _ptr(u), _ptr(v), None if tp is None else _ptr(tp), float(psize),
+                                        float(scale), _precision(precision), _ptr(out), o))
+    return out
+
+
+def frame_chi2_seed(cache, image, u, v, vis, sigma, psize, scale, tap=None, gains=None, precision=KS_MIXED, order="screen"):
+    """frame_chi2_seed! (device_visibilities.jl:97-111): chi^2 of the (gained) model visibilities
+    against the data and the adjoint seed of the weighted residuals, (chi2, seed (npix, 4))."""
+    img = np.ascontiguousarray(image, dtype=np.float64).reshape(cache.npix, 4)
+    u = np.ascontiguousarray(u, dtype=np.float64); v = np.ascontiguousarray(v, dtype=np.float64)
+    tp = None if tap is None else np.ascontiguousarray(tap, dtype=np.float64)
+    gp = None if gains is None else _complex_pairs(gains)
+    dp = _complex_pairs(vis)
+    sg = np.ascontiguousarray(sigma, dtype=np.float64).reshape(u.size, 4)
+    seed = np.empty((cache.npix, 4))
+    chi2 = ctypes.c_double()
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_frame_chi2_seed(cache._ctx, _ptr(img), o, u.size, _ptr(u), _ptr(v), None if tp is None else _ptr(tp),
+                                               None if gp is None else _ptr(gp), _ptr(dp), _ptr(sg), float(psize), float(scale),
+                                               _precision(precision), ctypes.byref(chi2), _ptr(seed)))
+    return chi2.value, seed
 
 
 def unsort(cache, x):

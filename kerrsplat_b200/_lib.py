@@ -57,6 +57,12 @@ SIGNATURES = [
     ("ks_thin_image", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _VP, ctypes.c_int32]),
     ("ks_render", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
                                  ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _VP, ctypes.c_int32]),
+    ("ks_visibilities", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_int64, _VP, _VP, _VP, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int32, _VP]),
+    ("ks_vis_seed", ctypes.c_int, [_VP, _VP, ctypes.c_int64, _VP, _VP, _VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, _VP,
+                                   ctypes.c_int32]),
+    ("ks_frame_chi2_seed", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_int64, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int32, _D, _VP]),
 ]
 # library extensions outside include/kerrsplat_b200.h's reference-facing set
 EXTRA_SIGNATURES = [

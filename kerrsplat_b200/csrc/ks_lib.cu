@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/kerrsplat_b200.h"
+#include "ks_dft.cuh"
 #include "ks_transfer.cuh"
 
 using namespace ks;
@@ -585,6 +586,11 @@ __global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, 
     }
 }
 
+__global__ void k_inverse_perm(const long long* __restrict__ perm, long long npix, long long* __restrict__ inv) {
+    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j < npix) inv[perm[j]] = j;
+}
+
 // sorted slot -> output order, for `nvec` blocks of npix rows of `width` doubles
 __global__ void k_unsort(const double* __restrict__ src, const long long* __restrict__ perm, long long npix, int width, int nvec,
                          int to_screen, double* __restrict__ dst) {
@@ -625,6 +631,7 @@ struct ks_context {
     Spacetime st{};
     DevBuf alpha, beta, key, key2, idx, perm, plan, nanch, aoff, anchors, resid_t, resid_phi, scratch;
     DevBuf tab, combos, out_sorted, stage_in, stage_out, counters, seg_out, work, stream_buf;
+    DevBuf inv_perm, dft_tu, dft_tv, dft_a, dft_t, dft_c, dft_s, dft_in[8], dft_partial;
     bool count_events = false;
     bool geo64 = true;    // mixed path: FP64 march feeding the FP32 transport (false: KS_MIXED_FP32 march)
     long long total_anchors = 0;
@@ -862,8 +869,10 @@ int ks_context_destroy(ks_context* c) {
     if (!c) return KS_OK;
     cudaSetDevice(c->device);
     for (DevBuf* b : {&c->alpha, &c->beta, &c->key, &c->key2, &c->idx, &c->perm, &c->plan, &c->nanch, &c->aoff, &c->anchors,
-                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out, &c->counters, &c->seg_out, &c->work, &c->stream_buf})
+                      &c->resid_t, &c->resid_phi, &c->scratch, &c->tab, &c->combos, &c->out_sorted, &c->stage_in, &c->stage_out, &c->counters, &c->seg_out, &c->work, &c->stream_buf, &c->inv_perm, &c->dft_tu, &c->dft_tv,
+                      &c->dft_a, &c->dft_t, &c->dft_c, &c->dft_s, &c->dft_partial})
         b->release();
+    for (DevBuf& b : c->dft_in) b.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -985,6 +994,10 @@ int ks_regenerate(ks_context* c, double a, double theta_o, int32_t nsamples, int
     c->launches++;
     KS_CUDA(c, cudaGetLastError());
     k_anchor_prefix<<<nblocks(n), kBlock, 0, c->stream>>>(n, npad, c->plan.as<double>(), c->aoff.as<long long>(), c->anchors.as<double>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, c->inv_perm.ensure(n * sizeof(long long)));
+    k_inverse_perm<<<nblocks(n), kBlock, 0, c->stream>>>(c->perm.as<long long>(), n, c->inv_perm.as<long long>());
     c->launches++;
     KS_CUDA(c, cudaGetLastError());
     KS_CUDA(c, c->resid_t.ensure(n * sizeof(double)));
@@ -1212,6 +1225,187 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     c->kernel_ms += ms;
     return KS_OK;
 }
+
+// ---- visibilities (device_visibilities.jl:53-111) ------------------------------------------------
+
+namespace {
+
+// Stage the DFT inputs (host or device) into device buffers; returns device pointers.
+int dft_stage(ks_context* c, int slot, const double* src, size_t count, const double** dev) {
+    if (!src) { *dev = nullptr; return KS_OK; }
+    return stage_in(c, c->dft_in[slot], src, count * sizeof(double), reinterpret_cast<const void**>(dev));
+}
+
+int dft_checks(ks_context* c, int64_t nuv, double psize, double scale, int32_t precision) {
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first (the screen and its sort order)");
+    if (nuv < 1) return fail(c, KS_ERR_ARGUMENT, "need at least one baseline");
+    if (!(std::isfinite(psize) && psize > 0 && std::isfinite(scale))) return fail(c, KS_ERR_NONFINITE, "pixel size and scale must be finite");
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    return KS_OK;
+}
+
+// The twiddle tables of the separable transform: Tu[i][2k + c] (l_i, u_k) and Tv[j][2k + c] (m_j, v_k).
+int dft_twiddles(ks_context* c, int64_t nuv, const double* du, const double* dv, double psize) {
+    const int na = c->nalpha, nb = c->nbeta;
+    KS_CUDA(c, c->dft_tu.ensure(size_t(na) * 2 * nuv * sizeof(float)));
+    KS_CUDA(c, c->dft_tv.ensure(size_t(nb) * 2 * nuv * sizeof(float)));
+    ksdft::k_twiddle<<<nblocks((long long)na * nuv, 256), 256, 0, c->stream>>>(na, -1.0, psize, nuv, du, c->dft_tu.as<float>(), 2 * nuv);
+    ksdft::k_twiddle<<<nblocks((long long)nb * nuv, 256), 256, 0, c->stream>>>(nb, 1.0, psize, nuv, dv, c->dft_tv.as<float>(), 2 * nuv);
+    c->launches += 2;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
+void gemm(ks_context* c, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb, float* C, long long ldc) {
+    dim3 grid(unsigned((N + ksdft::BN - 1) / ksdft::BN), unsigned((M + ksdft::BM - 1) / ksdft::BM));
+    ksdft::k_gemm_3xtf32<<<grid, ksdft::NTHREADS, 0, c->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+    c->launches++;
+    c->kernel_launches++;
+}
+
+// V (nuv x 4 complex) of a device image
+int dft_forward(ks_context* c, const double* dimg, int32_t order, int64_t nuv, const double* du, const double* dv, const double* dtap,
+                double psize, double scale, int32_t precision, double* dV) {
+    const int na = c->nalpha, nb = c->nbeta;
+    const long long* inv = order == KS_ORDER_SORTED ? c->inv_perm.as<long long>() : nullptr;
+    if (precision == KS_FP64) {
+        ksdft::k_vis_direct<<<nblocks(nuv, 64), 64, 0, c->stream>>>(na, nb, dimg, inv, nuv, du, dv, dtap, psize, scale, dV);
+        c->launches++;
+        c->kernel_launches++;
+        KS_CUDA(c, cudaGetLastError());
+        return KS_OK;
+    }
+    int s = dft_twiddles(c, nuv, du, dv, psize);
+    if (s) return s;
+    KS_CUDA(c, c->dft_a.ensure(size_t(4) * nb * na * sizeof(float)));
+    KS_CUDA(c, c->dft_t.ensure(size_t(4) * nb * 2 * nuv * sizeof(float)));
+    ksdft::k_pack_image<<<nblocks((long long)na * nb * 4, 256), 256, 0, c->stream>>>(dimg, inv, na, nb, c->dft_a.as<float>());
+    c->launches++;
+    gemm(c, 4 * nb, int(2 * nuv), na, c->dft_a.as<float>(), na, c->dft_tu.as<float>(), 2 * nuv, c->dft_t.as<float>(), 2 * nuv);
+    ksdft::k_vis_combine<<<nblocks(nuv * 4, 128), 128, 0, c->stream>>>(nb, nuv, c->dft_t.as<float>(), 2 * nuv, c->dft_tv.as<float>(),
+                                                                       2 * nuv, dtap, scale, dV);
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
+// seed (npix x 4) of device weights w (nuv x 4 complex)
+int dft_adjoint(ks_context* c, const double* dw, int64_t nuv, const double* du, const double* dv, const double* dtap, double psize,
+                double scale, int32_t precision, double* dseed, int32_t order, bool have_twiddles) {
+    const int na = c->nalpha, nb = c->nbeta;
+    const long long* inv = order == KS_ORDER_SORTED ? c->inv_perm.as<long long>() : nullptr;
+    if (precision == KS_FP64) {
+        ksdft::k_seed_direct<<<nblocks((long long)na * nb, 64), 64, 0, c->stream>>>(na, nb, inv, nuv, dw, du, dv, dtap, psize, scale, dseed);
+        c->launches++;
+        c->kernel_launches++;
+        KS_CUDA(c, cudaGetLastError());
+        return KS_OK;
+    }
+    if (!have_twiddles) {
+        int s = dft_twiddles(c, nuv, du, dv, psize);
+        if (s) return s;
+    }
+    KS_CUDA(c, c->dft_c.ensure(size_t(2) * nuv * 4 * nb * sizeof(float)));
+    KS_CUDA(c, c->dft_s.ensure(size_t(na) * 4 * nb * sizeof(float)));
+    ksdft::k_seed_rhs<<<nblocks(nuv * 4 * nb, 256), 256, 0, c->stream>>>(nb, nuv, c->dft_tv.as<float>(), 2 * nuv, dw, dtap, scale,
+                                                                        c->dft_c.as<float>(), 4 * nb);
+    c->launches++;
+    gemm(c, na, 4 * nb, int(2 * nuv), c->dft_tu.as<float>(), 2 * nuv, c->dft_c.as<float>(), 4 * nb, c->dft_s.as<float>(), 4 * nb);
+    ksdft::k_unpack_seed<<<nblocks((long long)na * nb * 4, 256), 256, 0, c->stream>>>(c->dft_s.as<float>(), 4 * nb, na, nb, inv, dseed);
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
+// copy `count` doubles from the device buffer `src` to `dst` (host or device)
+int deliver(ks_context* c, const double* src, double* dst, size_t count) {
+    KS_CUDA(c, cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyDefault, c->stream));
+    return KS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ks_visibilities(ks_context* c, const double* image, int32_t order, int64_t nuv, const double* u, const double* v, const double* tap,
+                    double psize, double scale, int32_t precision, double* V) {
+    if (!c || !image || !u || !v || !V) return KS_ERR_ARGUMENT;
+    int s = dft_checks(c, nuv, psize, scale, precision);
+    if (s) return s;
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const double *dimg, *du, *dv, *dtap;
+    if ((s = dft_stage(c, 0, image, size_t(c->npix) * 4, &dimg)) || (s = dft_stage(c, 1, u, nuv, &du)) || (s = dft_stage(c, 2, v, nuv, &dv)) ||
+        (s = dft_stage(c, 3, tap, tap ? nuv : 0, &dtap)))
+        return s;
+    KS_CUDA(c, c->dft_in[4].ensure(size_t(nuv) * 8 * sizeof(double)));
+    cudaEventRecord(c->ev0, c->stream);
+    if ((s = dft_forward(c, dimg, order, nuv, du, dv, dtap, psize, scale, precision, c->dft_in[4].as<double>()))) return s;
+    cudaEventRecord(c->ev1, c->stream);
+    if ((s = deliver(c, c->dft_in[4].as<double>(), V, size_t(nuv) * 8))) return s;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->kernel_ms += ms;
+    return KS_OK;
+}
+
+int ks_vis_seed(ks_context* c, const double* w, int64_t nuv, const double* u, const double* v, const double* tap, double psize, double scale,
+                int32_t precision, double* seed, int32_t order) {
+    if (!c || !w || !u || !v || !seed) return KS_ERR_ARGUMENT;
+    int s = dft_checks(c, nuv, psize, scale, precision);
+    if (s) return s;
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const double *dw, *du, *dv, *dtap;
+    if ((s = dft_stage(c, 0, w, size_t(nuv) * 8, &dw)) || (s = dft_stage(c, 1, u, nuv, &du)) || (s = dft_stage(c, 2, v, nuv, &dv)) ||
+        (s = dft_stage(c, 3, tap, tap ? nuv : 0, &dtap)))
+        return s;
+    KS_CUDA(c, c->dft_in[5].ensure(size_t(c->npix) * 4 * sizeof(double)));
+    if ((s = dft_adjoint(c, dw, nuv, du, dv, dtap, psize, scale, precision, c->dft_in[5].as<double>(), order, false))) return s;
+    if ((s = deliver(c, c->dft_in[5].as<double>(), seed, size_t(c->npix) * 4))) return s;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KS_OK;
+}
+
+int ks_frame_chi2_seed(ks_context* c, const double* image, int32_t order, int64_t nuv, const double* u, const double* v, const double* tap,
+                       const double* g, const double* vis, const double* sigma, double psize, double scale, int32_t precision,
+                       double* chi2, double* seed) {
+    if (!c || !image || !u || !v || !vis || !sigma || !chi2 || !seed) return KS_ERR_ARGUMENT;
+    int s = dft_checks(c, nuv, psize, scale, precision);
+    if (s) return s;
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const double *dimg, *du, *dv, *dtap, *dg, *dvis, *dsig;
+    if ((s = dft_stage(c, 0, image, size_t(c->npix) * 4, &dimg)) || (s = dft_stage(c, 1, u, nuv, &du)) || (s = dft_stage(c, 2, v, nuv, &dv)) ||
+        (s = dft_stage(c, 3, tap, tap ? nuv : 0, &dtap)) || (s = dft_stage(c, 6, g, g ? 2 * nuv : 0, &dg)) ||
+        (s = dft_stage(c, 7, vis, size_t(nuv) * 8, &dvis)))
+        return s;
+    KS_CUDA(c, c->dft_in[4].ensure(size_t(nuv) * 8 * sizeof(double) * 2 + size_t(nuv) * 4 * sizeof(double)));
+    double* dV = c->dft_in[4].as<double>();
+    double* dW = dV + nuv * 8;
+    double* dS = dW + nuv * 8;
+    KS_CUDA(c, cudaMemcpyAsync(dS, sigma, size_t(nuv) * 4 * sizeof(double), cudaMemcpyDefault, c->stream));
+    dsig = dS;
+    KS_CUDA(c, c->dft_in[5].ensure(size_t(c->npix) * 4 * sizeof(double)));
+    if ((s = dft_forward(c, dimg, order, nuv, du, dv, dtap, psize, scale, precision, dV))) return s;
+    const int nblk = int((nuv * 4 + 255) / 256);
+    KS_CUDA(c, c->dft_partial.ensure(size_t(nblk) * sizeof(double)));
+    ksdft::k_chi2_weights<<<nblk, 256, 0, c->stream>>>(nuv, dV, dg, dvis, dsig, dW, c->dft_partial.as<double>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    if ((s = dft_adjoint(c, dW, nuv, du, dv, dtap, psize, scale, precision, c->dft_in[5].as<double>(), order, precision != KS_FP64))) return s;
+    std::vector<double> part(nblk);
+    KS_CUDA(c, cudaMemcpyAsync(part.data(), c->dft_partial.p, nblk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if ((s = deliver(c, c->dft_in[5].as<double>(), seed, size_t(c->npix) * 4))) return s;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    double x = 0.0;
+    for (double p : part) x += p;   // fixed order: deterministic
+    *chi2 = x;
+    return KS_OK;
+}
+
+}  // extern "C"
 
 // ---- the allocation-free thin image -------------------------------------------------------------
 

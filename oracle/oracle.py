@@ -157,3 +157,41 @@ def ellipf(phi, m):
     out = np.empty_like(phi)
     load().kso_ellipf(ctypes.c_long(phi.size), _p(phi), _p(m), _p(out))
     return out
+
+
+# ---- visibilities: numpy FP64 restatement of src/Fit/device_visibilities.jl:53-111 ----------------
+
+def pixel_offsets(na, nb, psize):
+    """l (east is -alpha) and m of every screen pixel p = i + j na (device_visibilities.jl:53-58)."""
+    i = np.arange(na * nb) % na
+    j = np.arange(na * nb) // na
+    return -((i + 1) - (na + 1) / 2) * psize, ((j + 1) - (nb + 1) / 2) * psize
+
+
+def visibilities(image, na, nb, u, v, tap, psize, scale):
+    """V_k = tap_k sum_j I_j scale exp(2 pi i (u_k l_j + v_k m_j)); image (npix, 4) in screen order
+    (vis_kernel!, device_visibilities.jl:61-73). Returns (nuv, 4) complex."""
+    l, m = pixel_offsets(na, nb, psize)
+    ph = 2 * np.pi * (np.outer(u, l) + np.outer(v, m))
+    E = np.exp(1j * ph) * scale
+    V = E @ np.asarray(image, dtype=np.float64)
+    return V * (np.ones(len(u)) if tap is None else np.asarray(tap))[:, None]
+
+
+def vis_seed(w, na, nb, u, v, tap, psize, scale):
+    """seed_j = sum_k Re[w_k conj(dV_k/dI_j)] (seed_kernel!, device_visibilities.jl:76-88); w (nuv, 4)
+    complex. Returns (npix, 4) in screen order."""
+    l, m = pixel_offsets(na, nb, psize)
+    ph = 2 * np.pi * (np.outer(u, l) + np.outer(v, m))
+    f = scale * (np.ones(len(u)) if tap is None else np.asarray(tap))
+    E = np.exp(-1j * ph) * f[:, None]
+    return np.real(E.T @ np.asarray(w))
+
+
+def frame_chi2_seed(image, na, nb, u, v, tap, g, vis, sigma, psize, scale):
+    """chi^2 of the gained model against the data and the adjoint seed (device_visibilities.jl:97-111)."""
+    V = visibilities(image, na, nb, u, v, tap, psize, scale)
+    gg = np.ones(len(u)) if g is None else np.asarray(g)
+    r = (gg[:, None] * V - vis) / sigma
+    w = 2 * np.conj(gg)[:, None] * r / sigma
+    return float(np.sum(np.abs(r) ** 2)), vis_seed(w, na, nb, u, v, tap, psize, scale)
