@@ -137,6 +137,28 @@ int ks_frame_chi2_seed(ks_context* ctx, const double* image, int32_t order, int6
                        const double* tap, const double* g, const double* vis, const double* sigma, double psize, double scale,
                        int32_t precision, double* chi2, double* seed);
 
+/* The gradient of l = sum dstokes . Stokes with respect to every splat parameter (the dual sweep:
+ * polarized_tails! + polarized_dual_sweep!, src/Splats/dual_gradient.jl:190-249, as driven by
+ * sweep_passes, src/Fit/Fit.jl:451-485). Thermal polarized splats (KS_THERMAL21) only, as in the
+ * reference. dstokes has the layout of ks_render's out (npix x 4 x nframes x nfreq, pixels in
+ * `order`), the adjoint of the observed Stokes vectors in cgs. dparams receives 21 x nsplat per set,
+ * column-major, the sets concatenated; with `accumulate` the gradient is added to it. KS_FP64 runs
+ * the reference's structure (stored FP64 samples, backward tails, forward duals, per-ray slots);
+ * KS_MIXED the FP32 transport with a per-segment reverse pass. Deterministic: no atomics. */
+int ks_adjoint(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+               int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* dstokes, int32_t order,
+               double* dparams, int32_t accumulate);
+
+/* chi2_gradient! (src/Fit/Fit.jl:502-534) with the image-domain residuals of _frame_seed! (Fit.jl:537-577):
+ * chi^2 = sum over unmasked pixels, Stokes and (frame, frequency) of ((image - data) / sigma)^2 and
+ * its gradient, in one forward and one reverse pass. data and sigma have the layout of ks_render's out
+ * in screen order (sigma may be NULL: then sigma_scalar for every entry); mask (npix x nframes x nfreq
+ * bytes, screen order, nonzero = used) may be NULL. chi2 (one double), image (optional, screen order)
+ * and dparams (as ks_adjoint) are outputs. */
+int ks_chi2_gradient(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+                     int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* data, const double* sigma,
+                     double sigma_scalar, const uint8_t* mask, double* chi2, double* dparams, int32_t accumulate, double* image);
+
 /* ---- library extensions with no counterpart in the reference (measurement and streams) ---- */
 
 /* The CUDA stream every call of this context runs on (a cudaStream_t). */
@@ -145,6 +167,10 @@ int ks_context_stream(ks_context* ctx, void** stream);
 /* Device time (CUDA events on the context stream) of the render kernels since the last reset,
  * their launch count, and the launch count of every kernel of this library. */
 int ks_kernel_stats(ks_context* ctx, double* render_ms, long long* render_launches, long long* all_launches, int reset);
+
+/* Device time (CUDA events) of the adjoint calls (ks_adjoint, ks_chi2_gradient) since the last reset
+ * and the launch count of their reverse-pass kernels. */
+int ks_adjoint_stats(ks_context* ctx, double* adjoint_ms, long long* launches, int reset);
 
 /* Count work events during ks_render (samples, valid samples, splat tests, weights evaluated,
  * coefficient evaluations, local frames, transfer steps); ks_event_counts reads the 7 counters of

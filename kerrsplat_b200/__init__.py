@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "adjoint", "chi2_gradient", "sweep_passes", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -373,6 +373,104 @@ def render(cache, model, times, nus, L, nmax=-1, slab=0.0, precision=KS_FP64, or
     cache._check(cache._lib.ks_render(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision),
                                       int(nmax), float(slab), _ptr(out), o))
     return out
+
+
+def _grad_like(model):
+    """dparams of a model: one (21, nsplat) float64 array per set, concatenated column-major."""
+    return [np.zeros((_lib.NROWS[s.kind], s.nsplat)) for s in model.sets()]
+
+
+def _grad_buffer(model, dparams):
+    if dparams is None:
+        return None, np.zeros(sum(_lib.NROWS[s.kind] * s.nsplat for s in model.sets()))
+    if hasattr(dparams, "data_ptr"):
+        return dparams, dparams
+    d = np.asarray(dparams)
+    if d.dtype != np.float64 or not (d.ndim == 1 or (d.ndim == 2 and d.flags.f_contiguous)):
+        raise ValueError("dparams must be a float64 array laid out like the parameters (flat, or 21 x nsplat column-major)")
+    return dparams, d
+
+
+def _split_grad(model, flat):
+    out, q = [], 0
+    for s in model.sets():
+        nr = _lib.NROWS[s.kind]
+        out.append(np.asarray(flat[q:q + nr * s.nsplat]).reshape(s.nsplat, nr).T.copy())
+        q += nr * s.nsplat
+    return out[0] if len(out) == 1 else out
+
+
+def adjoint(cache, model, times, nus, L, dstokes, nmax=-1, slab=0.0, precision=KS_FP64, order="screen", dparams=None):
+    """The gradient of sum(dstokes * Stokes) with respect to every splat parameter (the dual sweep,
+    dual_gradient.jl:190-249): `dstokes` has the shape of `render`'s output, (nfreq, nframes, npix, 4).
+    Returns (21, nsplat) per set; with `dparams` given (float64, the parameters' layout) the gradient
+    is added to it in place (the reference's `dparams .+= ...`). Thermal polarized splats only."""
+    times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+    nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+    nt, nf = int(times.shape[0]), int(nus.shape[0])
+    ds = _as_f64(dstokes)
+    if tuple(ds.shape) != (nf, nt, cache.npix, 4):
+        raise ValueError(f"dstokes must have shape {(nf, nt, cache.npix, 4)}, got {tuple(ds.shape)}")
+    arr, nsets, _keep = _set_array(model)
+    user, buf = _grad_buffer(model, dparams)
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_adjoint(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision), int(nmax),
+                                       float(slab), _ptr(ds), o, _ptr(buf), 1 if user is not None else 0))
+    return user if user is not None else _split_grad(model, buf)
+
+
+def chi2_gradient(cache, model, times, nus, L, data, sigma, mask=None, nmax=-1, slab=0.0, precision=KS_FP64, dparams=None,
+                  return_image=False):
+    """chi2_gradient! (Fit.jl:502-534) for image-domain data: chi^2 = sum ((image - data)/sigma)^2 over
+    unmasked pixels, Stokes, frames and frequencies, and its gradient with respect to every splat
+    parameter, in one forward and one reverse pass on the GPU. `data` (and `sigma` unless it is a
+    scalar) have the shape of `render`'s screen-order output; `mask` is (nfreq, nframes, npix) bools.
+    Returns (chi2, grad) -- grad as `adjoint` returns it -- and the model image with `return_image`."""
+    times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+    nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+    nt, nf = int(times.shape[0]), int(nus.shape[0])
+    shape = (nf, nt, cache.npix, 4)
+    d = _as_f64(data)
+    if tuple(d.shape) != shape:
+        raise ValueError(f"data must have shape {shape}, got {tuple(d.shape)}")
+    if np.isscalar(sigma):
+        sg, ss = None, float(sigma)
+        if not (np.isfinite(ss) and ss > 0):
+            raise ValueError("sigma must be positive")
+    else:
+        sg, ss = _as_f64(sigma), 0.0
+        if tuple(sg.shape) != shape:
+            raise ValueError(f"sigma must have shape {shape}, got {tuple(sg.shape)}")
+    mk = None
+    if mask is not None:
+        mk = np.ascontiguousarray(mask, dtype=np.uint8) if not hasattr(mask, "data_ptr") else mask
+        if tuple(mk.shape) != shape[:3]:
+            raise ValueError(f"mask must have shape {shape[:3]}")
+    arr, nsets, _keep = _set_array(model)
+    user, buf = _grad_buffer(model, dparams)
+    chi2 = ctypes.c_double(0.0)
+    img = _out_like(d, shape) if return_image else None
+    cache._check(cache._lib.ks_chi2_gradient(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision),
+                                             int(nmax), float(slab), _ptr(d), _ptr(sg) if sg is not None else None, ss,
+                                             _ptr(mk) if mk is not None else None, ctypes.addressof(chi2), _ptr(buf),
+                                             1 if user is not None else 0, _ptr(img) if img is not None else None))
+    g = user if user is not None else _split_grad(model, buf)
+    return (chi2.value, g, img) if return_image else (chi2.value, g)
+
+
+def sweep_passes(cache, model, L, nmax=-1, slab=0.0, precision=KS_FP64):
+    """The two passes of the gradient as closures (sweep_passes, Fit.jl:451-485): `forward(t, nu)`
+    returns the model image (nfreq = 1, screen order, (npix, 4) per frame) and `reverse(dstokes, t, nu)`
+    returns the gradient of sum(dstokes * image). Each pass is one GPU call; the reverse pass runs its
+    own forward pass, so the pair is stateless."""
+    def forward(t, nu):
+        return render(cache, model, np.atleast_1d(t), [nu], L, nmax=nmax, slab=slab, precision=precision)[0]
+
+    def reverse(dstokes, t, nu):
+        ds = np.asarray(dstokes, dtype=np.float64).reshape(1, len(np.atleast_1d(t)), cache.npix, 4)
+        return adjoint(cache, model, np.atleast_1d(t), [nu], L, ds, nmax=nmax, slab=slab, precision=precision)
+
+    return forward, reverse
 
 
 def polarized_image(cache, model, t_obs, nu, L, nmax=-1, slab=0.0, precision=KS_FP64):

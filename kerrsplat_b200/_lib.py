@@ -63,6 +63,11 @@ SIGNATURES = [
                                    ctypes.c_int32]),
     ("ks_frame_chi2_seed", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_int64, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_int32, _D, _VP]),
+    ("ks_adjoint", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
+                                  ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _VP, ctypes.c_int32, _VP, ctypes.c_int32]),
+    ("ks_chi2_gradient", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
+                                        ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _VP, _VP, ctypes.c_double, _VP,
+                                        _VP, _VP, ctypes.c_int32, _VP]),
 ]
 # library extensions outside include/kerrsplat_b200.h's reference-facing set
 EXTRA_SIGNATURES = [
@@ -70,6 +75,7 @@ EXTRA_SIGNATURES = [
     ("ks_kernel_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     ("ks_set_event_counting", ctypes.c_int, [_VP, ctypes.c_int]),
     ("ks_event_counts", ctypes.c_int, [_VP, _VP]),
+    ("ks_adjoint_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     ("ks_thin_image_noalloc", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _VP, ctypes.c_int32]),
 ]
 

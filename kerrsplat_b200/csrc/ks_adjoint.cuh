@@ -1,0 +1,807 @@
+// ks_adjoint.cuh -- the adjoint of the polarized transport with respect to the splat parameters
+// (the reference's dual sweep, src/Splats/dual_gradient.jl, for PolarizedSplats).
+//
+// Along a ray the observed invariant Stokes vector is the tail T_1 of T_k = E_k + O_k T_{k+1}
+// (T_{N+1} = 0); for l = w_1 . T_1 the adjoint in front of sample k is w_k = O_{k-1}^T ... O_1^T w_1
+// and the sample's step enters l through w_k^T (O_k T_{k+1} + Ej_k j_k). So
+//   j-bar = Ej^T w exactly (E is linear in j), and (alpha-bar, rho-bar) are the partials of
+//   w^T (O T + Ej j) by seven forward-mode duals through the step operator (sample_adjoint,
+//   transport.jl:221-245);
+//   each splat's coefficients c_i enter through c-bar . c_i: the fluid rows (logTe, logB, thB, phB,
+//   u1, u2, u3) by seven duals through the frame and the thermal fits, ln n_e as c-bar . c_i itself
+//   (every coefficient is proportional to the density), and the thirteen geometric rows (centre,
+//   log-widths, quaternion, t0, logw, omega) as c-bar . c_i times the partials of ln G, here in
+//   closed form (element_adjoint!, dual_gradient.jl:43-76).
+// Samples that the forward pass skips (invalid, inside r_h (1 + 1e-3), beyond the half-orbit cutoff,
+// or with no active element) have O = 1, E = 0 and no adjoint; culled splats and weights below the
+// cutoff contribute nothing, as in the reference.
+//
+// FP64 plain path (the reference's structure, one thread per (ray, frame x frequency)):
+//   k_kstop (winding_cutoff_kernel!, dual_gradient.jl:81-97) -> k_tails (polarized_tails_kernel!,
+//   129-147; writes the image) -> k_dual_plain (polarized_dual_kernel!, 151-178; per-ray gradient
+//   slots) -> k_slot_reduce (the deterministic sum over rays, 239-241).
+#pragma once
+#include "ks_transfer.cuh"
+
+namespace ks {
+
+// ---- per-splat constants of the gradient (FP64) ------------------------------------------------
+enum GradTab { GT_DF0, GT_DKR, GT_DBT0, GT_DBT1, GT_DBT2, GT_DBP0, GT_DBP1, GT_DBP2, GT_QW, GT_QX, GT_QY, GT_QZ, GT_QN, GT_COUNT };
+
+// gradient rows of a THERMAL21 column (polarized.jl:17-19, 0-based)
+enum GradRow { GR_X, GR_Y, GR_Z, GR_S1, GR_S2, GR_S3, GR_Q1, GR_Q2, GR_Q3, GR_Q4, GR_T0, GR_LOGW, GR_LOGNE, GR_LOGTE, GR_LOGB,
+               GR_THB, GR_PHB, GR_U1, GR_U2, GR_U3, GR_OMEGA, GR_COUNT };
+
+// ---- the step adjoint (sample_adjoint, transport.jl:221-245) -------------------------------------
+// in: j (4), alpha (4), rho (3) of the sample summed over elements, Dl the step length; w the adjoint
+// in front of the sample, R the tail behind it. out: O (for w <- O^T w), E = Ej j, and c-bar =
+// (j-bar 4, alpha-bar 4, rho-bar 3).
+template <class T>
+__device__ __forceinline__ void sample_adjoint(const MomentCoeffs& MC, const T* in, T Dl, const T w[4], const T R[4], T O[16], T E[4],
+                                               T cb[11]) {
+    using D = Dual<T, 7>;
+    D al[4], rh[3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) al[q] = D::seed(in[4 + q], q);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) rh[q] = D::seed(in[8 + q], 4 + q);
+    D Od[16], Ejd[16];
+    step_operator(MC, al, rh, D(Dl), Od, Ejd);
+    D qd(T(0));
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        D row = Od[4 * r] * R[0] + Od[4 * r + 1] * R[1] + Od[4 * r + 2] * R[2] + Od[4 * r + 3] * R[3] +
+                Ejd[4 * r] * in[0] + Ejd[4 * r + 1] * in[1] + Ejd[4 * r + 2] * in[2] + Ejd[4 * r + 3] * in[3];
+        qd += row * w[r];
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) O[q] = Od[q].v;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) E[r] = Ejd[4 * r].v * in[0] + Ejd[4 * r + 1].v * in[1] + Ejd[4 * r + 2].v * in[2] + Ejd[4 * r + 3].v * in[3];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) cb[c] = Ejd[c].v * w[0] + Ejd[4 + c].v * w[1] + Ejd[8 + c].v * w[2] + Ejd[12 + c].v * w[3];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) cb[4 + q] = qd.d[q];
+}
+
+// ---- one thermal splat's share of the gradient at one sample (element_adjoint!) --------------------
+// p: the splat's table row (in T), gt: its gradient constants (FP64), F: the sample's frame data,
+// (x, y, z) its quasi-Cartesian KS position, t = t_obs - t~ the emission time. For each of the
+// first nc frequencies nu[c] whose bit is set in `act`, cb(c, q) = cb[c * cstride + q * qstride] is
+// the sample's c-bar at that frequency. Adds sum_c c-bar . dc/d(row) into g[21]; returns whether the
+// splat contributes (inside its support, weight above the cutoff, emitting or absorbing). The frame
+// and its partials are shared by the frequencies.
+template <class T, int CH>
+__device__ __forceinline__ bool element_adjoint(const T* p, const double* __restrict__ gt, const SampleFrame<T>& F, T x, T y, T z, T t,
+                                                T alpha, T beta, T a_sin_tho, const T* nu, int nc, unsigned act, const T* cb, int cstride,
+                                                int qstride, T g[GR_COUNT]) {
+    // the weight and its geometric partials (Splats.jl:58-93, polarized.jl:22-29)
+    const T ph = p[ST_OMEGA] * (t - p[ST_T0]);
+    T sp, cp;
+    sincos(ph, &sp, &cp);
+    const T cx = p[ST_CX] * cp - p[ST_CY] * sp, cy = p[ST_CX] * sp + p[ST_CY] * cp;
+    const T d0 = x - cx, d1 = y - cy, d2 = z - p[ST_CZ];
+    if (d0 * d0 + d1 * d1 + d2 * d2 > p[ST_SUPP]) return false;   // outside_support (polarized.jl:110-120)
+    const T dr[3] = {d0 * cp + d1 * sp, -d0 * sp + d1 * cp, d2};
+    const T* R = p + ST_R0;   // R[3 i + j]: u_j = sum_i R[3 i + j] dr_i
+    T u[3], e[3];
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) u[jj] = R[jj] * dr[0] + R[3 + jj] * dr[1] + R[6 + jj] * dr[2];
+    e[0] = u[0] * p[ST_ES1]; e[1] = u[1] * p[ST_ES2]; e[2] = u[2] * p[ST_ES3];
+    const T tt = (t - p[ST_T0]) * p[ST_INVW];
+    const T q = (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] + tt * tt) / T(2);
+    const T G = exp(-q);
+    if (!(G > T(kWEIGHT_CUTOFF))) return false;
+
+    // the fluid rows as seven forward-mode duals (splat_coefficients, polarized.jl:140-150)
+    using D = Dual<T, 7>;
+    D Te(p[ST_TE]), f0(p[ST_F0]), kr(p[ST_KR]), Bm(p[ST_BMAG]);
+    Te.d[0] = p[ST_TE]; f0.d[0] = T(gt[GT_DF0]); kr.d[0] = T(gt[GT_DKR]);
+    Bm.d[1] = p[ST_BMAG];
+    D bx(p[ST_BHX]), by(p[ST_BHY]), bz(p[ST_BHZ]);
+    bx.d[2] = T(gt[GT_DBT0]); by.d[2] = T(gt[GT_DBT1]); bz.d[2] = T(gt[GT_DBT2]);
+    bx.d[3] = T(gt[GT_DBP0]); by.d[3] = T(gt[GT_DBP1]); bz.d[3] = T(gt[GT_DBP2]);
+    const D u1 = D::seed(p[ST_U1], 4), u2 = D::seed(p[ST_U2], 5), u3 = D::seed(p[ST_U3], 6);
+    SampleFrame<D> Fd;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { Fd.pu[k] = D(F.pu[k]); Fd.pz[k] = D(F.pz[k]); }
+    Fd.lapse_inv = D(F.lapse_inv); Fd.om_lapse = D(F.om_lapse); Fd.sDS = D(F.sDS); Fd.misS = D(F.misS); Fd.ivarpi = D(F.ivarpi);
+    Fd.r = D(F.r); Fd.sth = D(F.sth); Fd.cth = D(F.cth); Fd.a = D(F.a);
+    const LFrame<D> lf = local_frame(Fd, u1, u2, u3, bx, by, bz, p[ST_BZERO] != T(0), D(alpha), D(beta), D(a_sin_tho));
+    const D thb = safe_acos(lf.cosB);
+    const D s2c = sin(T(2) * lf.chi), c2c = cos(T(2) * lf.chi);
+    const D ne(p[ST_NE] * G);
+    T sc = T(0);
+    T fl[7] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
+    bool any = false;
+#pragma unroll 1
+    for (int c = 0; c < CH; ++c) {
+        if (c >= nc || !((act >> c) & 1u)) continue;
+        const T* cbc = cb + c * cstride;
+        const D nuf = D(nu[c]) / lf.g;
+        const Coef<D> cf = thermal(ne, Te, f0, kr, Bm, nuf, thb);
+        // screen_coefficients (transport.jl:265-270)
+        if (!(cf.jI > T(0) || cf.aI > T(0) || cf.rQ != T(0) || cf.rV != T(0))) continue;
+        const D fe = cap_factor(cf.jI, cf.jQ, cf.jV, D(T(0.99)));
+        const D fa = cap_factor(cf.aI, cf.aQ, cf.aV, D(T(0.99)));
+        const D nh = nuf / T(kNU0);
+        const D i2 = D(T(1)) / (nh * nh);
+        const D jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+        const D qd = (cf.jI * i2) * cbc[0] + (jQ * c2c) * cbc[qstride] + (jQ * s2c) * cbc[2 * qstride] + (cf.jV * fe * i2) * cbc[3 * qstride] +
+                     (nh * cf.aI) * cbc[4 * qstride] + (aQ * c2c) * cbc[5 * qstride] + (aQ * s2c) * cbc[6 * qstride] +
+                     (cf.aV * fa * nh) * cbc[7 * qstride] + (rQ * c2c) * cbc[8 * qstride] + (rQ * s2c) * cbc[9 * qstride] +
+                     (nh * cf.rV) * cbc[10 * qstride];
+        sc += qd.v;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) fl[k] += qd.d[k];
+        any = true;
+    }
+    if (!any) return false;
+
+    // geometric rows: g += sc * d(ln G)/d(row) = -sc * dq/d(row)
+    const T gu[3] = {e[0] * p[ST_ES1], e[1] * p[ST_ES2], e[2] * p[ST_ES3]};   // dq/du
+    T gdr[3];                                                                  // dq/d(dr)
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii) gdr[ii] = R[3 * ii] * gu[0] + R[3 * ii + 1] * gu[1] + R[3 * ii + 2] * gu[2];
+    g[GR_X] += sc * gdr[0];
+    g[GR_Y] += sc * gdr[1];
+    g[GR_Z] += sc * gdr[2];
+    g[GR_S1] += sc * e[0] * e[0];
+    g[GR_S2] += sc * e[1] * e[1];
+    g[GR_S3] += sc * e[2] * e[2];
+    g[GR_LOGW] += sc * tt * tt;
+    // the pattern phase: dq/dph through dr = rot(-ph) x - p (xy components)
+    const T dqdph = gdr[0] * (dr[1] + p[ST_CY]) - gdr[1] * (dr[0] + p[ST_CX]);
+    g[GR_OMEGA] -= sc * dqdph * (t - p[ST_T0]);
+    g[GR_T0] -= sc * (-dqdph * p[ST_OMEGA] - tt * p[ST_INVW]);
+    // the quaternion through the rotation matrix and the normalisation
+    T GM[9];
+#pragma unroll
+    for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) GM[3 * ii + jj] = dr[ii] * gu[jj];
+    const T w = T(gt[GT_QW]), qx = T(gt[GT_QX]), qy = T(gt[GT_QY]), qz = T(gt[GT_QZ]);
+    T gq[4];
+    gq[0] = T(2) * (-qz * GM[1] + qy * GM[2] + qz * GM[3] - qx * GM[5] - qy * GM[6] + qx * GM[7]);
+    gq[1] = T(2) * (qy * GM[1] + qz * GM[2] + qy * GM[3] - T(2) * qx * GM[4] - w * GM[5] + qz * GM[6] + w * GM[7] - T(2) * qx * GM[8]);
+    gq[2] = T(2) * (-T(2) * qy * GM[0] + qx * GM[1] + w * GM[2] + qx * GM[3] + qz * GM[5] - w * GM[6] + qz * GM[7] - T(2) * qy * GM[8]);
+    gq[3] = T(2) * (-T(2) * qz * GM[0] - w * GM[1] + qx * GM[2] + w * GM[3] - T(2) * qz * GM[4] + qy * GM[5] + qx * GM[6] + qy * GM[7]);
+    const T dotq = w * gq[0] + qx * gq[1] + qy * gq[2] + qz * gq[3];
+    const T inv_n = T(1.0 / gt[GT_QN]);
+    g[GR_Q1] -= sc * (gq[0] - w * dotq) * inv_n;
+    g[GR_Q2] -= sc * (gq[1] - qx * dotq) * inv_n;
+    g[GR_Q3] -= sc * (gq[2] - qy * dotq) * inv_n;
+    g[GR_Q4] -= sc * (gq[3] - qz * dotq) * inv_n;
+    // ln n_e and the fluid rows
+    g[GR_LOGNE] += sc;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) g[GR_LOGTE + k] += fl[k];
+    return true;
+}
+
+// The summed screen-basis coefficients of the thermal splats at one sample and frequency
+// (accumulate_elements, transport.jl:254-276); false when no element is active. Same arithmetic as
+// the forward consumer.
+template <class T>
+__device__ __forceinline__ bool sample_coefficients(const T* tab, int ntot, const SampleFrame<T>& F, T x, T y, T z, T t, T alpha, T beta,
+                                                    T a_sin_tho, T nu, T out[11]) {
+#pragma unroll
+    for (int q = 0; q < 11; ++q) out[q] = T(0);
+    bool active = false;
+    for (int i = 0; i < ntot; ++i) {
+        const T* p = tab + i * ST_COUNT;
+        T q;
+        if (!splat_exponent(p, t, x, y, z, true, q)) continue;
+        T G = exp(-q);
+        if (!(G > T(kWEIGHT_CUTOFF))) continue;
+        LFrame<T> lf = local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != T(0), alpha, beta, a_sin_tho);
+        T nuf = nu / lf.g;
+        T thb = acos(fmin(T(1), fmax(T(-1), lf.cosB)));
+        Coef<T> cf = thermal(p[ST_NE] * G, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
+        if (!(cf.jI > T(0) || cf.aI > T(0) || cf.rQ != T(0) || cf.rV != T(0))) continue;
+        T fe = cap_factor(cf.jI, cf.jQ, cf.jV, T(0.99));
+        T fa = cap_factor(cf.aI, cf.aQ, cf.aV, T(0.99));
+        T nh = nuf / T(kNU0);
+        T i2 = T(1) / (nh * nh);
+        T s2c = sin(T(2) * lf.chi), c2c = cos(T(2) * lf.chi);
+        T jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+        out[0] += cf.jI * i2; out[1] += jQ * c2c; out[2] += jQ * s2c; out[3] += cf.jV * fe * i2;
+        out[4] += nh * cf.aI; out[5] += aQ * c2c; out[6] += aQ * s2c; out[7] += cf.aV * fa * nh;
+        out[8] += rQ * c2c; out[9] += rQ * s2c; out[10] += nh * cf.rV;
+        active = true;
+    }
+    return active;
+}
+
+// A stored FP64 sample (the reference's GeodesicSamples, direct_march.jl:71-88), [k - 1][npix] arrays.
+struct StoredSamples {
+    const double *t, *r, *th, *ph;
+    const unsigned char* fl;
+};
+
+// What one stored sample gives the consumer: position, emission-time offset, frame data.
+struct SampleGeo {
+    double x, y, z, sth, cth, ts, r, th;
+    bool usable, nur, nuth;
+};
+__device__ __forceinline__ SampleGeo stored_geo(const StoredSamples& S, long long q, double a, double rh_lo) {
+    SampleGeo g;
+    const unsigned f = S.fl[q];
+    g.r = S.r[q]; g.th = S.th[q]; g.ts = S.t[q];
+    g.usable = (f & 1u) && g.r > rh_lo;
+    g.nur = (f & 2u) != 0; g.nuth = (f & 4u) != 0;
+    g.x = g.y = g.z = g.sth = g.cth = 0.0;
+    if (g.usable) ks_coords(a, g.r, g.th, S.ph[q], g.x, g.y, g.z, g.sth, g.cth);
+    return g;
+}
+
+}  // namespace ks
+
+namespace {
+
+using namespace ks;
+
+// Per-splat constants of the gradient of THERMAL21 splats: d(K0/K2)/d(logTe), d(K1/K2)/d(logTe) at
+// x = 1/Theta_e (dK0/dx = -K1, dK1/dx = -K0 - K1/x), the derivatives of the field direction by its
+// angles, and the normalised quaternion with its norm.
+__global__ void k_grad_table(int nsplat, int first, const double* __restrict__ params, double* __restrict__ gtab) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsplat) return;
+    const double* p = params + 21LL * i;
+    double* o = gtab + (long long)(first + i) * GT_COUNT;
+    const double Te = exp(p[13]);
+    const double xb = 1.0 / Te;
+    double k0, k1;
+    besselk01(xb, k0, k1);
+    const double k2 = k0 + 2.0 * k1 / xb;
+    if (k2 > 0) {
+        const double dk0 = -k1, dk1 = -k0 - k1 / xb;
+        const double dk2 = dk0 + 2.0 * dk1 / xb - 2.0 * k1 / (xb * xb);
+        const double df0dx = (dk0 * k2 - k0 * dk2) / (k2 * k2), dkrdx = (dk1 * k2 - k1 * dk2) / (k2 * k2);
+        o[GT_DF0] = -xb * df0dx;   // dx/dlogTe = -x
+        o[GT_DKR] = -xb * dkrdx;
+    } else {
+        o[GT_DF0] = 0.0; o[GT_DKR] = 0.0;
+    }
+    const double st = sin(p[15]), ct = cos(p[15]), sp = sin(p[16]), cp = cos(p[16]);
+    o[GT_DBT0] = ct * cp; o[GT_DBT1] = ct * sp; o[GT_DBT2] = -st;
+    o[GT_DBP0] = -st * sp; o[GT_DBP1] = st * cp; o[GT_DBP2] = 0.0;
+    const double n = sqrt(p[6] * p[6] + p[7] * p[7] + p[8] * p[8] + p[9] * p[9]);
+    o[GT_QW] = p[6] / n; o[GT_QX] = p[7] / n; o[GT_QY] = p[8] / n; o[GT_QZ] = p[9] / n; o[GT_QN] = n;
+}
+
+// winding_cutoff_kernel! (dual_gradient.jl:81-97): the first sample of each ray beyond its nmax-th
+// passage through |z| < slab (N + 1 when there is none)
+__global__ void k_kstop(StoredSamples S, long long npix, int N, double rh_lo, int nmax, double slab, int* __restrict__ kstop) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    double zprev = 0.0;
+    int wn = 0;
+    bool inside = false, crossed = false, zset = false;
+    int stop = N + 1;
+    for (int k = 1; k <= N; ++k) {
+        const long long q = (long long)(k - 1) * npix + j;
+        const double r = S.r[q];
+        if (!((S.fl[q] & 1u) && r > rh_lo)) continue;
+        const double z = r * cos(S.th[q]);
+        // WindingState (step.jl:379-398)
+        if (!zset) { zprev = z; zset = true; inside = fabs(z) < slab; crossed = false; }
+        else {
+            const bool inside_now = fabs(z) < slab;
+            const bool crossing = zprev * z < 0.0;
+            if (inside || inside_now) {
+                crossed = crossed || crossing;
+                if (inside && !inside_now) { if (crossed) wn += 1; crossed = false; }
+                else if (!inside && inside_now) { crossed = crossing; }
+                inside = inside_now;
+            } else if (crossing) {
+                wn += 1;
+            }
+            zprev = z;
+        }
+        if (wn > nmax) { stop = k; break; }
+    }
+    kstop[j] = stop;
+}
+
+// polarized_tails_kernel! (dual_gradient.jl:129-147), FP64: one thread per (ray, combination);
+// tails[((c * (N + 1) + k) * 4 + s) * npix + j] = T_{k+1} (k = 0..N), img the observed Stokes vectors.
+__global__ void __launch_bounds__(128) k_tails(PlanView P, Spacetime st, long long npix, StoredSamples S, const int* __restrict__ kstop,
+                                               const double* __restrict__ tab64, int ntot, const double* __restrict__ ct,
+                                               const double* __restrict__ cnu, int ncombo, double L, double* __restrict__ tails,
+                                               double* __restrict__ img) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* tab = reinterpret_cast<double*>(smem);
+    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = tab64[q];
+    __syncthreads();
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= npix * ncombo) return;
+    const long long j = idx % npix;
+    const int c = int(idx / npix);
+    const int N = st.N;
+    const double a = st.a, rh_lo = st.rh * (1 + 1e-3);
+    const double nu = cnu[c], t_obs = ct[c], nh = nu / kNU0, Lnu = L / nh;
+    const double alpha = P.get(PF_ALPHA, j), beta = P.get(PF_BETA, j), eta = P.get(PF_ETA, j), lam = P.get(PF_LAM, j);
+    const double dtau = P.get(PF_DTAU, j), a_sin_tho = a * sin(st.thetao);
+    const int stop = kstop ? kstop[j] : N + 1;
+    double* tl = tails + (long long)c * (N + 1) * 4 * npix + j;
+    double T4[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int s = 0; s < 4; ++s) tl[((long long)N * 4 + s) * npix] = 0.0;
+    for (int k = N; k >= 1; --k) {
+        if (k < stop) {
+            const SampleGeo g = stored_geo(S, (long long)(k - 1) * npix + j, a, rh_lo);
+            if (g.usable) {
+                SampleFrame<double> F = sample_frame(a, g.r, g.th, g.sth, g.cth, eta, lam, g.nur, g.nuth);
+                double in[11];
+                if (sample_coefficients(tab, ntot, F, g.x, g.y, g.z, t_obs - g.ts, alpha, beta, a_sin_tho, nu, in)) {
+                    const double Sg = g.r * g.r + a * a * cos(g.th) * cos(g.th);
+                    double O[16], E[4];
+                    transfer_step(c_moments, in, in + 4, in + 8, Lnu * Sg * dtau, O, E);
+                    double Tn[4];
+                    for (int r = 0; r < 4; ++r) Tn[r] = E[r] + O[4 * r] * T4[0] + O[4 * r + 1] * T4[1] + O[4 * r + 2] * T4[2] + O[4 * r + 3] * T4[3];
+                    for (int r = 0; r < 4; ++r) T4[r] = Tn[r];
+                }
+            }
+        }
+        for (int s = 0; s < 4; ++s) tl[((long long)(k - 1) * 4 + s) * npix] = T4[s];
+    }
+    const double n3 = nh * nh * nh;
+    for (int s = 0; s < 4; ++s) img[((long long)c * npix + j) * 4 + s] = T4[s] * n3;
+}
+
+// polarized_dual_kernel! (dual_gradient.jl:151-178), FP64: one thread per (ray, combination),
+// forward over the samples; the ray's share of every splat's gradient into its own slots
+// grad[(row * ntot + i) * nrc + c * npix + j].
+__global__ void __launch_bounds__(128) k_dual_plain(PlanView P, Spacetime st, long long npix, StoredSamples S, const int* __restrict__ kstop,
+                                                    const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
+                                                    const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L,
+                                                    const double* __restrict__ tails, const double* __restrict__ dstokes,
+                                                    double* __restrict__ grad) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* tab = reinterpret_cast<double*>(smem);
+    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = tab64[q];
+    __syncthreads();
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= npix * ncombo) return;
+    const long long j = idx % npix;
+    const int c = int(idx / npix);
+    const long long nrc = npix * ncombo;
+    const int N = st.N;
+    const double a = st.a, rh_lo = st.rh * (1 + 1e-3);
+    const double nu = cnu[c], t_obs = ct[c], nh = nu / kNU0, Lnu = L / nh, n3 = nh * nh * nh;
+    const double alpha = P.get(PF_ALPHA, j), beta = P.get(PF_BETA, j), eta = P.get(PF_ETA, j), lam = P.get(PF_LAM, j);
+    const double dtau = P.get(PF_DTAU, j), a_sin_tho = a * sin(st.thetao);
+    const int stop = kstop ? kstop[j] : N + 1;
+    const double* tl = tails + (long long)c * (N + 1) * 4 * npix + j;
+    double w[4];
+    for (int s = 0; s < 4; ++s) w[s] = dstokes[((long long)c * npix + j) * 4 + s] * n3;
+    const int kend = min(stop - 1, N);
+    for (int k = 1; k <= kend; ++k) {
+        const SampleGeo g = stored_geo(S, (long long)(k - 1) * npix + j, a, rh_lo);
+        if (!g.usable) continue;
+        SampleFrame<double> F = sample_frame(a, g.r, g.th, g.sth, g.cth, eta, lam, g.nur, g.nuth);
+        const double t = t_obs - g.ts;
+        double in[11];
+        if (!sample_coefficients(tab, ntot, F, g.x, g.y, g.z, t, alpha, beta, a_sin_tho, nu, in)) continue;
+        const double Sg = g.r * g.r + a * a * cos(g.th) * cos(g.th);
+        double R[4];
+        for (int s = 0; s < 4; ++s) R[s] = tl[((long long)k * 4 + s) * npix];
+        double O[16], E[4], cb[11];
+        sample_adjoint(c_moments, in, Lnu * Sg * dtau, w, R, O, E, cb);
+        for (int i = 0; i < ntot; ++i) {
+            double gi[GR_COUNT];
+            for (int r = 0; r < GR_COUNT; ++r) gi[r] = 0.0;
+            if (!element_adjoint<double, 1>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, F, g.x, g.y, g.z, t, alpha, beta, a_sin_tho,
+                                            &nu, 1, 1u, cb, 0, 1, gi))
+                continue;
+            for (int r = 0; r < GR_COUNT; ++r) grad[((long long)r * ntot + i) * nrc + idx] += gi[r];
+        }
+        double wn[4];
+        for (int s = 0; s < 4; ++s) wn[s] = O[s] * w[0] + O[4 + s] * w[1] + O[8 + s] * w[2] + O[12 + s] * w[3];
+        for (int s = 0; s < 4; ++s) w[s] = wn[s];
+    }
+}
+
+// The deterministic sum of the per-ray slots (one block per (row, splat), a fixed tree), into the
+// column-major parameter layout dparams[i * 21 + row].
+__global__ void k_slot_reduce(const double* __restrict__ grad, long long nrc, int ntot, double* __restrict__ out) {
+    __shared__ double sh[256];
+    const int ri = blockIdx.x;   // row * ntot + i
+    const double* g = grad + (long long)ri * nrc;
+    double s = 0.0;
+    for (long long q = threadIdx.x; q < nrc; q += blockDim.x) s += g[q];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const int row = ri / ntot, i = ri % ntot;
+        out[(long long)i * GR_COUNT + row] = sh[0];
+    }
+}
+
+// Image-domain chi^2 and its seed (_frame_seed!, src/Fit/Fit.jl:537-577): for every sorted ray j and
+// combination c, r = (image - data) / sigma with data, sigma and mask in screen order; chi^2 = sum r^2
+// over unmasked pixels and Stokes, seed = 2 r / sigma (zero where masked). Per-block partial sums.
+__global__ void k_chi2_seed(const double* __restrict__ img, const long long* __restrict__ perm, long long npix, int ncombo,
+                            const double* __restrict__ data, const double* __restrict__ sigma, double sigma_s,
+                            const unsigned char* __restrict__ mask, double* __restrict__ seed, double* __restrict__ partial) {
+    __shared__ double sh[256];
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double acc = 0.0;
+    if (idx < npix * ncombo) {
+        const long long j = idx % npix, c = idx / npix;
+        const long long scr = c * npix + perm[j];
+        const bool use = mask ? mask[scr] != 0 : true;
+        for (int s = 0; s < 4; ++s) {
+            double sd = 0.0;
+            if (use) {
+                const double sg = sigma ? sigma[scr * 4 + s] : sigma_s;
+                const double r = (img[idx * 4 + s] - data[scr * 4 + s]) / sg;
+                acc += r * r;
+                sd = 2.0 * r / sg;
+            }
+            seed[idx * 4 + s] = sd;
+        }
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// sum of n partials in a fixed order (one block)
+__global__ void k_sum_partials(const double* __restrict__ partial, long long n, double* __restrict__ out) {
+    __shared__ double sh[256];
+    double s = 0.0;
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) s += partial[q];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+// screen- or sorted-order adjoint seeds (ks_adjoint's dstokes) into sorted order
+__global__ void k_sort_seed(const double* __restrict__ src, const long long* __restrict__ perm, long long npix, int ncombo, int screen,
+                            double* __restrict__ dst) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= npix * ncombo) return;
+    const long long j = idx % npix, c = idx / npix;
+    const long long sidx = screen ? c * npix + perm[j] : idx;
+    for (int s = 0; s < 4; ++s) dst[idx * 4 + s] = src[sidx * 4 + s];
+}
+
+}  // namespace
+
+// ---- the mixed path: a per-segment reverse pass over the FP32 sample stream --------------------------
+//
+// The forward pass (k_consume with MixedJob::gstate) stores, at every active (sample, ray, frequency),
+// the state P_k of the segment before the sample and the summed coefficients c_k. k_adj_bounds turns
+// the segments' (P, S) into the adjoint at each segment's start, w_s = (P_0 ... P_{s-1})^T w_1, and
+// the tail behind each segment's end, T_s = S_{s+1} + P_{s+1} T_{s+1}. k_adjoint_mixed then walks
+// each work unit (32 rays x one segment x one frame x CH frequencies) from its last sample to its
+// first: w_k = P_k^T w_s, the step adjoint (seven duals through the step operator) spread over the
+// warp, T <- E + O T, and the element adjoints of the (ray, splat) pairs that pass the support test,
+// 32 at a time, their 21 rows summed per splat in list order into the warp's accumulator (shared
+// memory). Each unit writes its own partial sums; k_unit_reduce adds the units in a fixed order.
+
+namespace {
+
+using namespace ks;
+
+__device__ __noinline__ void sample_adjoint_ool(const float* in, float Dl, const float* w, const float* R, float* O, float* E, float* cb) {
+    float o[16], e[4], c[11];
+    sample_adjoint(c_moments, in, Dl, w, R, o, e, c);
+#pragma unroll
+    for (int q = 0; q < 16; ++q) O[q] = o[q];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) E[q] = e[q];
+#pragma unroll
+    for (int q = 0; q < 11; ++q) cb[q] = c[q];
+}
+
+// s: the owner lane's column of the warp's sample data ([field][32]); cb: the owner's c-bar column of
+// [CH][11][32]; nu: the unit's frequencies
+template <int CH>
+__device__ __noinline__ void element_adjoint_ool(const float* p, const double* gt, const float* s, float t_obs, float a, float a_sin_tho,
+                                                 const float* nu, int nc, unsigned act, const float* cb, float* g) {
+    SampleFrame<float> F;
+    F.pu[0] = s[SF_PU0 * 32]; F.pu[1] = s[SF_PU1 * 32]; F.pu[2] = s[SF_PU2 * 32]; F.pu[3] = s[SF_PU3 * 32];
+    F.pz[0] = s[SF_PZ0 * 32]; F.pz[1] = s[SF_PZ1 * 32]; F.pz[2] = s[SF_PZ2 * 32]; F.pz[3] = s[SF_PZ3 * 32];
+    F.lapse_inv = s[SF_LI * 32]; F.om_lapse = s[SF_OL * 32]; F.sDS = s[SF_SDS * 32]; F.misS = s[SF_MIS * 32]; F.ivarpi = s[SF_IVP * 32];
+    F.r = s[SF_R * 32]; F.sth = s[SF_STH * 32]; F.cth = s[SF_CTH * 32]; F.a = a;
+    float gl[GR_COUNT];
+#pragma unroll
+    for (int r = 0; r < GR_COUNT; ++r) gl[r] = 0.f;
+    element_adjoint<float, CH>(p, gt, F, s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], t_obs - s[SF_T * 32], s[SF_ALPHA * 32], s[SF_BETA * 32],
+                               a_sin_tho, nu, nc, act, cb, 11 * 32, 32, gl);
+#pragma unroll
+    for (int r = 0; r < GR_COUNT; ++r) g[r] = gl[r];
+}
+
+template <int CH>
+struct AdjSmem {
+    static constexpr int kSampleBytes = 32 * kSF * 4;
+    static constexpr int kItemBytes = 32 * 32 * 2;        // (lane, splat) pair list
+    static constexpr int kCbBytes = 32 * CH * 11 * 4;     // c-bar per lane and frequency
+    static constexpr int kTwBytes = 32 * CH * 8 * 4;      // T (4) and w (4) per lane and frequency
+    static constexpr int kGitemBytes = 32 * GR_COUNT * 4; // the rows of each evaluated pair
+    static constexpr int kMetaBytes = 32 * 4 * 2;
+    static constexpr int kFixed = kSampleBytes + kItemBytes + kCbBytes + kTwBytes + kGitemBytes + kMetaBytes;
+    __host__ __device__ static size_t acc_bytes(int ntot) { return (size_t(ntot) * GR_COUNT * 4 + 15) / 16 * 16; }
+    __host__ __device__ static size_t warp_bytes(int ntot) { return size_t(kFixed) + acc_bytes(ntot); }
+    __host__ __device__ static size_t bytes(int ntot, int warps) {
+        return (size_t(ntot) * ST_COUNT * 4 + 15) / 16 * 16 + size_t(warps) * warp_bytes(ntot);
+    }
+};
+
+// the adjoint at each segment's start and the tail behind its end, per (ray, combination):
+// bnd[((combo nseg + s) 8 + q) npix + j], q = 0..3 w, 4..7 T
+__global__ void k_adj_bounds(MixedJob job, const double* __restrict__ cnu, const float* __restrict__ seg_out, const double* __restrict__ seeds,
+                             float* __restrict__ bnd) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ncombo = (long long)job.nframes * job.nfreq;
+    if (q >= job.npix * ncombo) return;
+    const long long combo = q / job.npix, j = q % job.npix;
+    const int v = int(combo / job.nframes);
+    const double nh = cnu[v] / kNU0, n3 = nh * nh * nh;
+    const float* base = seg_out + ((combo * job.nseg) * job.npix + j) * 20;
+    float* b = bnd + (combo * job.nseg) * 8 * job.npix + j;
+    double w[4];
+    for (int s = 0; s < 4; ++s) w[s] = seeds[(combo * job.npix + j) * 4 + s] * n3;
+    for (int sg = 0; sg < job.nseg; ++sg) {
+        const float* PS = base + (long long)sg * job.npix * 20;
+        for (int s = 0; s < 4; ++s) b[((long long)sg * 8 + s) * job.npix] = float(w[s]);
+        double wn[4];
+        for (int s = 0; s < 4; ++s) wn[s] = PS[s] * w[0] + PS[4 + s] * w[1] + PS[8 + s] * w[2] + PS[12 + s] * w[3];
+        for (int s = 0; s < 4; ++s) w[s] = wn[s];
+    }
+    double T4[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int sg = job.nseg - 1; sg >= 0; --sg) {
+        const float* PS = base + (long long)sg * job.npix * 20;
+        for (int s = 0; s < 4; ++s) b[((long long)sg * 8 + 4 + s) * job.npix] = float(T4[s]);
+        double Tn[4];
+        for (int r = 0; r < 4; ++r) Tn[r] = PS[16 + r] + PS[4 * r] * T4[0] + PS[4 * r + 1] * T4[1] + PS[4 * r + 2] * T4[2] + PS[4 * r + 3] * T4[3];
+        for (int r = 0; r < 4; ++r) T4[r] = Tn[r];
+    }
+}
+
+template <int CH, int NT>
+__global__ void __launch_bounds__(NT, 1)
+k_adjoint_mixed(Spacetime st, MixedJob job, const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
+                const double* __restrict__ ct, const double* __restrict__ cnu, const double* __restrict__ plan_f, const float* __restrict__ stream,
+                const float* __restrict__ gstate, const unsigned char* __restrict__ gact, const float* __restrict__ bnd,
+                unsigned long long* __restrict__ work, float* __restrict__ gunit) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* tab = reinterpret_cast<float*>(smem);
+    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wb = smem + (size_t(ntot) * ST_COUNT * 4 + 15) / 16 * 16 + size_t(warp) * AdjSmem<CH>::warp_bytes(ntot);
+    float* sf = reinterpret_cast<float*>(wb);
+    uint16_t* items = reinterpret_cast<uint16_t*>(wb + AdjSmem<CH>::kSampleBytes);
+    float* cbs = reinterpret_cast<float*>(wb + AdjSmem<CH>::kSampleBytes + AdjSmem<CH>::kItemBytes);
+    float* tw = cbs + 32 * CH * 11;                 // [c][8][32]: w 0..3, T 4..7
+    float* gitem = tw + 32 * CH * 8;                // [item][21]
+    int* meta_off = reinterpret_cast<int*>(gitem + 32 * GR_COUNT);
+    unsigned* meta_bits = reinterpret_cast<unsigned*>(meta_off + 32);
+    float* gacc = reinterpret_cast<float*>(meta_bits + 32);   // [splat][21]
+    __syncthreads();
+    const unsigned full = 0xffffffffu;
+    const int N = st.N;
+    const long long npad = job.npad, npix = job.npix;
+    const float a = float(st.a), a_sin_tho = float(st.a * sin(st.thetao));
+    const long long gsz = (long long)ntot * GR_COUNT;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(work, 1ull);
+        u = __shfl_sync(full, u, 0);
+        if (u >= (unsigned long long)job.total) break;
+        const long long ur = job.total - 1 - (long long)u;          // the forward pass's order: last rays first
+        const long long per_chunk = (long long)job.nseg * job.nframes * job.nvc;
+        const long long wg = ur / per_chunk;
+        const long long rem = ur % per_chunk;
+        const int seg = int(rem / (job.nframes * job.nvc));
+        const int y = int(rem % (job.nframes * job.nvc));
+        const int f = y / job.nvc, v0 = (y % job.nvc) * CH;
+        const long long jbase = wg * 32;
+        const long long j0 = jbase + lane;
+        const bool live = j0 < npix;
+        const long long j = live ? j0 : npix - 1;
+        const int k0 = 1 + seg * job.seg_len;
+        const int k1 = min(N + 1, k0 + job.seg_len);
+        const int nc = min(CH, job.nfreq - v0);
+        const float t_obs = float(ct[f]);
+        float nu[CH], Lnu[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const int v = min(v0 + c, job.nfreq - 1);
+            nu[c] = float(cnu[v]);
+            Lnu[c] = float(job.L / (cnu[v] / kNU0));
+        }
+        const float dtau = float(plan_f[(long long)PF_DTAU * npad + j]);
+        const float alpha = float(plan_f[(long long)PF_ALPHA * npad + j]), beta = float(plan_f[(long long)PF_BETA * npad + j]);
+        const float eta = float(plan_f[(long long)PF_ETA * npad + j]), lam = float(plan_f[(long long)PF_LAM * npad + j]);
+        // this lane's w (segment start) and T (segment end) per frequency
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const long long combo = (long long)min(v0 + c, job.nfreq - 1) * job.nframes + f;
+            const float* b = bnd + (combo * job.nseg + seg) * 8 * npix + j;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) tw[(c * 8 + q) * 32 + lane] = (live && c < nc) ? b[(long long)q * npix] : 0.f;
+        }
+        for (long long q = lane; q < gsz; q += 32) gacc[q] = 0.f;
+        __syncwarp();
+        for (int k = k1 - 1; k >= k0; --k) {
+            const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + j;
+            const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
+            unsigned actbits = 0u;
+            if (live && (flags & 8u)) {
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    if (c >= nc) break;
+                    const long long combo = (long long)(v0 + c) * job.nframes + f;
+                    if (gact[(combo * N + (k - 1)) * npad + j]) actbits |= 1u << c;
+                }
+            }
+            if (__ballot_sync(full, actbits != 0u) == 0u) continue;
+            float x = 0.f, yy = 0.f, z = 0.f, ts = 0.f, rho = 0.f;
+            if (actbits) {
+                x = sp[SM_X * npad]; yy = sp[SM_Y * npad]; z = sp[SM_Z * npad]; ts = sp[SM_T * npad];
+                const float r = sp[SM_R * npad], sth = sp[SM_STH * npad], cth = sp[SM_CTH * npad];
+                rho = sqrtf(x * x + yy * yy);
+                SampleFrame<float> F = sample_frame(a, r, 0.f, sth, cth, eta, lam, (flags & 2u) != 0u, (flags & 4u) != 0u);
+                float* mys = sf + lane;
+                mys[SF_X * 32] = x; mys[SF_Y * 32] = yy; mys[SF_Z * 32] = z; mys[SF_T * 32] = ts;
+                mys[SF_PU0 * 32] = F.pu[0]; mys[SF_PU1 * 32] = F.pu[1]; mys[SF_PU2 * 32] = F.pu[2]; mys[SF_PU3 * 32] = F.pu[3];
+                mys[SF_PZ0 * 32] = F.pz[0]; mys[SF_PZ1 * 32] = F.pz[1]; mys[SF_PZ2 * 32] = F.pz[2]; mys[SF_PZ3 * 32] = F.pz[3];
+                mys[SF_LI * 32] = F.lapse_inv; mys[SF_OL * 32] = F.om_lapse; mys[SF_SDS * 32] = F.sDS; mys[SF_MIS * 32] = F.misS;
+                mys[SF_IVP * 32] = F.ivarpi;
+                mys[SF_R * 32] = r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
+                mys[SF_SG * 32] = (r * r + a * a * cth * cth) * dtau;
+                mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
+            }
+            // 1. step adjoints of the (lane, frequency) pairs, spread over the warp
+            const int n2 = __popc(actbits);
+            int incl2 = n2;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                int v = __shfl_up_sync(full, incl2, d);
+                if (lane >= d) incl2 += v;
+            }
+            const int off2 = incl2 - n2;
+            const int total2 = __shfl_sync(full, incl2, 31);
+            meta_off[lane] = off2;
+            meta_bits[lane] = actbits;
+            __syncwarp();
+            for (int base = 0; base < total2; base += 32) {
+                const int g = base + lane;
+                if (g < total2) {
+                    int o = 0;
+#pragma unroll
+                    for (int d = 16; d >= 1; d >>= 1)
+                        if (o + d < 32 && meta_off[o + d] <= g) o += d;
+                    unsigned bits = meta_bits[o];
+                    const int jj = g - meta_off[o];
+                    for (int q = 0; q < jj; ++q) bits &= bits - 1;
+                    const int c = __ffs(bits) - 1;
+                    const long long combo = (long long)(v0 + c) * job.nframes + f;
+                    const float* gs = gstate + ((combo * N + (k - 1)) * 27) * npad + jbase + o;
+                    float Pm[16], in[11];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) Pm[q] = gs[q * npad];
+#pragma unroll
+                    for (int q = 0; q < 11; ++q) in[q] = gs[(16 + q) * npad];
+                    float* twc = tw + c * 8 * 32 + o;
+                    float wk[4], R[4];
+#pragma unroll
+                    for (int s = 0; s < 4; ++s)
+                        wk[s] = Pm[s] * twc[0] + Pm[4 + s] * twc[32] + Pm[8 + s] * twc[64] + Pm[12 + s] * twc[96];
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) R[s] = twc[(4 + s) * 32];
+                    float Lc = Lnu[0];
+#pragma unroll
+                    for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;
+                    float O[16], E[4], cb[11];
+                    sample_adjoint_ool(in, Lc * sf[SF_SG * 32 + o], wk, R, O, E, cb);
+                    float* cbo = cbs + c * 11 * 32 + o;
+#pragma unroll
+                    for (int q = 0; q < 11; ++q) cbo[q * 32] = cb[q];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                        twc[(4 + r) * 32] = E[r] + O[4 * r] * R[0] + O[4 * r + 1] * R[1] + O[4 * r + 2] * R[2] + O[4 * r + 3] * R[3];
+                }
+            }
+            __syncwarp();
+            // 2. element adjoints of the (lane, splat) pairs inside the support and above the cutoff
+            const float t = t_obs - ts;
+            for (int s0 = 0; s0 < ntot; s0 += 32) {
+                unsigned mask = 0u;
+                if (actbits) {
+                    const int nb = min(32, ntot - s0);
+                    for (int b = 0; b < nb; ++b) {
+                        const float* p = tab + (s0 + b) * ST_COUNT;
+                        const float dr = rho - p[ST_RHO], dz = z - p[ST_CZ];
+                        if (dr * dr + dz * dz > p[ST_SUPP]) continue;
+                        float q;
+                        if (!splat_exponent(p, t, x, yy, z, true, q)) continue;
+                        if (q < kQCUT) mask |= 1u << b;
+                    }
+                }
+                const int n = __popc(mask);
+                int incl = n;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    int v = __shfl_up_sync(full, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                const int off = incl - n;
+                const int total = __shfl_sync(full, incl, 31);
+                if (total == 0) continue;
+                {
+                    unsigned m = mask;
+                    int kk = off;
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        items[kk++] = uint16_t((lane << 5) | b);
+                    }
+                }
+                __syncwarp();
+                for (int base = 0; base < total; base += 32) {
+                    const int kk = base + lane;
+                    float g[GR_COUNT];
+#pragma unroll
+                    for (int r = 0; r < GR_COUNT; ++r) g[r] = 0.f;
+                    if (kk < total) {
+                        const int it = items[kk];
+                        const int o = it >> 5, i = s0 + (it & 31);
+                        element_adjoint_ool<CH>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, sf + o, t_obs, a, a_sin_tho, nu, nc,
+                                                meta_bits[o], cbs + o, g);
+                    }
+#pragma unroll
+                    for (int r = 0; r < GR_COUNT; ++r) gitem[lane * GR_COUNT + r] = g[r];
+                    __syncwarp();
+                    if (lane < GR_COUNT) {
+                        const int m = min(32, total - base);
+                        for (int q = 0; q < m; ++q) {
+                            const int i = s0 + (items[base + q] & 31);
+                            gacc[i * GR_COUNT + lane] += gitem[q * GR_COUNT + lane];
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        float* gu = gunit + ur * gsz;
+        for (long long q = lane; q < gsz; q += 32) gu[q] = gacc[q];
+        __syncwarp();
+    }
+}
+
+// The sum over work units in a fixed order: stage 1 adds the units of each chunk (one thread per
+// gradient entry and chunk), stage 2 the chunks.
+__global__ void k_unit_reduce1(const float* __restrict__ gunit, long long nunits, long long gsz, int per_chunk, double* __restrict__ part) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= gsz) return;
+    const long long u0 = (long long)blockIdx.y * per_chunk, u1 = min(nunits, u0 + per_chunk);
+    double s = 0.0;
+    for (long long uu = u0; uu < u1; ++uu) s += gunit[uu * gsz + e];
+    part[(long long)blockIdx.y * gsz + e] = s;
+}
+__global__ void k_unit_reduce2(const double* __restrict__ part, int nchunks, long long gsz, double* __restrict__ out) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= gsz) return;
+    double s = 0.0;
+    for (int ch = 0; ch < nchunks; ++ch) s += part[(long long)ch * gsz + e];
+    out[e] = s;
+}
+
+}  // namespace

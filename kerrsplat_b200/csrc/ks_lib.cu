@@ -586,6 +586,12 @@ __global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, 
     }
 }
 
+}  // namespace
+
+#include "ks_adjoint.cuh"
+
+namespace {
+
 __global__ void k_inverse_perm(const long long* __restrict__ perm, long long npix, long long* __restrict__ inv) {
     long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j < npix) inv[perm[j]] = j;
@@ -632,6 +638,16 @@ struct ks_context {
     DevBuf alpha, beta, key, key2, idx, perm, plan, nanch, aoff, anchors, resid_t, resid_phi, scratch;
     DevBuf tab, combos, out_sorted, stage_in, stage_out, counters, seg_out, work, stream_buf;
     DevBuf inv_perm, dft_tu, dft_tv, dft_a, dft_t, dft_c, dft_s, dft_in[8], dft_partial;
+    // adjoint: gradient table, stored FP64 samples (plain path), cutoffs, tails, per-ray slots,
+    // seeds, chi^2 partials; mixed path: per-sample states, activity, segment bounds, unit partials
+    DevBuf gtab, samples, kstop, tails, slots, dgrad, seeds, chi_part, chi_val, dstage;
+    DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part;
+    bool samples_ready = false;
+    MixedJob last_job{};                    // the segmentation of the last mixed forward pass
+    float* fwd_gstate = nullptr;            // set during the adjoint's forward pass only
+    unsigned char* fwd_gact = nullptr;
+    double adjoint_ms = 0.0;
+    long long adjoint_launches = 0;
     bool count_events = false;
     bool geo64 = true;    // mixed path: FP64 march feeding the FP32 transport (false: KS_MIXED_FP32 march)
     long long total_anchors = 0;
@@ -733,6 +749,57 @@ int nrows_of(int kind) {
     }
 }
 
+// The concatenated splat table of a scene (and, with `grad`, the gradient table of its THERMAL21
+// splats): validates the sets, stages each set's parameters and runs k_splat_table / k_grad_table.
+int build_tables(ks_context* c, const ks_splat_set* sets, int nsets, int* ntot_out, bool grad) {
+    int ntot = 0;
+    for (int s = 0; s < nsets; ++s) {
+        int nr = nrows_of(sets[s].kind);
+        if (nr < 0 || sets[s].kind == KS_THIN14) return fail(c, KS_ERR_ARGUMENT, "set %d: unsupported kind %d", s, sets[s].kind);
+        if (sets[s].kind == KS_KNOT21) return fail(c, KS_ERR_ARGUMENT, "set %d: knot splats are not supported by ks_render yet", s);
+        if (grad && sets[s].kind != KS_THERMAL21)
+            return fail(c, KS_ERR_ARGUMENT, "set %d: the adjoint covers thermal polarized splats (KS_THERMAL21) only", s);
+        if (sets[s].nsplat < 0 || (sets[s].nsplat > 0 && !sets[s].params)) return fail(c, KS_ERR_ARGUMENT, "set %d: bad parameters", s);
+        if (sets[s].kind == KS_KAPPA22 && sets[s].nsplat > 0 && !sets[s].hyp) return fail(c, KS_ERR_ARGUMENT, "set %d: kappa sets need hyp", s);
+        ntot += sets[s].nsplat;
+    }
+    KS_CUDA(c, c->tab.ensure(size_t(std::max(ntot, 1)) * ST_COUNT * sizeof(double)));
+    if (grad) KS_CUDA(c, c->gtab.ensure(size_t(std::max(ntot, 1)) * GT_COUNT * sizeof(double)));
+    int first = 0;
+    for (int s = 0; s < nsets; ++s) {
+        const ks_splat_set& S = sets[s];
+        if (S.nsplat == 0) continue;
+        const int nr = nrows_of(S.kind);
+        const void* dh = nullptr;
+        // each set is staged into its own device buffer
+        std::vector<double> hp(size_t(nr) * S.nsplat);
+        KS_CUDA(c, cudaMemcpy(hp.data(), S.params, hp.size() * sizeof(double), cudaMemcpyDefault));
+        for (double v : hp) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "set %d: non-finite parameter", s);
+        DevBuf tmp;
+        KS_CUDA(c, tmp.ensure(hp.size() * sizeof(double) + size_t(S.nsplat) * sizeof(double)));
+        KS_CUDA(c, cudaMemcpyAsync(tmp.p, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        if (S.kind == KS_KAPPA22) {
+            double* hd = tmp.as<double>() + hp.size();
+            KS_CUDA(c, cudaMemcpyAsync(hd, S.hyp, S.nsplat * sizeof(double), cudaMemcpyDefault, c->stream));
+            dh = hd;
+        }
+        SetDesc d{S.kind, nr, S.nsplat, first, tmp.as<const double>(), (const double*)dh, S.gamma_max > 0 ? S.gamma_max : 1e5};
+        k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+        if (grad) {
+            k_grad_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(S.nsplat, first, tmp.as<const double>(), c->gtab.as<double>());
+            c->launches++;
+            KS_CUDA(c, cudaGetLastError());
+        }
+        KS_CUDA(c, cudaStreamSynchronize(c->stream));
+        tmp.release();
+        first += S.nsplat;
+    }
+    *ntot_out = ntot;
+    return KS_OK;
+}
+
 template <int CH, int NT, int KM>
 int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int per_sm) {
     MixedJob job = job0;
@@ -750,6 +817,9 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     job.total = base_units * job.nseg;
     const double* dt = c->combos.as<double>();
     const double* dn = dt + job.nframes;
+    job.gstate = c->fwd_gstate;
+    job.gact = c->fwd_gact;
+    c->last_job = job;
     const size_t seg_bytes = size_t(job.nframes) * job.nfreq * job.nseg * c->npix * 20 * sizeof(float);
     KS_CUDA(c, c->seg_out.ensure(seg_bytes));
     KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
@@ -1006,6 +1076,7 @@ int ks_regenerate(ks_context* c, double a, double theta_o, int32_t nsamples, int
     KS_CUDA(c, cudaMemsetAsync(c->resid_phi.p, 0, n * sizeof(double), c->stream));
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
     c->regenerated = true;
+    c->samples_ready = false;
     return KS_OK;
 }
 
@@ -1135,44 +1206,11 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     for (double v : ht) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite observation time");
     for (double v : hnu) if (!(std::isfinite(v) && v > 0)) return fail(c, KS_ERR_NONFINITE, "frequencies must be finite and positive");
     int ntot = 0;
-    for (int s = 0; s < nsets; ++s) {
-        int nr = nrows_of(sets[s].kind);
-        if (nr < 0 || sets[s].kind == KS_THIN14) return fail(c, KS_ERR_ARGUMENT, "set %d: unsupported kind %d", s, sets[s].kind);
-        if (sets[s].kind == KS_KNOT21) return fail(c, KS_ERR_ARGUMENT, "set %d: knot splats are not supported by ks_render yet", s);
-        if (sets[s].nsplat < 0 || (sets[s].nsplat > 0 && !sets[s].params)) return fail(c, KS_ERR_ARGUMENT, "set %d: bad parameters", s);
-        if (sets[s].kind == KS_KAPPA22 && sets[s].nsplat > 0 && !sets[s].hyp) return fail(c, KS_ERR_ARGUMENT, "set %d: kappa sets need hyp", s);
-        ntot += sets[s].nsplat;
+    {
+        int st_ = build_tables(c, sets, nsets, &ntot, false);
+        if (st_) return st_;
     }
     const long long n = c->npix;
-    KS_CUDA(c, c->tab.ensure(size_t(std::max(ntot, 1)) * ST_COUNT * sizeof(double)));
-    int first = 0;
-    for (int s = 0; s < nsets; ++s) {
-        const ks_splat_set& S = sets[s];
-        if (S.nsplat == 0) continue;
-        int nr = nrows_of(S.kind);
-        const void* dp = nullptr;
-        const void* dh = nullptr;
-        // each set is staged into its own slice of the staging buffer
-        std::vector<double> hp(size_t(nr) * S.nsplat);
-        KS_CUDA(c, cudaMemcpy(hp.data(), S.params, hp.size() * sizeof(double), cudaMemcpyDefault));
-        for (double v : hp) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "set %d: non-finite parameter", s);
-        DevBuf tmp;
-        KS_CUDA(c, tmp.ensure(hp.size() * sizeof(double) + size_t(S.nsplat) * sizeof(double)));
-        KS_CUDA(c, cudaMemcpyAsync(tmp.p, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        dp = tmp.p;
-        if (S.kind == KS_KAPPA22) {
-            double* hd = tmp.as<double>() + hp.size();
-            KS_CUDA(c, cudaMemcpyAsync(hd, S.hyp, S.nsplat * sizeof(double), cudaMemcpyDefault, c->stream));
-            dh = hd;
-        }
-        SetDesc d{S.kind, nr, S.nsplat, first, (const double*)dp, (const double*)dh, S.gamma_max > 0 ? S.gamma_max : 1e5};
-        k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
-        c->launches++;
-        KS_CUDA(c, cudaGetLastError());
-        KS_CUDA(c, cudaStreamSynchronize(c->stream));
-        tmp.release();
-        first += S.nsplat;
-    }
     const int ncombo = nframes * nfreq;
     std::vector<double> hc(2 * size_t(ncombo));
     for (int fv = 0; fv < nfreq; ++fv)
@@ -1223,6 +1261,310 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->kernel_ms += ms;
+    return KS_OK;
+}
+
+}  // extern "C"
+
+// ---- the adjoint (src/Splats/dual_gradient.jl, src/Fit/Fit.jl:451-577) --------------------------------
+
+namespace {
+
+__global__ void k_accumulate(double* __restrict__ dst, const double* __restrict__ src, long long n, int accumulate) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q < n) dst[q] = (accumulate ? dst[q] : 0.0) + src[q];
+}
+
+// The stored FP64 samples of every ray (the reference's store_samples cache, built once per regenerate).
+int ensure_samples(ks_context* c, StoredSamples* S) {
+    const long long n = c->npix;
+    const size_t ns = size_t(n) * c->st.N;
+    KS_CUDA(c, c->samples.ensure(ns * (4 * sizeof(double) + 1)));
+    double* d = c->samples.as<double>();
+    unsigned char* fl = reinterpret_cast<unsigned char*>(d + 4 * ns);
+    if (!c->samples_ready) {
+        k_march_store<<<nblocks(n), kBlock, 0, c->stream>>>(plan_view(c), c->st, n, d, d + ns, d + 2 * ns, d + 3 * ns, fl,
+                                                              c->resid_t.as<double>(), c->resid_phi.as<double>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+        c->samples_ready = true;
+    }
+    *S = StoredSamples{d, d + ns, d + 2 * ns, d + 3 * ns, fl};
+    return KS_OK;
+}
+
+// Stage `count` elements of `src` (host or device) into `buf`; returns the device pointer.
+template <class U>
+int stage_dev(ks_context* c, DevBuf& buf, const U* src, size_t count, const U** dev) {
+    if (!src) { *dev = nullptr; return KS_OK; }
+    const void* d = nullptr;
+    int s = stage_in(c, buf, src, count * sizeof(U), &d);
+    *dev = reinterpret_cast<const U*>(d);
+    return s;
+}
+
+// Occupancy of k_adjoint_mixed<CH, NT> with its shared memory for `ntot` splats (0 if it does not fit).
+template <int CH, int NT>
+int adjoint_blocks(ks_context* c, int ntot) {
+    const size_t smem = AdjSmem<CH>::bytes(ntot, NT / 32);
+    if (smem > 227 * 1024) return 0;
+    if (cudaFuncSetAttribute(k_adjoint_mixed<CH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_mixed<CH, NT>, NT, smem) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return per_sm;
+}
+
+template <int CH, int NT>
+int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* dt, const double* dn) {
+    int nsm = 0;
+    KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    const MixedJob& job = c->last_job;
+    const long long ncombo = (long long)job.nframes * job.nfreq;
+    KS_CUDA(c, c->adj_bnd.ensure(size_t(ncombo) * job.nseg * 8 * c->npix * sizeof(float)));
+    k_adj_bounds<<<nblocks(c->npix * ncombo, 256), 256, 0, c->stream>>>(job, dn, c->seg_out.as<float>(), c->seeds.as<double>(),
+                                                                        c->adj_bnd.as<float>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    const long long gsz = (long long)ntot * GR_COUNT;
+    KS_CUDA(c, c->adj_unit.ensure(size_t(job.total) * gsz * sizeof(float)));
+    KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
+    KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
+    constexpr int W = NT / 32;
+    const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
+    const size_t smem = AdjSmem<CH>::bytes(ntot, W);
+    k_adjoint_mixed<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(c->st, job, c->tab.as<double>(), c->gtab.as<double>(), ntot, dt, dn,
+                                                                    c->plan.as<double>(), c->stream_buf.as<float>(), job.gstate, job.gact,
+                                                                    c->adj_bnd.as<float>(), c->work.as<unsigned long long>(),
+                                                                    c->adj_unit.as<float>());
+    c->launches++;
+    c->adjoint_launches++;
+    KS_CUDA(c, cudaGetLastError());
+    const int per_chunk = 256;
+    const int nchunks = int((job.total + per_chunk - 1) / per_chunk);
+    KS_CUDA(c, c->adj_part.ensure(size_t(nchunks) * gsz * sizeof(double)));
+    k_unit_reduce1<<<dim3(nblocks(gsz, 128), nchunks), 128, 0, c->stream>>>(c->adj_unit.as<float>(), job.total, gsz, per_chunk,
+                                                                             c->adj_part.as<double>());
+    k_unit_reduce2<<<nblocks(gsz, 128), 128, 0, c->stream>>>(c->adj_part.as<double>(), nchunks, gsz, c->dgrad.as<double>());
+    c->launches += 2;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
+template <int CH>
+int launch_adjoint_mixed_ch(ks_context* c, int ntot, const double* dt, const double* dn) {
+    const int w256 = adjoint_blocks<CH, 256>(c, ntot) * 8, w128 = adjoint_blocks<CH, 128>(c, ntot) * 4,
+              w64 = adjoint_blocks<CH, 64>(c, ntot) * 2, w32 = adjoint_blocks<CH, 32>(c, ntot);
+    const int best = std::max(std::max(w256, w128), std::max(w64, w32));
+    if (best <= 0) return fail(c, KS_ERR_ARGUMENT, "too many splats for the mixed adjoint (%d)", ntot);
+    if (w256 == best) return launch_adjoint_mixed_nt<CH, 256>(c, ntot, w256 / 8, dt, dn);
+    if (w128 == best) return launch_adjoint_mixed_nt<CH, 128>(c, ntot, w128 / 4, dt, dn);
+    if (w64 == best) return launch_adjoint_mixed_nt<CH, 64>(c, ntot, w64 / 2, dt, dn);
+    return launch_adjoint_mixed_nt<CH, 32>(c, ntot, w32, dt, dn);
+}
+
+// The forward image with the state the reverse pass needs (FP64: stored samples, cutoffs, tails),
+// the seeds (given, or those of chi^2), the reverse pass and the reduction into dparams.
+int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double* times, int nframes, const double* nus, int nfreq,
+                double L, int precision, int nmax, double slab, const double* dstokes, int order, const double* data,
+                const double* sigma, double sigma_s, const uint8_t* mask, double* chi2_out, double* dparams, int accumulate,
+                double* image) {
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    if (nsets < 0 || (nsets > 0 && !sets)) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
+    if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d for the adjoint", precision);
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
+    if (!std::isfinite(slab)) return fail(c, KS_ERR_NONFINITE, "non-finite slab");
+    if (!dparams) return fail(c, KS_ERR_ARGUMENT, "dparams is required");
+    if (data && !sigma && !(std::isfinite(sigma_s) && sigma_s > 0))
+        return fail(c, KS_ERR_ARGUMENT, "chi^2 needs sigma (an array, or a finite positive scalar)");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    std::vector<double> ht(nframes), hnu(nfreq);
+    KS_CUDA(c, cudaMemcpy(ht.data(), times, nframes * sizeof(double), cudaMemcpyDefault));
+    KS_CUDA(c, cudaMemcpy(hnu.data(), nus, nfreq * sizeof(double), cudaMemcpyDefault));
+    for (double v : ht) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite observation time");
+    for (double v : hnu) if (!(std::isfinite(v) && v > 0)) return fail(c, KS_ERR_NONFINITE, "frequencies must be finite and positive");
+    int ntot = 0;
+    {
+        int s = build_tables(c, sets, nsets, &ntot, true);
+        if (s) return s;
+    }
+    const long long n = c->npix;
+    const int N = c->st.N;
+    const int ncombo = nframes * nfreq;
+    const long long nrc = n * ncombo;
+    // the times, the frequencies (the mixed forward pass), then per combination fv * nframes + ft its
+    // time and frequency (the plain path)
+    std::vector<double> hc(ht);
+    hc.insert(hc.end(), hnu.begin(), hnu.end());
+    hc.resize(size_t(nframes) + nfreq + 2 * size_t(ncombo));
+    for (int fv = 0; fv < nfreq; ++fv)
+        for (int ft = 0; ft < nframes; ++ft) {
+            hc[nframes + nfreq + size_t(fv) * nframes + ft] = ht[ft];
+            hc[nframes + nfreq + ncombo + size_t(fv) * nframes + ft] = hnu[fv];
+        }
+    KS_CUDA(c, c->combos.ensure(hc.size() * sizeof(double)));
+    KS_CUDA(c, cudaMemcpyAsync(c->combos.p, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double* dtimes = c->combos.as<double>();
+    const double* dfreqs = dtimes + nframes;
+    const double* dct = dfreqs + nfreq;
+    const double* dcn = dct + ncombo;
+    KS_CUDA(c, c->out_sorted.ensure(size_t(nrc) * 4 * sizeof(double)));
+    KS_CUDA(c, c->seeds.ensure(size_t(nrc) * 4 * sizeof(double)));
+    KS_CUDA(c, c->dgrad.ensure(size_t(std::max(ntot, 1)) * GR_COUNT * sizeof(double)));
+    cudaEventRecord(c->ev0, c->stream);
+    const bool mixed = precision == KS_MIXED;
+    // 1. forward pass with the reverse pass's state
+    StoredSamples S{};
+    const int* kst = nullptr;
+    const size_t tab_smem = size_t(ntot) * ST_COUNT * sizeof(double);
+    if (mixed) {
+        c->geo64 = true;
+        const size_t rows = size_t(ncombo) * N * c->npad;
+        KS_CUDA(c, c->adj_state.ensure(rows * 27 * sizeof(float)));
+        KS_CUDA(c, c->adj_act.ensure(rows));
+        KS_CUDA(c, cudaMemsetAsync(c->adj_act.p, 0, rows, c->stream));
+        c->fwd_gstate = c->adj_state.as<float>();
+        c->fwd_gact = c->adj_act.as<unsigned char>();
+        int s = launch_mixed(c, ntot, ht.data(), nframes, nfreq, L, nmax, slab, true);
+        c->fwd_gstate = nullptr;
+        c->fwd_gact = nullptr;
+        if (s) return s;
+    } else {
+    if (tab_smem > 200 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for the FP64 adjoint (%d)", ntot);
+    {
+        int s = ensure_samples(c, &S);
+        if (s) return s;
+    }
+    if (nmax >= 0) {
+        KS_CUDA(c, c->kstop.ensure(size_t(n) * sizeof(int)));
+        k_kstop<<<nblocks(n), kBlock, 0, c->stream>>>(S, n, N, c->st.rh * (1 + 1e-3), nmax, slab, c->kstop.as<int>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+        kst = c->kstop.as<int>();
+    }
+    KS_CUDA(c, c->tails.ensure(size_t(ncombo) * (N + 1) * 4 * n * sizeof(double)));
+    KS_CUDA(c, cudaFuncSetAttribute(k_tails, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_smem));
+    k_tails<<<nblocks(nrc), kBlock, tab_smem, c->stream>>>(plan_view(c), c->st, n, S, kst, c->tab.as<double>(), ntot, dct, dcn, ncombo, L,
+                                                          c->tails.as<double>(), c->out_sorted.as<double>());
+    c->launches++;
+    c->adjoint_launches++;
+    KS_CUDA(c, cudaGetLastError());
+    }
+    // 2. seeds
+    const long long nblk = (nrc + 255) / 256;
+    if (data) {
+        const double *dd = nullptr, *ds = nullptr;
+        const uint8_t* dm = nullptr;
+        KS_CUDA(c, c->dstage.ensure(size_t(nrc) * 4 * sizeof(double) * (sigma ? 2 : 1) + size_t(nrc)));
+        // host data, sigma and mask share one staging buffer
+        const bool hd = !is_device_ptr(data), hs = sigma && !is_device_ptr(sigma), hm = mask && !is_device_ptr(mask);
+        double* st0 = c->dstage.as<double>();
+        if (hd) { KS_CUDA(c, cudaMemcpyAsync(st0, data, size_t(nrc) * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream)); dd = st0; }
+        else dd = data;
+        if (sigma) {
+            if (hs) { KS_CUDA(c, cudaMemcpyAsync(st0 + nrc * 4, sigma, size_t(nrc) * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream)); ds = st0 + nrc * 4; }
+            else ds = sigma;
+        }
+        if (mask) {
+            uint8_t* m0 = reinterpret_cast<uint8_t*>(st0 + nrc * 4 * (sigma ? 2 : 1));
+            if (hm) { KS_CUDA(c, cudaMemcpyAsync(m0, mask, size_t(nrc), cudaMemcpyHostToDevice, c->stream)); dm = m0; }
+            else dm = mask;
+        }
+        KS_CUDA(c, c->chi_part.ensure(size_t(nblk) * sizeof(double)));
+        KS_CUDA(c, c->chi_val.ensure(sizeof(double)));
+        k_chi2_seed<<<unsigned(nblk), 256, 0, c->stream>>>(c->out_sorted.as<double>(), c->perm.as<long long>(), n, ncombo, dd, ds, sigma_s, dm,
+                                                           c->seeds.as<double>(), c->chi_part.as<double>());
+        k_sum_partials<<<1, 256, 0, c->stream>>>(c->chi_part.as<double>(), nblk, c->chi_val.as<double>());
+        c->launches += 2;
+        KS_CUDA(c, cudaGetLastError());
+    } else {
+        const double* dsd = nullptr;
+        {
+            int s = stage_dev(c, c->dstage, dstokes, size_t(nrc) * 4, &dsd);
+            if (s) return s;
+        }
+        k_sort_seed<<<nblocks(nrc, 256), 256, 0, c->stream>>>(dsd, c->perm.as<long long>(), n, ncombo, order == KS_ORDER_SCREEN ? 1 : 0,
+                                                              c->seeds.as<double>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
+    // 3. reverse pass and the deterministic reduction
+    if (ntot > 0 && mixed) {
+        const int nf = nfreq;
+        int s = nf >= 4 ? launch_adjoint_mixed_ch<4>(c, ntot, dtimes, dfreqs)
+                        : (nf == 3 ? launch_adjoint_mixed_ch<3>(c, ntot, dtimes, dfreqs) : launch_adjoint_mixed_ch<1>(c, ntot, dtimes, dfreqs));
+        if (s) return s;
+    } else if (ntot > 0) {
+        const size_t slot_bytes = size_t(GR_COUNT) * ntot * nrc * sizeof(double);
+        KS_CUDA(c, c->slots.ensure(slot_bytes));
+        KS_CUDA(c, cudaMemsetAsync(c->slots.p, 0, slot_bytes, c->stream));
+        KS_CUDA(c, cudaFuncSetAttribute(k_dual_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_smem));
+        k_dual_plain<<<nblocks(nrc), kBlock, tab_smem, c->stream>>>(plan_view(c), c->st, n, S, kst, c->tab.as<double>(), c->gtab.as<double>(),
+                                                                   ntot, dct, dcn, ncombo, L, c->tails.as<double>(), c->seeds.as<double>(),
+                                                                   c->slots.as<double>());
+        c->launches++;
+        c->adjoint_launches++;
+        KS_CUDA(c, cudaGetLastError());
+        k_slot_reduce<<<unsigned(GR_COUNT * ntot), 256, 0, c->stream>>>(c->slots.as<double>(), nrc, ntot, c->dgrad.as<double>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    // 4. results
+    const long long ng = (long long)ntot * GR_COUNT;
+    if (ng > 0) {
+        if (is_device_ptr(dparams)) {
+            k_accumulate<<<nblocks(ng, 256), 256, 0, c->stream>>>(dparams, c->dgrad.as<double>(), ng, accumulate);
+            c->launches++;
+            KS_CUDA(c, cudaGetLastError());
+        } else {
+            std::vector<double> hg(ng);
+            KS_CUDA(c, cudaMemcpyAsync(hg.data(), c->dgrad.p, ng * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            KS_CUDA(c, cudaStreamSynchronize(c->stream));
+            for (long long q = 0; q < ng; ++q) dparams[q] = (accumulate ? dparams[q] : 0.0) + hg[q];
+        }
+    }
+    if (data && chi2_out) KS_CUDA(c, cudaMemcpyAsync(chi2_out, c->chi_val.p, sizeof(double), cudaMemcpyDefault, c->stream));
+    if (image) {
+        int s = emit(c, c->out_sorted.as<double>(), 4, ncombo, KS_ORDER_SCREEN, image);
+        if (s) return s;
+    }
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->adjoint_ms += ms;
+    return KS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ks_adjoint(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+               int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* dstokes, int32_t order,
+               double* dparams, int32_t accumulate) {
+    if (!c || !dstokes) return KS_ERR_ARGUMENT;
+    return adjoint_run(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, dstokes, order, nullptr, nullptr, 0.0,
+                       nullptr, nullptr, dparams, accumulate, nullptr);
+}
+
+int ks_chi2_gradient(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+                     int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* data, const double* sigma,
+                     double sigma_scalar, const uint8_t* mask, double* chi2, double* dparams, int32_t accumulate, double* image) {
+    if (!c || !data) return KS_ERR_ARGUMENT;
+    return adjoint_run(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, nullptr, KS_ORDER_SCREEN, data, sigma,
+                       sigma_scalar, mask, chi2, dparams, accumulate, image);
+}
+
+int ks_adjoint_stats(ks_context* c, double* adjoint_ms, long long* launches, int reset) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (adjoint_ms) *adjoint_ms = c->adjoint_ms;
+    if (launches) *launches = c->adjoint_launches;
+    if (reset) { c->adjoint_ms = 0.0; c->adjoint_launches = 0; }
     return KS_OK;
 }
 

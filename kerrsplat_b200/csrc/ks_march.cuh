@@ -67,10 +67,10 @@ __device__ __forceinline__ MarchRay<T> load_ray(const PlanView& P, const Spaceti
 
 // ---- per-sample geometry (recurrence.jl:169-308, quadrature.jl:110-215) ---------------------------
 
-template <class T> __device__ __forceinline__ T kpi();
+template <class T> __device__ __forceinline__ T kpi() { return T(kPi); }
 template <> __device__ __forceinline__ double kpi<double>() { return kPi; }
 template <> __device__ __forceinline__ float kpi<float>() { return 3.14159265358979323846f; }
-template <class T> __device__ __forceinline__ T keps();
+template <class T> __device__ __forceinline__ T keps() { return T(kEps); }
 template <> __device__ __forceinline__ double keps<double>() { return kEps; }
 template <> __device__ __forceinline__ float keps<float>() { return 1.1920929e-7f; }
 

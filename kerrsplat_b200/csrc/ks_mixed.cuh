@@ -108,6 +108,13 @@ struct MixedSink {
     unsigned* meta_bits;   // and active-frequency bits [32]
     float zprev; int wn; bool inside, crossed, zset;
     unsigned int ev[7];
+    // the adjoint's forward pass (null otherwise): at every active (sample, lane, frequency) the state
+    // P before the sample (16) and the summed coefficients (11) into gstate[((combo N + k - 1) 27 +
+    // field) npad + ray], and gact[(combo N + k - 1) npad + ray] = 1
+    float* gstate;
+    unsigned char* gact;
+    long long gnpad, jbase;
+    int gN, kcur, gframes, gf, gv0;
 
     __device__ void init() {
         for (int c = 0; c < CH; ++c) {
@@ -300,6 +307,12 @@ struct MixedSink {
                 float Dl = Lc * sf[SF_SG * 32 + o];   // the owner's Sigma dtau
                 float O[16], E[4];
                 transfer_step_ool(in, Dl, O, E);
+                if (gstate) {
+                    const long long combo = (long long)(gv0 + c) * gframes + gf;
+                    float* gs = gstate + ((combo * gN + (kcur - 1)) * 27 + 16) * gnpad + jbase + o;
+#pragma unroll
+                    for (int q = 0; q < 11; ++q) gs[q * gnpad] = in[q];
+                }
 #pragma unroll
                 for (int q = 0; q < 16; ++q) sres[q * 32 + lane] = O[q];
 #pragma unroll
@@ -321,6 +334,14 @@ struct MixedSink {
                     float P[16], S4[4];
 #pragma unroll
                     for (int q = 0; q < 16; ++q) P[q] = st[q * 32];
+                    if (gstate) {
+                        const long long combo = (long long)(gv0 + c) * gframes + gf;
+                        const long long row = combo * gN + (kcur - 1);
+                        float* gs = gstate + row * 27 * gnpad + jbase + lane;
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) gs[q * gnpad] = P[q];
+                        gact[row * gnpad + jbase + lane] = 1;
+                    }
 #pragma unroll
                     for (int q = 0; q < 4; ++q) S4[q] = st[(16 + q) * 32];
 #pragma unroll
@@ -392,6 +413,8 @@ struct MixedJob {
     int nmax;
     float slab;
     double L;
+    float* gstate = nullptr;          // the adjoint's per-sample states (see MixedSink)
+    unsigned char* gact = nullptr;
 };
 
 template <int CH, int NT, int KM>
@@ -442,6 +465,8 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         sink.eta = float(P.get(PF_ETA, j)); sink.lam = float(P.get(PF_LAM, j));
         sink.a_sin_tho = float(st.a * sin(st.thetao)); sink.slab = job.slab; sink.nmax = job.nmax;
         sink.lane = lane; sink.live = live;
+        sink.gstate = job.gstate; sink.gact = job.gact; sink.gnpad = npad; sink.jbase = w * 32;
+        sink.gN = N; sink.gframes = job.nframes; sink.gf = f; sink.gv0 = v0;
         sink.sf = reinterpret_cast<float*>(wb);
         sink.items = reinterpret_cast<uint16_t*>(wb + MixedSmem<CH>::kSampleBytes);
         sink.sres = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes);
@@ -453,6 +478,7 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         sink.init();
         const float* sp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
         for (int k = k0; k < k1; ++k, sp += SM_COUNT * npad) {
+            sink.kcur = k;
             const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
             sink.consume((flags & 8u) != 0u, sp[SM_X * npad], sp[SM_Y * npad], sp[SM_Z * npad], sp[SM_T * npad], sp[SM_R * npad],
                          sp[SM_STH * npad], sp[SM_CTH * npad], (flags & 2u) != 0u, (flags & 4u) != 0u);

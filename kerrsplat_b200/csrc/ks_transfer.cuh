@@ -9,6 +9,7 @@
 // depends on the sample. The formulas are written in the scalar type T so that FP32 runs them
 // without leaving FP32's range (the reference's own constraint, coefficients.jl:147-152).
 #pragma once
+#include "ks_dual.cuh"
 #include "ks_march.cuh"
 
 namespace ks {
@@ -56,6 +57,24 @@ __device__ __forceinline__ float fexp(float x) { return __expf(x); }
 __device__ __forceinline__ double fexp(double x) { return exp(x); }
 __device__ __forceinline__ float flog(float x) { return __logf(x); }
 __device__ __forceinline__ double flog(double x) { return log(x); }
+// the same for dual numbers (the adjoint's forward-mode derivatives)
+template <class T, int N> __device__ __forceinline__ Dual<T, N> fexp(const Dual<T, N>& x) { T e = fexp(x.v); return dchain(x, e, e); }
+template <class T, int N> __device__ __forceinline__ Dual<T, N> flog(const Dual<T, N>& x) { return dchain(x, flog(x.v), T(1) / x.v); }
+template <class T, int N>
+__device__ __forceinline__ Dual<T, N> fpow(const Dual<T, N>& x, const Dual<T, N>& y) {
+    Dual<T, N> r;
+    r.v = fpow(x.v, y.v);
+    bool ydep = false;
+#pragma unroll
+    for (int i = 0; i < N; ++i) ydep = ydep || (y.d[i] != T(0));
+    const T dx = x.v != T(0) ? y.v * r.v / x.v : (y.v == T(1) ? T(1) : T(0));
+    const T dy = ydep ? r.v * flog(x.v) : T(0);
+#pragma unroll
+    for (int i = 0; i < N; ++i) r.d[i] = dx * x.d[i] + (ydep ? dy * y.d[i] : T(0));
+    return r;
+}
+// a power-of-two rescaling is exact: constant in the partials
+template <class T, int N> __device__ __forceinline__ Dual<T, N> pow2_below(const Dual<T, N>& v) { return Dual<T, N>(pow2_below(v.v)); }
 
 // ---- coefficients.jl ------------------------------------------------------------------------------
 template <class T>
@@ -67,7 +86,7 @@ __device__ __forceinline__ T planck(T nu, T Te) {
     T nh = nu / T(kNU0);
     T pref = T(kPLANCK0) * nh * nh * nh;
     if (x < T(2e-3)) return pref / (x / T(24) * (T(24) + x * (T(12) + x * (T(4) + x))));
-    if constexpr (sizeof(T) == 4) return pref / expm1f(x);   // no cancellation in FP32
+    if constexpr (is_f32<T>) return pref / expm1(x);   // no cancellation in FP32
     return pref / (exp(x) - T(1));
 }
 
@@ -178,7 +197,7 @@ __device__ __forceinline__ Coef<T> kappa(T ne, T kap, T w, T hyp, T g43, T g2, T
     T NhighV = -T(0.765625) * fpow(fpow(st, T(-2.5)) - T(1), T(11.0 / 25)) * (fpow(kap, T(-11.0 / 25)) / w) * fpow(X, T(-0.5)) * hk - small;
     T xV = T(3) * fpow(kap, T(-1.5));
     T sg = ct > T(0) ? T(1) : (ct < T(0) ? T(-1) : T(0));
-    const T small2 = sizeof(T) == 8 ? T(1e-80) : T(0);   // small^2 (zero in FP32)
+    const T small2 = is_f32<T> ? T(0) : T(1e-80);   // small^2 (zero in FP32)
     T jV = fabs(NhighV) < small2 ? T(0)
          : -(pref * NlowV * X13 * fpow(T(1) + fpow(X, xV * (T(3) * kap - T(4)) / T(6)) * fpow(NlowV / NhighV, xV), T(-1) / xV)) * sg;
     T apref = ne * T(kEE) / (B * st);
@@ -311,9 +330,10 @@ __device__ __forceinline__ LFrame<T> local_frame(const SampleFrame<T>& F, T u1, 
 struct MomentCoeffs { double c[10][24]; float cf[10][24]; };
 
 template <class T>
-__device__ __forceinline__ T mcoef(const MomentCoeffs& MC, int n, int m);
-template <> __device__ __forceinline__ double mcoef<double>(const MomentCoeffs& MC, int n, int m) { return MC.c[n][m]; }
-template <> __device__ __forceinline__ float mcoef<float>(const MomentCoeffs& MC, int n, int m) { return MC.cf[n][m]; }
+__device__ __forceinline__ T mcoef(const MomentCoeffs& MC, int n, int m) {
+    if constexpr (is_f32<T>) return T(MC.cf[n][m]);
+    else return T(MC.c[n][m]);
+}
 
 template <class T>
 __device__ __forceinline__ T moment_n(const MomentCoeffs& MC, T a, int n) {
@@ -369,12 +389,15 @@ template <class T> __device__ __forceinline__ T phi_fn(const MomentCoeffs& MC, T
     return -expm1(-a) / a;
 }
 
-template <class T> __device__ __forceinline__ T lin_thr();
-template <> __device__ __forceinline__ double lin_thr<double>() { return 1e-200; }
-template <> __device__ __forceinline__ float lin_thr<float>() { return 1e-25f; }
-template <class T> __device__ __forceinline__ T cub_thr();
-template <> __device__ __forceinline__ double cub_thr<double>() { return 1e-17; }
-template <> __device__ __forceinline__ float cub_thr<float>() { return 1.1920929e-7f / 20.0f; }
+// step.jl:147-153, in the scalar type of T (duals compare their values)
+template <class T> __device__ __forceinline__ scalar_t<T> lin_thr() {
+    if constexpr (is_f32<T>) return 1e-25f;
+    else return 1e-200;
+}
+template <class T> __device__ __forceinline__ scalar_t<T> cub_thr() {
+    if constexpr (is_f32<T>) return 1.1920929e-7f / 20.0f;
+    else return 1e-17;
+}
 
 template <class T>
 __device__ __forceinline__ T sinhc_excess(T b) {
@@ -414,10 +437,9 @@ __device__ __forceinline__ void kmats(T aQ, T aU, T aV, T rQ, T rU, T rV, T K1[1
         }
 }
 
-// The exact step (step.jl:27-124): O = exp(-K D) and E = (int_0^D exp(-K u) du) j.
+// The step operator (step.jl:45-124): O = exp(-K D) and Ej = int_0^D exp(-K u) du, both 4x4 row-major.
 template <class T>
-__device__ __forceinline__ void transfer_step(const MomentCoeffs& MC, const T j4[4], const T al[4], const T rh[3], T Dlen,
-                                              T O[16], T E[4]) {
+__device__ __forceinline__ void step_operator(const MomentCoeffs& MC, const T al[4], const T rh[3], T Dlen, T O[16], T Ej[16]) {
     const T s = pow2_below(Dlen);
     const T D = Dlen / s;
     T aI = al[0] * s, aQ = al[1] * s, aU = al[2] * s, aV = al[3] * s;
@@ -426,7 +448,6 @@ __device__ __forceinline__ void transfer_step(const MomentCoeffs& MC, const T j4
     T r2 = rQ * rQ + rU * rU + rV * rV;
     T a = aI * D;
     T K1[16], K2[16], K3[16];
-    T Ej[16];
     if ((a2 + r2) * D * D < lin_thr<T>()) {
         T e = exp(-a);
         T ph = phi_fn(MC, a), m1 = moment_n(MC, a, 1);
@@ -507,8 +528,19 @@ __device__ __forceinline__ void transfer_step(const MomentCoeffs& MC, const T j4
             }
         }
     }
+    // the rescaled emission integral (s is a power of two: exact)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) E[i] = s * (Ej[4 * i] * j4[0] + Ej[4 * i + 1] * j4[1] + Ej[4 * i + 2] * j4[2] + Ej[4 * i + 3] * j4[3]);
+    for (int i = 0; i < 16; ++i) Ej[i] = s * Ej[i];
+}
+
+// The exact step (step.jl:27-30): O = exp(-K D) and E = (int_0^D exp(-K u) du) j.
+template <class T>
+__device__ __forceinline__ void transfer_step(const MomentCoeffs& MC, const T j4[4], const T al[4], const T rh[3], T Dlen,
+                                              T O[16], T E[4]) {
+    T Ej[16];
+    step_operator(MC, al, rh, Dlen, O, Ej);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) E[i] = Ej[4 * i] * j4[0] + Ej[4 * i + 1] * j4[1] + Ej[4 * i + 2] * j4[2] + Ej[4 * i + 3] * j4[3];
 }
 
 // ---- splats -------------------------------------------------------------------------------------

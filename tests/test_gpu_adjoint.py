@@ -1,0 +1,167 @@
+"""GPU parity of the adjoint (the dual sweep, src/Splats/dual_gradient.jl; chi2_gradient!,
+src/Fit/Fit.jl:502-577) against central finite differences of the CPU oracle's polarized image, the
+check the reference's own gradient gates make (test/test_polarized_splats.jl:318-364; the
+reference's Enzyme gradient cannot run here).
+
+Tolerances: the FP64 adjoint against the FD gradient within 1e-5 per parameter (relative, with a
+floor of 1e-4 of the largest component; the FD step is 1e-7 relative, so its own error is ~1e-8);
+the mixed (FP32 transport) adjoint within 1e-3 of the FP64 adjoint in the relative L2 norm over all
+parameters, and per parameter above 1e-2 of the largest component.
+"""
+import numpy as np
+import pytest
+
+import kerrsplat_b200 as ks
+from kerrsplat_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+NS, RES, N = 5, 10, 64
+
+
+@pytest.fixture(scope="module")
+def scene():
+    c = scenes.config2(res=RES, N=N)
+    rng = np.random.Generator(np.random.PCG64(21))
+    p = scenes.thermal_params(rng, NS, c["a"], rlo=3.0, rhi=8.0)
+    # large splats close to the hole so that every one of them is seen by the small screen
+    p[3:6] = np.log(rng.uniform(1.0, 2.5, (3, NS)))
+    cam = ks.Camera((-10.0, 10.0), (-10.0, 10.0), RES)
+    cache = ks.GeodesicCache(cam, N)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    times, nus = np.array([0.0, 5.0]), np.array([86e9, 345e9])
+    ds = np.random.Generator(np.random.PCG64(22)).standard_normal((len(nus), len(times), cam.npix, 4))
+    return dict(c=c, p=p, cam=cam, cache=cache, times=times, nus=nus, ds=ds, N=N)
+
+
+def oracle_loss(oracle, s, p, nmax=-1, slab=0.0):
+    c, cam = s["c"], s["cam"]
+    tot = 0.0
+    for v, nu in enumerate(s["nus"]):
+        for f, t in enumerate(s["times"]):
+            img = oracle.polarized_image(c["a"], c["theta_o"], cam.alpha, cam.beta, s["N"], c["M"], [("thermal", p, None)], t, nu, c["L"],
+                                         nmax=nmax, slab=slab)
+            tot += float(np.sum(s["ds"][v, f] * img))
+    return tot
+
+
+def fd_gradient(oracle, s, nmax=-1, slab=0.0):
+    p0 = s["p"]
+    g = np.zeros_like(p0)
+    for i in range(p0.shape[1]):
+        for r in range(p0.shape[0]):
+            h = 1e-7 * max(abs(p0[r, i]), 1.0)
+            pp, pm = p0.copy(), p0.copy()
+            pp[r, i] += h
+            pm[r, i] -= h
+            g[r, i] = (oracle_loss(oracle, s, pp, nmax, slab) - oracle_loss(oracle, s, pm, nmax, slab)) / (2 * h)
+    return g
+
+
+def compare(g, ref, tol):
+    floor = 1e-4 * np.abs(ref).max()
+    err = np.abs(g - ref) / (np.abs(ref) + floor)
+    return err.max(), np.unravel_index(err.argmax(), err.shape)
+
+
+@pytest.fixture(scope="module")
+def fd(scene, oracle):
+    oracle.set_threads(8)
+    return fd_gradient(oracle, scene)
+
+
+def test_fp64_adjoint_matches_finite_differences(scene, fd):
+    s = scene
+    g = ks.adjoint(s["cache"], ks.PolarizedSplats(s["p"]), s["times"], s["nus"], s["c"]["L"], s["ds"], precision=ks.KS_FP64)
+    assert np.abs(fd).max() > 0
+    err, where = compare(g, fd, 1e-5)
+    print("fp64 adjoint vs FD: max rel err", err, "at (row, splat)", where)
+    assert err < 1e-5, (err, where, g[where], fd[where])
+
+
+def test_fp64_adjoint_is_deterministic_and_accumulates(scene):
+    s = scene
+    m = ks.PolarizedSplats(s["p"])
+    g1 = ks.adjoint(s["cache"], m, s["times"], s["nus"], s["c"]["L"], s["ds"], precision=ks.KS_FP64)
+    g2 = ks.adjoint(s["cache"], m, s["times"], s["nus"], s["c"]["L"], s["ds"], precision=ks.KS_FP64)
+    assert np.array_equal(g1, g2)
+    acc = np.asfortranarray(np.ones_like(g1))
+    ks.adjoint(s["cache"], m, s["times"], s["nus"], s["c"]["L"], s["ds"], precision=ks.KS_FP64, dparams=acc)
+    assert np.array_equal(acc, 1.0 + g1)
+
+
+def test_chi2_gradient_matches_adjoint_of_its_seed(scene, oracle):
+    s = scene
+    c, cam = s["c"], s["cam"]
+    m = ks.PolarizedSplats(s["p"])
+    img = np.asarray(ks.render(s["cache"], m, s["times"], s["nus"], c["L"], precision=ks.KS_FP64))
+    rng = np.random.Generator(np.random.PCG64(23))
+    sigma = 0.05 * np.abs(img).max() * (1.0 + rng.uniform(0, 1, img.shape))
+    data = img * (1 + 0.1 * rng.standard_normal(img.shape))
+    mask = rng.uniform(0, 1, img.shape[:3]) > 0.2
+    chi2, g, model = ks.chi2_gradient(s["cache"], m, s["times"], s["nus"], c["L"], data, sigma, mask=mask, precision=ks.KS_FP64,
+                                      return_image=True)
+    r = (img - data) / sigma * mask[..., None]
+    assert np.allclose(model, img, rtol=1e-12, atol=1e-12 * np.abs(img).max())
+    assert abs(chi2 - np.sum(r * r)) <= 1e-10 * np.sum(r * r)
+    ga = ks.adjoint(s["cache"], m, s["times"], s["nus"], c["L"], 2 * r / sigma, precision=ks.KS_FP64)
+    assert np.allclose(g, ga, rtol=1e-9, atol=1e-12 * np.abs(ga).max())
+    # a scalar sigma
+    chi2s, gs = ks.chi2_gradient(s["cache"], m, s["times"], s["nus"], c["L"], data, 0.1 * np.abs(img).max(), precision=ks.KS_FP64)
+    rs = (img - data) / (0.1 * np.abs(img).max())
+    assert abs(chi2s - np.sum(rs * rs)) <= 1e-10 * np.sum(rs * rs)
+
+
+def test_truncated_adjoint_matches_finite_differences(oracle):
+    # the half-orbit cutoff (winding_cutoff_kernel!): nmax = 0, a thin slab
+    c = scenes.config2(res=8, N=48)
+    rng = np.random.Generator(np.random.PCG64(24))
+    p = scenes.thermal_params(rng, 2, c["a"], rlo=3.0, rhi=6.0)
+    p[3:6] = np.log(rng.uniform(1.0, 2.0, (3, 2)))
+    cam = ks.Camera((-8.0, 8.0), (-8.0, 8.0), 8)
+    cache = ks.GeodesicCache(cam, 48)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    s = dict(c=c, p=p, cam=cam, times=np.array([0.0]), nus=np.array([230e9]), N=48)
+    s["ds"] = rng.standard_normal((1, 1, cam.npix, 4))
+    fdg = fd_gradient(oracle, s, nmax=0, slab=0.5)
+    g = ks.adjoint(cache, ks.PolarizedSplats(p), s["times"], s["nus"], c["L"], s["ds"], nmax=0, slab=0.5, precision=ks.KS_FP64)
+    err, where = compare(g, fdg, 1e-5)
+    print("truncated fp64 adjoint vs FD:", err, where)
+    assert err < 1e-5, (err, where)
+
+
+def rel_l2(x, y):
+    return float(np.linalg.norm(np.asarray(x) - np.asarray(y)) / max(np.linalg.norm(y), 1e-300))
+
+
+def test_mixed_adjoint_matches_fp64(scene, fd):
+    s = scene
+    m = ks.PolarizedSplats(s["p"])
+    g64 = ks.adjoint(s["cache"], m, s["times"], s["nus"], s["c"]["L"], s["ds"], precision=ks.KS_FP64)
+    g32 = ks.adjoint(s["cache"], m, s["times"], s["nus"], s["c"]["L"], s["ds"], precision=ks.KS_MIXED)
+    e64, e_fd = rel_l2(g32, g64), rel_l2(g32, fd)
+    print("mixed adjoint: rel L2 vs fp64", e64, "vs FD", e_fd)
+    assert e64 < 1e-3 and e_fd < 1e-3, (e64, e_fd)
+    g32b = ks.adjoint(s["cache"], m, s["times"], s["nus"], s["c"]["L"], s["ds"], precision=ks.KS_MIXED)
+    assert np.array_equal(g32, g32b)   # deterministic: fixed-order reductions, no atomics on the sums
+
+
+@pytest.mark.parametrize("nus", [[86e9, 230e9, 345e9], [86e9, 230e9, 345e9, 690e9]])
+def test_mixed_chi2_gradient_matches_fp64(nus):
+    # three and four frequencies share a work unit of the mixed kernels (the configuration-2/3 layout)
+    c = scenes.config2(res=12, N=96)
+    rng = np.random.Generator(np.random.PCG64(25))
+    p = scenes.thermal_params(rng, 6, c["a"], rlo=3.0, rhi=9.0)
+    p[3:6] = np.log(rng.uniform(0.8, 2.0, (3, 6)))
+    cam = ks.Camera((-12.0, 12.0), (-12.0, 12.0), 12)
+    cache = ks.GeodesicCache(cam, 96)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    m = ks.PolarizedSplats(p)
+    img = np.asarray(ks.render(cache, m, [0.0], nus, c["L"], precision=ks.KS_FP64))
+    data = img * (1 + 0.05 * rng.standard_normal(img.shape))
+    sigma = 0.01 * np.abs(img).max()
+    chi64, g64 = ks.chi2_gradient(cache, m, [0.0], nus, c["L"], data, sigma, precision=ks.KS_FP64)
+    chi32, g32 = ks.chi2_gradient(cache, m, [0.0], nus, c["L"], data, sigma, precision=ks.KS_MIXED)
+    print("chi2", chi64, chi32, "grad rel L2", rel_l2(g32, g64))
+    assert abs(chi32 - chi64) <= 1e-3 * chi64
+    assert rel_l2(g32, g64) < 1e-3
