@@ -159,6 +159,15 @@ int ks_chi2_gradient(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, c
                      int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* data, const double* sigma,
                      double sigma_scalar, const uint8_t* mask, double* chi2, double* dparams, int32_t accumulate, double* image);
 
+/* sample_adjoint (src/Transfer/transport.jl:221-245) of n independent samples in FP64: for the summed
+ * coefficients in (j 4, alpha 4, rho 3 per sample), the step length Dl, the adjoint w in front of the
+ * sample and the tail R behind it, out[31 i ..] = O (16, row-major), E (4) and c-bar = (j-bar 4,
+ * alpha-bar 4, rho-bar 3), the partials of w^T (O R + E). method 0: the structured form of the mixed
+ * path's reverse pass; 1: seven forward-mode duals through the step operator (the reference's form,
+ * used by the FP64 adjoint). Arrays host or device. */
+int ks_sample_adjoint(ks_context* ctx, int64_t n, const double* in, const double* Dl, const double* w, const double* R, int32_t method,
+                      double* out);
+
 /* ---- library extensions with no counterpart in the reference (measurement and streams) ---- */
 
 /* The CUDA stream every call of this context runs on (a cudaStream_t). */

@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "adjoint", "chi2_gradient", "sweep_passes", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -456,6 +456,20 @@ def chi2_gradient(cache, model, times, nus, L, data, sigma, mask=None, nmax=-1, 
                                              1 if user is not None else 0, _ptr(img) if img is not None else None))
     g = user if user is not None else _split_grad(model, buf)
     return (chi2.value, g, img) if return_image else (chi2.value, g)
+
+
+def sample_adjoint(cache, coeffs, Dl, w, R, method=0):
+    """sample_adjoint (transport.jl:221-245) of n samples on the GPU (FP64): coeffs (n, 11) = (j, alpha,
+    rho), Dl (n,), w and R (n, 4). Returns O (n, 4, 4), E (n, 4) and c-bar (n, 11). method 0 is the
+    structured form (the mixed reverse pass), 1 the seven forward-mode duals (the FP64 reverse pass)."""
+    coeffs = np.ascontiguousarray(coeffs, dtype=np.float64).reshape(-1, 11)
+    n = coeffs.shape[0]
+    Dl = np.ascontiguousarray(Dl, dtype=np.float64).reshape(n)
+    w = np.ascontiguousarray(w, dtype=np.float64).reshape(n, 4)
+    R = np.ascontiguousarray(R, dtype=np.float64).reshape(n, 4)
+    out = np.empty((n, 31))
+    cache._check(cache._lib.ks_sample_adjoint(cache._ctx, n, _ptr(coeffs), _ptr(Dl), _ptr(w), _ptr(R), int(method), _ptr(out)))
+    return out[:, :16].reshape(n, 4, 4), out[:, 16:20], out[:, 20:]
 
 
 def sweep_passes(cache, model, L, nmax=-1, slab=0.0, precision=KS_FP64):

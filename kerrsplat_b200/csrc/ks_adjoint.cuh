@@ -64,6 +64,164 @@ __device__ __forceinline__ void sample_adjoint(const MomentCoeffs& MC, const T* 
     for (int q = 0; q < 7; ++q) cb[4 + q] = qd.d[q];
 }
 
+// ---- the step adjoint in structured form (the mixed path) -----------------------------------------
+// In every branch of the step operator O = sum_n o_n K^n and Ej = s sum_n e_n K^n (n = 0..3), with K
+// the rescaled matrix K' of step_operator (without alpha_I) and scalar coefficients that depend on
+// alpha, rho only through the invariants a = aI D, a2 = |alpha_QUV|^2, r2 = |rho|^2, ar = alpha.rho
+// (step.jl:64-124). So q = w^T (O R + Ej j) has
+//   dq/dtheta = sum_n [do_n/dtheta <w, K^n R> + o_n <w, dK^n/dtheta R>] + s (the same with e_n and j),
+// the coefficient partials by four duals in (a, a2, r2, ar), and dK/dtheta a constant sparse matrix:
+// <w, dK^2 v> = <w, G K v> + <K^T w, G v>, <w, dK^3 v> = <w, G K^2 v> + <K^T w, G K v> + <K^2T w, G v>.
+
+// the coefficients (o_n, e_n) of the rescaled step at the scaled invariants; same branches and
+// thresholds as step_operator
+template <class TD>
+__device__ __forceinline__ void step_coefficients(const MomentCoeffs& MC, TD a, TD a2, TD r2, TD ar, scalar_t<TD> D, TD o[4], TD e[4]) {
+    using S = scalar_t<TD>;
+    if ((a2 + r2) * D * D < lin_thr<TD>()) {
+        const TD ex = exp(-a), ph = phi_fn(MC, a), m1 = moment_n(MC, a, 1);
+        o[0] = ex; o[1] = -D * ex; o[2] = TD(S(0)); o[3] = TD(S(0));
+        e[0] = D * ph; e[1] = -(D * D) * m1; e[2] = TD(S(0)); e[3] = TD(S(0));
+        return;
+    }
+    const TD h = (a2 - r2) / S(2);
+    const TD rt2 = h * h + ar * ar;
+    const TD root = rt2 > S(0) ? sqrt(rt2) : TD(S(0));
+    TD L1sq, L2sq;
+    if (h >= S(0)) { L1sq = h + root; L2sq = L1sq > S(0) ? ar * ar / L1sq : TD(S(0)); }
+    else { L2sq = root - h; L1sq = L2sq > S(0) ? ar * ar / L2sq : TD(S(0)); }
+    const TD L1 = L1sq > S(0) ? sqrt(L1sq) : TD(S(0)), L2 = L2sq > S(0) ? sqrt(L2sq) : TD(S(0));
+    const TD b1 = L1 * D, b2 = L2 * D;
+    const TD Th = L1sq + L2sq;
+    const TD ex = exp(-a);
+    TD M[10];
+    moments(MC, a, M);
+    if (Th * D * D * ((a2 + r2) * D * D + S(1)) < cub_thr<TD>()) {
+        o[0] = ex; o[1] = -D * ex; o[2] = (D * D / S(2)) * ex; o[3] = -(D * D * D / S(6)) * ex;
+        e[0] = D * M[0]; e[1] = -(D * D) * M[1]; e[2] = (D * D * D / S(2)) * M[2]; e[3] = -(D * D * D * D / S(6)) * M[3];
+        return;
+    }
+    TD ecosh, esinhb, ecoshm1;
+    if (b1 < S(1)) {
+        const TD sh = sinh(b1 / S(2));
+        ecosh = ex * cosh(b1);
+        esinhb = ex * (fabs(b1) < S(0.1) ? sinhc_excess(b1) + S(1) : sinh(b1) / b1);
+        ecoshm1 = ex * S(2) * sh * sh;
+    } else {
+        const TD em = exp(-(a - b1)), ep = exp(-(a + b1));
+        ecosh = (em + ep) / S(2); esinhb = (em - ep) / (S(2) * b1); ecoshm1 = (em - S(2) * ex + ep) / S(2);
+    }
+    const TD sb2 = sin(b2), cb2 = cos(b2), sh2 = sin(b2 / S(2));
+    const TD c0 = (L2sq * ecosh + L1sq * ex * cb2) / Th;
+    const TD c2 = (ecoshm1 + ex * S(2) * sh2 * sh2) / Th;
+    const TD sincb2 = fabs(b2) < S(0.1) ? S(1) - sinc_deficit(b2) : sb2 / b2;
+    const TD so = D * esinhb, sn = D * ex * sincb2;
+    const TD ph_a = fabs(a) < S(1) ? M[0] : -expm1(-a) / a;
+    const TD icoshm1 = b1 < S(0.1) ? b1 * b1 * (M[2] / S(2) + b1 * b1 * (M[4] / S(24) + b1 * b1 * (M[6] / S(720) + b1 * b1 * M[8] / S(40320))))
+                                   : (phi_fn(MC, a - b1) + phi_fn(MC, a + b1)) / S(2) - ph_a;
+    const TD vser = b2 * b2 * (M[2] / S(2) - b2 * b2 * (M[4] / S(24) - b2 * b2 * (M[6] / S(720) - b2 * b2 * M[8] / S(40320))));
+    const TD icos_closed = (a - ex * (a * cb2 - b2 * sb2)) / (a * a + b2 * b2);
+    const TD iversin = b2 < S(0.1) ? vser : ph_a - icos_closed;
+    const TD icos = b2 < S(0.1) ? ph_a - vser : icos_closed;
+    const TD sdser = b2 * b2 * (M[3] / S(6) - b2 * b2 * (M[5] / S(120) - b2 * b2 * (M[7] / S(5040) - b2 * b2 * M[9] / S(362880))));
+    const TD isinc = b2 < S(0.1) ? M[1] - sdser : (S(1) - ex * (a * sb2 / b2 + cb2)) / (a * a + b2 * b2);
+    const TD ishx = b1 < S(0.1) ? b1 * b1 * (M[3] / S(6) + b1 * b1 * (M[5] / S(120) + b1 * b1 * (M[7] / S(5040) + b1 * b1 * M[9] / S(362880))))
+                                : (phi_fn(MC, a - b1) - phi_fn(MC, a + b1)) / (S(2) * b1) - M[1];
+    const TD Ich = D * (ph_a + icoshm1);
+    const TD Ic = D * icos;
+    const TD Ish = D * D * (M[1] + ishx);
+    const TD Is = D * D * isinc;
+    const TD C0 = (L2sq * Ich + L1sq * Ic) / Th;
+    const TD C2 = D * (icoshm1 + iversin) / Th;
+    o[0] = c0; o[1] = -(so * L2sq + sn * L1sq) / Th; o[2] = c2; o[3] = (sn - so) / Th;
+    e[0] = C0; e[1] = -(Ish * L2sq + Is * L1sq) / Th; e[2] = C2; e[3] = (Is - Ish) / Th;
+}
+
+// <x, G_theta y> for the six sparse generators G = dK/dtheta, theta = aQ, aU, aV, rQ, rU, rV
+template <class T>
+__device__ __forceinline__ void kgen_forms(const T x[4], const T y[4], T out[6]) {
+    out[0] = x[0] * y[1] + x[1] * y[0];
+    out[1] = x[0] * y[2] + x[2] * y[0];
+    out[2] = x[0] * y[3] + x[3] * y[0];
+    out[3] = x[2] * y[3] - x[3] * y[2];
+    out[4] = x[3] * y[1] - x[1] * y[3];
+    out[5] = x[1] * y[2] - x[2] * y[1];
+}
+
+template <class T>
+__device__ __forceinline__ void kmul(const T K[16], const T v[4], T out[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = K[4 * i] * v[0] + K[4 * i + 1] * v[1] + K[4 * i + 2] * v[2] + K[4 * i + 3] * v[3];
+}
+template <class T>
+__device__ __forceinline__ void kmul_t(const T K[16], const T v[4], T out[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = K[i] * v[0] + K[4 + i] * v[1] + K[8 + i] * v[2] + K[12 + i] * v[3];
+}
+template <class T>
+__device__ __forceinline__ T dot4(const T x[4], const T y[4]) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2] + x[3] * y[3]; }
+
+// sample_adjoint (transport.jl:221-245) with the structured partials; same outputs as sample_adjoint
+template <class T>
+__device__ __forceinline__ void sample_adjoint_structured(const MomentCoeffs& MC, const T* in, T Dl, const T w[4], const T R[4], T O[16],
+                                                          T E[4], T cb[11]) {
+    T Ej[16];
+    step_operator(MC, in + 4, in + 8, Dl, O, Ej);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) E[r] = Ej[4 * r] * in[0] + Ej[4 * r + 1] * in[1] + Ej[4 * r + 2] * in[2] + Ej[4 * r + 3] * in[3];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) cb[c] = Ej[c] * w[0] + Ej[4 + c] * w[1] + Ej[8 + c] * w[2] + Ej[12 + c] * w[3];
+    const T s = pow2_below(Dl);
+    const T D = Dl / s;
+    const T aI = in[4] * s, aQ = in[5] * s, aU = in[6] * s, aV = in[7] * s, rQ = in[8] * s, rU = in[9] * s, rV = in[10] * s;
+    using D4 = Dual<T, 4>;
+    const D4 a = D4::seed(aI * D, 0), a2 = D4::seed(aQ * aQ + aU * aU + aV * aV, 1), r2 = D4::seed(rQ * rQ + rU * rU + rV * rV, 2),
+             ar = D4::seed(aQ * rQ + aU * rU + aV * rV, 3);
+    D4 o[4], e[4];
+    step_coefficients(MC, a, a2, r2, ar, D, o, e);
+    T K[16];
+    K[0] = 0; K[1] = aQ; K[2] = aU; K[3] = aV; K[4] = aQ; K[5] = 0; K[6] = rV; K[7] = -rU;
+    K[8] = aU; K[9] = -rV; K[10] = 0; K[11] = rQ; K[12] = aV; K[13] = rU; K[14] = -rQ; K[15] = 0;
+    const T* jv = in;
+    T KR[4], K2R[4], K3R[4], Kj[4], K2j[4], K3j[4], Kw[4], K2w[4];
+    kmul(K, R, KR); kmul(K, KR, K2R); kmul(K, K2R, K3R);
+    kmul(K, jv, Kj); kmul(K, Kj, K2j); kmul(K, K2j, K3j);
+    kmul_t(K, w, Kw); kmul_t(K, Kw, K2w);
+    const T P[4] = {dot4(w, R), dot4(w, KR), dot4(w, K2R), dot4(w, K3R)};
+    const T J[4] = {dot4(w, jv), dot4(w, Kj), dot4(w, K2j), dot4(w, K3j)};
+    // through the invariants
+    T dx[4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+        T acc = T(0);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc += o[n].d[x] * P[n] + s * e[n].d[x] * J[n];
+        dx[x] = acc;
+    }
+    T g[7];
+    g[0] = dx[0] * D;                                   // aI
+    g[1] = dx[1] * T(2) * aQ + dx[3] * rQ;              // aQ
+    g[2] = dx[1] * T(2) * aU + dx[3] * rU;
+    g[3] = dx[1] * T(2) * aV + dx[3] * rV;
+    g[4] = dx[2] * T(2) * rQ + dx[3] * aQ;              // rQ
+    g[5] = dx[2] * T(2) * rU + dx[3] * aU;
+    g[6] = dx[2] * T(2) * rV + dx[3] * aV;
+    // through the explicit K of K^1, K^2, K^3
+    T f1[6], f2a[6], f2b[6], f3a[6], f3b[6], f3c[6];
+    T h1[6], h2a[6], h2b[6], h3a[6], h3b[6], h3c[6];
+    kgen_forms(w, R, f1); kgen_forms(w, KR, f2a); kgen_forms(Kw, R, f2b);
+    kgen_forms(w, K2R, f3a); kgen_forms(Kw, KR, f3b); kgen_forms(K2w, R, f3c);
+    kgen_forms(w, jv, h1); kgen_forms(w, Kj, h2a); kgen_forms(Kw, jv, h2b);
+    kgen_forms(w, K2j, h3a); kgen_forms(Kw, Kj, h3b); kgen_forms(K2w, jv, h3c);
+#pragma unroll
+    for (int t = 0; t < 6; ++t)
+        g[1 + t] += o[1].v * f1[t] + o[2].v * (f2a[t] + f2b[t]) + o[3].v * (f3a[t] + f3b[t] + f3c[t]) +
+                    s * (e[1].v * h1[t] + e[2].v * (h2a[t] + h2b[t]) + e[3].v * (h3a[t] + h3b[t] + h3c[t]));
+    // d/d(alpha_true) = s d/d(alpha_scaled)
+#pragma unroll
+    for (int t = 0; t < 7; ++t) cb[4 + t] = s * g[t];
+}
+
 // ---- one thermal splat's share of the gradient at one sample (element_adjoint!) --------------------
 // p: the splat's table row (in T), gt: its gradient constants (FP64), F: the sample's frame data,
 // (x, y, z) its quasi-Cartesian KS position, t = t_obs - t~ the emission time. For each of the
@@ -402,6 +560,21 @@ __global__ void __launch_bounds__(128) k_dual_plain(PlanView P, Spacetime st, lo
     }
 }
 
+// sample_adjoint of n independent samples (FP64): method 0 the structured partials, 1 the seven duals
+// through the step operator; out[31 i ..] = O (16), E (4), c-bar (11)
+__global__ void k_sample_adjoint(long long n, const double* __restrict__ in, const double* __restrict__ Dl, const double* __restrict__ w,
+                                 const double* __restrict__ R, int method, double* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double O[16], E[4], cb[11];
+    if (method == 0) sample_adjoint_structured(c_moments, in + 11 * i, Dl[i], w + 4 * i, R + 4 * i, O, E, cb);
+    else sample_adjoint(c_moments, in + 11 * i, Dl[i], w + 4 * i, R + 4 * i, O, E, cb);
+    double* o = out + 31 * i;
+    for (int q = 0; q < 16; ++q) o[q] = O[q];
+    for (int q = 0; q < 4; ++q) o[16 + q] = E[q];
+    for (int q = 0; q < 11; ++q) o[20 + q] = cb[q];
+}
+
 // The deterministic sum of the per-ray slots (one block per (row, splat), a fixed tree), into the
 // column-major parameter layout dparams[i * 21 + row].
 __global__ void k_slot_reduce(const double* __restrict__ grad, long long nrc, int ntot, double* __restrict__ out) {
@@ -486,27 +659,17 @@ __global__ void k_sort_seed(const double* __restrict__ src, const long long* __r
 // The forward pass (k_consume with MixedJob::gstate) stores, at every active (sample, ray, frequency),
 // the state P_k of the segment before the sample and the summed coefficients c_k. k_adj_bounds turns
 // the segments' (P, S) into the adjoint at each segment's start, w_s = (P_0 ... P_{s-1})^T w_1, and
-// the tail behind each segment's end, T_s = S_{s+1} + P_{s+1} T_{s+1}. k_adjoint_mixed then walks
-// each work unit (32 rays x one segment x one frame x CH frequencies) from its last sample to its
-// first: w_k = P_k^T w_s, the step adjoint (seven duals through the step operator) spread over the
-// warp, T <- E + O T, and the element adjoints of the (ray, splat) pairs that pass the support test,
-// 32 at a time, their 21 rows summed per splat in list order into the warp's accumulator (shared
-// memory). Each unit writes its own partial sums; k_unit_reduce adds the units in a fixed order.
+// the tail behind each segment's end, T_s = S_{s+1} + P_{s+1} T_{s+1}. k_adj_steps walks each work
+// unit (32 rays x one segment x one frame x CH frequencies) from its last sample to its first:
+// w_k = P_k^T w_s, the step adjoint (structured partials) spread over the warp, T <- E + O T, and
+// c-bar stored in place of c_k. k_adj_elements then evaluates the element adjoints of the (ray,
+// splat) pairs that pass the support test, 32 at a time, their 21 rows summed per splat in list
+// order into the warp's accumulator (shared memory). Each unit writes its own partial sums;
+// k_unit_reduce adds the units in a fixed order. Two kernels keep each one's code small.
 
 namespace {
 
 using namespace ks;
-
-__device__ __noinline__ void sample_adjoint_ool(const float* in, float Dl, const float* w, const float* R, float* O, float* E, float* cb) {
-    float o[16], e[4], c[11];
-    sample_adjoint(c_moments, in, Dl, w, R, o, e, c);
-#pragma unroll
-    for (int q = 0; q < 16; ++q) O[q] = o[q];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) E[q] = e[q];
-#pragma unroll
-    for (int q = 0; q < 11; ++q) cb[q] = c[q];
-}
 
 // s: the owner lane's column of the warp's sample data ([field][32]); cb: the owner's c-bar column of
 // [CH][11][32]; nu: the unit's frequencies
@@ -526,22 +689,6 @@ __device__ __noinline__ void element_adjoint_ool(const float* p, const double* g
 #pragma unroll
     for (int r = 0; r < GR_COUNT; ++r) g[r] = gl[r];
 }
-
-template <int CH>
-struct AdjSmem {
-    static constexpr int kSampleBytes = 32 * kSF * 4;
-    static constexpr int kItemBytes = 32 * 32 * 2;        // (lane, splat) pair list
-    static constexpr int kCbBytes = 32 * CH * 11 * 4;     // c-bar per lane and frequency
-    static constexpr int kTwBytes = 32 * CH * 8 * 4;      // T (4) and w (4) per lane and frequency
-    static constexpr int kGitemBytes = 32 * GR_COUNT * 4; // the rows of each evaluated pair
-    static constexpr int kMetaBytes = 32 * 4 * 2;
-    static constexpr int kFixed = kSampleBytes + kItemBytes + kCbBytes + kTwBytes + kGitemBytes + kMetaBytes;
-    __host__ __device__ static size_t acc_bytes(int ntot) { return (size_t(ntot) * GR_COUNT * 4 + 15) / 16 * 16; }
-    __host__ __device__ static size_t warp_bytes(int ntot) { return size_t(kFixed) + acc_bytes(ntot); }
-    __host__ __device__ static size_t bytes(int ntot, int warps) {
-        return (size_t(ntot) * ST_COUNT * 4 + 15) / 16 * 16 + size_t(warps) * warp_bytes(ntot);
-    }
-};
 
 // the adjoint at each segment's start and the tail behind its end, per (ray, combination):
 // bnd[((combo nseg + s) 8 + q) npix + j], q = 0..3 w, 4..7 T
@@ -574,29 +721,187 @@ __global__ void k_adj_bounds(MixedJob job, const double* __restrict__ cnu, const
     }
 }
 
+// The per-lane state of the step phase (T and w per frequency) and of the element phase.
+template <int CH>
+struct AdjSmem {
+    // step phase: T (4) and w (4) per lane and frequency, meta
+    static constexpr int kTwBytes = 32 * CH * 8 * 4;
+    static constexpr int kMetaBytes = 32 * 4 * 2;
+    static constexpr int kStepWarp = kTwBytes + kMetaBytes;
+    // element phase: sample data, pair list, c-bar per lane and frequency, the rows of each evaluated
+    // pair, then the warp's gradient accumulator [splat][21]
+    static constexpr int kSampleBytes = 32 * kSF * 4;
+    static constexpr int kItemBytes = 32 * 32 * 2;
+    static constexpr int kCbBytes = 32 * CH * 11 * 4;
+    static constexpr int kGitemBytes = 32 * GR_COUNT * 4;
+    static constexpr int kFixed = kSampleBytes + kItemBytes + kCbBytes + kGitemBytes + kMetaBytes;
+    __host__ __device__ static size_t acc_bytes(int ntot) { return (size_t(ntot) * GR_COUNT * 4 + 15) / 16 * 16; }
+    __host__ __device__ static size_t tab_bytes(int ntot) { return (size_t(ntot) * ST_COUNT * 4 + 15) / 16 * 16; }
+    __host__ __device__ static size_t warp_bytes(int ntot) { return size_t(kFixed) + acc_bytes(ntot); }
+    __host__ __device__ static size_t bytes(int ntot, int warps) { return tab_bytes(ntot) + size_t(warps) * warp_bytes(ntot); }
+    __host__ __device__ static size_t step_bytes(int warps) { return size_t(warps) * kStepWarp; }
+};
+
+// The work unit of a persistent warp, decoded as k_consume decodes it (last rays first).
+struct AdjUnit {
+    long long ur, jbase, j;
+    int seg, f, v0, k0, k1, nc;
+    bool live;
+};
+template <int CH>
+__device__ __forceinline__ AdjUnit adj_unit(const MixedJob& job, unsigned long long u, int lane, int N) {
+    AdjUnit U;
+    U.ur = job.total - 1 - (long long)u;
+    const long long per_chunk = (long long)job.nseg * job.nframes * job.nvc;
+    const long long wg = U.ur / per_chunk;
+    const long long rem = U.ur % per_chunk;
+    U.seg = int(rem / (job.nframes * job.nvc));
+    const int y = int(rem % (job.nframes * job.nvc));
+    U.f = y / job.nvc;
+    U.v0 = (y % job.nvc) * CH;
+    U.jbase = wg * 32;
+    const long long j0 = U.jbase + lane;
+    U.live = j0 < job.npix;
+    U.j = U.live ? j0 : job.npix - 1;
+    U.k0 = 1 + U.seg * job.seg_len;
+    U.k1 = min(N + 1, U.k0 + job.seg_len);
+    U.nc = min(CH, job.nfreq - U.v0);
+    return U;
+}
+
+// The step phase: every work unit walks its segment from the last sample to the first, carrying T
+// per (lane, frequency); the (lane, frequency) pairs with an active sample are spread over the warp,
+// each computes w_k = P_k^T w_s and the step adjoint, writes c-bar over the stored coefficients
+// (fields 16..26 of its gstate row) and advances T <- E + O T.
+template <int CH, int NT>
+__global__ void __launch_bounds__(NT)
+k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const double* __restrict__ plan_f, const float* __restrict__ stream,
+            float* __restrict__ gstate, const unsigned char* __restrict__ gact, const float* __restrict__ bnd,
+            unsigned long long* __restrict__ work) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wb = smem + size_t(warp) * AdjSmem<CH>::kStepWarp;
+    float* tw = reinterpret_cast<float*>(wb);                        // [c][8][32]: w 0..3, T 4..7
+    int* meta_off = reinterpret_cast<int*>(wb + AdjSmem<CH>::kTwBytes);
+    unsigned* meta_bits = reinterpret_cast<unsigned*>(meta_off + 32);
+    const unsigned full = 0xffffffffu;
+    const int N = st.N;
+    const long long npad = job.npad, npix = job.npix;
+    const float a = float(st.a);
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(work, 1ull);
+        u = __shfl_sync(full, u, 0);
+        if (u >= (unsigned long long)job.total) break;
+        const AdjUnit U = adj_unit<CH>(job, u, lane, N);
+        float Lnu[CH];
+#pragma unroll
+        for (int c = 0; c < CH; ++c) Lnu[c] = float(job.L / (cnu[min(U.v0 + c, job.nfreq - 1)] / kNU0));
+        const float dtau_o = float(plan_f[(long long)PF_DTAU * npad + U.j]);
+#pragma unroll
+        for (int c = 0; c < CH; ++c) {
+            const long long combo = (long long)min(U.v0 + c, job.nfreq - 1) * job.nframes + U.f;
+            const float* b = bnd + (combo * job.nseg + U.seg) * 8 * npix + U.j;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) tw[(c * 8 + q) * 32 + lane] = (U.live && c < U.nc) ? b[(long long)q * npix] : 0.f;
+        }
+        __syncwarp();
+        for (int k = U.k1 - 1; k >= U.k0; --k) {
+            const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
+            unsigned actbits = 0u;
+            if (U.live && (__float_as_uint(sp[SM_FLAGS * npad]) & 8u)) {
+#pragma unroll
+                for (int c = 0; c < CH; ++c) {
+                    if (c >= U.nc) break;
+                    const long long combo = (long long)(U.v0 + c) * job.nframes + U.f;
+                    if (gact[(combo * N + (k - 1)) * npad + U.j]) actbits |= 1u << c;
+                }
+            }
+            const int n2 = __popc(actbits);
+            int incl2 = n2;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                int v = __shfl_up_sync(full, incl2, d);
+                if (lane >= d) incl2 += v;
+            }
+            const int total2 = __shfl_sync(full, incl2, 31);
+            if (total2 == 0) continue;
+            // Sigma dtau of this lane's sample, for the worker that takes its steps
+            const float rr = sp[SM_R * npad], cth = sp[SM_CTH * npad];
+            const float sgd = (rr * rr + a * a * cth * cth) * dtau_o;
+            meta_off[lane] = incl2 - n2;
+            meta_bits[lane] = actbits;
+            __syncwarp();
+            for (int base = 0; base < total2; base += 32) {
+                const int g = base + lane;
+                int o = 0;
+                if (g < total2) {
+#pragma unroll
+                    for (int d = 16; d >= 1; d >>= 1)
+                        if (o + d < 32 && meta_off[o + d] <= g) o += d;
+                }
+                const float sg_o = __shfl_sync(full, sgd, o);
+                if (g < total2) {
+                    unsigned bits = meta_bits[o];
+                    const int jj = g - meta_off[o];
+                    for (int q = 0; q < jj; ++q) bits &= bits - 1;
+                    const int c = __ffs(bits) - 1;
+                    const long long combo = (long long)(U.v0 + c) * job.nframes + U.f;
+                    float* gs = gstate + ((combo * N + (k - 1)) * 27) * npad + U.jbase + o;
+                    float Pm[16], in[11];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) Pm[q] = gs[q * npad];
+#pragma unroll
+                    for (int q = 0; q < 11; ++q) in[q] = gs[(16 + q) * npad];
+                    float* twc = tw + c * 8 * 32 + o;
+                    float wk[4], R[4];
+#pragma unroll
+                    for (int s4 = 0; s4 < 4; ++s4)
+                        wk[s4] = Pm[s4] * twc[0] + Pm[4 + s4] * twc[32] + Pm[8 + s4] * twc[64] + Pm[12 + s4] * twc[96];
+#pragma unroll
+                    for (int s4 = 0; s4 < 4; ++s4) R[s4] = twc[(4 + s4) * 32];
+                    float Lc = Lnu[0];
+#pragma unroll
+                    for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;
+                    float O[16], E[4], cb[11];
+                    sample_adjoint_structured(c_moments, in, Lc * sg_o, wk, R, O, E, cb);
+#pragma unroll
+                    for (int q = 0; q < 11; ++q) gs[(16 + q) * npad] = cb[q];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                        twc[(4 + r) * 32] = E[r] + O[4 * r] * R[0] + O[4 * r + 1] * R[1] + O[4 * r + 2] * R[2] + O[4 * r + 3] * R[3];
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// The element phase: every work unit visits its samples (in order); the lanes with an active sample
+// test the splats against the support, the passing (lane, splat) pairs are evaluated 32 at a time
+// with the sample's c-bar (read back from gstate), and their 21 rows are summed per splat in list
+// order into the warp's accumulator; the unit writes its partial sums to gunit.
 template <int CH, int NT>
 __global__ void __launch_bounds__(NT, 1)
-k_adjoint_mixed(Spacetime st, MixedJob job, const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
-                const double* __restrict__ ct, const double* __restrict__ cnu, const double* __restrict__ plan_f, const float* __restrict__ stream,
-                const float* __restrict__ gstate, const unsigned char* __restrict__ gact, const float* __restrict__ bnd,
-                unsigned long long* __restrict__ work, float* __restrict__ gunit) {
+k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
+               const double* __restrict__ ct, const double* __restrict__ cnu, const double* __restrict__ plan_f, const float* __restrict__ stream,
+               const float* __restrict__ gstate, const unsigned char* __restrict__ gact, unsigned long long* __restrict__ work,
+               float* __restrict__ gunit) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* tab = reinterpret_cast<float*>(smem);
     for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wb = smem + (size_t(ntot) * ST_COUNT * 4 + 15) / 16 * 16 + size_t(warp) * AdjSmem<CH>::warp_bytes(ntot);
+    unsigned char* wb = smem + AdjSmem<CH>::tab_bytes(ntot) + size_t(warp) * AdjSmem<CH>::warp_bytes(ntot);
     float* sf = reinterpret_cast<float*>(wb);
     uint16_t* items = reinterpret_cast<uint16_t*>(wb + AdjSmem<CH>::kSampleBytes);
     float* cbs = reinterpret_cast<float*>(wb + AdjSmem<CH>::kSampleBytes + AdjSmem<CH>::kItemBytes);
-    float* tw = cbs + 32 * CH * 11;                 // [c][8][32]: w 0..3, T 4..7
-    float* gitem = tw + 32 * CH * 8;                // [item][21]
-    int* meta_off = reinterpret_cast<int*>(gitem + 32 * GR_COUNT);
-    unsigned* meta_bits = reinterpret_cast<unsigned*>(meta_off + 32);
-    float* gacc = reinterpret_cast<float*>(meta_bits + 32);   // [splat][21]
+    float* gitem = cbs + 32 * CH * 11;                  // [item][21]
+    unsigned* meta_bits = reinterpret_cast<unsigned*>(gitem + 32 * GR_COUNT);
+    float* gacc = reinterpret_cast<float*>(wb + AdjSmem<CH>::kFixed);   // [splat][21]
     __syncthreads();
     const unsigned full = 0xffffffffu;
     const int N = st.N;
-    const long long npad = job.npad, npix = job.npix;
+    const long long npad = job.npad;
     const float a = float(st.a), a_sin_tho = float(st.a * sin(st.thetao));
     const long long gsz = (long long)ntot * GR_COUNT;
     for (;;) {
@@ -604,51 +909,26 @@ k_adjoint_mixed(Spacetime st, MixedJob job, const double* __restrict__ tab64, co
         if (lane == 0) u = atomicAdd(work, 1ull);
         u = __shfl_sync(full, u, 0);
         if (u >= (unsigned long long)job.total) break;
-        const long long ur = job.total - 1 - (long long)u;          // the forward pass's order: last rays first
-        const long long per_chunk = (long long)job.nseg * job.nframes * job.nvc;
-        const long long wg = ur / per_chunk;
-        const long long rem = ur % per_chunk;
-        const int seg = int(rem / (job.nframes * job.nvc));
-        const int y = int(rem % (job.nframes * job.nvc));
-        const int f = y / job.nvc, v0 = (y % job.nvc) * CH;
-        const long long jbase = wg * 32;
-        const long long j0 = jbase + lane;
-        const bool live = j0 < npix;
-        const long long j = live ? j0 : npix - 1;
-        const int k0 = 1 + seg * job.seg_len;
-        const int k1 = min(N + 1, k0 + job.seg_len);
-        const int nc = min(CH, job.nfreq - v0);
-        const float t_obs = float(ct[f]);
-        float nu[CH], Lnu[CH];
+        const AdjUnit U = adj_unit<CH>(job, u, lane, N);
+        const float t_obs = float(ct[U.f]);
+        float nu[CH];
 #pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const int v = min(v0 + c, job.nfreq - 1);
-            nu[c] = float(cnu[v]);
-            Lnu[c] = float(job.L / (cnu[v] / kNU0));
-        }
-        const float dtau = float(plan_f[(long long)PF_DTAU * npad + j]);
-        const float alpha = float(plan_f[(long long)PF_ALPHA * npad + j]), beta = float(plan_f[(long long)PF_BETA * npad + j]);
-        const float eta = float(plan_f[(long long)PF_ETA * npad + j]), lam = float(plan_f[(long long)PF_LAM * npad + j]);
-        // this lane's w (segment start) and T (segment end) per frequency
-#pragma unroll
-        for (int c = 0; c < CH; ++c) {
-            const long long combo = (long long)min(v0 + c, job.nfreq - 1) * job.nframes + f;
-            const float* b = bnd + (combo * job.nseg + seg) * 8 * npix + j;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) tw[(c * 8 + q) * 32 + lane] = (live && c < nc) ? b[(long long)q * npix] : 0.f;
-        }
+        for (int c = 0; c < CH; ++c) nu[c] = float(cnu[min(U.v0 + c, job.nfreq - 1)]);
+        const float dtau = float(plan_f[(long long)PF_DTAU * npad + U.j]);
+        const float alpha = float(plan_f[(long long)PF_ALPHA * npad + U.j]), beta = float(plan_f[(long long)PF_BETA * npad + U.j]);
+        const float eta = float(plan_f[(long long)PF_ETA * npad + U.j]), lam = float(plan_f[(long long)PF_LAM * npad + U.j]);
         for (long long q = lane; q < gsz; q += 32) gacc[q] = 0.f;
         __syncwarp();
-        for (int k = k1 - 1; k >= k0; --k) {
-            const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + j;
+        for (int k = U.k0; k < U.k1; ++k) {
+            const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
             const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
             unsigned actbits = 0u;
-            if (live && (flags & 8u)) {
+            if (U.live && (flags & 8u)) {
 #pragma unroll
                 for (int c = 0; c < CH; ++c) {
-                    if (c >= nc) break;
-                    const long long combo = (long long)(v0 + c) * job.nframes + f;
-                    if (gact[(combo * N + (k - 1)) * npad + j]) actbits |= 1u << c;
+                    if (c >= U.nc) break;
+                    const long long combo = (long long)(U.v0 + c) * job.nframes + U.f;
+                    if (gact[(combo * N + (k - 1)) * npad + U.j]) actbits |= 1u << c;
                 }
             }
             if (__ballot_sync(full, actbits != 0u) == 0u) continue;
@@ -667,60 +947,17 @@ k_adjoint_mixed(Spacetime st, MixedJob job, const double* __restrict__ tab64, co
                 mys[SF_R * 32] = r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
                 mys[SF_SG * 32] = (r * r + a * a * cth * cth) * dtau;
                 mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
-            }
-            // 1. step adjoints of the (lane, frequency) pairs, spread over the warp
-            const int n2 = __popc(actbits);
-            int incl2 = n2;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                int v = __shfl_up_sync(full, incl2, d);
-                if (lane >= d) incl2 += v;
-            }
-            const int off2 = incl2 - n2;
-            const int total2 = __shfl_sync(full, incl2, 31);
-            meta_off[lane] = off2;
-            meta_bits[lane] = actbits;
-            __syncwarp();
-            for (int base = 0; base < total2; base += 32) {
-                const int g = base + lane;
-                if (g < total2) {
-                    int o = 0;
+                for (int c = 0; c < CH; ++c) {
+                    if (!((actbits >> c) & 1u)) continue;
+                    const long long combo = (long long)(U.v0 + c) * job.nframes + U.f;
+                    const float* gs = gstate + ((combo * N + (k - 1)) * 27 + 16) * npad + U.j;
 #pragma unroll
-                    for (int d = 16; d >= 1; d >>= 1)
-                        if (o + d < 32 && meta_off[o + d] <= g) o += d;
-                    unsigned bits = meta_bits[o];
-                    const int jj = g - meta_off[o];
-                    for (int q = 0; q < jj; ++q) bits &= bits - 1;
-                    const int c = __ffs(bits) - 1;
-                    const long long combo = (long long)(v0 + c) * job.nframes + f;
-                    const float* gs = gstate + ((combo * N + (k - 1)) * 27) * npad + jbase + o;
-                    float Pm[16], in[11];
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) Pm[q] = gs[q * npad];
-#pragma unroll
-                    for (int q = 0; q < 11; ++q) in[q] = gs[(16 + q) * npad];
-                    float* twc = tw + c * 8 * 32 + o;
-                    float wk[4], R[4];
-#pragma unroll
-                    for (int s = 0; s < 4; ++s)
-                        wk[s] = Pm[s] * twc[0] + Pm[4 + s] * twc[32] + Pm[8 + s] * twc[64] + Pm[12 + s] * twc[96];
-#pragma unroll
-                    for (int s = 0; s < 4; ++s) R[s] = twc[(4 + s) * 32];
-                    float Lc = Lnu[0];
-#pragma unroll
-                    for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;
-                    float O[16], E[4], cb[11];
-                    sample_adjoint_ool(in, Lc * sf[SF_SG * 32 + o], wk, R, O, E, cb);
-                    float* cbo = cbs + c * 11 * 32 + o;
-#pragma unroll
-                    for (int q = 0; q < 11; ++q) cbo[q * 32] = cb[q];
-#pragma unroll
-                    for (int r = 0; r < 4; ++r)
-                        twc[(4 + r) * 32] = E[r] + O[4 * r] * R[0] + O[4 * r + 1] * R[1] + O[4 * r + 2] * R[2] + O[4 * r + 3] * R[3];
+                    for (int q = 0; q < 11; ++q) cbs[(c * 11 + q) * 32 + lane] = gs[q * npad];
                 }
             }
+            meta_bits[lane] = actbits;
             __syncwarp();
-            // 2. element adjoints of the (lane, splat) pairs inside the support and above the cutoff
             const float t = t_obs - ts;
             for (int s0 = 0; s0 < ntot; s0 += 32) {
                 unsigned mask = 0u;
@@ -763,7 +1000,7 @@ k_adjoint_mixed(Spacetime st, MixedJob job, const double* __restrict__ tab64, co
                     if (kk < total) {
                         const int it = items[kk];
                         const int o = it >> 5, i = s0 + (it & 31);
-                        element_adjoint_ool<CH>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, sf + o, t_obs, a, a_sin_tho, nu, nc,
+                        element_adjoint_ool<CH>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, sf + o, t_obs, a, a_sin_tho, nu, U.nc,
                                                 meta_bits[o], cbs + o, g);
                     }
 #pragma unroll
@@ -780,7 +1017,7 @@ k_adjoint_mixed(Spacetime st, MixedJob job, const double* __restrict__ tab64, co
                 }
             }
         }
-        float* gu = gunit + ur * gsz;
+        float* gu = gunit + U.ur * gsz;
         for (long long q = lane; q < gsz; q += 32) gu[q] = gacc[q];
         __syncwarp();
     }

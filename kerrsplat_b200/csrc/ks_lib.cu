@@ -1303,17 +1303,17 @@ int stage_dev(ks_context* c, DevBuf& buf, const U* src, size_t count, const U** 
     return s;
 }
 
-// Occupancy of k_adjoint_mixed<CH, NT> with its shared memory for `ntot` splats (0 if it does not fit).
+// Occupancy of k_adj_elements<CH, NT> with its shared memory for `ntot` splats (0 if it does not fit).
 template <int CH, int NT>
 int adjoint_blocks(ks_context* c, int ntot) {
     const size_t smem = AdjSmem<CH>::bytes(ntot, NT / 32);
     if (smem > 227 * 1024) return 0;
-    if (cudaFuncSetAttribute(k_adjoint_mixed<CH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(k_adj_elements<CH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_mixed<CH, NT>, NT, smem) != cudaSuccess) { cudaGetLastError(); return 0; }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_elements<CH, NT>, NT, smem) != cudaSuccess) { cudaGetLastError(); return 0; }
     return per_sm;
 }
 
@@ -1330,18 +1330,33 @@ int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* d
     KS_CUDA(c, cudaGetLastError());
     const long long gsz = (long long)ntot * GR_COUNT;
     KS_CUDA(c, c->adj_unit.ensure(size_t(job.total) * gsz * sizeof(float)));
-    KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
-    KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
-    constexpr int W = NT / 32;
-    const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
-    const size_t smem = AdjSmem<CH>::bytes(ntot, W);
-    k_adjoint_mixed<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(c->st, job, c->tab.as<double>(), c->gtab.as<double>(), ntot, dt, dn,
-                                                                    c->plan.as<double>(), c->stream_buf.as<float>(), job.gstate, job.gact,
-                                                                    c->adj_bnd.as<float>(), c->work.as<unsigned long long>(),
-                                                                    c->adj_unit.as<float>());
-    c->launches++;
-    c->adjoint_launches++;
-    KS_CUDA(c, cudaGetLastError());
+    KS_CUDA(c, c->work.ensure(2 * sizeof(unsigned long long)));
+    KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, 2 * sizeof(unsigned long long), c->stream));
+    // the step phase
+    {
+        constexpr int NS = 256, WS = NS / 32;
+        const size_t smem = AdjSmem<CH>::step_bytes(WS);
+        int per = 0;
+        KS_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_adj_steps<CH, NS>, NS, smem));
+        const long long grid = std::min<long long>(job.total / WS + 1, (long long)nsm * std::max(per, 1));
+        k_adj_steps<CH, NS><<<unsigned(grid), NS, smem, c->stream>>>(c->st, job, dn, c->plan.as<double>(), c->stream_buf.as<float>(),
+                                                                    job.gstate, job.gact, c->adj_bnd.as<float>(), c->work.as<unsigned long long>());
+        c->launches++;
+        c->adjoint_launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
+    // the element phase
+    {
+        constexpr int W = NT / 32;
+        const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
+        const size_t smem = AdjSmem<CH>::bytes(ntot, W);
+        k_adj_elements<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(c->st, job, c->tab.as<double>(), c->gtab.as<double>(), ntot, dt, dn,
+                                                                       c->plan.as<double>(), c->stream_buf.as<float>(), job.gstate, job.gact,
+                                                                       c->work.as<unsigned long long>() + 1, c->adj_unit.as<float>());
+        c->launches++;
+        c->adjoint_launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
     const int per_chunk = 256;
     const int nchunks = int((job.total + per_chunk - 1) / per_chunk);
     KS_CUDA(c, c->adj_part.ensure(size_t(nchunks) * gsz * sizeof(double)));
@@ -1356,13 +1371,12 @@ int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* d
 template <int CH>
 int launch_adjoint_mixed_ch(ks_context* c, int ntot, const double* dt, const double* dn) {
     const int w256 = adjoint_blocks<CH, 256>(c, ntot) * 8, w128 = adjoint_blocks<CH, 128>(c, ntot) * 4,
-              w64 = adjoint_blocks<CH, 64>(c, ntot) * 2, w32 = adjoint_blocks<CH, 32>(c, ntot);
-    const int best = std::max(std::max(w256, w128), std::max(w64, w32));
+              w64 = adjoint_blocks<CH, 64>(c, ntot) * 2;
+    const int best = std::max(std::max(w256, w128), w64);
     if (best <= 0) return fail(c, KS_ERR_ARGUMENT, "too many splats for the mixed adjoint (%d)", ntot);
     if (w256 == best) return launch_adjoint_mixed_nt<CH, 256>(c, ntot, w256 / 8, dt, dn);
     if (w128 == best) return launch_adjoint_mixed_nt<CH, 128>(c, ntot, w128 / 4, dt, dn);
-    if (w64 == best) return launch_adjoint_mixed_nt<CH, 64>(c, ntot, w64 / 2, dt, dn);
-    return launch_adjoint_mixed_nt<CH, 32>(c, ntot, w32, dt, dn);
+    return launch_adjoint_mixed_nt<CH, 64>(c, ntot, w64 / 2, dt, dn);
 }
 
 // The forward image with the state the reverse pass needs (FP64: stored samples, cutoffs, tails),
@@ -1558,6 +1572,30 @@ int ks_chi2_gradient(ks_context* c, const ks_splat_set* sets, int32_t nsets, con
     if (!c || !data) return KS_ERR_ARGUMENT;
     return adjoint_run(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, nullptr, KS_ORDER_SCREEN, data, sigma,
                        sigma_scalar, mask, chi2, dparams, accumulate, image);
+}
+
+int ks_sample_adjoint(ks_context* c, int64_t n, const double* in, const double* Dl, const double* w, const double* R, int32_t method,
+                      double* out) {
+    if (!c || n < 0 || (n > 0 && (!in || !Dl || !w || !R || !out))) return KS_ERR_ARGUMENT;
+    if (method != 0 && method != 1) return fail(c, KS_ERR_ARGUMENT, "method must be 0 (structured) or 1 (duals)");
+    if (n == 0) return KS_OK;
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const size_t sizes[4] = {size_t(n) * 11, size_t(n), size_t(n) * 4, size_t(n) * 4};
+    const double* src[4] = {in, Dl, w, R};
+    const double* dev[4];
+    for (int q = 0; q < 4; ++q) {
+        int s = stage_dev(c, c->dft_in[q], src[q], sizes[q], &dev[q]);
+        if (s) return s;
+    }
+    const bool dout = is_device_ptr(out);
+    double* o = out;
+    if (!dout) { KS_CUDA(c, c->stage_out.ensure(size_t(n) * 31 * sizeof(double))); o = c->stage_out.as<double>(); }
+    k_sample_adjoint<<<nblocks(n), kBlock, 0, c->stream>>>(n, dev[0], dev[1], dev[2], dev[3], method, o);
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    if (!dout) KS_CUDA(c, cudaMemcpyAsync(out, o, size_t(n) * 31 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KS_OK;
 }
 
 int ks_adjoint_stats(ks_context* c, double* adjoint_ms, long long* launches, int reset) {

@@ -114,3 +114,11 @@ def kappa_params(rng, n, a):
     p[13] = rng.uniform(3.0, 6.0, n)
     p[14] = np.log(np.exp(rng.uniform(np.log(1.0), np.log(50.0), n)))
     return p
+
+
+def config3_target(params, rng_seed=2):
+    """The perturbed parameters of the configuration-3 target: every parameter moved by 5% Gaussian
+    noise relative to max(|p|, 0.1); the caller renders them and adds 1% Gaussian pixel noise
+    (sigma = 0.01 max I)."""
+    rng = np.random.Generator(np.random.PCG64(rng_seed))
+    return params + 0.05 * np.maximum(np.abs(params), 0.1) * rng.standard_normal(params.shape), rng

@@ -165,3 +165,37 @@ def test_mixed_chi2_gradient_matches_fp64(nus):
     print("chi2", chi64, chi32, "grad rel L2", rel_l2(g32, g64))
     assert abs(chi32 - chi64) <= 1e-3 * chi64
     assert rel_l2(g32, g64) < 1e-3
+
+
+def test_sample_adjoint_structured_matches_duals_and_fd(oracle):
+    """sample_adjoint (transport.jl:221-245): the structured partials of the mixed path and the seven
+    forward-mode duals of the FP64 path against each other (1e-10) and against central differences of
+    the oracle's exact step (1e-6), over the linear, cubic and general branches of the step."""
+    rng = np.random.Generator(np.random.PCG64(26))
+    cam = ks.Camera((-1.0, 1.0), (-1.0, 1.0), 2)
+    cache = ks.GeodesicCache(cam, 8)
+    n = 60
+    scale = np.concatenate([np.full(20, 1e-12), np.full(20, 1e-3), np.full(20, 1.0)])   # linear, cubic, general
+    al = np.abs(rng.standard_normal((n, 4))) * scale[:, None]
+    al[:, 0] += 2 * np.linalg.norm(al[:, 1:], axis=1)
+    rh = rng.standard_normal((n, 3)) * scale[:, None] * 3
+    j = np.abs(rng.standard_normal((n, 4)))
+    coeffs = np.concatenate([j, al, rh], axis=1)
+    Dl = rng.uniform(0.2, 3.0, n)
+    w, R = rng.standard_normal((n, 4)), rng.standard_normal((n, 4))
+    O0, E0, c0 = ks.sample_adjoint(cache, coeffs, Dl, w, R, method=0)
+    O1, E1, c1 = ks.sample_adjoint(cache, coeffs, Dl, w, R, method=1)
+    assert np.allclose(O0, O1, rtol=0, atol=1e-15) and np.allclose(E0, E1, rtol=0, atol=1e-15)
+    den = np.abs(c1).max(axis=1, keepdims=True)
+    assert np.max(np.abs(c0 - c1) / den) < 1e-10
+    for i in range(n):
+        def q(cf):
+            O, E = oracle.transfer_step(cf[:4], cf[4:8], cf[8:11], Dl[i])
+            return float(w[i] @ (O @ R[i] + E))
+        for k in range(11):
+            h = 1e-6 * max(abs(coeffs[i, k]), 0.1)
+            cp, cm = coeffs[i].copy(), coeffs[i].copy()
+            cp[k] += h
+            cm[k] -= h
+            fdv = (q(cp) - q(cm)) / (2 * h)
+            assert abs(c0[i, k] - fdv) <= 1e-6 * den[i, 0] + 1e-6 * abs(fdv), (i, k, c0[i, k], fdv)
