@@ -84,6 +84,16 @@ int ks_camera_set(ks_context* ctx, const double* alpha, const double* beta, int6
  * ray for `nsamples` samples and anchor interval `anchor_M` (Recurrence(M)/Fused(M)). */
 int ks_regenerate(ks_context* ctx, double a, double theta_o, int32_t nsamples, int32_t anchor_M);
 
+/* regenerate! with a sample count per ray: ray j gets N_j = clamp(64 ceil(samples_per_mino tau_total_j / 64),
+ * nmin, nmax) samples at tau_k = k tau_total_j / (N_j + 1), k = 1..N_j, i.e. exactly the samples of a
+ * uniform-N run with N = N_j for that ray (the reference runs mixed counts as uniform-N tiles,
+ * tiles(), cache.jl:241-246). Every other entry point follows each ray's own count. */
+int ks_regenerate_uneven(ks_context* ctx, double a, double theta_o, double samples_per_mino, int32_t nmin, int32_t nmax,
+                         int32_t anchor_M);
+
+/* The sample count of every ray (sorted order), npix int32. */
+int ks_get_nsamples(ks_context* ctx, int32_t* nsamples);
+
 /* cache.perm / cache.ranges (cache.jl:73-76, pixel_constants.jl:167-176): perm[j] is the screen
  * index (0-based) of sorted slot j; ranges = {case2_begin, case2_end, case3_begin, case3_end,
  * case4_begin, case4_end} as half-open 0-based slot ranges. */

@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -169,6 +169,13 @@ class GeodesicCache:
         return self.camera.size
 
     @property
+    def nsamples_per_ray(self):
+        """Sample count of every ray in sorted order (all cache.nsamples unless regenerated uneven)."""
+        out = np.empty(self.npix, dtype=np.int32)
+        self._check(self._lib.ks_get_nsamples(self._ctx, _ptr(out)))
+        return out
+
+    @property
     def perm(self):
         """perm[j] = screen index (0-based) of sorted slot j."""
         out = np.empty(self.npix, dtype=np.int64)
@@ -227,14 +234,21 @@ class GeodesicCache:
         return s.value
 
 
-def regenerate(cache, a, theta_o, camera=None, marcher=None):
-    """regenerate!(cache, a, theta_o[, camera]; marcher) (cache.jl:153-180, 248-255)."""
+def regenerate(cache, a, theta_o, camera=None, marcher=None, uneven=None):
+    """regenerate!(cache, a, theta_o[, camera]; marcher) (cache.jl:153-180, 248-255). With
+    `uneven = (samples_per_mino, nmin)` every ray gets its own sample count
+    N_j = clamp(64 ceil(samples_per_mino tau_total_j / 64), nmin, cache.nsamples)."""
     if camera is not None:
         if camera.npix != cache.npix:
             raise ValueError(f"camera has {camera.npix} pixels, cache was built for {cache.npix}")
         cache.set_camera(camera)
     marcher = marcher or Fused(64)
-    cache._check(cache._lib.ks_regenerate(cache._ctx, float(a), float(theta_o), cache.nsamples, marcher.M))
+    if uneven is None:
+        cache._check(cache._lib.ks_regenerate(cache._ctx, float(a), float(theta_o), cache.nsamples, marcher.M))
+    else:
+        density, nmin = uneven
+        cache._check(cache._lib.ks_regenerate_uneven(cache._ctx, float(a), float(theta_o), float(density), int(nmin), cache.nsamples,
+                                                     marcher.M))
     cache.spin, cache.theta_o, cache.marcher = float(a), float(theta_o), marcher
     cache.generation += 1
     return cache
@@ -329,6 +343,26 @@ class KappaSplats(_Model):
         self.hyp = np.ascontiguousarray(hyp, dtype=np.float64)
 
 
+class KnotSplats(_Model):
+    """Thermal splats whose centres follow trajectory knots (trajectories.jl:80-129): `params` 21 rows
+    (rows 1-3 and the pattern rate are not used), `knots` (3, nknots, nsplat) quasi-Cartesian
+    Kerr-Schild centres at the increasing coordinate `times` (nknots); the centre at a sample's
+    emission time is interpolated linearly and clamped to the end knots."""
+    kind = _lib.KS_KNOT21
+
+    def __init__(self, params, knots, times):
+        self.params, self.nsplat = _colmajor(params, 21)
+        k = np.asarray(knots, dtype=np.float64)
+        t = np.ascontiguousarray(times, dtype=np.float64).ravel()
+        if k.ndim != 3 or k.shape[0] != 3 or k.shape[1] != t.size or k.shape[2] != self.nsplat:
+            raise ValueError(f"knots must be (3, {t.size}, {self.nsplat}), got {k.shape}")
+        if t.size > 1 and not np.all(np.diff(t) > 0):
+            raise ValueError("knot times must increase")
+        self.knots = np.ascontiguousarray(k.ravel(order="F"))   # x fastest, then knot, then splat
+        self.knot_times = t
+        self.nknots = int(t.size)
+
+
 class CompositeModel(_Model):
     """Union of models (transport.jl:348-358): the elements of `a` followed by those of `b`."""
 
@@ -352,9 +386,10 @@ def _set_array(model):
         arr[i].params = _ptr(m.params).value
         hyp = getattr(m, "hyp", None)
         arr[i].hyp = _ptr(hyp).value if hyp is not None else None
-        arr[i].knots = None
-        arr[i].knot_times = None
-        arr[i].nknots = 0
+        kn = getattr(m, "knots", None)
+        arr[i].knots = _ptr(kn).value if kn is not None else None
+        arr[i].knot_times = _ptr(m.knot_times).value if kn is not None else None
+        arr[i].nknots = getattr(m, "nknots", 0)
         arr[i].gamma_max = getattr(m, "gamma_max", 1e5)
         keep.append(m)
     return arr, len(sets), keep

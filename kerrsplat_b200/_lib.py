@@ -49,6 +49,9 @@ SIGNATURES = [
     ("ks_last_error", ctypes.c_char_p, [_VP]),
     ("ks_camera_set", ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32]),
     ("ks_regenerate", ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32]),
+    ("ks_regenerate_uneven", ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_int32]),
+    ("ks_get_nsamples", ctypes.c_int, [_VP, _VP]),
     ("ks_get_perm", ctypes.c_int, [_VP, _VP]),
     ("ks_get_ranges", ctypes.c_int, [_VP, _VP]),
     ("ks_get_residuals", ctypes.c_int, [_VP, _VP, _VP]),

@@ -68,10 +68,16 @@ __global__ void k_build_plan(Spacetime st, const double* __restrict__ alpha, con
     long long i = perm[j];
     RayC R = build_ray(st, alpha[i], beta[i]);
     auto put = [&](int field, double v) { f[field * npad + j] = v; };
-    double dtau = R.tau_total / (st.N + 1);
+    int Nj = st.N;
+    if (st.density > 0.0) {
+        const double want = 64.0 * ceil(st.density * R.tau_total / 64.0);
+        Nj = (want > 0.0) ? int(fmin(double(st.N), fmax(double(st.nmin), want))) : st.nmin;
+    }
+    double dtau = R.tau_total / (Nj + 1);
     double h = dtau / 2.0;
     int Man = anchor_interval(st.M, 1.0 - R.k);
-    int nanch = (st.N - 1) / Man + 1;
+    int nanch = (Nj - 1) / Man + 1;
+    put(PF_NSAMP, Nj);
     put(PF_ALPHA, R.alpha); put(PF_BETA, R.beta); put(PF_ETA, R.eta); put(PF_LAM, R.lam);
     put(PF_NUMREALS, R.numreals); put(PF_CASE, R.rcase);
     put(PF_K, R.k); put(PF_C, R.c); put(PF_FO, R.fo);
@@ -91,7 +97,7 @@ __global__ void k_build_plan(Spacetime st, const double* __restrict__ alpha, con
     // the interval that holds the radial turning point of a scattering ray (quadrature.jl:269)
     int turn_k = -1;
     if (R.scattering) {
-        for (int k = 2; k <= st.N; ++k) {
+        for (int k = 2; k <= Nj; ++k) {
             double ta = (k - 1) * dtau, tb = k * dtau;
             if (ta < R.fo && R.fo < tb) { turn_k = k; break; }
         }
@@ -247,6 +253,7 @@ struct SetDesc {
     const double* params;
     const double* hyp;
     double gmax;
+    int koff, nk;                     // knot splats: offset of the set's first knot record, knot count
 };
 
 __global__ void k_splat_table(SetDesc d, double* __restrict__ tab) {
@@ -269,6 +276,8 @@ __global__ void k_splat_table(SetDesc d, double* __restrict__ tab) {
     double smax = fmax(p[3], fmax(p[4], p[5]));
     o[ST_SUPP] = (-2.0 * log(kWEIGHT_CUTOFF)) * exp(2 * smax);
     o[ST_RHO] = sqrt(p[0] * p[0] + p[1] * p[1]);
+    o[ST_KOFF] = d.kind == KS_KNOT21 ? double(d.koff + 4 * d.nk * i) : 0.0;
+    o[ST_NK] = d.kind == KS_KNOT21 ? double(d.nk) : 0.0;
     if (d.kind == KS_THIN14) { o[ST_LOGA] = p[12]; return; }
     o[ST_NE] = exp(p[12]);
     double Bmag, thB, phB, u1, u2, u3;
@@ -421,6 +430,7 @@ __global__ void k_thin_noalloc(PlanView P, Spacetime st, long long npix, const d
 template <class T, int CH>
 struct PolSink {
     const T* tab; int ntot;
+    const T* knots;   // the knot array of knot splats (after the table)
     T t_obs[CH], nu[CH], nuh[CH], Lnu[CH];
     int nc;
     T a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
@@ -484,7 +494,7 @@ struct PolSink {
                 T t = t_obs[c] - s.t;
                 T q;
                 ev[2]++;
-                if (!splat_exponent(p, t, x, y, z, kind != KS_KNOT21, q)) continue;
+                if (!any_exponent(p, knots, t, x, y, z, q)) continue;
                 ev[3]++;
                 T G = exp(-q);
                 if (!(G > T(kWEIGHT_CUTOFF))) continue;
@@ -546,17 +556,17 @@ template <class T, int CH>
 __global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, long long npix, const double* __restrict__ tab64, int ntot,
                                                       const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L,
                                                       int nmax, double slab, double* __restrict__ out, double* __restrict__ resid_t,
-                                                      double* __restrict__ resid_phi, unsigned long long* __restrict__ counters) {
+                                                      double* __restrict__ resid_phi, unsigned long long* __restrict__ counters, int nkv) {
     extern __shared__ __align__(16) unsigned char smem[];
     T* tab = reinterpret_cast<T*>(smem);
-    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = T(tab64[q]);
+    for (int q = threadIdx.x; q < ntot * ST_COUNT + nkv; q += blockDim.x) tab[q] = T(tab64[q]);
     __syncthreads();
     long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (j >= npix) return;
     const int c0 = blockIdx.y * CH;
     MarchRay<T> R = load_ray<T>(P, st, j);
     PolSink<T, CH> sink;
-    sink.tab = tab; sink.ntot = ntot;
+    sink.tab = tab; sink.ntot = ntot; sink.knots = tab + ntot * ST_COUNT;
     sink.nc = min(CH, ncombo - c0);
     for (int c = 0; c < CH; ++c) {
         int cc = min(c0 + c, ncombo - 1);
@@ -643,6 +653,7 @@ struct ks_context {
     DevBuf gtab, samples, kstop, tails, slots, dgrad, seeds, chi_part, chi_val, dstage;
     DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part;
     bool samples_ready = false;
+    int nkv = 0;                            // knot values after the splat table in `tab`
     MixedJob last_job{};                    // the segmentation of the last mixed forward pass
     float* fwd_gstate = nullptr;            // set during the adjoint's forward pass only
     unsigned char* fwd_gact = nullptr;
@@ -756,14 +767,38 @@ int build_tables(ks_context* c, const ks_splat_set* sets, int nsets, int* ntot_o
     for (int s = 0; s < nsets; ++s) {
         int nr = nrows_of(sets[s].kind);
         if (nr < 0 || sets[s].kind == KS_THIN14) return fail(c, KS_ERR_ARGUMENT, "set %d: unsupported kind %d", s, sets[s].kind);
-        if (sets[s].kind == KS_KNOT21) return fail(c, KS_ERR_ARGUMENT, "set %d: knot splats are not supported by ks_render yet", s);
         if (grad && sets[s].kind != KS_THERMAL21)
             return fail(c, KS_ERR_ARGUMENT, "set %d: the adjoint covers thermal polarized splats (KS_THERMAL21) only", s);
         if (sets[s].nsplat < 0 || (sets[s].nsplat > 0 && !sets[s].params)) return fail(c, KS_ERR_ARGUMENT, "set %d: bad parameters", s);
         if (sets[s].kind == KS_KAPPA22 && sets[s].nsplat > 0 && !sets[s].hyp) return fail(c, KS_ERR_ARGUMENT, "set %d: kappa sets need hyp", s);
         ntot += sets[s].nsplat;
     }
-    KS_CUDA(c, c->tab.ensure(size_t(std::max(ntot, 1)) * ST_COUNT * sizeof(double)));
+    // the knot array of the knot sets (trajectories.jl:80-111): per splat its times, x, y, z
+    std::vector<double> kv;
+    std::vector<int> koff(nsets, 0);
+    for (int s = 0; s < nsets; ++s) {
+        const ks_splat_set& S = sets[s];
+        if (S.kind != KS_KNOT21 || S.nsplat == 0) continue;
+        if (!S.knots || !S.knot_times || S.nknots < 1) return fail(c, KS_ERR_ARGUMENT, "set %d: knot splats need knots and knot times", s);
+        const int nk = S.nknots;
+        std::vector<double> ht(nk), hk(size_t(3) * nk * S.nsplat);
+        KS_CUDA(c, cudaMemcpy(ht.data(), S.knot_times, ht.size() * sizeof(double), cudaMemcpyDefault));
+        KS_CUDA(c, cudaMemcpy(hk.data(), S.knots, hk.size() * sizeof(double), cudaMemcpyDefault));
+        for (int k = 0; k < nk; ++k)
+            if (!std::isfinite(ht[k]) || (k > 0 && !(ht[k] > ht[k - 1]))) return fail(c, KS_ERR_ARGUMENT, "set %d: knot times must increase", s);
+        for (double v : hk) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "set %d: non-finite knot", s);
+        koff[s] = int(kv.size());
+        for (int i = 0; i < S.nsplat; ++i) {
+            kv.insert(kv.end(), ht.begin(), ht.end());
+            for (int d = 0; d < 3; ++d)
+                for (int k = 0; k < nk; ++k) kv.push_back(hk[d + 3 * (k + size_t(nk) * i)]);
+        }
+    }
+    c->nkv = int(kv.size());
+    KS_CUDA(c, c->tab.ensure((size_t(std::max(ntot, 1)) * ST_COUNT + kv.size()) * sizeof(double)));
+    if (!kv.empty())
+        KS_CUDA(c, cudaMemcpyAsync(c->tab.as<double>() + size_t(ntot) * ST_COUNT, kv.data(), kv.size() * sizeof(double),
+                                   cudaMemcpyHostToDevice, c->stream));
     if (grad) KS_CUDA(c, c->gtab.ensure(size_t(std::max(ntot, 1)) * GT_COUNT * sizeof(double)));
     int first = 0;
     for (int s = 0; s < nsets; ++s) {
@@ -783,7 +818,8 @@ int build_tables(ks_context* c, const ks_splat_set* sets, int nsets, int* ntot_o
             KS_CUDA(c, cudaMemcpyAsync(hd, S.hyp, S.nsplat * sizeof(double), cudaMemcpyDefault, c->stream));
             dh = hd;
         }
-        SetDesc d{S.kind, nr, S.nsplat, first, tmp.as<const double>(), (const double*)dh, S.gamma_max > 0 ? S.gamma_max : 1e5};
+        SetDesc d{S.kind, nr, S.nsplat, first, tmp.as<const double>(), (const double*)dh, S.gamma_max > 0 ? S.gamma_max : 1e5, koff[s],
+                  S.kind == KS_KNOT21 ? S.nknots : 0};
         k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
         c->launches++;
         KS_CUDA(c, cudaGetLastError());
@@ -805,7 +841,7 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     MixedJob job = job0;
     const int N = c->st.N;
     constexpr int W = NT / 32;
-    const size_t smem = MixedSmem<CH>::bytes(ntot, W);
+    const size_t smem = MixedSmem<CH>::bytes(ntot, W, c->nkv);
     // split the sample range into segments until there are about eight work units per resident
     // warp, so that the most expensive unit is short
     const long long resident = (long long)nsm * per_sm * W;
@@ -841,7 +877,7 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
 // Occupancy of k_consume<CH, NT, KM> with its shared memory for `ntot` splats (0 if it does not fit).
 template <int CH, int NT, int KM>
 int consume_blocks(ks_context* c, int ntot) {
-    const size_t smem = MixedSmem<CH>::bytes(ntot, NT / 32);
+    const size_t smem = MixedSmem<CH>::bytes(ntot, NT / 32, c->nkv);
     if (smem > 227 * 1024) return 0;
     if (cudaFuncSetAttribute(k_consume<CH, NT, KM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
@@ -872,6 +908,7 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     job.nvc = (nfreq + CH - 1) / CH;
     job.nchunks = (c->npix + 31) / 32;
     job.nmax = nmax; job.slab = float(slab); job.L = L;
+    job.nkv = c->nkv;
     // the block size with the most resident warps (the per-warp shared memory sets the limit)
     const int w384 = consume_blocks<CH, 384, KM>(c, ntot) * 12, w256 = consume_blocks<CH, 256, KM>(c, ntot) * 8,
               w128 = consume_blocks<CH, 128, KM>(c, ntot) * 4;
@@ -1005,7 +1042,36 @@ int ks_camera_set(ks_context* c, const double* alpha, const double* beta, int64_
     return KS_OK;
 }
 
+namespace {
+int regenerate_impl(ks_context* c, double a, double theta_o, int32_t nsamples, int32_t anchor_M, double density, int32_t nmin);
+}
+
 int ks_regenerate(ks_context* c, double a, double theta_o, int32_t nsamples, int32_t anchor_M) {
+    return regenerate_impl(c, a, theta_o, nsamples, anchor_M, 0.0, 0);
+}
+
+int ks_regenerate_uneven(ks_context* c, double a, double theta_o, double samples_per_mino, int32_t nmin, int32_t nmax, int32_t anchor_M) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (!(std::isfinite(samples_per_mino) && samples_per_mino > 0)) return fail(c, KS_ERR_ARGUMENT, "samples per unit Mino time must be positive");
+    if (nmin < 1 || nmax < nmin) return fail(c, KS_ERR_ARGUMENT, "need 1 <= nmin <= nmax");
+    return regenerate_impl(c, a, theta_o, nmax, anchor_M, samples_per_mino, nmin);
+}
+
+int ks_get_nsamples(ks_context* c, int32_t* out) {
+    if (!c || !out) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    std::vector<double> f(c->npix);
+    KS_CUDA(c, cudaMemcpy(f.data(), c->plan.as<double>() + size_t(PF_NSAMP) * c->npad, c->npix * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int32_t> o(c->npix);
+    for (long long j = 0; j < c->npix; ++j) o[j] = int32_t(f[j]);
+    KS_CUDA(c, cudaMemcpy(out, o.data(), o.size() * sizeof(int32_t), cudaMemcpyDefault));
+    return KS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int regenerate_impl(ks_context* c, double a, double theta_o, int32_t nsamples, int32_t anchor_M, double density, int32_t nmin) {
     if (!c) return KS_ERR_ARGUMENT;
     if (c->npix <= 0) return fail(c, KS_ERR_ARGUMENT, "set a camera before regenerate");
     if (!std::isfinite(a) || !std::isfinite(theta_o)) return fail(c, KS_ERR_NONFINITE, "non-finite spin or inclination");
@@ -1019,6 +1085,7 @@ int ks_regenerate(ks_context* c, double a, double theta_o, int32_t nsamples, int
     st.rp = 1.0 + std::sqrt(1.0 - a * a); st.rmn = 1.0 - std::sqrt(1.0 - a * a); st.rh = st.rp;
     st.abscos = std::fabs(std::cos(theta_o)); st.cos2 = std::cos(theta_o) * std::cos(theta_o);
     st.N = nsamples; st.M = anchor_M;
+    st.density = density; st.nmin = nmin;
     KS_CUDA(c, c->key.ensure(n)); KS_CUDA(c, c->key2.ensure(n));
     KS_CUDA(c, c->idx.ensure(n * sizeof(long long))); KS_CUDA(c, c->perm.ensure(n * sizeof(long long)));
     k_root_case<<<nblocks(n), kBlock, 0, c->stream>>>(st, c->alpha.as<double>(), c->beta.as<double>(), n, c->key.as<unsigned char>(),
@@ -1079,6 +1146,9 @@ int ks_regenerate(ks_context* c, double a, double theta_o, int32_t nsamples, int
     c->samples_ready = false;
     return KS_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int ks_get_perm(ks_context* c, int64_t* perm) {
     if (!c || !perm) return KS_ERR_ARGUMENT;
@@ -1127,6 +1197,7 @@ int ks_march_samples(ks_context* c, double* t, double* r, double* theta, double*
     KS_CUDA(c, c->stage_out.ensure(ns * (4 * sizeof(double) + 1)));
     double* d = c->stage_out.as<double>();
     unsigned char* fl = reinterpret_cast<unsigned char*>(d + 4 * ns);
+    KS_CUDA(c, cudaMemsetAsync(d, 0, ns * (4 * sizeof(double) + 1), c->stream));   // samples past a ray's count: zero
     k_march_store<<<nblocks(n), kBlock, 0, c->stream>>>(plan_view(c), c->st, n, d, d + ns, d + 2 * ns, d + 3 * ns, fl,
                                                           c->resid_t.as<double>(), c->resid_phi.as<double>());
     c->launches++;
@@ -1235,14 +1306,14 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     cudaEventRecord(c->ev0, c->stream);
     if (precision == KS_FP64) {
         // the plain path: one march per (frame, frequency), as the reference's polarized_cube does
-        size_t smem = size_t(ntot) * ST_COUNT * sizeof(double);
+        size_t smem = (size_t(ntot) * ST_COUNT + c->nkv) * sizeof(double);
         if (smem > 220 * 1024) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
         KS_CUDA(c, cudaFuncSetAttribute(k_polarized<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         for (int cc = 0; cc < ncombo; ++cc) {
             k_polarized<double, 1><<<dim3(nblocks(n), 1), kBlock, smem, c->stream>>>(
                 plan_view(c), c->st, n, c->tab.as<double>(), ntot, dct + cc, dcn + cc, 1, L, nmax, slab,
                 c->out_sorted.as<double>() + size_t(cc) * n * 4, c->resid_t.as<double>(), c->resid_phi.as<double>(),
-                c->count_events ? c->counters.as<unsigned long long>() : nullptr);
+                c->count_events ? c->counters.as<unsigned long long>() : nullptr, c->nkv);
             c->launches++;
             c->kernel_launches++;
         }
@@ -1283,6 +1354,7 @@ int ensure_samples(ks_context* c, StoredSamples* S) {
     double* d = c->samples.as<double>();
     unsigned char* fl = reinterpret_cast<unsigned char*>(d + 4 * ns);
     if (!c->samples_ready) {
+        KS_CUDA(c, cudaMemsetAsync(fl, 0, ns, c->stream));   // samples past a ray's count stay invalid
         k_march_store<<<nblocks(n), kBlock, 0, c->stream>>>(plan_view(c), c->st, n, d, d + ns, d + 2 * ns, d + 3 * ns, fl,
                                                               c->resid_t.as<double>(), c->resid_phi.as<double>());
         c->launches++;

@@ -26,7 +26,7 @@ struct MarchRay {
     T a, lam, eta, rp, rmn, sp, sm, Qt, Qtm, Qphi, Qphim, r4, qC, qn, sqrt_eps, gc, mp, K2;
     T vabsalpha, valpha2, vabsbeta, vabscos, vcos2;
     JS<T> dr, dth;
-    int turn_k, Manchor, nanch;
+    int turn_k, Manchor, nanch, nsamp;
     long long anchor_off;
 };
 
@@ -61,6 +61,7 @@ __device__ __forceinline__ MarchRay<T> load_ray(const PlanView& P, const Spaceti
     R.turn_k = int(P.get(PF_TURN_K, j));
     R.Manchor = int(P.get(PF_MANCHOR, j));
     R.nanch = int(P.get(PF_NANCH, j));
+    R.nsamp = int(P.get(PF_NSAMP, j));
     R.anchor_off = P.anchor_off[j];
     return R;
 }
@@ -210,11 +211,12 @@ __device__ __forceinline__ JS<T> load_js(const double* rec, int off) {
     return {T(rec[off]), T(rec[off + 1]), T(rec[off + 2])};
 }
 
-// March ray j with N samples and call f(k, sample) for k = 1..N; returns the largest anchor residuals.
+// March ray j with its N samples and call f(k, sample) for k = 1..N; returns the largest anchor residuals.
 template <class T, class F>
 __device__ __forceinline__ void march(const PlanView& P, const Spacetime& st, long long j, const MarchRay<T>& R,
                                       F& f, double& resid_t, double& resid_phi) {
-    const int N = st.N;
+    const int N = R.nsamp;
+    (void)st;
     const double dtau = R.dtau;
     const double h = dtau / 2.0;
     const double* A0 = P.anchors + R.anchor_off * AF_COUNT;
@@ -291,6 +293,8 @@ __device__ __forceinline__ void march(const PlanView& P, const Spacetime& st, lo
 // their anchor spacing. With k_begin = 1 this is the stream of march() (quadrature.jl:231-296).
 template <class T, class F>
 __device__ __forceinline__ void march_range(const PlanView& P, long long j, const MarchRay<T>& R, F& f, int k_begin, int k_end) {
+    if (k_end > R.nsamp + 1) k_end = R.nsamp + 1;
+    if (k_begin >= k_end) return;
     const double dtau = R.dtau;
     const double h = dtau / 2.0;
     int m = (k_begin - 1) / R.Manchor;

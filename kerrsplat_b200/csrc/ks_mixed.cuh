@@ -37,7 +37,9 @@ struct MixedSmem {
     static constexpr int kMetaBytes = 32 * 4 * 2;
     static constexpr int kStateBytes = 32 * CH * 20 * 4;                                        // P (16) and S (4) per lane and frequency
     static constexpr int kWarpBytes = kSampleBytes + kItemBytes + kResBytes + kMetaBytes + kStateBytes;
-    static size_t bytes(int ntot, int warps) { return size_t(ntot) * ST_COUNT * 4 + size_t(warps) * kWarpBytes; }
+    // the splat table and the knot array (nkv floats) come first
+    __host__ __device__ static size_t tab_bytes(int ntot, int nkv) { return (size_t(ntot) * ST_COUNT * 4 + size_t(nkv) * 4 + 15) / 16 * 16; }
+    static size_t bytes(int ntot, int warps, int nkv = 0) { return tab_bytes(ntot, nkv) + size_t(warps) * kWarpBytes; }
 };
 
 // Out-of-line pieces of the consumer: one copy of each in the instruction cache (inlined into the
@@ -92,6 +94,7 @@ __device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float*
 template <int CH, int KM>
 struct MixedSink {
     const float* tab; int ntot;
+    const float* knots;   // the knot array of knot splats (after the table)
     float t_obs;
     float nu[CH], Lnu[CH];
     int nc;
@@ -115,6 +118,7 @@ struct MixedSink {
     unsigned char* gact;
     long long gnpad, jbase;
     int gN, kcur, gframes, gf, gv0;
+    int nsamp;        // this lane's samples
 
     __device__ void init() {
         for (int c = 0; c < CH; ++c) {
@@ -149,7 +153,8 @@ struct MixedSink {
         const float* p = tab + i * ST_COUNT;
         const int kind = int(p[ST_KIND]);
         float q;
-        splat_exponent(p, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], false, q);
+        if (kind == KS_KNOT21) knot_exponent(p, knots, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], q);
+        else splat_exponent(p, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], false, q);
         float G = __expf(-q);
         LFrame<float> lf = local_frame_ool(s, p, a, a_sin_tho);
         float thb = acosf(fminf(1.f, fmaxf(-1.f, lf.cosB)));
@@ -175,8 +180,9 @@ struct MixedSink {
     // quasi-Cartesian Kerr-Schild position, ts the regularized lookback time t~.
     __device__ void consume(bool usable, float x, float y, float z, float ts, float r, float sth, float cth, bool nur, bool nuth) {
         const unsigned full = 0xffffffffu;
-        ev[0]++;
-        bool valid = live && usable;
+        const bool inrange = kcur <= nsamp;   // a ray with fewer samples than the unit's segment
+        if (inrange) ev[0]++;
+        bool valid = live && inrange && usable;
         if (valid) ev[1]++;
         if (valid && nmax >= 0) valid = wind_ok(r * cth);
         unsigned vmask = __ballot_sync(full, valid);
@@ -215,8 +221,12 @@ struct MixedSink {
                     // farther than the support radius from that circle is outside the support sphere
                     // at every time (no trigonometry needed)
                     const float dr = rho - p[ST_RHO], dz = z - p[ST_CZ];
-                    if (dr * dr + dz * dz > p[ST_SUPP] && int(p[ST_KIND]) != KS_KNOT21) continue;
-                    if (!splat_exponent(p, t, x, y, z, int(p[ST_KIND]) != KS_KNOT21, q)) continue;
+                    if (int(p[ST_KIND]) != KS_KNOT21) {
+                        if (dr * dr + dz * dz > p[ST_SUPP]) continue;
+                        if (!splat_exponent(p, t, x, y, z, true, q)) continue;
+                    } else {
+                        knot_exponent(p, knots, t, x, y, z, q);
+                    }
                     ev[3]++;
                     if (q < kQCUT) mask |= 1u << b;
                 }
@@ -415,6 +425,7 @@ struct MixedJob {
     double L;
     float* gstate = nullptr;          // the adjoint's per-sample states (see MixedSink)
     unsigned char* gact = nullptr;
+    int nkv = 0;                      // knot values after the splat table
 };
 
 template <int CH, int NT, int KM>
@@ -424,8 +435,8 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
           float* __restrict__ seg_out, unsigned long long* __restrict__ counters) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* tab = reinterpret_cast<float*>(smem);
-    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
-    unsigned char* wbase = smem + size_t(ntot) * ST_COUNT * 4;
+    for (int q = threadIdx.x; q < ntot * ST_COUNT + job.nkv; q += blockDim.x) tab[q] = float(tab64[q]);
+    unsigned char* wbase = smem + MixedSmem<CH>::tab_bytes(ntot, job.nkv);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* wb = wbase + size_t(warp) * MixedSmem<CH>::kWarpBytes;
     __syncthreads();
@@ -449,9 +460,11 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         const bool live = j0 < job.npix;
         const long long j = live ? j0 : job.npix - 1;
         const int k0 = 1 + seg * job.seg_len;
-        const int k1 = min(N + 1, k0 + job.seg_len);
+        // the unit ends at the largest sample count of its rays (uneven counts)
+        const int kmax = __reduce_max_sync(0xffffffffu, int(P.get(PF_NSAMP, j)));
+        const int k1 = min(min(N + 1, k0 + job.seg_len), kmax + 1);
         MixedSink<CH, KM> sink;
-        sink.tab = tab; sink.ntot = ntot;
+        sink.tab = tab; sink.ntot = ntot; sink.knots = tab + ntot * ST_COUNT;
         sink.t_obs = float(ct[f]);
         sink.nc = min(CH, job.nfreq - v0);
         for (int c = 0; c < CH; ++c) {
@@ -465,6 +478,7 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         sink.eta = float(P.get(PF_ETA, j)); sink.lam = float(P.get(PF_LAM, j));
         sink.a_sin_tho = float(st.a * sin(st.thetao)); sink.slab = job.slab; sink.nmax = job.nmax;
         sink.lane = lane; sink.live = live;
+        sink.nsamp = int(P.get(PF_NSAMP, j));
         sink.gstate = job.gstate; sink.gact = job.gact; sink.gnpad = npad; sink.jbase = w * 32;
         sink.gN = N; sink.gframes = job.nframes; sink.gf = f; sink.gv0 = v0;
         sink.sf = reinterpret_cast<float*>(wb);

@@ -19,7 +19,10 @@ namespace ks {
 
 struct Spacetime {
     double a, thetao, rp, rmn, rh, abscos, cos2;
-    int N, M;
+    int N, M;        // N: samples per ray (with uneven counts, the largest)
+    // uneven counts: N_j = clamp(64 ceil(density tau_total_j / 64), nmin, N); density 0 = uniform N
+    double density;
+    int nmin;
 };
 
 enum PlanField {
@@ -37,6 +40,7 @@ enum PlanField {
     PF_PTT_SN, PF_PTT_CN, PF_PTT_DN,                                     // polar state at fo
     PF_MANCHOR, PF_NANCH,
     PF_R1RE, PF_R1IM, PF_R2RE, PF_R2IM, PF_R3RE, PF_R3IM, PF_R4RE, PF_R4IM,
+    PF_NSAMP,                                    // samples of this ray
     PF_COUNT
 };
 

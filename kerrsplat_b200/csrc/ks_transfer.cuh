@@ -30,6 +30,7 @@ enum SplatTab {
     ST_P, ST_GMIN, ST_GMAX, ST_GSPAN, ST_GAMJ, ST_GAMA,
     ST_KAP, ST_W, ST_HYP, ST_G43, ST_G2, ST_GQ, ST_GP, ST_GK2, ST_KB,
     ST_KIND, ST_RHO,
+    ST_KOFF, ST_NK,           // knot splats: offset of the splat's knot record in the knot array, knot count
     ST_COUNT
 };
 
@@ -563,6 +564,44 @@ __device__ __forceinline__ bool splat_exponent(const T* p, T t, T x, T y, T z, b
     T tt = (t - p[ST_T0]) * p[ST_INVW];
     q = (e0 * e0 + e1 * e1 + e2 * e2 + tt * tt) / T(2);
     return true;
+}
+
+// knot_centre (trajectories.jl:93-111): the centre interpolated linearly between the knots at time t,
+// clamped to the end knots; kn = [times (nk), x (nk), y (nk), z (nk)] with increasing times
+template <class T>
+__device__ __forceinline__ void knot_centre(const T* kn, int nk, T t, T& cx, T& cy, T& cz) {
+    const T* ts = kn;
+    const T *X = kn + nk, *Y = kn + 2 * nk, *Z = kn + 3 * nk;
+    if (t <= ts[0]) { cx = X[0]; cy = Y[0]; cz = Z[0]; return; }
+    if (t >= ts[nk - 1]) { cx = X[nk - 1]; cy = Y[nk - 1]; cz = Z[nk - 1]; return; }
+    int k = 0;
+    while (k < nk - 2 && ts[k + 1] <= t) ++k;
+    const T w = (t - ts[k]) / (ts[k + 1] - ts[k]);
+    cx = (T(1) - w) * X[k] + w * X[k + 1];
+    cy = (T(1) - w) * Y[k] + w * Y[k + 1];
+    cz = (T(1) - w) * Z[k] + w * Z[k + 1];
+}
+
+// The weight exponent of a knot splat (KnotSplats element, trajectories.jl:113-129): the centre from
+// its knots at the emission time, no pattern rotation and no support cull; knots = the knot array.
+template <class T>
+__device__ __forceinline__ void knot_exponent(const T* p, const T* knots, T t, T x, T y, T z, T& q) {
+    T cx, cy, cz;
+    knot_centre(knots + int(p[ST_KOFF]), int(p[ST_NK]), t, cx, cy, cz);
+    const T d0 = x - cx, d1 = y - cy, d2 = z - cz;
+    const T u0 = p[ST_R0] * d0 + p[ST_R3] * d1 + p[ST_R6] * d2;
+    const T u1 = p[ST_R1] * d0 + p[ST_R4] * d1 + p[ST_R7] * d2;
+    const T u2 = p[ST_R2] * d0 + p[ST_R5] * d1 + p[ST_R8] * d2;
+    const T e0 = u0 * p[ST_ES1], e1 = u1 * p[ST_ES2], e2 = u2 * p[ST_ES3];
+    const T tt = (t - p[ST_T0]) * p[ST_INVW];
+    q = (e0 * e0 + e1 * e1 + e2 * e2 + tt * tt) / T(2);
+}
+
+// The exponent of any splat of a polarized scene: false when the support sphere culls it.
+template <class T>
+__device__ __forceinline__ bool any_exponent(const T* p, const T* knots, T t, T x, T y, T z, T& q) {
+    if (int(p[ST_KIND]) == KS_KNOT21) { knot_exponent(p, knots, t, x, y, z, q); return true; }
+    return splat_exponent(p, t, x, y, z, true, q);
 }
 
 }  // namespace ks

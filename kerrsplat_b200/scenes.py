@@ -122,3 +122,100 @@ def config3_target(params, rng_seed=2):
     (sigma = 0.01 max I)."""
     rng = np.random.Generator(np.random.PCG64(rng_seed))
     return params + 0.05 * np.maximum(np.abs(params), 0.1) * rng.standard_normal(params.shape), rng
+
+
+# ---- trajectory knots (host preprocessing, trajectories.jl:9-68) ------------------------------------
+
+def boyer_lindquist(a, x, y, z):
+    """BL (r, theta, phi) of a quasi-Cartesian Kerr-Schild point (trajectories.jl:9-18)."""
+    r = np.sqrt(x * x + y * y + z * z)
+    th = np.arccos(np.clip(z / r, -1.0, 1.0))
+    temp = np.sqrt(1 - a * a)
+    rp, rm = 1 + temp, 1 - temp
+    eps = np.finfo(float).eps
+    phks = np.arctan2(y, x)
+    ph = phks - a / (2 * temp) * np.log(np.abs((r - rp + eps) / (r - rm + eps))) + np.arctan2(a, r)
+    return r, th, ph
+
+
+def quasi_cartesian_kerr_schild(a, r, th, ph):
+    """coordinates.jl:22-31."""
+    temp = np.sqrt(1 - a * a)
+    rp, rm = 1 + temp, 1 - temp
+    eps = np.finfo(float).eps
+    phks = ph + a / (2 * temp) * np.log(np.abs((r - rp + eps) / (r - rm + eps))) - np.arctan2(a, r)
+    return r * np.sin(th) * np.cos(phks), r * np.sin(th) * np.sin(phks), r * np.cos(th)
+
+
+def coordinate_velocity(a, r, th, u):
+    """(dr/dt, dtheta/dt, dphi/dt) of ZAMO 3-velocity u along (r-hat, phi-hat, -theta-hat)
+    (trajectories.jl:21-25): the BL 4-velocity from the ZAMO tetrad."""
+    g = np.sqrt(1 + u[0] ** 2 + u[1] ** 2 + u[2] ** 2)
+    s2 = np.sin(th) ** 2
+    Sg = r * r + a * a * np.cos(th) ** 2
+    D = r * r - 2 * r + a * a
+    A = (r * r + a * a) ** 2 - a * a * D * s2
+    lapse = np.sqrt(Sg * D / A)
+    om = 2 * a * r / A
+    varpi = np.sqrt(A / Sg) * np.sqrt(s2)
+    ut = g / lapse
+    ur = np.sqrt(D / Sg) * u[0]
+    uth = -u[2] / np.sqrt(Sg)
+    uph = om / lapse * g + u[1] / varpi
+    return np.array([ur / ut, uth / ut, uph / ut])
+
+
+def trajectory_knots(params, a, times, substeps=4):
+    """Centres of every splat at the coordinate `times`, integrated from the centre at t0 with the
+    splat's ZAMO velocity by RK4 in BL coordinates, `substeps` steps per knot interval, forward and
+    backward from t0 (trajectories.jl:35-68). Returns (3, nknots, nsplat) KS positions."""
+    times = np.asarray(times, dtype=np.float64)
+    n = params.shape[1]
+    knots = np.empty((3, times.size, n))
+    dt_knot = abs(times[-1] - times[0]) / max(times.size - 1, 1)
+    for i in range(n):
+        u = params[17:20, i]
+        t0 = params[10, i]
+        q0 = np.array(boyer_lindquist(a, *params[0:3, i]))
+
+        def integrate(q, t_from, t_to):
+            m = max(1, int(np.ceil(abs(t_to - t_from) / dt_knot * substeps)))
+            h = (t_to - t_from) / m
+            for _ in range(m):
+                k1 = coordinate_velocity(a, q[0], q[1], u)
+                k2 = coordinate_velocity(a, *(q + h / 2 * k1)[:2], u)
+                k3 = coordinate_velocity(a, *(q + h / 2 * k2)[:2], u)
+                k4 = coordinate_velocity(a, *(q + h * k3)[:2], u)
+                q = q + h / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+            return q
+
+        order = np.argsort(times)
+        kt0 = int(np.searchsorted(times[order], t0))
+        q, tprev = q0, t0
+        for k in range(kt0, times.size):
+            q = integrate(q, tprev, times[order[k]]); tprev = times[order[k]]
+            knots[:, order[k], i] = quasi_cartesian_kerr_schild(a, *q)
+        q, tprev = q0, t0
+        for k in range(kt0 - 1, -1, -1):
+            q = integrate(q, tprev, times[order[k]]); tprev = times[order[k]]
+            knots[:, order[k], i] = quasi_cartesian_kerr_schild(a, *q)
+    return knots
+
+
+def config4(res=512, N=2048, nframes=32, density=768.0, nmin=128):
+    """Batched movie: a = 0.94, theta_o = 163 deg, +-15 M, frames t_obs = 10 f M (f < nframes),
+    86/230/345/690 GHz, uneven samples per ray (N_j = clamp(64 ceil(768 tau_j / 64), 128, 2048)),
+    256 splats of seed 3: 85 thermal on 4 trajectory knots spanning the emission times, 85 power-law
+    (p ~ U[2.5, 3.5], gamma_min = 10), 86 kappa (kappa ~ U[3, 6])."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    a, tho = 0.94, np.deg2rad(163.0)
+    pt = thermal_params(rng, 85, a)
+    pp = powerlaw_params(rng, 85, a)
+    pk = kappa_params(rng, 86, a)
+    times = 10.0 * np.arange(nframes)
+    # knots over the emission times of the movie: lookbacks reach ~ -60 M before the first frame
+    ktimes = np.linspace(times[0] - 80.0, times[-1] + 20.0, 4)
+    knots = trajectory_knots(pt, a, ktimes)
+    return dict(a=a, theta_o=tho, camera=Camera((-15.0, 15.0), (-15.0, 15.0), res), N=N, M=64, density=density, nmin=nmin,
+                thermal=pt, powerlaw=pp, kappa=pk, knots=knots, knot_times=ktimes, times=times,
+                nus=np.array([86e9, 230e9, 345e9, 690e9]), L=gravitational_radius(4.0e6))

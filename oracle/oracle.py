@@ -89,20 +89,27 @@ NROWS = {1: 21, 2: 22, 3: 22, 4: 21}
 
 
 def polarized_image(a, theta_o, alpha, beta, N, M, sets, t_obs, nu, L, nmax=-1, slab=0.0, gmax=1e5):
-    """sets: list of (kind, params (nrows, nsplat), hyp or None). Returns (npix, 4) cgs, screen order."""
+    """sets: list of (kind, params (nrows, nsplat), hyp or None[, knots (3, nknots, nsplat), knot_times]).
+    Returns (npix, 4) cgs, screen order."""
     alpha, beta = _d(alpha), _d(beta)
     n = alpha.size
     ns = len(sets)
-    kinds = (ctypes.c_int * ns)(*[KIND[k] if isinstance(k, str) else k for k, _, _ in sets])
+    kinds = (ctypes.c_int * ns)(*[KIND[st[0]] if isinstance(st[0], str) else st[0] for st in sets])
     nrows = (ctypes.c_int * ns)(*[NROWS[kinds[i]] for i in range(ns)])
-    keep = [np.ascontiguousarray(np.asarray(p, dtype=np.float64).T) for _, p, _ in sets]
+    keep = [np.ascontiguousarray(np.asarray(st[1], dtype=np.float64).T) for st in sets]
     nsplat = (ctypes.c_int * ns)(*[k.shape[0] for k in keep])
     params = (ctypes.c_void_p * ns)(*[k.ctypes.data for k in keep])
-    hyps = [None if h is None else _d(h) for _, _, h in sets]
+    hyps = [None if st[2] is None else _d(st[2]) for st in sets]
     hyp = (ctypes.c_void_p * ns)(*[None if h is None else h.ctypes.data for h in hyps])
+    # knots (3, nknots, nsplat) in the reference's column-major order: x fastest
+    kn = [np.asfortranarray(np.asarray(st[3], dtype=np.float64)).ravel(order="F") if len(st) > 3 else None for st in sets]
+    kt = [_d(st[4]) if len(st) > 4 else None for st in sets]
+    knots = (ctypes.c_void_p * ns)(*[None if k is None else k.ctypes.data for k in kn])
+    ktimes = (ctypes.c_void_p * ns)(*[None if k is None else k.ctypes.data for k in kt])
+    nknots = (ctypes.c_int * ns)(*[0 if k is None else k.size for k in kt])
     out = np.empty((n, 4))
     load().kso_polarized_image(ctypes.c_double(a), ctypes.c_double(theta_o), _p(alpha), _p(beta), ctypes.c_long(n), int(N), int(M),
-                               ns, kinds, nrows, nsplat, params, hyp, None, None, None, ctypes.c_double(gmax),
+                               ns, kinds, nrows, nsplat, params, hyp, knots, ktimes, nknots, ctypes.c_double(gmax),
                                ctypes.c_double(t_obs), ctypes.c_double(nu), ctypes.c_double(L), int(nmax), ctypes.c_double(slab), _p(out))
     return out
 

@@ -61,3 +61,73 @@ def test_winding_truncation_matches_oracle(oracle, nmax):
     print("winding", nmax, errs)
     # the all-FP32 march is held to 1e-3: its error comes from the march (axis-grazing rays), not the transport
     assert errs[ks.KS_FP64] < 1e-10 and errs[ks.KS_MIXED] < 1e-4 and errs[ks.KS_MIXED_FP32] < 1e-3, errs
+
+
+@pytest.mark.parametrize("prec,tol", [(ks.KS_FP64, 1e-10), (ks.KS_MIXED, 1e-4)])
+def test_knot_splats_match_oracle(oracle, prec, tol):
+    # KnotSplats (trajectories.jl:80-129): centres interpolated between trajectory knots at each
+    # emission time, beside pattern-rotating thermal splats; two frames, two frequencies
+    a, tho = 0.94, np.deg2rad(163.0)
+    rng = np.random.Generator(np.random.PCG64(32))
+    pk = scenes.thermal_params(rng, 4, a, rlo=3.0, rhi=7.0)
+    pk[3:6] = np.log(rng.uniform(0.8, 2.0, (3, 4)))
+    ktimes = np.array([-80.0, -30.0, 20.0, 60.0])
+    knots = scenes.trajectory_knots(pk, a, ktimes)
+    pt = scenes.thermal_params(rng, 3, a)
+    model = ks.CompositeModel(ks.KnotSplats(pk, knots, ktimes), ks.PolarizedSplats(pt))
+    cam = ks.Camera((-12.0, 12.0), (-12.0, 12.0), 16)
+    cache = ks.GeodesicCache(cam, 96)
+    ks.regenerate(cache, a, tho)
+    L = ks.gravitational_radius(4e6)
+    times, nus = [0.0, 20.0], [230e9, 690e9]
+    out = np.asarray(ks.render(cache, model, times, nus, L, precision=prec))
+    sets = [("knot", pk, None, knots, ktimes), ("thermal", pt, None)]
+    errs = {}
+    for v, nu in enumerate(nus):
+        for f, t in enumerate(times):
+            ref = oracle.polarized_image(a, tho, cam.alpha, cam.beta, 96, 64, sets, t, nu, L)
+            assert np.abs(ref).max() > 0
+            errs[(nu, t)] = rel_l2(out[v, f], ref)
+    # the knot splats alone are seen (their rows 1-3 are not used: moving them changes nothing)
+    pk2 = pk.copy()
+    pk2[0:3] += 50.0
+    out2 = np.asarray(ks.render(cache, ks.CompositeModel(ks.KnotSplats(pk2, knots, ktimes), ks.PolarizedSplats(pt)), times, nus, L,
+                                precision=prec))
+    print("knots", prec, errs)
+    assert max(errs.values()) < tol, errs
+    assert np.array_equal(out, out2)
+
+
+@pytest.mark.parametrize("prec,tol", [(ks.KS_FP64, 1e-10), (ks.KS_MIXED, 1e-4)])
+def test_uneven_sample_counts_match_oracle(oracle, prec, tol):
+    # every ray marched with its own N_j = clamp(64 ceil(768 tau_j / 64), 64, 256): identical to a
+    # uniform run at N = N_j for that ray (the reference's tiles, cache.jl:241-246)
+    c = scenes.config2(res=16, N=256)
+    rng = np.random.Generator(np.random.PCG64(33))
+    p = scenes.thermal_params(rng, 6, c["a"], rlo=3.0, rhi=9.0)
+    cam = ks.Camera((-14.0, 14.0), (-14.0, 14.0), 16)
+    cache = ks.GeodesicCache(cam, 256)
+    ks.regenerate(cache, c["a"], c["theta_o"], uneven=(768.0, 64))
+    nsorted = cache.nsamples_per_ray
+    nscreen = np.empty_like(nsorted)
+    nscreen[cache.perm] = nsorted
+    counts = np.unique(nscreen)
+    assert counts.size >= 2 and counts.min() >= 64 and counts.max() <= 256
+    times, nus = [0.0], [86e9, 345e9]
+    out = np.asarray(ks.render(cache, ks.PolarizedSplats(p), times, nus, c["L"], precision=prec))
+    errs = {}
+    for v, nu in enumerate(nus):
+        ref = np.zeros((cam.npix, 4))
+        for Nj in counts:
+            m = nscreen == Nj
+            ref[m] = oracle.polarized_image(c["a"], c["theta_o"], cam.alpha[m], cam.beta[m], int(Nj), 64, [("thermal", p, None)], 0.0, nu,
+                                            c["L"])
+        errs[nu] = rel_l2(out[v, 0], ref)
+    # the sample count the metric uses
+    cache.count_events(True)
+    ks.render(cache, ks.PolarizedSplats(p), times, nus, c["L"], precision=prec)
+    ev = cache.event_counts()
+    cache.count_events(False)
+    print("uneven", prec, counts, errs, ev["samples"], int(nsorted.sum()) * len(nus))
+    assert max(errs.values()) < tol, errs
+    assert ev["samples"] == int(nsorted.sum()) * len(nus)
