@@ -169,6 +169,20 @@ int ks_chi2_gradient(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, c
                      int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* data, const double* sigma,
                      double sigma_scalar, const uint8_t* mask, double* chi2, double* dparams, int32_t accumulate, double* image);
 
+/* J v of the image (jvp!, src/Fit/gauss_newton.jl:91-118, whose tails pass runs on parameters carrying
+ * duals along v): the directional derivatives of the observed Stokes images along ndir directions
+ * `dirs` (ndir x nparams, each direction laid out like dparams of ks_adjoint), into dimage
+ * (ndir x nfreq x nframes x npix x 4, pixels in `order`; the image itself into `image` when not NULL).
+ * Thermal polarized splats only; KS_FP64 carries FP64 duals, KS_MIXED FP32 duals; eight directions per
+ * pass (jacobian!'s chunk, gauss_newton.jl:432-479). */
+int ks_jvp(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+           int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* dirs, int32_t ndir, double* dimage,
+           int32_t order, double* image);
+
+/* normal_matrix(J) (src/Fit/gauss_newton.jl:486-494): A = J^T J of a row-major m x n Jacobian (FP64),
+ * A n x n. KS_FP64: FP64 tiles; KS_MIXED: the 3xTF32 tensor-core GEMM with FP32 accumulation. */
+int ks_normal_matrix(ks_context* ctx, const double* J, int64_t m, int64_t n, int32_t precision, double* A);
+
 /* sample_adjoint (src/Transfer/transport.jl:221-245) of n independent samples in FP64: for the summed
  * coefficients in (j 4, alpha 4, rho 3 per sample), the step length Dl, the adjoint w in front of the
  * sample and the tail R behind it, out[31 i ..] = O (16, row-major), E (4) and c-bar = (j-bar 4,

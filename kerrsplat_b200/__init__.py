@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -491,6 +491,39 @@ def chi2_gradient(cache, model, times, nus, L, data, sigma, mask=None, nmax=-1, 
                                              1 if user is not None else 0, _ptr(img) if img is not None else None))
     g = user if user is not None else _split_grad(model, buf)
     return (chi2.value, g, img) if return_image else (chi2.value, g)
+
+
+def jvp(cache, model, times, nus, L, dirs, nmax=-1, slab=0.0, precision=KS_FP64, order="screen", return_image=False):
+    """J v of the image (jvp!, gauss_newton.jl:91-118) along each direction in `dirs`: an array of
+    (ndir, 21, nsplat) (or (21, nsplat) for one direction; several sets: (ndir, nparams) flat, each
+    direction laid out like `adjoint`'s dparams). Returns (ndir, nfreq, nframes, npix, 4)."""
+    times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+    nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+    nt, nf = int(times.shape[0]), int(nus.shape[0])
+    nparams = sum(_lib.NROWS[s.kind] * s.nsplat for s in model.sets())
+    d = np.asarray(dirs, dtype=np.float64)
+    if d.ndim == 2 and d.shape[0] == 21 and len(model.sets()) == 1 and d.shape[1] == model.sets()[0].nsplat:
+        d = d[None]
+    if d.ndim == 3:   # (ndir, 21, nsplat) -> column-major per direction
+        d = np.ascontiguousarray(np.transpose(d, (0, 2, 1))).reshape(d.shape[0], -1)
+    d = np.ascontiguousarray(d.reshape(-1, nparams))
+    nd = d.shape[0]
+    arr, nsets, _keep = _set_array(model)
+    out = np.empty((nd, nf, nt, cache.npix, 4))
+    img = np.empty((nf, nt, cache.npix, 4)) if return_image else None
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_jvp(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision), int(nmax),
+                                   float(slab), _ptr(d), nd, _ptr(out), o, _ptr(img) if img is not None else None))
+    return (out, img) if return_image else out
+
+
+def normal_matrix(cache, J, precision=KS_FP64):
+    """normal_matrix(J) (gauss_newton.jl:486-494): J^T J of an (m, n) Jacobian on the GPU."""
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    m, n = J.shape
+    A = np.empty((n, n))
+    cache._check(cache._lib.ks_normal_matrix(cache._ctx, _ptr(J), m, n, _precision(precision), _ptr(A)))
+    return A
 
 
 def sample_adjoint(cache, coeffs, Dl, w, R, method=0):

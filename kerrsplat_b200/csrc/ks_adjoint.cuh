@@ -1042,3 +1042,234 @@ __global__ void k_unit_reduce2(const double* __restrict__ part, int nchunks, lon
 }
 
 }  // namespace
+
+// ---- forward mode: J v of the image (jvp!, src/Fit/gauss_newton.jl:91-118) ---------------------------
+//
+// The reference runs its tails pass on parameters that carry duals along v. Here the splat table of the
+// THERMAL21 splats is built as duals (each entry with its K directional derivatives), the march stays
+// plain (the geodesics do not depend on the splats), and the consumer composes (P, S) on duals: the
+// weight, the frame, the thermal fits, the cap, the invariants, the rotation and the exact step are
+// the same templates as the forward path, instantiated on Dual<S, K>.
+
+namespace {
+
+using namespace ks;
+
+// One THERMAL21 column and K tangent directions v[k * 21 + row] -> the dual table row. The cull radii
+// (ST_SUPP, ST_RHO) keep their values: the cull is a threshold, not a function of the parameters.
+template <class S, int K>
+__global__ void k_dual_table(int nsplat, const double* __restrict__ params, const double* __restrict__ dirs, long long dir_stride,
+                             const double* __restrict__ tab, const double* __restrict__ gtab, Dual<S, K>* __restrict__ dtab) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nsplat) return;
+    using D = Dual<double, K>;
+    const double* p = params + 21LL * i;
+    D q[21];
+    for (int r = 0; r < 21; ++r) {
+        q[r] = D(p[r]);
+        for (int k = 0; k < K; ++k) q[r].d[k] = dirs[k * dir_stride + 21LL * i + r];
+    }
+    const double* t0 = tab + (long long)i * ST_COUNT;
+    const double* g = gtab + (long long)i * GT_COUNT;
+    D o[ST_COUNT];
+    for (int e = 0; e < ST_COUNT; ++e) o[e] = D(t0[e]);
+    o[ST_CX] = q[0]; o[ST_CY] = q[1]; o[ST_CZ] = q[2];
+    o[ST_T0] = q[10]; o[ST_OMEGA] = q[20];
+    o[ST_ES1] = exp(-q[3]); o[ST_ES2] = exp(-q[4]); o[ST_ES3] = exp(-q[5]);
+    const D n = sqrt(q[6] * q[6] + q[7] * q[7] + q[8] * q[8] + q[9] * q[9]);
+    const D w = q[6] / n, x = q[7] / n, y = q[8] / n, z = q[9] / n;
+    o[ST_R0] = 1.0 - 2.0 * (y * y + z * z); o[ST_R1] = 2.0 * (x * y - w * z); o[ST_R2] = 2.0 * (x * z + w * y);
+    o[ST_R3] = 2.0 * (x * y + w * z); o[ST_R4] = 1.0 - 2.0 * (x * x + z * z); o[ST_R5] = 2.0 * (y * z - w * x);
+    o[ST_R6] = 2.0 * (x * z - w * y); o[ST_R7] = 2.0 * (y * z + w * x); o[ST_R8] = 1.0 - 2.0 * (x * x + y * y);
+    o[ST_INVW] = exp(-q[11]);
+    o[ST_NE] = exp(q[12]);
+    o[ST_TE] = exp(q[13]);
+    for (int k = 0; k < K; ++k) { o[ST_F0].d[k] = g[GT_DF0] * q[13].d[k]; o[ST_KR].d[k] = g[GT_DKR] * q[13].d[k]; }
+    o[ST_BMAG] = exp(q[14]);
+    if (t0[ST_BZERO] == 0.0) {
+        o[ST_BHX] = sin(q[15]) * cos(q[16]); o[ST_BHY] = sin(q[15]) * sin(q[16]); o[ST_BHZ] = cos(q[15]);
+    }
+    o[ST_U1] = q[17]; o[ST_U2] = q[18]; o[ST_U3] = q[19];
+    Dual<S, K>* out = dtab + (long long)i * ST_COUNT;
+    for (int e = 0; e < ST_COUNT; ++e) {
+        out[e].v = S(o[e].v);
+        for (int k = 0; k < K; ++k) out[e].d[k] = S(o[e].d[k]);
+    }
+}
+
+// The consumer of the JVP: RadiativeTransport on the dual table (transport.jl:171-198, step.jl:347).
+template <class S, int K>
+struct JvpSink {
+    using D = Dual<S, K>;
+    const D* tab; int ntot;
+    S t_obs, nu, Lnu, a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
+    int nmax;
+    D P[16], Sv[4];
+    S zprev; int wn; bool inside, crossed, zset;
+
+    __device__ void init() {
+        for (int q = 0; q < 16; ++q) P[q] = D(S((q % 5 == 0) ? 1 : 0));
+        for (int q = 0; q < 4; ++q) Sv[q] = D(S(0));
+        wn = 0; inside = false; crossed = false; zset = false; zprev = S(0);
+    }
+    __device__ void wind(S z) {   // step.jl:379-398
+        if (!zset) { zprev = z; zset = true; inside = fabs(z) < slab; crossed = false; return; }
+        bool inside_now = fabs(z) < slab;
+        bool crossing = zprev * z < S(0);
+        if (inside || inside_now) {
+            crossed = crossed || crossing;
+            if (inside && !inside_now) { if (crossed) wn += 1; crossed = false; }
+            else if (!inside && inside_now) { crossed = crossing; }
+            inside = inside_now;
+        } else if (crossing) {
+            wn += 1;
+        }
+        zprev = z;
+    }
+    __device__ void operator()(int, const Sample<double>& s64) {
+        const S r = S(s64.r), th = S(s64.theta), ph = S(s64.phi), ts = S(s64.t);
+        if (!(s64.ok && r > rh_lo)) return;
+        if (nmax >= 0) {
+            wind(r * cos(th));
+            if (wn > nmax) return;
+        }
+        S x, y, z, sth, cth;
+        ks_coords(a, r, th, ph, x, y, z, sth, cth);
+        const S t = t_obs - ts;
+        D in[11];
+        for (int q = 0; q < 11; ++q) in[q] = D(S(0));
+        bool active = false, have_frame = false;
+        SampleFrame<D> F;
+        for (int i = 0; i < ntot; ++i) {
+            const D* p = tab + (long long)i * ST_COUNT;
+            D q;
+            if (!splat_exponent(p, D(t), D(x), D(y), D(z), true, q)) continue;
+            const D G = exp(-q);
+            if (!(G > S(kWEIGHT_CUTOFF))) continue;
+            if (!have_frame) {
+                const SampleFrame<S> F0 = sample_frame(a, r, th, sth, cth, eta, lam, s64.nur, s64.nutheta);
+                for (int k = 0; k < 4; ++k) { F.pu[k] = D(F0.pu[k]); F.pz[k] = D(F0.pz[k]); }
+                F.lapse_inv = D(F0.lapse_inv); F.om_lapse = D(F0.om_lapse); F.sDS = D(F0.sDS); F.misS = D(F0.misS); F.ivarpi = D(F0.ivarpi);
+                F.r = D(F0.r); F.sth = D(F0.sth); F.cth = D(F0.cth); F.a = D(F0.a);
+                have_frame = true;
+            }
+            const LFrame<D> lf = local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != S(0),
+                                             D(alpha), D(beta), D(a_sin_tho));
+            const D nuf = D(nu) / lf.g;
+            const D thb = safe_acos(lf.cosB);
+            const Coef<D> cf = thermal(p[ST_NE] * G, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
+            if (!(cf.jI > S(0) || cf.aI > S(0) || cf.rQ != S(0) || cf.rV != S(0))) continue;
+            const D fe = cap_factor(cf.jI, cf.jQ, cf.jV, D(S(0.99)));
+            const D fa = cap_factor(cf.aI, cf.aQ, cf.aV, D(S(0.99)));
+            const D nh = nuf / S(kNU0);
+            const D i2 = D(S(1)) / (nh * nh);
+            const D s2c = sin(S(2) * lf.chi), c2c = cos(S(2) * lf.chi);
+            const D jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+            in[0] += cf.jI * i2; in[1] += jQ * c2c; in[2] += jQ * s2c; in[3] += cf.jV * fe * i2;
+            in[4] += nh * cf.aI; in[5] += aQ * c2c; in[6] += aQ * s2c; in[7] += cf.aV * fa * nh;
+            in[8] += rQ * c2c; in[9] += rQ * s2c; in[10] += nh * cf.rV;
+            active = true;
+        }
+        if (!active) return;
+        const S Sg = r * r + a * a * cos(th) * cos(th);
+        D O[16], E[4];
+        transfer_step(c_moments, in, in + 4, in + 8, D(Lnu * Sg * dtau), O, E);
+        D Pn[16];
+        for (int rr = 0; rr < 4; ++rr) {
+            Sv[rr] += P[4 * rr] * E[0] + P[4 * rr + 1] * E[1] + P[4 * rr + 2] * E[2] + P[4 * rr + 3] * E[3];
+            for (int q = 0; q < 4; ++q)
+                Pn[4 * rr + q] = P[4 * rr] * O[q] + P[4 * rr + 1] * O[4 + q] + P[4 * rr + 2] * O[8 + q] + P[4 * rr + 3] * O[12 + q];
+        }
+        for (int q = 0; q < 16; ++q) P[q] = Pn[q];
+    }
+};
+
+// One thread per (ray, combination): the image's K directional derivatives (sorted order)
+// out[((d * ncombo + c) * npix + j) * 4 + s], and the image itself in img.
+template <class S, int K>
+__global__ void __launch_bounds__(64) k_jvp(PlanView P, Spacetime st, long long npix, const Dual<S, K>* __restrict__ dtab, int ntot,
+                                            const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L, int nmax,
+                                            double slab, double* __restrict__ img, double* __restrict__ out) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= npix * ncombo) return;
+    const long long j = idx % npix;
+    const int c = int(idx / npix);
+    MarchRay<double> R = load_ray<double>(P, st, j);
+    JvpSink<S, K> sink;
+    sink.tab = dtab; sink.ntot = ntot;
+    sink.t_obs = S(ct[c]); sink.nu = S(cnu[c]);
+    const double nh = cnu[c] / kNU0;
+    sink.Lnu = S(L / nh);
+    sink.a = S(st.a); sink.rh_lo = S(st.rh * (1 + 1e-3)); sink.dtau = S(R.dtau);
+    sink.alpha = S(P.get(PF_ALPHA, j)); sink.beta = S(P.get(PF_BETA, j)); sink.eta = S(R.eta); sink.lam = S(R.lam);
+    sink.a_sin_tho = S(st.a * sin(st.thetao)); sink.slab = S(slab); sink.nmax = nmax;
+    sink.init();
+    double rt, rp;
+    march(P, st, j, R, sink, rt, rp);
+    const double n3 = nh * nh * nh;
+    for (int s = 0; s < 4; ++s) {
+        img[(c * npix + j) * 4 + s] = double(sink.Sv[s].v) * n3;
+        for (int d = 0; d < K; ++d) out[(((long long)d * ncombo + c) * npix + j) * 4 + s] = double(sink.Sv[s].d[d]) * n3;
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// A = J^T J (normal_matrix, gauss_newton.jl:486-494) of a row-major m x n FP64 Jacobian, FP64 tiles
+// of 32 x 32 with the shared k-slab; only the upper triangle's tiles are computed and mirrored.
+__global__ void k_normal_fp64(long long m, int n, const double* __restrict__ J, double* __restrict__ A) {
+    __shared__ double Ja[32][33], Jb[32][33];
+    const int bi = blockIdx.y, bj = blockIdx.x;
+    if (bj < bi) return;
+    const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long k0 = 0; k0 < m; k0 += 32) {
+        for (int q = 0; q < 4; ++q) {
+            const int kk = ty + 8 * q;
+            const long long r = k0 + kk;
+            const int ca = bi * 32 + tx, cb = bj * 32 + tx;
+            Ja[kk][tx] = (r < m && ca < n) ? J[r * n + ca] : 0.0;
+            Jb[kk][tx] = (r < m && cb < n) ? J[r * n + cb] : 0.0;
+        }
+        __syncthreads();
+        for (int kk = 0; kk < 32; ++kk) {
+            const double b = Jb[kk][tx];
+            for (int q = 0; q < 4; ++q) acc[q] += Ja[kk][ty + 8 * q] * b;
+        }
+        __syncthreads();
+    }
+    for (int q = 0; q < 4; ++q) {
+        const int i = bi * 32 + ty + 8 * q, j = bj * 32 + tx;
+        if (i < n && j < n) { A[(long long)i * n + j] = acc[q]; A[(long long)j * n + i] = acc[q]; }
+    }
+}
+
+__global__ void k_to_f32(long long n, const double* __restrict__ x, float* __restrict__ y) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q < n) y[q] = float(x[q]);
+}
+// row-major m x n (double) -> row-major n x m (float)
+__global__ void k_transpose_f32(long long m, int n, const double* __restrict__ x, float* __restrict__ y) {
+    __shared__ float t[32][33];
+    const long long r0 = (long long)blockIdx.y * 32;
+    const int c0 = blockIdx.x * 32;
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+        const long long r = r0 + q;
+        const int cc = c0 + threadIdx.x;
+        t[q][threadIdx.x] = (r < m && cc < n) ? float(x[r * n + cc]) : 0.f;
+    }
+    __syncthreads();
+    for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+        const int cc = c0 + q;
+        const long long r = r0 + threadIdx.x;
+        if (cc < n && r < m) y[(long long)cc * m + r] = t[threadIdx.x][q];
+    }
+}
+__global__ void k_to_f64(long long n, const float* __restrict__ x, double* __restrict__ y) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q < n) y[q] = double(x[q]);
+}
+
+}  // namespace

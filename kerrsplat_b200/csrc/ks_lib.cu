@@ -254,6 +254,7 @@ struct SetDesc {
     const double* hyp;
     double gmax;
     int koff, nk;                     // knot splats: offset of the set's first knot record, knot count
+    const double* knots;              // the knot array (device)
 };
 
 __global__ void k_splat_table(SetDesc d, double* __restrict__ tab) {
@@ -278,6 +279,20 @@ __global__ void k_splat_table(SetDesc d, double* __restrict__ tab) {
     o[ST_RHO] = sqrt(p[0] * p[0] + p[1] * p[1]);
     o[ST_KOFF] = d.kind == KS_KNOT21 ? double(d.koff + 4 * d.nk * i) : 0.0;
     o[ST_NK] = d.kind == KS_KNOT21 ? double(d.nk) : 0.0;
+    if (d.kind == KS_KNOT21) {
+        // every interpolated centre lies in the box of the knots: a point farther than the box's
+        // half-diagonal plus the support radius from its centre is outside the support at any time
+        const double* kn = d.knots + d.koff + 4 * d.nk * i;
+        double lo[3], hi[3], half2 = 0.0;
+        for (int q = 0; q < 3; ++q) {
+            lo[q] = hi[q] = kn[(q + 1) * d.nk];
+            for (int k = 1; k < d.nk; ++k) { lo[q] = fmin(lo[q], kn[(q + 1) * d.nk + k]); hi[q] = fmax(hi[q], kn[(q + 1) * d.nk + k]); }
+            half2 += 0.25 * (hi[q] - lo[q]) * (hi[q] - lo[q]);
+        }
+        o[ST_CX] = 0.5 * (lo[0] + hi[0]); o[ST_CY] = 0.5 * (lo[1] + hi[1]); o[ST_CZ] = 0.5 * (lo[2] + hi[2]);
+        const double rb = sqrt(half2) + sqrt(o[ST_SUPP]);
+        o[ST_RHO] = rb * rb;   // the bounding radius squared (knot splats use no pattern circle)
+    }
     if (d.kind == KS_THIN14) { o[ST_LOGA] = p[12]; return; }
     o[ST_NE] = exp(p[12]);
     double Bmag, thB, phB, u1, u2, u3;
@@ -651,7 +666,7 @@ struct ks_context {
     // adjoint: gradient table, stored FP64 samples (plain path), cutoffs, tails, per-ray slots,
     // seeds, chi^2 partials; mixed path: per-sample states, activity, segment bounds, unit partials
     DevBuf gtab, samples, kstop, tails, slots, dgrad, seeds, chi_part, chi_val, dstage;
-    DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part;
+    DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part, jvp_tab, jvp_in, jvp_out;
     bool samples_ready = false;
     int nkv = 0;                            // knot values after the splat table in `tab`
     MixedJob last_job{};                    // the segmentation of the last mixed forward pass
@@ -819,7 +834,7 @@ int build_tables(ks_context* c, const ks_splat_set* sets, int nsets, int* ntot_o
             dh = hd;
         }
         SetDesc d{S.kind, nr, S.nsplat, first, tmp.as<const double>(), (const double*)dh, S.gamma_max > 0 ? S.gamma_max : 1e5, koff[s],
-                  S.kind == KS_KNOT21 ? S.nknots : 0};
+                  S.kind == KS_KNOT21 ? S.nknots : 0, c->tab.as<const double>() + size_t(ntot) * ST_COUNT};
         k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
         c->launches++;
         KS_CUDA(c, cudaGetLastError());
@@ -1340,6 +1355,10 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
 // ---- the adjoint (src/Splats/dual_gradient.jl, src/Fit/Fit.jl:451-577) --------------------------------
 
 namespace {
+void gemm(ks_context* c, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb, float* C, long long ldc);
+}
+
+namespace {
 
 __global__ void k_accumulate(double* __restrict__ dst, const double* __restrict__ src, long long n, int accumulate) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1646,6 +1665,154 @@ int ks_chi2_gradient(ks_context* c, const ks_splat_set* sets, int32_t nsets, con
                        sigma_scalar, mask, chi2, dparams, accumulate, image);
 }
 
+}  // extern "C"
+
+namespace {
+
+// J v of the image for one chunk of K directions (dirs: K x nparams, each laid out like dparams)
+template <class S, int K>
+int jvp_chunk(ks_context* c, int ntot, const double* dparams_dev, const double* ddirs, long long dstride, const double* dct,
+              const double* dcn, int ncombo, double L, int nmax, double slab, double* img_sorted, double* out_sorted) {
+    KS_CUDA(c, c->jvp_tab.ensure(size_t(std::max(ntot, 1)) * ST_COUNT * sizeof(Dual<S, K>)));
+    Dual<S, K>* dt = c->jvp_tab.as<Dual<S, K>>();
+    if (ntot > 0) {
+        k_dual_table<S, K><<<nblocks(ntot, 64), 64, 0, c->stream>>>(ntot, dparams_dev, ddirs, dstride, c->tab.as<double>(),
+                                                                    c->gtab.as<double>(), dt);
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
+    const long long nrc = c->npix * ncombo;
+    k_jvp<S, K><<<nblocks(nrc, 64), 64, 0, c->stream>>>(plan_view(c), c->st, c->npix, dt, ntot, dct, dcn, ncombo, L, nmax, slab, img_sorted,
+                                                        out_sorted);
+    c->launches++;
+    c->adjoint_launches++;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ks_jvp(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus, int32_t nfreq,
+           double L, int32_t precision, int32_t nmax, double slab, const double* dirs, int32_t ndir, double* dimage, int32_t order,
+           double* image) {
+    if (!c || !dirs || !dimage || ndir < 1) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    if (nsets < 1 || !sets) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
+    if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d for the JVP", precision);
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    std::vector<double> ht(nframes), hnu(nfreq);
+    KS_CUDA(c, cudaMemcpy(ht.data(), times, nframes * sizeof(double), cudaMemcpyDefault));
+    KS_CUDA(c, cudaMemcpy(hnu.data(), nus, nfreq * sizeof(double), cudaMemcpyDefault));
+    for (double v : ht) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite observation time");
+    for (double v : hnu) if (!(std::isfinite(v) && v > 0)) return fail(c, KS_ERR_NONFINITE, "frequencies must be finite and positive");
+    int ntot = 0;
+    {
+        int s = build_tables(c, sets, nsets, &ntot, true);
+        if (s) return s;
+    }
+    // the raw parameters of all sets, concatenated (21 x ntot) on the device
+    const long long np = (long long)ntot * 21;
+    std::vector<double> hp(np);
+    {
+        long long off = 0;
+        for (int s = 0; s < nsets; ++s) {
+            const size_t cnt = size_t(21) * sets[s].nsplat;
+            if (cnt) KS_CUDA(c, cudaMemcpy(hp.data() + off, sets[s].params, cnt * sizeof(double), cudaMemcpyDefault));
+            off += cnt;
+        }
+    }
+    const int K = ndir == 1 ? 1 : 8;
+    const int nchunk = (ndir + K - 1) / K;
+    // directions padded to whole chunks
+    std::vector<double> hd(size_t(nchunk) * K * np, 0.0);
+    KS_CUDA(c, cudaMemcpy(hd.data(), dirs, size_t(ndir) * np * sizeof(double), cudaMemcpyDefault));
+    for (double v : hd) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite direction");
+    KS_CUDA(c, c->jvp_in.ensure((hp.size() + hd.size() + 1) * sizeof(double)));
+    double* dp = c->jvp_in.as<double>();
+    KS_CUDA(c, cudaMemcpyAsync(dp, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    KS_CUDA(c, cudaMemcpyAsync(dp + np, hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const int ncombo = nframes * nfreq;
+    std::vector<double> hc(2 * size_t(ncombo));
+    for (int fv = 0; fv < nfreq; ++fv)
+        for (int ft = 0; ft < nframes; ++ft) {
+            hc[size_t(fv) * nframes + ft] = ht[ft];
+            hc[ncombo + size_t(fv) * nframes + ft] = hnu[fv];
+        }
+    KS_CUDA(c, c->combos.ensure(hc.size() * sizeof(double)));
+    KS_CUDA(c, cudaMemcpyAsync(c->combos.p, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double* dct = c->combos.as<double>();
+    const double* dcn = dct + ncombo;
+    const long long nrc = c->npix * ncombo;
+    KS_CUDA(c, c->out_sorted.ensure(size_t(nrc) * 4 * sizeof(double)));
+    KS_CUDA(c, c->jvp_out.ensure(size_t(K) * nrc * 4 * sizeof(double)));
+    cudaEventRecord(c->ev0, c->stream);
+    for (int ch = 0; ch < nchunk; ++ch) {
+        const double* dd = dp + np + (long long)ch * K * np;
+        int s;
+        if (precision == KS_FP64)
+            s = K == 1 ? jvp_chunk<double, 1>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>())
+                       : jvp_chunk<double, 8>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>());
+        else
+            s = K == 1 ? jvp_chunk<float, 1>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>())
+                       : jvp_chunk<float, 8>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>());
+        if (s) return s;
+        const int nd = std::min(K, ndir - ch * K);
+        s = emit(c, c->jvp_out.as<double>(), 4, int(nd * ncombo), order, dimage + (long long)ch * K * nrc * 4);
+        if (s) return s;
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    if (image) {
+        int s = emit(c, c->out_sorted.as<double>(), 4, ncombo, order, image);
+        if (s) return s;
+    }
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->adjoint_ms += ms;
+    return KS_OK;
+}
+
+int ks_normal_matrix(ks_context* c, const double* J, int64_t m, int64_t n, int32_t precision, double* A) {
+    if (!c || !J || !A || m < 1 || n < 1) return KS_ERR_ARGUMENT;
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    if (n > (1 << 16)) return fail(c, KS_ERR_ARGUMENT, "too many columns (%lld)", (long long)n);
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const double* dJ = nullptr;
+    {
+        int s = stage_dev(c, c->dstage, J, size_t(m) * n, &dJ);
+        if (s) return s;
+    }
+    const bool dev = is_device_ptr(A);
+    double* dA = A;
+    if (!dev) { KS_CUDA(c, c->stage_out.ensure(size_t(n) * n * sizeof(double))); dA = c->stage_out.as<double>(); }
+    const int nb = int((n + 31) / 32);
+    if (precision == KS_FP64) {
+        k_normal_fp64<<<dim3(nb, nb), dim3(32, 8), 0, c->stream>>>(m, int(n), dJ, dA);
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+    } else {
+        // 3xTF32 tensor-core GEMM: A = J^T J from a transposed FP32 copy
+        KS_CUDA(c, c->dft_a.ensure(size_t(m) * n * 2 * sizeof(float) + size_t(n) * n * sizeof(float)));
+        float* Jt = c->dft_a.as<float>();
+        float* Jf = Jt + size_t(m) * n;
+        float* Af = Jf + size_t(m) * n;
+        k_transpose_f32<<<dim3(nb, unsigned((m + 31) / 32)), dim3(32, 8), 0, c->stream>>>(m, int(n), dJ, Jt);
+        k_to_f32<<<nblocks(m * n, 256), 256, 0, c->stream>>>(m * n, dJ, Jf);
+        gemm(c, int(n), int(n), int(m), Jt, m, Jf, n, Af, n);
+        k_to_f64<<<nblocks(n * n, 256), 256, 0, c->stream>>>(n * n, Af, dA);
+        c->launches += 3;
+        KS_CUDA(c, cudaGetLastError());
+    }
+    if (!dev) KS_CUDA(c, cudaMemcpyAsync(A, dA, size_t(n) * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return KS_OK;
+}
+
 int ks_sample_adjoint(ks_context* c, int64_t n, const double* in, const double* Dl, const double* w, const double* R, int32_t method,
                       double* out) {
     if (!c || n < 0 || (n > 0 && (!in || !Dl || !w || !R || !out))) return KS_ERR_ARGUMENT;
@@ -1677,6 +1844,8 @@ int ks_adjoint_stats(ks_context* c, double* adjoint_ms, long long* launches, int
     if (reset) { c->adjoint_ms = 0.0; c->adjoint_launches = 0; }
     return KS_OK;
 }
+
+}  // extern "C"
 
 // ---- visibilities (device_visibilities.jl:53-111) ------------------------------------------------
 
@@ -1878,6 +2047,8 @@ static int noalloc_table(ks_context* c, double** tab) {
     *tab = static_cast<double*>(g_noalloc_addr[c->device]);
     return KS_OK;
 }
+
+extern "C" {
 
 int ks_thin_image_noalloc(ks_context* c, const double* params, int32_t nsplat, double t_obs, int32_t precision, double* out,
                           int32_t order) {

@@ -225,6 +225,8 @@ struct MixedSink {
                         if (dr * dr + dz * dz > p[ST_SUPP]) continue;
                         if (!splat_exponent(p, t, x, y, z, true, q)) continue;
                     } else {
+                        const float dx = x - p[ST_CX], dy = y - p[ST_CY], dz2 = z - p[ST_CZ];
+                        if (dx * dx + dy * dy + dz2 * dz2 > p[ST_RHO]) continue;   // outside the knots' bounding sphere
                         knot_exponent(p, knots, t, x, y, z, q);
                     }
                     ev[3]++;

@@ -131,7 +131,9 @@ __device__ __forceinline__ Coef<T> thermal(T ne, T Te, T f0, T kr, T B, T nu, T 
 // the splat's Gamma-function products, gspan = gmin^(1-p) - gmax^(1-p)
 template <class T>
 __device__ __forceinline__ Coef<T> powerlaw(T ne, T p, T gmin, T gspan, T gamj, T gama, T B, T nu, T th) {
-    T st = sin(th), ct = cos(th);
+    // the fits divide by sin(theta) and raise it to negative powers: a field along the ray (a pitch
+    // angle that rounds to 0 or pi, common in FP32) is evaluated 1e-6 from the axis
+    T st = fmax(sin(th), T(1e-6)), ct = cos(th);
     const T PI = kpi<T>();
     T nc = T(kEE) * B / (T(2) * PI * T(kME) * T(kCL));
     T pref = ne * T(kEE) * T(kEE) * nc / T(kCL);
@@ -176,7 +178,7 @@ __device__ __forceinline__ T kappa_rhoV_fit(int i, T w, T X) {
 // gk2 = Gamma(2 + k/2), kb = K0/(K2 + 1e-40) at 1/w (per splat)
 template <class T>
 __device__ __forceinline__ Coef<T> kappa(T ne, T kap, T w, T hyp, T g43, T g2, T gq, T gp, T gk2, T kb, T B, T nu, T th) {
-    T st = sin(th), ct = cos(th);
+    T st = fmax(sin(th), T(1e-6)), ct = cos(th);   // as powerlaw: a field along the ray is evaluated 1e-6 from the axis
     const T PI = kpi<T>();
     const T small = T(1e-40);  // FP32: subnormal-flushes to 0; the guard below then reads |N_high| < 0
     T nc = T(kEE) * B / (T(2) * PI * T(kME) * T(kCL));
@@ -600,7 +602,12 @@ __device__ __forceinline__ void knot_exponent(const T* p, const T* knots, T t, T
 // The exponent of any splat of a polarized scene: false when the support sphere culls it.
 template <class T>
 __device__ __forceinline__ bool any_exponent(const T* p, const T* knots, T t, T x, T y, T z, T& q) {
-    if (int(p[ST_KIND]) == KS_KNOT21) { knot_exponent(p, knots, t, x, y, z, q); return true; }
+    if (int(p[ST_KIND]) == KS_KNOT21) {
+        const T dx = x - p[ST_CX], dy = y - p[ST_CY], dz = z - p[ST_CZ];
+        if (dx * dx + dy * dy + dz * dz > p[ST_RHO]) return false;   // outside the knots' bounding sphere
+        knot_exponent(p, knots, t, x, y, z, q);
+        return true;
+    }
     return splat_exponent(p, t, x, y, z, true, q);
 }
 

@@ -199,3 +199,43 @@ def test_sample_adjoint_structured_matches_duals_and_fd(oracle):
             cm[k] -= h
             fdv = (q(cp) - q(cm)) / (2 * h)
             assert abs(c0[i, k] - fdv) <= 1e-6 * den[i, 0] + 1e-6 * abs(fdv), (i, k, c0[i, k], fdv)
+
+
+@pytest.mark.parametrize("prec,tol", [(ks.KS_FP64, 1e-6), (ks.KS_MIXED, 2e-3)])
+def test_jvp_matches_finite_differences_and_adjoint(scene, oracle, prec, tol):
+    """jvp! (gauss_newton.jl:91-118): J v of the image along random directions against central
+    differences of the oracle image, and <dstokes, J v> = <J^T dstokes, v> against the adjoint."""
+    s = scene
+    c, cam = s["c"], s["cam"]
+    m = ks.PolarizedSplats(s["p"])
+    rng = np.random.Generator(np.random.PCG64(27))
+    dirs = rng.standard_normal((3, 21, NS)) * np.maximum(np.abs(s["p"]), 0.1)[None]
+    jv = ks.jvp(s["cache"], m, s["times"], s["nus"], c["L"], dirs, precision=prec)
+    g = ks.adjoint(s["cache"], m, s["times"], s["nus"], c["L"], s["ds"], precision=ks.KS_FP64)
+    for d in range(3):
+        h = 1e-7
+        fd = np.zeros_like(jv[d])
+        for v, nu in enumerate(s["nus"]):
+            for f, t in enumerate(s["times"]):
+                ip = oracle.polarized_image(c["a"], c["theta_o"], cam.alpha, cam.beta, N, c["M"], [("thermal", s["p"] + h * dirs[d], None)], t,
+                                            nu, c["L"])
+                im = oracle.polarized_image(c["a"], c["theta_o"], cam.alpha, cam.beta, N, c["M"], [("thermal", s["p"] - h * dirs[d], None)], t,
+                                            nu, c["L"])
+                fd[v, f] = (ip - im) / (2 * h)
+        e = rel_l2(jv[d], fd)
+        dual = float(np.sum(s["ds"] * jv[d]))
+        ref = float(np.sum(g * dirs[d]))
+        print("jvp", prec, d, "rel L2 vs FD", e, "duality", dual, ref)
+        assert e < tol, (d, e)
+        assert abs(dual - ref) <= tol * abs(ref) + 1e-30, (d, dual, ref)
+
+
+@pytest.mark.parametrize("prec,tol", [(ks.KS_FP64, 1e-12), (ks.KS_MIXED, 1e-5)])
+def test_normal_matrix(prec, tol):
+    cam = ks.Camera((-1.0, 1.0), (-1.0, 1.0), 2)
+    cache = ks.GeodesicCache(cam, 8)
+    rng = np.random.Generator(np.random.PCG64(28))
+    J = rng.standard_normal((1000, 77)) * np.exp(rng.uniform(-2, 2, 77))[None]
+    A = ks.normal_matrix(cache, J, precision=prec)
+    ref = J.T @ J
+    assert np.max(np.abs(A - ref)) <= tol * np.abs(ref).max()
