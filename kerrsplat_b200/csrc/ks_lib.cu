@@ -924,6 +924,7 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     job.nchunks = (c->npix + 31) / 32;
     job.nmax = nmax; job.slab = float(slab); job.L = L;
     job.nkv = c->nkv;
+    job.ch = CH;
     // the block size with the most resident warps (the per-warp shared memory sets the limit)
     const int w384 = consume_blocks<CH, 384, KM>(c, ntot) * 12, w256 = consume_blocks<CH, 256, KM>(c, ntot) * 8,
               w128 = consume_blocks<CH, 128, KM>(c, ntot) * 4;
@@ -936,16 +937,21 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     (void)M;
 }
 
+// The frequencies of a work unit: all of them (up to four) share the march and the splat tests. (Two
+// frequencies per unit, which doubles the resident warps of a 256-splat table, measured 8% slower on
+// the movie: the tests it repeats cost more than the occupancy it gains.)
+template <int KM>
+int launch_mixed_km(ks_context* c, int ntot, int nframes, int nfreq, double L, int nmax, double slab) {
+    if (nfreq >= 4) return launch_mixed_ch<4, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (nfreq == 3) return launch_mixed_ch<3, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (nfreq == 2) return launch_mixed_ch<2, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
+    return launch_mixed_ch<1, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
+}
+
 int launch_mixed(ks_context* c, int ntot, const double* ht, int nframes, int nfreq, double L, int nmax, double slab, bool thermal_only) {
     (void)ht;
-    if (thermal_only) {
-        if (nfreq >= 4) return launch_mixed_ch<4, 1>(c, ntot, nframes, nfreq, L, nmax, slab);
-        if (nfreq == 3) return launch_mixed_ch<3, 1>(c, ntot, nframes, nfreq, L, nmax, slab);
-        return launch_mixed_ch<1, 1>(c, ntot, nframes, nfreq, L, nmax, slab);
-    }
-    if (nfreq >= 4) return launch_mixed_ch<4, 7>(c, ntot, nframes, nfreq, L, nmax, slab);
-    if (nfreq == 3) return launch_mixed_ch<3, 7>(c, ntot, nframes, nfreq, L, nmax, slab);
-    return launch_mixed_ch<1, 7>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (ntot > 32 * kMaxSplatWords) return fail(c, KS_ERR_ARGUMENT, "the mixed path takes at most %d splats (%d)", 32 * kMaxSplatWords, ntot);
+    return thermal_only ? launch_mixed_km<1>(c, ntot, nframes, nfreq, L, nmax, slab) : launch_mixed_km<7>(c, ntot, nframes, nfreq, L, nmax, slab);
 }
 
 // Write `nvec` x npix x width doubles from the sorted device buffer to `out` (host or device) in `order`.
@@ -1599,9 +1605,11 @@ int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double
     }
     // 3. reverse pass and the deterministic reduction
     if (ntot > 0 && mixed) {
-        const int nf = nfreq;
-        int s = nf >= 4 ? launch_adjoint_mixed_ch<4>(c, ntot, dtimes, dfreqs)
-                        : (nf == 3 ? launch_adjoint_mixed_ch<3>(c, ntot, dtimes, dfreqs) : launch_adjoint_mixed_ch<1>(c, ntot, dtimes, dfreqs));
+        // the reverse pass groups frequencies as the forward pass did
+        const int ch = c->last_job.ch;
+        int s = ch == 4 ? launch_adjoint_mixed_ch<4>(c, ntot, dtimes, dfreqs)
+                        : (ch == 3 ? launch_adjoint_mixed_ch<3>(c, ntot, dtimes, dfreqs)
+                                   : (ch == 2 ? launch_adjoint_mixed_ch<2>(c, ntot, dtimes, dfreqs) : launch_adjoint_mixed_ch<1>(c, ntot, dtimes, dfreqs)));
         if (s) return s;
     } else if (ntot > 0) {
         const size_t slot_bytes = size_t(GR_COUNT) * ntot * nrc * sizeof(double);

@@ -27,6 +27,49 @@ constexpr float kQCUT = 13.815510557964274f;   // -ln(WEIGHT_CUTOFF): G > 1e-6 <
 enum SampleField { SF_X, SF_Y, SF_Z, SF_T, SF_PU0, SF_PU1, SF_PU2, SF_PU3, SF_PZ0, SF_PZ1, SF_PZ2, SF_PZ3,
                    SF_LI, SF_OL, SF_SDS, SF_MIS, SF_IVP, SF_R, SF_STH, SF_CTH, SF_SG, SF_ALPHA, SF_BETA, SF_COUNT };
 constexpr int kSF = SF_COUNT;                   // floats per lane of sample data
+constexpr int kMaxSplatWords = 16;              // candidate masks cover up to 512 splats
+
+// The bounds of a work unit's samples (quasi-Cartesian KS box, cylindrical radius and height) and the
+// splats whose support can reach them: a pattern-rotating splat's support lies within its support
+// radius of the circle its centre runs on (rho = ST_RHO, z = ST_CZ), a knot splat's within its
+// bounding sphere (centre ST_CX..CZ, radius^2 ST_RHO). Splats outside are below the weight cutoff at
+// every sample of the unit, so the per-sample tests skip them (the same result, fewer tests).
+struct UnitBox { float xlo, xhi, ylo, yhi, zlo, zhi, rlo, rhi; };
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, d));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, d));
+    return v;
+}
+
+// the candidate mask words of a unit (all lanes call it; cand gets ceil(ntot / 32) words)
+__device__ __forceinline__ void unit_candidates(const float* tab, int ntot, const UnitBox& b, int lane, unsigned* cand) {
+    for (int s0 = 0; s0 < ntot; s0 += 32) {
+        const int i = s0 + lane;
+        bool keep = false;
+        if (i < ntot && b.xlo <= b.xhi) {
+            const float* p = tab + i * ST_COUNT;
+            if (int(p[ST_KIND]) == KS_KNOT21) {
+                const float dx = fmaxf(fmaxf(b.xlo - p[ST_CX], p[ST_CX] - b.xhi), 0.f);
+                const float dy = fmaxf(fmaxf(b.ylo - p[ST_CY], p[ST_CY] - b.yhi), 0.f);
+                const float dz = fmaxf(fmaxf(b.zlo - p[ST_CZ], p[ST_CZ] - b.zhi), 0.f);
+                keep = dx * dx + dy * dy + dz * dz <= p[ST_RHO] * 1.0001f;
+            } else {
+                const float dr = fmaxf(fmaxf(b.rlo - p[ST_RHO], p[ST_RHO] - b.rhi), 0.f);
+                const float dz = fmaxf(fmaxf(b.zlo - p[ST_CZ], p[ST_CZ] - b.zhi), 0.f);
+                keep = dr * dr + dz * dz <= p[ST_SUPP] * 1.0001f;
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) cand[s0 >> 5] = m;
+    }
+    __syncwarp();
+}
 
 template <int CH>
 struct MixedSmem {
@@ -34,7 +77,7 @@ struct MixedSmem {
     static constexpr int kSampleBytes = 32 * kSF * 4;
     static constexpr int kItemBytes = 32 * 32 * 2 > 32 * 20 * 4 ? 32 * 32 * 2 : 32 * 20 * 4;   // item list | step results
     static constexpr int kResBytes = 32 * CH * 12 * 4;                                          // pair results | step inputs
-    static constexpr int kMetaBytes = 32 * 4 * 2;
+    static constexpr int kMetaBytes = 32 * 4 * 2 + kMaxSplatWords * 4;                           // step offsets, bits; candidate mask
     static constexpr int kStateBytes = 32 * CH * 20 * 4;                                        // P (16) and S (4) per lane and frequency
     static constexpr int kWarpBytes = kSampleBytes + kItemBytes + kResBytes + kMetaBytes + kStateBytes;
     // the splat table and the knot array (nkv floats) come first
@@ -109,6 +152,7 @@ struct MixedSink {
     float* state;     // this lane's P/S column of the warp's [CH * 20][32] array
     int* meta_off;    // this warp's first step item per lane [32]
     unsigned* meta_bits;   // and active-frequency bits [32]
+    const unsigned* cand;  // the unit's candidate splats (unit_candidates)
     float zprev; int wn; bool inside, crossed, zset;
     unsigned int ev[7];
     // the adjoint's forward pass (null otherwise): at every active (sample, lane, frequency) the state
@@ -209,11 +253,15 @@ struct MixedSink {
             for (int q = 0; q < 11; ++q) acc[c][q] = 0.f;
         __syncwarp();
         for (int s0 = 0; s0 < ntot; s0 += 32) {
-            // 1. tests: support sphere, then the weight cutoff
+            const unsigned cm = cand[s0 >> 5];
+            if (cm == 0u) continue;
+            // 1. tests of the unit's candidates: support sphere, then the weight cutoff
             unsigned mask = 0u;
             if (valid) {
-                const int nb = min(32, ntot - s0);
-                for (int b = 0; b < nb; ++b) {
+                unsigned cb = cm;
+                while (cb) {
+                    const int b = __ffs(cb) - 1;
+                    cb &= cb - 1;
                     const float* p = tab + (s0 + b) * ST_COUNT;
                     float q;
                     ev[2]++;
@@ -428,6 +476,7 @@ struct MixedJob {
     float* gstate = nullptr;          // the adjoint's per-sample states (see MixedSink)
     unsigned char* gact = nullptr;
     int nkv = 0;                      // knot values after the splat table
+    int ch = 1;                       // frequencies per work unit
 };
 
 template <int CH, int NT, int KM>
@@ -489,9 +538,26 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         sink.res = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes);
         sink.meta_off = reinterpret_cast<int*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes + MixedSmem<CH>::kResBytes);
         sink.meta_bits = reinterpret_cast<unsigned*>(sink.meta_off + 32);
+        unsigned* cand = sink.meta_bits + 32;
+        sink.cand = cand;
         sink.state = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes + MixedSmem<CH>::kResBytes +
                                               MixedSmem<CH>::kMetaBytes) + lane;
         sink.init();
+        {
+            // the unit's bounds and candidate splats
+            UnitBox b{3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f};
+            const float* bp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
+            for (int k = k0; k < k1; ++k, bp += SM_COUNT * npad) {
+                if (!live || k > sink.nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
+                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
+                const float rho = sqrtf(x * x + y * y);
+                b.xlo = fminf(b.xlo, x); b.xhi = fmaxf(b.xhi, x); b.ylo = fminf(b.ylo, y); b.yhi = fmaxf(b.yhi, y);
+                b.zlo = fminf(b.zlo, z); b.zhi = fmaxf(b.zhi, z); b.rlo = fminf(b.rlo, rho); b.rhi = fmaxf(b.rhi, rho);
+            }
+            b.xlo = warp_min(b.xlo); b.xhi = warp_max(b.xhi); b.ylo = warp_min(b.ylo); b.yhi = warp_max(b.yhi);
+            b.zlo = warp_min(b.zlo); b.zhi = warp_max(b.zhi); b.rlo = warp_min(b.rlo); b.rhi = warp_max(b.rhi);
+            unit_candidates(tab, ntot, b, lane, cand);
+        }
         const float* sp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
         for (int k = k0; k < k1; ++k, sp += SM_COUNT * npad) {
             sink.kcur = k;
