@@ -179,6 +179,16 @@ int ks_jvp(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const doubl
            int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* dirs, int32_t ndir, double* dimage,
            int32_t order, double* image);
 
+/* The image's derivatives with respect to the spacetime block (a, theta_o, ln L) that
+ * spacetime_valgrad (src/Fit/joint.jl:74-82) takes with three-partial duals through regenerate! and the
+ * transport: dimage (3 x nfreq x nframes x npix x 4, screen order) = d/da, d/dtheta_o by central
+ * differences of the render with steps h_a, h_theta (four regenerates, the context regenerated back at
+ * (a, theta_o) before the call returns), and d/d(ln L) exactly (a dual on the step length, through the
+ * J v pass) for thermal scenes, by central differences otherwise. image (optional): the image. */
+int ks_spacetime_derivatives(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes,
+                             const double* nus, int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, double h_a,
+                             double h_theta, double* dimage, double* image);
+
 /* normal_matrix(J) (src/Fit/gauss_newton.jl:486-494): A = J^T J of a row-major m x n Jacobian (FP64),
  * A n x n. KS_FP64: FP64 tiles; KS_MIXED: the 3xTF32 tensor-core GEMM with FP32 accumulation. */
 int ks_normal_matrix(ks_context* ctx, const double* J, int64_t m, int64_t n, int32_t precision, double* A);

@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -514,6 +514,22 @@ def jvp(cache, model, times, nus, L, dirs, nmax=-1, slab=0.0, precision=KS_FP64,
     o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
     cache._check(cache._lib.ks_jvp(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision), int(nmax),
                                    float(slab), _ptr(d), nd, _ptr(out), o, _ptr(img) if img is not None else None))
+    return (out, img) if return_image else out
+
+
+def spacetime_derivatives(cache, model, times, nus, L, h_a=1e-5, h_theta=1e-5, nmax=-1, slab=0.0, precision=KS_FP64, return_image=False):
+    """d(image)/d(a, theta_o, ln L) (the spacetime block of spacetime_valgrad, joint.jl:74-82): array
+    (3, nfreq, nframes, npix, 4) in screen order; a and theta_o by central differences with steps
+    h_a, h_theta, ln L exactly for thermal scenes."""
+    times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+    nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+    nt, nf = int(times.shape[0]), int(nus.shape[0])
+    arr, nsets, _keep = _set_array(model)
+    out = np.empty((3, nf, nt, cache.npix, 4))
+    img = np.empty((nf, nt, cache.npix, 4)) if return_image else None
+    cache._check(cache._lib.ks_spacetime_derivatives(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision),
+                                                     int(nmax), float(slab), float(h_a), float(h_theta), _ptr(out),
+                                                     _ptr(img) if img is not None else None))
     return (out, img) if return_image else out
 
 

@@ -1104,6 +1104,7 @@ struct JvpSink {
     const D* tab; int ntot;
     S t_obs, nu, Lnu, a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
     int nmax;
+    int lnL_dir;      // >= 0: the direction that carries d/d(ln L) (the step length scales with L)
     D P[16], Sv[4];
     S zprev; int wn; bool inside, crossed, zset;
 
@@ -1172,8 +1173,10 @@ struct JvpSink {
         }
         if (!active) return;
         const S Sg = r * r + a * a * cos(th) * cos(th);
+        D Dl(Lnu * Sg * dtau);
+        if (lnL_dir >= 0) Dl.d[lnL_dir] = Dl.v;
         D O[16], E[4];
-        transfer_step(c_moments, in, in + 4, in + 8, D(Lnu * Sg * dtau), O, E);
+        transfer_step(c_moments, in, in + 4, in + 8, Dl, O, E);
         D Pn[16];
         for (int rr = 0; rr < 4; ++rr) {
             Sv[rr] += P[4 * rr] * E[0] + P[4 * rr + 1] * E[1] + P[4 * rr + 2] * E[2] + P[4 * rr + 3] * E[3];
@@ -1189,7 +1192,7 @@ struct JvpSink {
 template <class S, int K>
 __global__ void __launch_bounds__(64) k_jvp(PlanView P, Spacetime st, long long npix, const Dual<S, K>* __restrict__ dtab, int ntot,
                                             const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L, int nmax,
-                                            double slab, double* __restrict__ img, double* __restrict__ out) {
+                                            double slab, double* __restrict__ img, double* __restrict__ out, int lnL_dir) {
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (idx >= npix * ncombo) return;
     const long long j = idx % npix;
@@ -1203,6 +1206,7 @@ __global__ void __launch_bounds__(64) k_jvp(PlanView P, Spacetime st, long long 
     sink.a = S(st.a); sink.rh_lo = S(st.rh * (1 + 1e-3)); sink.dtau = S(R.dtau);
     sink.alpha = S(P.get(PF_ALPHA, j)); sink.beta = S(P.get(PF_BETA, j)); sink.eta = S(R.eta); sink.lam = S(R.lam);
     sink.a_sin_tho = S(st.a * sin(st.thetao)); sink.slab = S(slab); sink.nmax = nmax;
+    sink.lnL_dir = lnL_dir;
     sink.init();
     double rt, rp;
     march(P, st, j, R, sink, rt, rp);

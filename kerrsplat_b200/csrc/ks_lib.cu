@@ -666,7 +666,7 @@ struct ks_context {
     // adjoint: gradient table, stored FP64 samples (plain path), cutoffs, tails, per-ray slots,
     // seeds, chi^2 partials; mixed path: per-sample states, activity, segment bounds, unit partials
     DevBuf gtab, samples, kstop, tails, slots, dgrad, seeds, chi_part, chi_val, dstage;
-    DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part, jvp_tab, jvp_in, jvp_out;
+    DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part, jvp_tab, jvp_in, jvp_out, st_buf;
     bool samples_ready = false;
     int nkv = 0;                            // knot values after the splat table in `tab`
     MixedJob last_job{};                    // the segmentation of the last mixed forward pass
@@ -1680,7 +1680,7 @@ namespace {
 // J v of the image for one chunk of K directions (dirs: K x nparams, each laid out like dparams)
 template <class S, int K>
 int jvp_chunk(ks_context* c, int ntot, const double* dparams_dev, const double* ddirs, long long dstride, const double* dct,
-              const double* dcn, int ncombo, double L, int nmax, double slab, double* img_sorted, double* out_sorted) {
+              const double* dcn, int ncombo, double L, int nmax, double slab, double* img_sorted, double* out_sorted, int lnL_dir = -1) {
     KS_CUDA(c, c->jvp_tab.ensure(size_t(std::max(ntot, 1)) * ST_COUNT * sizeof(Dual<S, K>)));
     Dual<S, K>* dt = c->jvp_tab.as<Dual<S, K>>();
     if (ntot > 0) {
@@ -1691,7 +1691,7 @@ int jvp_chunk(ks_context* c, int ntot, const double* dparams_dev, const double* 
     }
     const long long nrc = c->npix * ncombo;
     k_jvp<S, K><<<nblocks(nrc, 64), 64, 0, c->stream>>>(plan_view(c), c->st, c->npix, dt, ntot, dct, dcn, ncombo, L, nmax, slab, img_sorted,
-                                                        out_sorted);
+                                                        out_sorted, lnL_dir);
     c->launches++;
     c->adjoint_launches++;
     KS_CUDA(c, cudaGetLastError());
@@ -1702,10 +1702,15 @@ int jvp_chunk(ks_context* c, int ntot, const double* dparams_dev, const double* 
 
 extern "C" {
 
-int ks_jvp(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus, int32_t nfreq,
-           double L, int32_t precision, int32_t nmax, double slab, const double* dirs, int32_t ndir, double* dimage, int32_t order,
-           double* image) {
-    if (!c || !dirs || !dimage || ndir < 1) return KS_ERR_ARGUMENT;
+}  // extern "C"
+
+namespace {
+
+// ks_jvp; with lnL, one direction: d/d(ln L) (dirs ignored), exact through a dual step length
+int jvp_impl(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus, int32_t nfreq,
+             double L, int32_t precision, int32_t nmax, double slab, const double* dirs, int32_t ndir, double* dimage, int32_t order,
+             double* image, bool lnL) {
+    if (!c || (!dirs && !lnL) || !dimage || ndir < 1) return KS_ERR_ARGUMENT;
     if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
     if (nsets < 1 || !sets) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
     if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
@@ -1738,7 +1743,7 @@ int ks_jvp(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double*
     const int nchunk = (ndir + K - 1) / K;
     // directions padded to whole chunks
     std::vector<double> hd(size_t(nchunk) * K * np, 0.0);
-    KS_CUDA(c, cudaMemcpy(hd.data(), dirs, size_t(ndir) * np * sizeof(double), cudaMemcpyDefault));
+    if (!lnL) KS_CUDA(c, cudaMemcpy(hd.data(), dirs, size_t(ndir) * np * sizeof(double), cudaMemcpyDefault));
     for (double v : hd) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite direction");
     KS_CUDA(c, c->jvp_in.ensure((hp.size() + hd.size() + 1) * sizeof(double)));
     double* dp = c->jvp_in.as<double>();
@@ -1762,12 +1767,13 @@ int ks_jvp(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double*
     for (int ch = 0; ch < nchunk; ++ch) {
         const double* dd = dp + np + (long long)ch * K * np;
         int s;
+        const int ld = lnL ? 0 : -1;
         if (precision == KS_FP64)
-            s = K == 1 ? jvp_chunk<double, 1>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>())
-                       : jvp_chunk<double, 8>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>());
+            s = K == 1 ? jvp_chunk<double, 1>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>(), ld)
+                       : jvp_chunk<double, 8>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>(), ld);
         else
-            s = K == 1 ? jvp_chunk<float, 1>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>())
-                       : jvp_chunk<float, 8>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>());
+            s = K == 1 ? jvp_chunk<float, 1>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>(), ld)
+                       : jvp_chunk<float, 8>(c, ntot, dp, dd, np, dct, dcn, ncombo, L, nmax, slab, c->out_sorted.as<double>(), c->jvp_out.as<double>(), ld);
         if (s) return s;
         const int nd = std::min(K, ndir - ch * K);
         s = emit(c, c->jvp_out.as<double>(), 4, int(nd * ncombo), order, dimage + (long long)ch * K * nrc * 4);
@@ -1782,6 +1788,84 @@ int ks_jvp(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double*
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->adjoint_ms += ms;
+    return KS_OK;
+}
+
+__global__ void k_central_diff(long long n, const double* __restrict__ plus, const double* __restrict__ minus, double inv2h,
+                               double* __restrict__ out) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q < n) out[q] = (plus[q] - minus[q]) * inv2h;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ks_jvp(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus, int32_t nfreq,
+           double L, int32_t precision, int32_t nmax, double slab, const double* dirs, int32_t ndir, double* dimage, int32_t order,
+           double* image) {
+    return jvp_impl(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, dirs, ndir, dimage, order, image, false);
+}
+
+int ks_spacetime_derivatives(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+                             int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, double h_a, double h_theta,
+                             double* dimage, double* image) {
+    if (!c || !dimage || !sets || nsets < 1) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    if (!(h_a > 0 && h_theta > 0 && std::isfinite(h_a) && std::isfinite(h_theta))) return fail(c, KS_ERR_ARGUMENT, "steps must be positive");
+    if (nframes < 1 || nfreq < 1) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    const Spacetime st0 = c->st;
+    if (!(st0.a - h_a > 0.0 && st0.a + h_a < 1.0)) return fail(c, KS_ERR_ARGUMENT, "a +- h_a must stay in (0, 1)");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const long long n4 = c->npix * (long long)nframes * nfreq * 4;
+    KS_CUDA(c, c->st_buf.ensure(size_t(n4) * 3 * sizeof(double)));
+    double* bp = c->st_buf.as<double>();
+    double* bm = bp + n4;
+    double* b3 = bm + n4;
+    const bool dev = is_device_ptr(dimage);
+    double* dd = dev ? dimage : nullptr;
+    std::vector<double> host;
+    if (!dev) { KS_CUDA(c, c->stage_out.ensure(size_t(n4) * 3 * sizeof(double))); dd = c->stage_out.as<double>(); }
+    const double steps[2] = {h_a, h_theta};
+    int status = KS_OK;
+    for (int q = 0; q < 2 && status == KS_OK; ++q) {
+        for (int sgn = 0; sgn < 2 && status == KS_OK; ++sgn) {
+            const double d = (sgn == 0 ? 1.0 : -1.0) * steps[q];
+            status = regenerate_impl(c, st0.a + (q == 0 ? d : 0.0), st0.thetao + (q == 1 ? d : 0.0), st0.N, st0.M, st0.density, st0.nmin);
+            if (status == KS_OK)
+                status = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, sgn == 0 ? bp : bm, KS_ORDER_SCREEN);
+        }
+        if (status == KS_OK) {
+            k_central_diff<<<nblocks(n4, 256), 256, 0, c->stream>>>(n4, bp, bm, 0.5 / steps[q], dd + q * n4);
+            c->launches++;
+        }
+    }
+    // back at (a, theta_o)
+    {
+        int s2 = regenerate_impl(c, st0.a, st0.thetao, st0.N, st0.M, st0.density, st0.nmin);
+        if (status == KS_OK) status = s2;
+    }
+    if (status) return status;
+    // d/d(ln L): exact through a dual step length for thermal scenes, else central differences in ln L
+    bool thermal = true;
+    for (int s = 0; s < nsets; ++s) thermal = thermal && sets[s].kind == KS_THERMAL21;
+    if (thermal) {
+        int s = jvp_impl(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, nullptr, 1, dd + 2 * n4, KS_ORDER_SCREEN,
+                         image ? b3 : nullptr, true);
+        if (s) return s;
+    } else {
+        const double h = 1e-5;
+        int s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L * std::exp(h), precision, nmax, slab, bp, KS_ORDER_SCREEN);
+        if (!s) s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L * std::exp(-h), precision, nmax, slab, bm, KS_ORDER_SCREEN);
+        if (!s && image) s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, b3, KS_ORDER_SCREEN);
+        if (s) return s;
+        k_central_diff<<<nblocks(n4, 256), 256, 0, c->stream>>>(n4, bp, bm, 0.5 / h, dd + 2 * n4);
+        c->launches++;
+    }
+    KS_CUDA(c, cudaGetLastError());
+    if (!dev) KS_CUDA(c, cudaMemcpyAsync(dimage, dd, size_t(n4) * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (image) KS_CUDA(c, cudaMemcpyAsync(image, b3, size_t(n4) * sizeof(double), cudaMemcpyDefault, c->stream));
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
     return KS_OK;
 }
 

@@ -239,3 +239,30 @@ def test_normal_matrix(prec, tol):
     A = ks.normal_matrix(cache, J, precision=prec)
     ref = J.T @ J
     assert np.max(np.abs(A - ref)) <= tol * np.abs(ref).max()
+
+
+def test_spacetime_derivatives_match_oracle(scene, oracle):
+    """The spacetime block (a, theta_o, ln L) of spacetime_valgrad (joint.jl:74-82): d/da and
+    d/dtheta_o against the oracle's central differences with the same steps (the same discretised
+    function, FP64: 1e-6), d/d(ln L) (a dual step length) against the oracle's central difference in
+    ln L (1e-6)."""
+    s = scene
+    c, cam = s["c"], s["cam"]
+    m = ks.PolarizedSplats(s["p"])
+    h = 1e-5
+    nu, t = s["nus"][:1], s["times"][:1]
+    d, img = ks.spacetime_derivatives(s["cache"], m, t, nu, c["L"], h_a=h, h_theta=h, precision=ks.KS_FP64, return_image=True)
+
+    def orc(a, th, L):
+        return oracle.polarized_image(a, th, cam.alpha, cam.beta, N, c["M"], [("thermal", s["p"], None)], t[0], nu[0], L)
+
+    a, th, L = c["a"], c["theta_o"], c["L"]
+    ref = [(orc(a + h, th, L) - orc(a - h, th, L)) / (2 * h), (orc(a, th + h, L) - orc(a, th - h, L)) / (2 * h),
+           (orc(a, th, L * np.exp(h)) - orc(a, th, L * np.exp(-h))) / (2 * h)]
+    errs = [rel_l2(d[q, 0, 0], ref[q]) for q in range(3)]
+    print("spacetime derivatives rel L2 (a, theta_o, ln L):", errs)
+    assert max(errs) < 1e-6, errs
+    assert rel_l2(img[0, 0], orc(a, th, L)) < 1e-10
+    # the context is back at (a, theta_o)
+    again = np.asarray(ks.render(s["cache"], m, t, nu, L, precision=ks.KS_FP64))[0, 0]
+    assert rel_l2(again, orc(a, th, L)) < 1e-10
