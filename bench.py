@@ -344,6 +344,70 @@ def run_movie(args):
     cache.close()
 
 
+def run_fit(args):
+    """The minibatched fit iteration (configuration 5): for each of the 16 parameter sets, the forward
+    image, the 3xTF32 DFT onto 2000 baselines, chi^2 against its noisy target, the adjoint DFT and the
+    reverse pass (ks_vis_chi2_gradient), and the Gauss-Newton normal-equation product along the
+    gradient, g^T J^T J g = |J g|^2 (one J v pass and one DFT): the curvature of the matrix-free
+    normal equations. One step = all sets; the FP64 plain path is timed on one set."""
+    import torch
+    import kerrsplat_b200 as ks
+    from kerrsplat_b200 import build, scenes
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    build.build(verbose=False)
+    c = scenes.config5(res=args.res, N=args.nsamples, nsets=args.sets)
+    cache = ks.GeodesicCache(c["camera"], c["N"], device=local)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    rng = c["rng"]
+    targets = []
+    for p in c["sets"]:
+        pt = p + 0.05 * np.maximum(np.abs(p), 0.1) * rng.standard_normal(p.shape)
+        img = np.asarray(ks.render(cache, ks.PolarizedSplats(pt), [c["t_obs"]], [c["nu"]], c["L"], precision=ks.KS_MIXED))[0, 0]
+        V = np.asarray(ks.visibilities(cache, img, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_MIXED))
+        sig = np.maximum(0.02 * np.abs(V), 1e-3 * np.abs(V).max())
+        noise = sig * (rng.standard_normal(V.shape) + 1j * rng.standard_normal(V.shape)) / np.sqrt(2)
+        targets.append((V + noise, sig))
+
+    def one_set(q, prec):
+        p, (vis, sig) = c["sets"][q], targets[q]
+        m = ks.PolarizedSplats(p)
+        chi2, g = ks.vis_chi2_gradient(cache, m, c["t_obs"], c["nu"], c["L"], c["u"], c["v"], vis, sig, c["psize"], c["scale"], precision=prec)
+        jv = ks.jvp(cache, m, [c["t_obs"]], [c["nu"]], c["L"], g, precision=prec)[0, 0, 0]
+        Vd = np.asarray(ks.visibilities(cache, jv, c["u"], c["v"], c["psize"], c["scale"], precision=prec))
+        curv = float(np.sum(np.abs(Vd / sig) ** 2))
+        return chi2, float(np.sum(g * g)), curv
+
+    for _ in range(args.warmup):
+        one_set(0, ks.KS_MIXED)
+    torch.cuda.synchronize()
+    per_set = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for q in range(len(c["sets"])):
+            t1 = time.perf_counter()
+            chi2, gg, curv = one_set(q, ks.KS_MIXED)
+            per_set.append({"splats": int(c["counts"][q]), "ms": (time.perf_counter() - t1) * 1e3, "chi2": chi2,
+                            "gn_step": -0.5 * gg / max(curv, 1e-300)})
+    ms_iter = (time.perf_counter() - t0) * 1e3 / args.steps
+    line = {"metric": "fit iterations/s (minibatched)", "value": 1e3 / ms_iter, "unit": "iterations/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_iter, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded PCG64 scene, cfg 5 distributions)",
+            "config": {"workload": f"minibatched fit {args.res}x{args.res} +-16M, a=0.7, theta_o=30deg, N={c['N']}, 230 GHz, "
+                                   f"{len(c['sets'])} thermal sets of {int(c['counts'].min())}-{int(c['counts'].max())} splats, "
+                                   f"{len(c['u'])} baselines, 3xTF32 DFT",
+                       "iteration": "per set: forward + DFT + chi^2 + adjoint DFT + reverse pass + J g + DFT (GN curvature g^T J^T J g)",
+                       "timing": "wall clock around the synchronous calls (host data)"},
+            "per_set": per_set[:len(c["sets"])]}
+    if args.fp64_steps > 0:
+        t1 = time.perf_counter()
+        one_set(0, ks.KS_FP64)
+        ms64 = (time.perf_counter() - t1) * 1e3
+        line["fp64_plain"] = {"set": 0, "splats": int(c["counts"][0]), "ms": ms64, "speedup_mixed_over_fp64": ms64 / per_set[0]["ms"]}
+    print(json.dumps(line), flush=True)
+    cache.close()
+
+
 def cpu_sample(c, nrays, seed=7):
     rng = np.random.Generator(np.random.PCG64(seed))
     idx = np.sort(rng.choice(c["camera"].npix, size=min(nrays, c["camera"].npix), replace=False))
@@ -404,14 +468,17 @@ def main():
     ap.add_argument("--no-gradient", action="store_true", help="skip the chi^2 + gradient measurement")
     ap.add_argument("--res", type=int, default=256, help="screen resolution (smaller cases for profiling)")
     ap.add_argument("--nsamples", type=int, default=1024)
-    ap.add_argument("--workload", default="polarized", choices=["polarized", "movie"],
-                    help="polarized: configurations 2 and 3 (the headline); movie: configuration 4")
+    ap.add_argument("--workload", default="polarized", choices=["polarized", "movie", "fit"],
+                    help="polarized: configurations 2 and 3 (the headline); movie: configuration 4; fit: configuration 5")
+    ap.add_argument("--sets", type=int, default=16, help="fit: parameter sets")
     ap.add_argument("--frames", type=int, default=32, help="movie frames")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "movie":
         run_movie(args)
+    elif args.workload == "fit":
+        run_fit(args)
     else:
         run_ours(args)
 

@@ -169,6 +169,17 @@ int ks_chi2_gradient(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, c
                      int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, const double* data, const double* sigma,
                      double sigma_scalar, const uint8_t* mask, double* chi2, double* dparams, int32_t accumulate, double* image);
 
+/* The visibility chi^2 of one frame and its gradient (timeresolved_gradient!'s device path,
+ * src/Fit/timeresolved.jl:115-138: the forward image, frame_chi2_seed!, device_visibilities.jl:97-111,
+ * and the reverse pass seeded by the adjoint transform), in one forward and one reverse pass: nuv
+ * baselines (u, v, tap, gains g as in ks_frame_chi2_seed; vis nuv x 4 complex, sigma nuv x 4), the DFT in
+ * the render's precision class (KS_MIXED: 3xTF32 tensor cores). chi2, dparams (as ks_adjoint) and the
+ * image (optional, screen order) are outputs. */
+int ks_vis_chi2_gradient(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, double t_obs, double nu, double L, int32_t precision,
+                         int32_t nmax, double slab, int64_t nuv, const double* u, const double* v, const double* tap, const double* g,
+                         const double* vis, const double* sigma, double psize, double scale, double* chi2, double* dparams,
+                         int32_t accumulate, double* image);
+
 /* J v of the image (jvp!, src/Fit/gauss_newton.jl:91-118, whose tails pass runs on parameters carrying
  * duals along v): the directional derivatives of the observed Stokes images along ndir directions
  * `dirs` (ndir x nparams, each direction laid out like dparams of ks_adjoint), into dimage

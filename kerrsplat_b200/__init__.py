@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -554,6 +554,30 @@ def sample_adjoint(cache, coeffs, Dl, w, R, method=0):
     out = np.empty((n, 31))
     cache._check(cache._lib.ks_sample_adjoint(cache._ctx, n, _ptr(coeffs), _ptr(Dl), _ptr(w), _ptr(R), int(method), _ptr(out)))
     return out[:, :16].reshape(n, 4, 4), out[:, 16:20], out[:, 20:]
+
+
+def vis_chi2_gradient(cache, model, t_obs, nu, L, u, v, vis, sigma, psize, scale, tap=None, gains=None, nmax=-1, slab=0.0,
+                      precision=KS_MIXED, dparams=None, return_image=False):
+    """The visibility chi^2 of one frame and its gradient (timeresolved_gradient!'s device path,
+    timeresolved.jl:115-138; frame_chi2_seed!, device_visibilities.jl:97-111) in one forward and one
+    reverse pass: vis (nuv, 4) complex data, sigma (nuv, 4). Returns (chi2, grad[, image])."""
+    u, v = _as_f64(u), _as_f64(v)
+    nuv = int(u.shape[0])
+    vi = _complex_pairs(vis)
+    sg = _as_f64(sigma)
+    tp = _as_f64(tap) if tap is not None else None
+    gg = _complex_pairs(gains) if gains is not None else None
+    arr, nsets, _keep = _set_array(model)
+    user, buf = _grad_buffer(model, dparams)
+    chi2 = ctypes.c_double(0.0)
+    img = np.empty((cache.npix, 4)) if return_image else None
+    cache._check(cache._lib.ks_vis_chi2_gradient(cache._ctx, arr, nsets, float(t_obs), float(nu), float(L), _precision(precision), int(nmax),
+                                                 float(slab), nuv, _ptr(u), _ptr(v), _ptr(tp) if tp is not None else None,
+                                                 _ptr(gg) if gg is not None else None, _ptr(vi), _ptr(sg), float(psize), float(scale),
+                                                 ctypes.addressof(chi2), _ptr(buf), 1 if user is not None else 0,
+                                                 _ptr(img) if img is not None else None))
+    g = user if user is not None else _split_grad(model, buf)
+    return (chi2.value, g, img) if return_image else (chi2.value, g)
 
 
 def sweep_passes(cache, model, L, nmax=-1, slab=0.0, precision=KS_FP64):

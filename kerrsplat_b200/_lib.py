@@ -70,6 +70,9 @@ SIGNATURES = [
                                   ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _VP, ctypes.c_int32, _VP, ctypes.c_int32]),
     ("ks_jvp", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
                               ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _VP, ctypes.c_int32, _VP, ctypes.c_int32, _VP]),
+    ("ks_vis_chi2_gradient", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int64, _VP, _VP, _VP,
+                                            _VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _VP, _VP, ctypes.c_int32, _VP]),
     ("ks_spacetime_derivatives", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
                                                 ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_double, _VP, _VP]),

@@ -507,23 +507,23 @@ __global__ void __launch_bounds__(128) k_tails(PlanView P, Spacetime st, long lo
     for (int s = 0; s < 4; ++s) img[((long long)c * npix + j) * 4 + s] = T4[s] * n3;
 }
 
-// polarized_dual_kernel! (dual_gradient.jl:151-178), FP64: one thread per (ray, combination),
-// forward over the samples; the ray's share of every splat's gradient into its own slots
-// grad[(row * ntot + i) * nrc + c * npix + j].
+// polarized_dual_kernel! (dual_gradient.jl:151-178), FP64: one thread per (ray, combination) of the
+// ray range [j0, j0 + nr), forward over the samples; the ray's share of every splat's gradient into
+// its own slots grad[(row * ntot + i) * (nr ncombo) + c * nr + (j - j0)].
 __global__ void __launch_bounds__(128) k_dual_plain(PlanView P, Spacetime st, long long npix, StoredSamples S, const int* __restrict__ kstop,
                                                     const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
                                                     const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L,
                                                     const double* __restrict__ tails, const double* __restrict__ dstokes,
-                                                    double* __restrict__ grad) {
+                                                    double* __restrict__ grad, long long j0, long long nr) {
     extern __shared__ __align__(16) unsigned char smem[];
     double* tab = reinterpret_cast<double*>(smem);
     for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = tab64[q];
     __syncthreads();
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (idx >= npix * ncombo) return;
-    const long long j = idx % npix;
-    const int c = int(idx / npix);
-    const long long nrc = npix * ncombo;
+    if (idx >= nr * ncombo) return;
+    const long long j = j0 + idx % nr;
+    const int c = int(idx / nr);
+    const long long nrc = nr * ncombo;
     const int N = st.N;
     const double a = st.a, rh_lo = st.rh * (1 + 1e-3);
     const double nu = cnu[c], t_obs = ct[c], nh = nu / kNU0, Lnu = L / nh, n3 = nh * nh * nh;
@@ -577,7 +577,7 @@ __global__ void k_sample_adjoint(long long n, const double* __restrict__ in, con
 
 // The deterministic sum of the per-ray slots (one block per (row, splat), a fixed tree), into the
 // column-major parameter layout dparams[i * 21 + row].
-__global__ void k_slot_reduce(const double* __restrict__ grad, long long nrc, int ntot, double* __restrict__ out) {
+__global__ void k_slot_reduce(const double* __restrict__ grad, long long nrc, int ntot, double* __restrict__ out, int accumulate) {
     __shared__ double sh[256];
     const int ri = blockIdx.x;   // row * ntot + i
     const double* g = grad + (long long)ri * nrc;
@@ -591,7 +591,8 @@ __global__ void k_slot_reduce(const double* __restrict__ grad, long long nrc, in
     }
     if (threadIdx.x == 0) {
         const int row = ri / ntot, i = ri % ntot;
-        out[(long long)i * GR_COUNT + row] = sh[0];
+        double* o = out + (long long)i * GR_COUNT + row;
+        *o = accumulate ? *o + sh[0] : sh[0];
     }
 }
 
@@ -734,11 +735,15 @@ struct AdjSmem {
     static constexpr int kItemBytes = 32 * 32 * 2;
     static constexpr int kCbBytes = 32 * CH * 11 * 4;
     static constexpr int kGitemBytes = 32 * GR_COUNT * 4;
-    static constexpr int kFixed = kSampleBytes + kItemBytes + kCbBytes + kGitemBytes + kMetaBytes;
+    static constexpr int kCandBytes = kMaxSplatWords * 4;
+    static constexpr int kFixed = kSampleBytes + kItemBytes + kCbBytes + kGitemBytes + kMetaBytes + kCandBytes;
     __host__ __device__ static size_t acc_bytes(int ntot) { return (size_t(ntot) * GR_COUNT * 4 + 15) / 16 * 16; }
     __host__ __device__ static size_t tab_bytes(int ntot) { return (size_t(ntot) * ST_COUNT * 4 + 15) / 16 * 16; }
-    __host__ __device__ static size_t warp_bytes(int ntot) { return size_t(kFixed) + acc_bytes(ntot); }
-    __host__ __device__ static size_t bytes(int ntot, int warps) { return tab_bytes(ntot) + size_t(warps) * warp_bytes(ntot); }
+    // the gradient accumulator is per warp in shared memory, or (large tables) the unit's own block of gunit
+    __host__ __device__ static size_t warp_bytes(int ntot, bool global_acc = false) { return size_t(kFixed) + (global_acc ? 0 : acc_bytes(ntot)); }
+    __host__ __device__ static size_t bytes(int ntot, int warps, bool global_acc = false) {
+        return tab_bytes(ntot) + size_t(warps) * warp_bytes(ntot, global_acc);
+    }
     __host__ __device__ static size_t step_bytes(int warps) { return size_t(warps) * kStepWarp; }
 };
 
@@ -886,18 +891,19 @@ __global__ void __launch_bounds__(NT, 1)
 k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
                const double* __restrict__ ct, const double* __restrict__ cnu, const double* __restrict__ plan_f, const float* __restrict__ stream,
                const float* __restrict__ gstate, const unsigned char* __restrict__ gact, unsigned long long* __restrict__ work,
-               float* __restrict__ gunit) {
+               float* __restrict__ gunit, int global_acc) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* tab = reinterpret_cast<float*>(smem);
     for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wb = smem + AdjSmem<CH>::tab_bytes(ntot) + size_t(warp) * AdjSmem<CH>::warp_bytes(ntot);
+    unsigned char* wb = smem + AdjSmem<CH>::tab_bytes(ntot) + size_t(warp) * AdjSmem<CH>::warp_bytes(ntot, global_acc != 0);
     float* sf = reinterpret_cast<float*>(wb);
     uint16_t* items = reinterpret_cast<uint16_t*>(wb + AdjSmem<CH>::kSampleBytes);
     float* cbs = reinterpret_cast<float*>(wb + AdjSmem<CH>::kSampleBytes + AdjSmem<CH>::kItemBytes);
     float* gitem = cbs + 32 * CH * 11;                  // [item][21]
     unsigned* meta_bits = reinterpret_cast<unsigned*>(gitem + 32 * GR_COUNT);
-    float* gacc = reinterpret_cast<float*>(wb + AdjSmem<CH>::kFixed);   // [splat][21]
+    unsigned* cand = meta_bits + 64;                    // the unit's candidate splats
+    float* gacc_smem = reinterpret_cast<float*>(wb + AdjSmem<CH>::kFixed);   // [splat][21]
     __syncthreads();
     const unsigned full = 0xffffffffu;
     const int N = st.N;
@@ -917,7 +923,24 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
         const float dtau = float(plan_f[(long long)PF_DTAU * npad + U.j]);
         const float alpha = float(plan_f[(long long)PF_ALPHA * npad + U.j]), beta = float(plan_f[(long long)PF_BETA * npad + U.j]);
         const float eta = float(plan_f[(long long)PF_ETA * npad + U.j]), lam = float(plan_f[(long long)PF_LAM * npad + U.j]);
+        float* gacc = global_acc ? gunit + U.ur * gsz : gacc_smem;
         for (long long q = lane; q < gsz; q += 32) gacc[q] = 0.f;
+        {
+            // the unit's bounds and candidate splats (as the forward pass)
+            UnitBox b{3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f};
+            const int nsamp = int(plan_f[(long long)PF_NSAMP * npad + U.j]);
+            for (int k = U.k0; k < U.k1; ++k) {
+                const float* bp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
+                if (!U.live || k > nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
+                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
+                const float rho = sqrtf(x * x + y * y);
+                b.xlo = fminf(b.xlo, x); b.xhi = fmaxf(b.xhi, x); b.ylo = fminf(b.ylo, y); b.yhi = fmaxf(b.yhi, y);
+                b.zlo = fminf(b.zlo, z); b.zhi = fmaxf(b.zhi, z); b.rlo = fminf(b.rlo, rho); b.rhi = fmaxf(b.rhi, rho);
+            }
+            b.xlo = warp_min(b.xlo); b.xhi = warp_max(b.xhi); b.ylo = warp_min(b.ylo); b.yhi = warp_max(b.yhi);
+            b.zlo = warp_min(b.zlo); b.zhi = warp_max(b.zhi); b.rlo = warp_min(b.rlo); b.rhi = warp_max(b.rhi);
+            unit_candidates(tab, ntot, b, lane, cand);
+        }
         __syncwarp();
         for (int k = U.k0; k < U.k1; ++k) {
             const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
@@ -960,10 +983,14 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
             __syncwarp();
             const float t = t_obs - ts;
             for (int s0 = 0; s0 < ntot; s0 += 32) {
+                const unsigned cm = cand[s0 >> 5];
+                if (cm == 0u) continue;
                 unsigned mask = 0u;
                 if (actbits) {
-                    const int nb = min(32, ntot - s0);
-                    for (int b = 0; b < nb; ++b) {
+                    unsigned cb2 = cm;
+                    while (cb2) {
+                        const int b = __ffs(cb2) - 1;
+                        cb2 &= cb2 - 1;
                         const float* p = tab + (s0 + b) * ST_COUNT;
                         const float dr = rho - p[ST_RHO], dz = z - p[ST_CZ];
                         if (dr * dr + dz * dz > p[ST_SUPP]) continue;
@@ -1017,8 +1044,10 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
                 }
             }
         }
-        float* gu = gunit + U.ur * gsz;
-        for (long long q = lane; q < gsz; q += 32) gu[q] = gacc[q];
+        if (!global_acc) {
+            float* gu = gunit + U.ur * gsz;
+            for (long long q = lane; q < gsz; q += 32) gu[q] = gacc[q];
+        }
         __syncwarp();
     }
 }

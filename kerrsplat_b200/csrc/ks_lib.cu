@@ -1362,6 +1362,20 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
 
 namespace {
 void gemm(ks_context* c, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb, float* C, long long ldc);
+int dft_stage(ks_context* c, int slot, const double* src, size_t count, const double** dev);
+int dft_checks(ks_context* c, int64_t nuv, double psize, double scale, int32_t precision);
+int dft_forward(ks_context* c, const double* dimg, int32_t order, int64_t nuv, const double* du, const double* dv, const double* dtap,
+                double psize, double scale, int32_t precision, double* dV);
+int dft_adjoint(ks_context* c, const double* dw, int64_t nuv, const double* du, const double* dv, const double* dtap, double psize,
+                double scale, int32_t precision, double* dseed, int32_t order, bool have_twiddles);
+
+// The visibility data of a frame (frame_chi2_seed!, device_visibilities.jl:97-111): nuv baselines,
+// the gains g (complex, may be NULL), the data vis and sigma per Stokes; all host or device.
+struct VisData {
+    int64_t nuv;
+    const double *u, *v, *tap, *g, *vis, *sigma;
+    double psize, scale;
+};
 }
 
 namespace {
@@ -1402,8 +1416,8 @@ int stage_dev(ks_context* c, DevBuf& buf, const U* src, size_t count, const U** 
 
 // Occupancy of k_adj_elements<CH, NT> with its shared memory for `ntot` splats (0 if it does not fit).
 template <int CH, int NT>
-int adjoint_blocks(ks_context* c, int ntot) {
-    const size_t smem = AdjSmem<CH>::bytes(ntot, NT / 32);
+int adjoint_blocks(ks_context* c, int ntot, bool global_acc) {
+    const size_t smem = AdjSmem<CH>::bytes(ntot, NT / 32, global_acc);
     if (smem > 227 * 1024) return 0;
     if (cudaFuncSetAttribute(k_adj_elements<CH, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
@@ -1415,7 +1429,7 @@ int adjoint_blocks(ks_context* c, int ntot) {
 }
 
 template <int CH, int NT>
-int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* dt, const double* dn) {
+int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* dt, const double* dn, bool global_acc) {
     int nsm = 0;
     KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     const MixedJob& job = c->last_job;
@@ -1446,10 +1460,11 @@ int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* d
     {
         constexpr int W = NT / 32;
         const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
-        const size_t smem = AdjSmem<CH>::bytes(ntot, W);
+        const size_t smem = AdjSmem<CH>::bytes(ntot, W, global_acc);
         k_adj_elements<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(c->st, job, c->tab.as<double>(), c->gtab.as<double>(), ntot, dt, dn,
                                                                        c->plan.as<double>(), c->stream_buf.as<float>(), job.gstate, job.gact,
-                                                                       c->work.as<unsigned long long>() + 1, c->adj_unit.as<float>());
+                                                                       c->work.as<unsigned long long>() + 1, c->adj_unit.as<float>(),
+                                                                       global_acc ? 1 : 0);
         c->launches++;
         c->adjoint_launches++;
         KS_CUDA(c, cudaGetLastError());
@@ -1467,13 +1482,22 @@ int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* d
 
 template <int CH>
 int launch_adjoint_mixed_ch(ks_context* c, int ntot, const double* dt, const double* dn) {
-    const int w256 = adjoint_blocks<CH, 256>(c, ntot) * 8, w128 = adjoint_blocks<CH, 128>(c, ntot) * 4,
-              w64 = adjoint_blocks<CH, 64>(c, ntot) * 2;
+    if (ntot > 32 * kMaxSplatWords) return fail(c, KS_ERR_ARGUMENT, "the mixed adjoint takes at most %d splats (%d)", 32 * kMaxSplatWords, ntot);
+    // the per-warp accumulator in shared memory while it leaves at least eight warps per SM, else the
+    // unit's block of global memory
+    bool global_acc = false;
+    int w256 = adjoint_blocks<CH, 256>(c, ntot, false) * 8, w128 = adjoint_blocks<CH, 128>(c, ntot, false) * 4,
+        w64 = adjoint_blocks<CH, 64>(c, ntot, false) * 2;
+    if (std::max(std::max(w256, w128), w64) < 8) {
+        global_acc = true;
+        w256 = adjoint_blocks<CH, 256>(c, ntot, true) * 8; w128 = adjoint_blocks<CH, 128>(c, ntot, true) * 4;
+        w64 = adjoint_blocks<CH, 64>(c, ntot, true) * 2;
+    }
     const int best = std::max(std::max(w256, w128), w64);
     if (best <= 0) return fail(c, KS_ERR_ARGUMENT, "too many splats for the mixed adjoint (%d)", ntot);
-    if (w256 == best) return launch_adjoint_mixed_nt<CH, 256>(c, ntot, w256 / 8, dt, dn);
-    if (w128 == best) return launch_adjoint_mixed_nt<CH, 128>(c, ntot, w128 / 4, dt, dn);
-    return launch_adjoint_mixed_nt<CH, 64>(c, ntot, w64 / 2, dt, dn);
+    if (w256 == best) return launch_adjoint_mixed_nt<CH, 256>(c, ntot, w256 / 8, dt, dn, global_acc);
+    if (w128 == best) return launch_adjoint_mixed_nt<CH, 128>(c, ntot, w128 / 4, dt, dn, global_acc);
+    return launch_adjoint_mixed_nt<CH, 64>(c, ntot, w64 / 2, dt, dn, global_acc);
 }
 
 // The forward image with the state the reverse pass needs (FP64: stored samples, cutoffs, tails),
@@ -1481,7 +1505,7 @@ int launch_adjoint_mixed_ch(ks_context* c, int ntot, const double* dt, const dou
 int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double* times, int nframes, const double* nus, int nfreq,
                 double L, int precision, int nmax, double slab, const double* dstokes, int order, const double* data,
                 const double* sigma, double sigma_s, const uint8_t* mask, double* chi2_out, double* dparams, int accumulate,
-                double* image) {
+                double* image, const VisData* vd = nullptr) {
     if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
     if (nsets < 0 || (nsets > 0 && !sets)) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
     if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
@@ -1567,7 +1591,38 @@ int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double
     }
     // 2. seeds
     const long long nblk = (nrc + 255) / 256;
-    if (data) {
+    double vis_chi2 = 0.0;
+    if (vd) {
+        // the visibilities of the image, chi^2 of the gained model and the adjoint transform of its
+        // weights (frame_chi2_seed!): the DFT in the render's precision class (3xTF32 for the mixed path)
+        if (ncombo != 1) return fail(c, KS_ERR_ARGUMENT, "visibility chi^2 takes one frame at one frequency");
+        const int dprec = mixed ? KS_MIXED : KS_FP64;
+        int s = dft_checks(c, vd->nuv, vd->psize, vd->scale, dprec);
+        if (s) return s;
+        const int64_t nuv = vd->nuv;
+        const double *du, *dv, *dtap, *dg, *dvis;
+        if ((s = dft_stage(c, 1, vd->u, nuv, &du)) || (s = dft_stage(c, 2, vd->v, nuv, &dv)) ||
+            (s = dft_stage(c, 3, vd->tap, vd->tap ? nuv : 0, &dtap)) || (s = dft_stage(c, 6, vd->g, vd->g ? 2 * nuv : 0, &dg)) ||
+            (s = dft_stage(c, 7, vd->vis, size_t(nuv) * 8, &dvis)))
+            return s;
+        KS_CUDA(c, c->dft_in[4].ensure(size_t(nuv) * 8 * sizeof(double) * 2 + size_t(nuv) * 4 * sizeof(double)));
+        double* dV = c->dft_in[4].as<double>();
+        double* dW = dV + nuv * 8;
+        double* dS = dW + nuv * 8;
+        KS_CUDA(c, cudaMemcpyAsync(dS, vd->sigma, size_t(nuv) * 4 * sizeof(double), cudaMemcpyDefault, c->stream));
+        if ((s = dft_forward(c, c->out_sorted.as<double>(), KS_ORDER_SORTED, nuv, du, dv, dtap, vd->psize, vd->scale, dprec, dV))) return s;
+        const int vblk = int((nuv * 4 + 255) / 256);
+        KS_CUDA(c, c->dft_partial.ensure(size_t(vblk) * sizeof(double)));
+        ksdft::k_chi2_weights<<<vblk, 256, 0, c->stream>>>(nuv, dV, dg, dvis, dS, dW, c->dft_partial.as<double>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+        if ((s = dft_adjoint(c, dW, nuv, du, dv, dtap, vd->psize, vd->scale, dprec, c->seeds.as<double>(), KS_ORDER_SORTED, dprec != KS_FP64)))
+            return s;
+        std::vector<double> part(vblk);
+        KS_CUDA(c, cudaMemcpyAsync(part.data(), c->dft_partial.p, vblk * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        KS_CUDA(c, cudaStreamSynchronize(c->stream));
+        for (double p : part) vis_chi2 += p;   // fixed order
+    } else if (data) {
         const double *dd = nullptr, *ds = nullptr;
         const uint8_t* dm = nullptr;
         KS_CUDA(c, c->dstage.ensure(size_t(nrc) * 4 * sizeof(double) * (sigma ? 2 : 1) + size_t(nrc)));
@@ -1612,19 +1667,26 @@ int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double
                                    : (ch == 2 ? launch_adjoint_mixed_ch<2>(c, ntot, dtimes, dfreqs) : launch_adjoint_mixed_ch<1>(c, ntot, dtimes, dfreqs)));
         if (s) return s;
     } else if (ntot > 0) {
-        const size_t slot_bytes = size_t(GR_COUNT) * ntot * nrc * sizeof(double);
-        KS_CUDA(c, c->slots.ensure(slot_bytes));
-        KS_CUDA(c, cudaMemsetAsync(c->slots.p, 0, slot_bytes, c->stream));
+        // per-ray slots in ray chunks of at most 4 GB, each reduced (in ray order) into dgrad
+        const long long per_ray = (long long)GR_COUNT * ntot * ncombo * (long long)sizeof(double);
+        const long long nr = std::max(1LL, std::min(n, (4LL << 30) / per_ray));
+        KS_CUDA(c, c->slots.ensure(size_t(nr) * per_ray));
         KS_CUDA(c, cudaFuncSetAttribute(k_dual_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_smem));
-        k_dual_plain<<<nblocks(nrc), kBlock, tab_smem, c->stream>>>(plan_view(c), c->st, n, S, kst, c->tab.as<double>(), c->gtab.as<double>(),
-                                                                   ntot, dct, dcn, ncombo, L, c->tails.as<double>(), c->seeds.as<double>(),
-                                                                   c->slots.as<double>());
-        c->launches++;
-        c->adjoint_launches++;
-        KS_CUDA(c, cudaGetLastError());
-        k_slot_reduce<<<unsigned(GR_COUNT * ntot), 256, 0, c->stream>>>(c->slots.as<double>(), nrc, ntot, c->dgrad.as<double>());
-        c->launches++;
-        KS_CUDA(c, cudaGetLastError());
+        for (long long j0 = 0; j0 < n; j0 += nr) {
+            const long long m = std::min(nr, n - j0);
+            KS_CUDA(c, cudaMemsetAsync(c->slots.p, 0, size_t(m) * per_ray, c->stream));
+            k_dual_plain<<<nblocks(m * ncombo), kBlock, tab_smem, c->stream>>>(plan_view(c), c->st, n, S, kst, c->tab.as<double>(),
+                                                                              c->gtab.as<double>(), ntot, dct, dcn, ncombo, L,
+                                                                              c->tails.as<double>(), c->seeds.as<double>(),
+                                                                              c->slots.as<double>(), j0, m);
+            c->launches++;
+            c->adjoint_launches++;
+            KS_CUDA(c, cudaGetLastError());
+            k_slot_reduce<<<unsigned(GR_COUNT * ntot), 256, 0, c->stream>>>(c->slots.as<double>(), m * ncombo, ntot, c->dgrad.as<double>(),
+                                                                            j0 > 0 ? 1 : 0);
+            c->launches++;
+            KS_CUDA(c, cudaGetLastError());
+        }
     }
     cudaEventRecord(c->ev1, c->stream);
     // 4. results
@@ -1642,6 +1704,7 @@ int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double
         }
     }
     if (data && chi2_out) KS_CUDA(c, cudaMemcpyAsync(chi2_out, c->chi_val.p, sizeof(double), cudaMemcpyDefault, c->stream));
+    if (vd && chi2_out) *chi2_out = vis_chi2;
     if (image) {
         int s = emit(c, c->out_sorted.as<double>(), 4, ncombo, KS_ORDER_SCREEN, image);
         if (s) return s;
@@ -1927,6 +1990,16 @@ int ks_sample_adjoint(ks_context* c, int64_t n, const double* in, const double* 
     if (!dout) KS_CUDA(c, cudaMemcpyAsync(out, o, size_t(n) * 31 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
     return KS_OK;
+}
+
+int ks_vis_chi2_gradient(ks_context* c, const ks_splat_set* sets, int32_t nsets, double t_obs, double nu, double L, int32_t precision,
+                         int32_t nmax, double slab, int64_t nuv, const double* u, const double* v, const double* tap, const double* g,
+                         const double* vis, const double* sigma, double psize, double scale, double* chi2, double* dparams,
+                         int32_t accumulate, double* image) {
+    if (!c || !u || !v || !vis || !sigma || nuv < 1) return KS_ERR_ARGUMENT;
+    const VisData vd{nuv, u, v, tap, g, vis, sigma, psize, scale};
+    return adjoint_run(c, sets, nsets, &t_obs, 1, &nu, 1, L, precision, nmax, slab, nullptr, KS_ORDER_SCREEN, nullptr, nullptr, 0.0,
+                       nullptr, chi2, dparams, accumulate, image, &vd);
 }
 
 int ks_adjoint_stats(ks_context* c, double* adjoint_ms, long long* launches, int reset) {

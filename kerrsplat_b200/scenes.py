@@ -219,3 +219,23 @@ def config4(res=512, N=2048, nframes=32, density=768.0, nmin=128):
     return dict(a=a, theta_o=tho, camera=Camera((-15.0, 15.0), (-15.0, 15.0), res), N=N, M=64, density=density, nmin=nmin,
                 thermal=pt, powerlaw=pp, kappa=pk, knots=knots, knot_times=ktimes, times=times,
                 nus=np.array([86e9, 230e9, 345e9, 690e9]), L=gravitational_radius(4.0e6))
+
+
+def config5(res=1024, N=512, nsets=16, nuv=2000):
+    """Minibatched fit: a = 0.7, theta_o = 30 deg, +-16 M, N = 512 (assumed), 230 GHz, seed 4; nsets
+    THERMAL21 sets with S ~ U{32..512} splats; nuv (u, v) points uniform in a disk of radius 10 G-lambda;
+    M = 6.5e9 Msun, D = 16.8 Mpc (pixel size psize = d(alpha) L / D); the target of each set is its own
+    scene with every parameter perturbed by 5% (config-3 rule), observed with 2% complex Gaussian noise
+    relative to |V| (sigma = 0.02 |V|, floored at 1e-3 of the largest |V|)."""
+    rng = np.random.Generator(np.random.PCG64(4))
+    a, tho = 0.7, np.deg2rad(30.0)
+    counts = rng.integers(32, 513, nsets)
+    sets = [thermal_params(rng, int(s), a) for s in counts]
+    rad = 10e9 * np.sqrt(rng.uniform(0.0, 1.0, nuv))
+    ang = rng.uniform(0.0, 2 * np.pi, nuv)
+    L = gravitational_radius(6.5e9)
+    D = 16.8e6 * 3.0857e18
+    dalpha = 32.0 / (res - 1)
+    psize = dalpha * L / D
+    return dict(a=a, theta_o=tho, camera=Camera((-16.0, 16.0), (-16.0, 16.0), res), N=N, M=64, sets=sets, counts=counts,
+                u=rad * np.cos(ang), v=rad * np.sin(ang), psize=psize, scale=psize ** 2 / 1e-23, L=L, nu=230e9, t_obs=0.0, rng=rng)

@@ -266,3 +266,62 @@ def test_spacetime_derivatives_match_oracle(scene, oracle):
     # the context is back at (a, theta_o)
     again = np.asarray(ks.render(s["cache"], m, t, nu, L, precision=ks.KS_FP64))[0, 0]
     assert rel_l2(again, orc(a, th, L)) < 1e-10
+
+
+def test_vis_chi2_gradient(scene, oracle):
+    """The visibility chi^2 gradient of one frame (timeresolved_gradient!'s device path): the FP64
+    call equals frame_chi2_seed followed by the adjoint seeded with its image seed (1e-9), a few
+    components equal central differences of the oracle chi^2 (numpy DFT of oracle images, 1e-5),
+    and the mixed call (3xTF32 DFT, FP32 transport) is within 1e-3 of FP64."""
+    s = scene
+    c, cam = s["c"], s["cam"]
+    m = ks.PolarizedSplats(s["p"])
+    t, nu = 0.0, 230e9
+    rng = np.random.Generator(np.random.PCG64(29))
+    nuv = 60
+    rad = np.sqrt(rng.uniform(0, 1, nuv)) * 2e9
+    ang = rng.uniform(0, 2 * np.pi, nuv)
+    u, v = rad * np.cos(ang), rad * np.sin(ang)
+    Dcm = 16.8e6 * 3.0857e18
+    psize = (20.0 / (RES - 1)) * c["L"] / Dcm
+    scale = psize ** 2 / 1e-23
+    img = np.asarray(ks.render(s["cache"], m, [t], [nu], c["L"], precision=ks.KS_FP64))[0, 0]
+    V = oracle.visibilities(img, RES, RES, u, v, None, psize, scale)
+    vis = V * (1 + 0.1 * (rng.standard_normal(V.shape) + 1j * rng.standard_normal(V.shape)))
+    sigma = 0.05 * np.abs(V).max() * np.ones((nuv, 4))
+    chi64, g64 = ks.vis_chi2_gradient(s["cache"], m, t, nu, c["L"], u, v, vis, sigma, psize, scale, precision=ks.KS_FP64)
+    chi_ref, seed = ks.frame_chi2_seed(s["cache"], img, u, v, vis, sigma, psize, scale, precision=ks.KS_FP64)
+    g_ref = ks.adjoint(s["cache"], m, [t], [nu], c["L"], np.asarray(seed).reshape(1, 1, cam.npix, 4), precision=ks.KS_FP64)
+    assert abs(chi64 - chi_ref) <= 1e-10 * chi_ref
+    assert rel_l2(g64, g_ref) < 1e-9
+
+    def ochi(p):
+        im = oracle.polarized_image(c["a"], c["theta_o"], cam.alpha, cam.beta, N, c["M"], [("thermal", p, None)], t, nu, c["L"])
+        return oracle.frame_chi2_seed(im, RES, RES, u, v, None, None, vis, sigma, psize, scale)[0]
+
+    for (r, i) in [(12, 1), (13, 2), (0, 0), (17, 3), (20, 1)]:
+        h = 1e-7 * max(abs(s["p"][r, i]), 1.0)
+        pp, pm = s["p"].copy(), s["p"].copy()
+        pp[r, i] += h
+        pm[r, i] -= h
+        fd = (ochi(pp) - ochi(pm)) / (2 * h)
+        assert abs(g64[r, i] - fd) <= 1e-5 * max(abs(fd), 1e-4 * np.abs(g64).max()), (r, i, g64[r, i], fd)
+    chi32, g32 = ks.vis_chi2_gradient(s["cache"], m, t, nu, c["L"], u, v, vis, sigma, psize, scale, precision=ks.KS_MIXED)
+    print("vis chi2", chi64, chi32, "grad rel L2 mixed vs fp64", rel_l2(g32, g64))
+    assert abs(chi32 - chi64) <= 1e-3 * chi64 and rel_l2(g32, g64) < 1e-3
+
+
+def test_mixed_adjoint_large_splat_table():
+    # 320 splats: the element kernel's per-unit gradient blocks live in global memory
+    c = scenes.config2(res=12, N=64)
+    rng = np.random.Generator(np.random.PCG64(30))
+    p = scenes.thermal_params(rng, 320, c["a"], rlo=3.0, rhi=10.0)
+    cam = ks.Camera((-12.0, 12.0), (-12.0, 12.0), 12)
+    cache = ks.GeodesicCache(cam, 64)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    m = ks.PolarizedSplats(p)
+    ds = rng.standard_normal((1, 1, cam.npix, 4))
+    g64 = ks.adjoint(cache, m, [0.0], [230e9], c["L"], ds, precision=ks.KS_FP64)
+    g32 = ks.adjoint(cache, m, [0.0], [230e9], c["L"], ds, precision=ks.KS_MIXED)
+    print("320 splats: mixed vs fp64", rel_l2(g32, g64))
+    assert np.abs(g64).max() > 0 and rel_l2(g32, g64) < 1e-3
