@@ -369,13 +369,18 @@ def run_fit(args):
         noise = sig * (rng.standard_normal(V.shape) + 1j * rng.standard_normal(V.shape)) / np.sqrt(2)
         targets.append((V + noise, sig))
 
-    def one_set(q, prec):
+    def one_set(q, prec, times=None):
         p, (vis, sig) = c["sets"][q], targets[q]
         m = ks.PolarizedSplats(p)
+        t0 = time.perf_counter()
         chi2, g = ks.vis_chi2_gradient(cache, m, c["t_obs"], c["nu"], c["L"], c["u"], c["v"], vis, sig, c["psize"], c["scale"], precision=prec)
+        t1 = time.perf_counter()
         jv = ks.jvp(cache, m, [c["t_obs"]], [c["nu"]], c["L"], g, precision=prec)[0, 0, 0]
+        t2 = time.perf_counter()
         Vd = np.asarray(ks.visibilities(cache, jv, c["u"], c["v"], c["psize"], c["scale"], precision=prec))
         curv = float(np.sum(np.abs(Vd / sig) ** 2))
+        if times is not None:
+            times.update({"chi2_grad_ms": (t1 - t0) * 1e3, "jvp_ms": (t2 - t1) * 1e3, "dft_ms": (time.perf_counter() - t2) * 1e3})
         return chi2, float(np.sum(g * g)), curv
 
     for _ in range(args.warmup):
@@ -386,9 +391,10 @@ def run_fit(args):
     for _ in range(args.steps):
         for q in range(len(c["sets"])):
             t1 = time.perf_counter()
-            chi2, gg, curv = one_set(q, ks.KS_MIXED)
-            per_set.append({"splats": int(c["counts"][q]), "ms": (time.perf_counter() - t1) * 1e3, "chi2": chi2,
-                            "gn_step": -0.5 * gg / max(curv, 1e-300)})
+            tm = {}
+            chi2, gg, curv = one_set(q, ks.KS_MIXED, tm)
+            per_set.append(dict({"splats": int(c["counts"][q]), "ms": (time.perf_counter() - t1) * 1e3, "chi2": chi2,
+                                 "gn_step": -0.5 * gg / max(curv, 1e-300)}, **tm))
     ms_iter = (time.perf_counter() - t0) * 1e3 / args.steps
     line = {"metric": "fit iterations/s (minibatched)", "value": 1e3 / ms_iter, "unit": "iterations/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_iter, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -401,9 +407,10 @@ def run_fit(args):
             "per_set": per_set[:len(c["sets"])]}
     if args.fp64_steps > 0:
         t1 = time.perf_counter()
-        one_set(0, ks.KS_FP64)
+        tm = {}
+        one_set(0, ks.KS_FP64, tm)
         ms64 = (time.perf_counter() - t1) * 1e3
-        line["fp64_plain"] = {"set": 0, "splats": int(c["counts"][0]), "ms": ms64, "speedup_mixed_over_fp64": ms64 / per_set[0]["ms"]}
+        line["fp64_plain"] = dict({"set": 0, "splats": int(c["counts"][0]), "ms": ms64, "speedup_mixed_over_fp64": ms64 / per_set[0]["ms"]}, **tm)
     print(json.dumps(line), flush=True)
     cache.close()
 
@@ -466,13 +473,17 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gradient", action="store_true", help="skip the chi^2 + gradient measurement")
-    ap.add_argument("--res", type=int, default=256, help="screen resolution (smaller cases for profiling)")
-    ap.add_argument("--nsamples", type=int, default=1024)
+    ap.add_argument("--res", type=int, default=None, help="screen resolution (default: the workload's; smaller cases for profiling)")
+    ap.add_argument("--nsamples", type=int, default=None, help="samples per ray (default: the workload's)")
     ap.add_argument("--workload", default="polarized", choices=["polarized", "movie", "fit"],
                     help="polarized: configurations 2 and 3 (the headline); movie: configuration 4; fit: configuration 5")
     ap.add_argument("--sets", type=int, default=16, help="fit: parameter sets")
     ap.add_argument("--frames", type=int, default=32, help="movie frames")
     args = ap.parse_args()
+    # the sizes of each workload's configuration unless given
+    dres, dn = {"polarized": (256, 1024), "movie": (512, 2048), "fit": (1024, 512)}[args.workload]
+    args.res = dres if args.res is None else args.res
+    args.nsamples = dn if args.nsamples is None else args.nsamples
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "movie":

@@ -73,104 +73,10 @@ __device__ __forceinline__ void sample_adjoint(const MomentCoeffs& MC, const T* 
 // the coefficient partials by four duals in (a, a2, r2, ar), and dK/dtheta a constant sparse matrix:
 // <w, dK^2 v> = <w, G K v> + <K^T w, G v>, <w, dK^3 v> = <w, G K^2 v> + <K^T w, G K v> + <K^2T w, G v>.
 
-// the coefficients (o_n, e_n) of the rescaled step at the scaled invariants; same branches and
-// thresholds as step_operator
-template <class TD>
-__device__ __forceinline__ void step_coefficients(const MomentCoeffs& MC, TD a, TD a2, TD r2, TD ar, scalar_t<TD> D, TD o[4], TD e[4]) {
-    using S = scalar_t<TD>;
-    if ((a2 + r2) * D * D < lin_thr<TD>()) {
-        const TD ex = exp(-a), ph = phi_fn(MC, a), m1 = moment_n(MC, a, 1);
-        o[0] = ex; o[1] = -D * ex; o[2] = TD(S(0)); o[3] = TD(S(0));
-        e[0] = D * ph; e[1] = -(D * D) * m1; e[2] = TD(S(0)); e[3] = TD(S(0));
-        return;
-    }
-    const TD h = (a2 - r2) / S(2);
-    const TD rt2 = h * h + ar * ar;
-    const TD root = rt2 > S(0) ? sqrt(rt2) : TD(S(0));
-    TD L1sq, L2sq;
-    if (h >= S(0)) { L1sq = h + root; L2sq = L1sq > S(0) ? ar * ar / L1sq : TD(S(0)); }
-    else { L2sq = root - h; L1sq = L2sq > S(0) ? ar * ar / L2sq : TD(S(0)); }
-    const TD L1 = L1sq > S(0) ? sqrt(L1sq) : TD(S(0)), L2 = L2sq > S(0) ? sqrt(L2sq) : TD(S(0));
-    const TD b1 = L1 * D, b2 = L2 * D;
-    const TD Th = L1sq + L2sq;
-    const TD ex = exp(-a);
-    TD M[10];
-    moments(MC, a, M);
-    if (Th * D * D * ((a2 + r2) * D * D + S(1)) < cub_thr<TD>()) {
-        o[0] = ex; o[1] = -D * ex; o[2] = (D * D / S(2)) * ex; o[3] = -(D * D * D / S(6)) * ex;
-        e[0] = D * M[0]; e[1] = -(D * D) * M[1]; e[2] = (D * D * D / S(2)) * M[2]; e[3] = -(D * D * D * D / S(6)) * M[3];
-        return;
-    }
-    TD ecosh, esinhb, ecoshm1;
-    if (b1 < S(1)) {
-        const TD sh = sinh(b1 / S(2));
-        ecosh = ex * cosh(b1);
-        esinhb = ex * (fabs(b1) < S(0.1) ? sinhc_excess(b1) + S(1) : sinh(b1) / b1);
-        ecoshm1 = ex * S(2) * sh * sh;
-    } else {
-        const TD em = exp(-(a - b1)), ep = exp(-(a + b1));
-        ecosh = (em + ep) / S(2); esinhb = (em - ep) / (S(2) * b1); ecoshm1 = (em - S(2) * ex + ep) / S(2);
-    }
-    const TD sb2 = sin(b2), cb2 = cos(b2), sh2 = sin(b2 / S(2));
-    const TD c0 = (L2sq * ecosh + L1sq * ex * cb2) / Th;
-    const TD c2 = (ecoshm1 + ex * S(2) * sh2 * sh2) / Th;
-    const TD sincb2 = fabs(b2) < S(0.1) ? S(1) - sinc_deficit(b2) : sb2 / b2;
-    const TD so = D * esinhb, sn = D * ex * sincb2;
-    const TD ph_a = fabs(a) < S(1) ? M[0] : -expm1(-a) / a;
-    const TD icoshm1 = b1 < S(0.1) ? b1 * b1 * (M[2] / S(2) + b1 * b1 * (M[4] / S(24) + b1 * b1 * (M[6] / S(720) + b1 * b1 * M[8] / S(40320))))
-                                   : (phi_fn(MC, a - b1) + phi_fn(MC, a + b1)) / S(2) - ph_a;
-    const TD vser = b2 * b2 * (M[2] / S(2) - b2 * b2 * (M[4] / S(24) - b2 * b2 * (M[6] / S(720) - b2 * b2 * M[8] / S(40320))));
-    const TD icos_closed = (a - ex * (a * cb2 - b2 * sb2)) / (a * a + b2 * b2);
-    const TD iversin = b2 < S(0.1) ? vser : ph_a - icos_closed;
-    const TD icos = b2 < S(0.1) ? ph_a - vser : icos_closed;
-    const TD sdser = b2 * b2 * (M[3] / S(6) - b2 * b2 * (M[5] / S(120) - b2 * b2 * (M[7] / S(5040) - b2 * b2 * M[9] / S(362880))));
-    const TD isinc = b2 < S(0.1) ? M[1] - sdser : (S(1) - ex * (a * sb2 / b2 + cb2)) / (a * a + b2 * b2);
-    const TD ishx = b1 < S(0.1) ? b1 * b1 * (M[3] / S(6) + b1 * b1 * (M[5] / S(120) + b1 * b1 * (M[7] / S(5040) + b1 * b1 * M[9] / S(362880))))
-                                : (phi_fn(MC, a - b1) - phi_fn(MC, a + b1)) / (S(2) * b1) - M[1];
-    const TD Ich = D * (ph_a + icoshm1);
-    const TD Ic = D * icos;
-    const TD Ish = D * D * (M[1] + ishx);
-    const TD Is = D * D * isinc;
-    const TD C0 = (L2sq * Ich + L1sq * Ic) / Th;
-    const TD C2 = D * (icoshm1 + iversin) / Th;
-    o[0] = c0; o[1] = -(so * L2sq + sn * L1sq) / Th; o[2] = c2; o[3] = (sn - so) / Th;
-    e[0] = C0; e[1] = -(Ish * L2sq + Is * L1sq) / Th; e[2] = C2; e[3] = (Is - Ish) / Th;
-}
-
-// <x, G_theta y> for the six sparse generators G = dK/dtheta, theta = aQ, aU, aV, rQ, rU, rV
-template <class T>
-__device__ __forceinline__ void kgen_forms(const T x[4], const T y[4], T out[6]) {
-    out[0] = x[0] * y[1] + x[1] * y[0];
-    out[1] = x[0] * y[2] + x[2] * y[0];
-    out[2] = x[0] * y[3] + x[3] * y[0];
-    out[3] = x[2] * y[3] - x[3] * y[2];
-    out[4] = x[3] * y[1] - x[1] * y[3];
-    out[5] = x[1] * y[2] - x[2] * y[1];
-}
-
-template <class T>
-__device__ __forceinline__ void kmul(const T K[16], const T v[4], T out[4]) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) out[i] = K[4 * i] * v[0] + K[4 * i + 1] * v[1] + K[4 * i + 2] * v[2] + K[4 * i + 3] * v[3];
-}
-template <class T>
-__device__ __forceinline__ void kmul_t(const T K[16], const T v[4], T out[4]) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) out[i] = K[i] * v[0] + K[4 + i] * v[1] + K[8 + i] * v[2] + K[12 + i] * v[3];
-}
-template <class T>
-__device__ __forceinline__ T dot4(const T x[4], const T y[4]) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2] + x[3] * y[3]; }
-
 // sample_adjoint (transport.jl:221-245) with the structured partials; same outputs as sample_adjoint
 template <class T>
 __device__ __forceinline__ void sample_adjoint_structured(const MomentCoeffs& MC, const T* in, T Dl, const T w[4], const T R[4], T O[16],
                                                           T E[4], T cb[11]) {
-    T Ej[16];
-    step_operator(MC, in + 4, in + 8, Dl, O, Ej);
-#pragma unroll
-    for (int r = 0; r < 4; ++r) E[r] = Ej[4 * r] * in[0] + Ej[4 * r + 1] * in[1] + Ej[4 * r + 2] * in[2] + Ej[4 * r + 3] * in[3];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) cb[c] = Ej[c] * w[0] + Ej[4 + c] * w[1] + Ej[8 + c] * w[2] + Ej[12 + c] * w[3];
     const T s = pow2_below(Dl);
     const T D = Dl / s;
     const T aI = in[4] * s, aQ = in[5] * s, aU = in[6] * s, aV = in[7] * s, rQ = in[8] * s, rU = in[9] * s, rV = in[10] * s;
@@ -189,6 +95,28 @@ __device__ __forceinline__ void sample_adjoint_structured(const MomentCoeffs& MC
     kmul_t(K, w, Kw); kmul_t(K, Kw, K2w);
     const T P[4] = {dot4(w, R), dot4(w, KR), dot4(w, K2R), dot4(w, K3R)};
     const T J[4] = {dot4(w, jv), dot4(w, Kj), dot4(w, K2j), dot4(w, K3j)};
+    // the values: O = sum o_n K^n, E = s sum e_n K^n j, j-bar = Ej^T w = s sum e_n (K^n)^T w
+    {
+        T K2[16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) K2[4 * i + jj] = K[4 * i] * K[jj] + K[4 * i + 1] * K[4 + jj] + K[4 * i + 2] * K[8 + jj] + K[4 * i + 3] * K[12 + jj];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const T k3 = K2[4 * i] * K[jj] + K2[4 * i + 1] * K[4 + jj] + K2[4 * i + 2] * K[8 + jj] + K2[4 * i + 3] * K[12 + jj];
+                O[4 * i + jj] = ((i == jj) ? o[0].v : T(0)) + o[1].v * K[4 * i + jj] + o[2].v * K2[4 * i + jj] + o[3].v * k3;
+            }
+        T K3w[4];
+        kmul_t(K, K2w, K3w);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            E[i] = s * (e[0].v * jv[i] + e[1].v * Kj[i] + e[2].v * K2j[i] + e[3].v * K3j[i]);
+            cb[i] = s * (e[0].v * w[i] + e[1].v * Kw[i] + e[2].v * K2w[i] + e[3].v * K3w[i]);
+        }
+    }
     // through the invariants
     T dx[4];
 #pragma unroll
@@ -266,8 +194,12 @@ __device__ __forceinline__ bool element_adjoint(const T* p, const double* __rest
     Fd.lapse_inv = D(F.lapse_inv); Fd.om_lapse = D(F.om_lapse); Fd.sDS = D(F.sDS); Fd.misS = D(F.misS); Fd.ivarpi = D(F.ivarpi);
     Fd.r = D(F.r); Fd.sth = D(F.sth); Fd.cth = D(F.cth); Fd.a = D(F.a);
     const LFrame<D> lf = local_frame(Fd, u1, u2, u3, bx, by, bz, p[ST_BZERO] != T(0), D(alpha), D(beta), D(a_sin_tho));
-    const D thb = safe_acos(lf.cosB);
-    const D s2c = sin(T(2) * lf.chi), c2c = cos(T(2) * lf.chi);
+    // the pitch angle's sine and cosine: FP32 from its cosine directly (no angle formed), FP64 through
+    // safe_acos as the reference does
+    D sbv, cbv;
+    if constexpr (is_f32<T>) pitch_sc(lf.cosB, sbv, cbv);
+    else { const D thb = safe_acos(lf.cosB); sbv = sin(thb); cbv = cos(thb); }
+    const D s2c = lf.s2c, c2c = lf.c2c;
     const D ne(p[ST_NE] * G);
     T sc = T(0);
     T fl[7] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
@@ -277,7 +209,7 @@ __device__ __forceinline__ bool element_adjoint(const T* p, const double* __rest
         if (c >= nc || !((act >> c) & 1u)) continue;
         const T* cbc = cb + c * cstride;
         const D nuf = D(nu[c]) / lf.g;
-        const Coef<D> cf = thermal(ne, Te, f0, kr, Bm, nuf, thb);
+        const Coef<D> cf = thermal_cs(ne, Te, f0, kr, Bm, nuf, sbv, cbv);
         // screen_coefficients (transport.jl:265-270)
         if (!(cf.jI > T(0) || cf.aI > T(0) || cf.rQ != T(0) || cf.rV != T(0))) continue;
         const D fe = cap_factor(cf.jI, cf.jQ, cf.jV, D(T(0.99)));
@@ -361,7 +293,7 @@ __device__ __forceinline__ bool sample_coefficients(const T* tab, int ntot, cons
         T fa = cap_factor(cf.aI, cf.aQ, cf.aV, T(0.99));
         T nh = nuf / T(kNU0);
         T i2 = T(1) / (nh * nh);
-        T s2c = sin(T(2) * lf.chi), c2c = cos(T(2) * lf.chi);
+        T s2c = lf.s2c, c2c = lf.c2c;
         T jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
         out[0] += cf.jI * i2; out[1] += jQ * c2c; out[2] += jQ * s2c; out[3] += cf.jV * fe * i2;
         out[4] += nh * cf.aI; out[5] += aQ * c2c; out[6] += aQ * s2c; out[7] += cf.aV * fa * nh;
@@ -1170,8 +1102,12 @@ struct JvpSink {
         for (int q = 0; q < 11; ++q) in[q] = D(S(0));
         bool active = false, have_frame = false;
         SampleFrame<D> F;
+        const S rho = sqrt(x * x + y * y);
         for (int i = 0; i < ntot; ++i) {
             const D* p = tab + (long long)i * ST_COUNT;
+            // the circle of the pattern rotation, on values first (exact: outside it the support test fails too)
+            const S dr = rho - p[ST_RHO].v, dz = z - p[ST_CZ].v;
+            if (dr * dr + dz * dz > p[ST_SUPP].v) continue;
             D q;
             if (!splat_exponent(p, D(t), D(x), D(y), D(z), true, q)) continue;
             const D G = exp(-q);
@@ -1186,14 +1122,16 @@ struct JvpSink {
             const LFrame<D> lf = local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != S(0),
                                              D(alpha), D(beta), D(a_sin_tho));
             const D nuf = D(nu) / lf.g;
-            const D thb = safe_acos(lf.cosB);
-            const Coef<D> cf = thermal(p[ST_NE] * G, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
+            D sbv, cbv;
+            if constexpr (is_f32<S>) pitch_sc(lf.cosB, sbv, cbv);
+            else { const D thb = safe_acos(lf.cosB); sbv = sin(thb); cbv = cos(thb); }
+            const Coef<D> cf = thermal_cs(p[ST_NE] * G, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, sbv, cbv);
             if (!(cf.jI > S(0) || cf.aI > S(0) || cf.rQ != S(0) || cf.rV != S(0))) continue;
             const D fe = cap_factor(cf.jI, cf.jQ, cf.jV, D(S(0.99)));
             const D fa = cap_factor(cf.aI, cf.aQ, cf.aV, D(S(0.99)));
             const D nh = nuf / S(kNU0);
             const D i2 = D(S(1)) / (nh * nh);
-            const D s2c = sin(S(2) * lf.chi), c2c = cos(S(2) * lf.chi);
+            const D s2c = lf.s2c, c2c = lf.c2c;
             const D jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
             in[0] += cf.jI * i2; in[1] += jQ * c2c; in[2] += jQ * s2c; in[3] += cf.jV * fe * i2;
             in[4] += nh * cf.aI; in[5] += aQ * c2c; in[6] += aQ * s2c; in[7] += cf.aV * fa * nh;

@@ -537,7 +537,7 @@ struct PolSink {
                 T fa = cap_factor(cf.aI, cf.aQ, cf.aV, T(0.99));
                 T nh = nuf / T(kNU0);
                 T i2 = T(1) / (nh * nh);
-                T s2c = sin(T(2) * lf.chi), c2c = cos(T(2) * lf.chi);
+                T s2c = lf.s2c, c2c = lf.c2c;
                 T jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
                 j4[c][0] += cf.jI * i2; j4[c][1] += jQ * c2c; j4[c][2] += jQ * s2c; j4[c][3] += cf.jV * fe * i2;
                 a4[c][0] += nh * cf.aI; a4[c][1] += aQ * c2c; a4[c][2] += aQ * s2c; a4[c][3] += cf.aV * fa * nh;

@@ -103,15 +103,15 @@ __device__ __noinline__ LFrame<float> local_frame_ool(const float* s, const floa
 // KM: the populations the scene contains (bit 0 thermal, 1 power law, 2 kappa); the kernel for a
 // thermal-only scene carries none of the other fits' code.
 template <int KM>
-__device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, float ne, float nuf, float thb, float s2c, float c2c,
+__device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, float ne, float nuf, float sb, float cb, float s2c, float c2c,
                                                      float* r) {
     Coef<float> cf;
     if ((KM & 2) && kind == KS_POWERLAW22)
-        cf = powerlaw(ne, p[ST_P], p[ST_GMIN], p[ST_GSPAN], p[ST_GAMJ], p[ST_GAMA], p[ST_BMAG], nuf, thb);
+        cf = powerlaw_cs(ne, p[ST_P], p[ST_GMIN], p[ST_GSPAN], p[ST_GAMJ], p[ST_GAMA], p[ST_BMAG], nuf, sb, cb);
     else if ((KM & 4) && kind == KS_KAPPA22)
-        cf = kappa(ne, p[ST_KAP], p[ST_W], p[ST_HYP], p[ST_G43], p[ST_G2], p[ST_GQ], p[ST_GP], p[ST_GK2], p[ST_KB], p[ST_BMAG], nuf, thb);
+        cf = kappa_cs(ne, p[ST_KAP], p[ST_W], p[ST_HYP], p[ST_G43], p[ST_G2], p[ST_GQ], p[ST_GP], p[ST_GK2], p[ST_KB], p[ST_BMAG], nuf, sb, cb);
     else
-        cf = thermal(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, thb);
+        cf = thermal_cs(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, sb, cb);
     bool on = cf.jI > 0.f || cf.aI > 0.f || cf.rQ != 0.f || cf.rV != 0.f;
     if (!on) { r[352] = 0.f; return; }
     float fe = cap_factor(cf.jI, cf.jQ, cf.jV, 0.99f);
@@ -127,7 +127,7 @@ __device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, f
 
 __device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float* O, float* E) {
     float o[16], e[4];
-    transfer_step(c_moments, in, in + 4, in + 8, Dl, o, e);
+    transfer_step_structured(c_moments, in, in + 4, in + 8, Dl, o, e);
 #pragma unroll
     for (int q = 0; q < 16; ++q) O[q] = o[q];
 #pragma unroll
@@ -201,10 +201,10 @@ struct MixedSink {
         else splat_exponent(p, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], false, q);
         float G = __expf(-q);
         LFrame<float> lf = local_frame_ool(s, p, a, a_sin_tho);
-        float thb = acosf(fminf(1.f, fmaxf(-1.f, lf.cosB)));
+        float sb, cb;
+        pitch_sc(lf.cosB, sb, cb);
         float ne = p[ST_NE] * G;
-        float s2c, c2c;
-        sincosf(2.f * lf.chi, &s2c, &c2c);
+        const float s2c = lf.s2c, c2c = lf.c2c;
         int act = 0;
 #pragma unroll 1
         for (int c = 0; c < CH; ++c) {
@@ -213,7 +213,7 @@ struct MixedSink {
             float nuc = nu[0];
 #pragma unroll
             for (int cc = 1; cc < CH; ++cc) nuc = (cc == c) ? nu[cc] : nuc;
-            screen_coefficients_ool<KM>(kind, p, ne, nuc / lf.g, thb, s2c, c2c, r);
+            screen_coefficients_ool<KM>(kind, p, ne, nuc / lf.g, sb, cb, s2c, c2c, r);
             act |= r[352] != 0.f;
         }
         ev[4] += act ? 1 : 0;

@@ -94,8 +94,7 @@ __device__ __forceinline__ T planck(T nu, T Te) {
 // coefficients.jl:101-145 with the Bessel ratios of the splat table (f0 = K0/K2, kr = K1/K2, both 1
 // where K2 underflows)
 template <class T>
-__device__ __forceinline__ Coef<T> thermal(T ne, T Te, T f0, T kr, T B, T nu, T th) {
-    T st = sin(th), ct = cos(th);
+__device__ __forceinline__ Coef<T> thermal_cs(T ne, T Te, T f0, T kr, T B, T nu, T st, T ct) {
     const T PI = kpi<T>();
     T w0 = T(kEE) * B / (T(kME) * T(kCL));
     T wp2 = T(4) * PI * ne * T(kEE) * T(kEE) / T(kME);
@@ -106,8 +105,19 @@ __device__ __forceinline__ Coef<T> thermal(T ne, T Te, T f0, T kr, T B, T nu, T 
         return {T(0), T(0), T(0), T(0), T(0), T(0), T(0), rV0};
     }
     T x = Te * sqrt(T(1.4142135623730951) * st * (T(1e3) * w0w));
+    T sw;   // 0.5 + 0.5 tanh((ln x - ln 120) / 0.1)
+    if constexpr (is_f32<T>) {
+        // = x^20 / (x^20 + 120^20): the same function without log and tanh, as p^20 / (1 + p^20) with
+        // p = x / 120 below 120 and 1 / (1 + q^20) with q = 120 / x above (no overflow, so duals stay finite)
+        const bool lo = x < T(120);
+        const T q = lo ? x / T(120) : T(120) / x;
+        const T q2 = q * q, q4 = q2 * q2, q5 = q4 * q, q10 = q5 * q5, q20 = q10 * q10;
+        sw = lo ? q20 / (T(1) + q20) : T(1) / (T(1) + q20);
+    } else {
+        sw = T(0.5) + T(0.5) * tanh((flog(x) - T(4.787491742782046 /* ln 120 */)) / T(0.1));
+    }
     T extraterm = (T(0.011) * fexp(-x / T(47.2)) - T(7.9370052598409974e-01 /* 2^(-1/3) */) / T(67.44733739010397 /* 3^(23/6) */) * PI * T(1e4) * fpow(x + T(1e-16), T(-8.0 / 3))) *
-                  (T(0.5) + T(0.5) * tanh((flog(x) - T(4.787491742782046 /* ln 120 */)) / T(0.1)));
+                  sw;
     T jffunc = T(2.011) * fexp(-fpow(x, T(1.035)) / T(4.7)) - cos(x / T(2)) * fexp(-fpow(x, T(1.2)) / T(2.73)) - T(0.011) * fexp(-x / T(47.2)) + extraterm;
     T eps11m22 = jffunc * wp2w2 * w0w * w0w * (kr + T(6) * Te) * st * st;
     T rQ = w / (T(2) * T(kCL)) * eps11m22;
@@ -130,10 +140,10 @@ __device__ __forceinline__ Coef<T> thermal(T ne, T Te, T f0, T kr, T B, T nu, T 
 // coefficients.jl:208-256 (Pandya+ 2016 power-law fits, Jones & O'Dell rotativities); gamj, gama are
 // the splat's Gamma-function products, gspan = gmin^(1-p) - gmax^(1-p)
 template <class T>
-__device__ __forceinline__ Coef<T> powerlaw(T ne, T p, T gmin, T gspan, T gamj, T gama, T B, T nu, T th) {
+__device__ __forceinline__ Coef<T> powerlaw_cs(T ne, T p, T gmin, T gspan, T gamj, T gama, T B, T nu, T st, T ct) {
     // the fits divide by sin(theta) and raise it to negative powers: a field along the ray (a pitch
     // angle that rounds to 0 or pi, common in FP32) is evaluated 1e-6 from the axis
-    T st = fmax(sin(th), T(1e-6)), ct = cos(th);
+    st = fmax(st, T(1e-6));
     const T PI = kpi<T>();
     T nc = T(kEE) * B / (T(2) * PI * T(kME) * T(kCL));
     T pref = ne * T(kEE) * T(kEE) * nc / T(kCL);
@@ -177,8 +187,8 @@ __device__ __forceinline__ T kappa_rhoV_fit(int i, T w, T X) {
 // kappa.jl:109-155; g43 = Gamma(k - 4/3), g2 = Gamma(k - 2), gq = Gamma(k/4 - 1/3), gp = Gamma(k/4 + 4/3),
 // gk2 = Gamma(2 + k/2), kb = K0/(K2 + 1e-40) at 1/w (per splat)
 template <class T>
-__device__ __forceinline__ Coef<T> kappa(T ne, T kap, T w, T hyp, T g43, T g2, T gq, T gp, T gk2, T kb, T B, T nu, T th) {
-    T st = fmax(sin(th), T(1e-6)), ct = cos(th);   // as powerlaw: a field along the ray is evaluated 1e-6 from the axis
+__device__ __forceinline__ Coef<T> kappa_cs(T ne, T kap, T w, T hyp, T g43, T g2, T gq, T gp, T gk2, T kb, T B, T nu, T st, T ct) {
+    st = fmax(st, T(1e-6));   // as powerlaw: a field along the ray is evaluated 1e-6 from the axis
     const T PI = kpi<T>();
     const T small = T(1e-40);  // FP32: subnormal-flushes to 0; the guard below then reads |N_high| < 0
     T nc = T(kEE) * B / (T(2) * PI * T(kME) * T(kCL));
@@ -235,6 +245,25 @@ __device__ __forceinline__ Coef<T> kappa(T ne, T kap, T w, T hyp, T g43, T g2, T
     return {jI, jQ, jV, aI, aQ, aV, rQ, rV};
 }
 
+// The fits at the pitch angle th (the reference's signatures): its sine and cosine.
+template <class T>
+__device__ __forceinline__ Coef<T> thermal(T ne, T Te, T f0, T kr, T B, T nu, T th) { return thermal_cs(ne, Te, f0, kr, B, nu, sin(th), cos(th)); }
+template <class T>
+__device__ __forceinline__ Coef<T> powerlaw(T ne, T p, T gmin, T gspan, T gamj, T gama, T B, T nu, T th) {
+    return powerlaw_cs(ne, p, gmin, gspan, gamj, gama, B, nu, sin(th), cos(th));
+}
+template <class T>
+__device__ __forceinline__ Coef<T> kappa(T ne, T kap, T w, T hyp, T g43, T g2, T gq, T gp, T gk2, T kb, T B, T nu, T th) {
+    return kappa_cs(ne, kap, w, hyp, g43, g2, gq, gp, gk2, kb, B, nu, sin(th), cos(th));
+}
+// The pitch angle's sine and cosine from its (clamped) cosine: sin(acos c) = sqrt((1 - c)(1 + c)).
+template <class T>
+__device__ __forceinline__ void pitch_sc(T cosB, T& st, T& ct) {
+    ct = fmin(T(1), fmax(T(-1), cosB));
+    const T s2 = (T(1) - ct) * (T(1) + ct);
+    st = s2 > T(0) ? sqrt(s2) : T(0);
+}
+
 // coefficients.jl:264-288
 template <class T>
 __device__ __forceinline__ T cap_factor(T I, T Q, T V, T fmax_) {
@@ -286,8 +315,12 @@ __device__ __forceinline__ SampleFrame<T> sample_frame(T a, T r, T th, T sth, T 
     return F;
 }
 
+// g, the pitch-angle cosine, the screen angle chi and the rotation by 2 chi (s2c = sin 2chi, c2c =
+// cos 2chi). In FP32 the rotation comes straight from the Walker-Penrose components (x, y) of
+// chi = atan2(y, x): cos 2chi = (x^2 - y^2) / (x^2 + y^2), sin 2chi = 2 x y / (x^2 + y^2), with
+// no angle formed; in FP64 chi is formed as the reference forms it.
 template <class T>
-struct LFrame { T g, cosB, chi; };
+struct LFrame { T g, cosB, chi, s2c, c2c; };
 
 // frames.jl:108-128 for one splat (fluid ZAMO 3-velocity u, unit field direction bh)
 template <class T>
@@ -307,7 +340,7 @@ __device__ __forceinline__ LFrame<T> local_frame(const SampleFrame<T>& F, T u1, 
     T cosB = k0 * bx + k1 * by + k2 * bz;
     T f0 = k1 * bz - k2 * by, f1 = k2 * bx - k0 * bz, f2 = k0 * by - k1 * bx;
     T fn = sqrt(f0 * f0 + f1 * f1 + f2 * f2);
-    if (!(fn > T(0))) return {g, cosB, T(0)};
+    if (!(fn > T(0))) return {g, cosB, T(0), T(0), T(1)};
     f0 /= fn; f1 /= fn; f2 /= fn;
     // f_zamo = Lambda(-u) (0, f)
     T fd = u1 * f0 + u2 * f1 + u3 * f2;
@@ -323,7 +356,16 @@ __device__ __forceinline__ LFrame<T> local_frame(const SampleFrame<T>& F, T u1, 
     // screen_direction (frames.jl:78-81)
     T mu = -(alpha + a_sin_tho);
     T ea = beta * kk2 - mu * kk1, eb = beta * kk1 + mu * kk2;
-    return {g, cosB, atan2(-ea, eb)};
+    if constexpr (is_f32<T>) {
+        const T y = -ea, x = eb;
+        const T r2 = x * x + y * y;
+        if (!(r2 > T(0))) return {g, cosB, T(0), T(0), T(1)};
+        const T ir = T(1) / r2;
+        return {g, cosB, T(0), T(2) * x * y * ir, (x * x - y * y) * ir};
+    } else {
+        const T chi = atan2(-ea, eb);
+        return {g, cosB, chi, sin(T(2) * chi), cos(T(2) * chi)};
+    }
 }
 
 // ---- step.jl --------------------------------------------------------------------------------------
@@ -368,16 +410,17 @@ __device__ __forceinline__ void moments(const MomentCoeffs& MC, T a, T M[10]) {
         for (int n = 1; n < 10; ++n) M[n] = (T(n) * M[n - 1] - e) / a;
     }
 }
-// FP32: one out-of-line copy of the series (it would otherwise be unrolled at every call site)
+// FP32: one out-of-line copy; for |a| < 1 the series of M_9 and the downward recurrence
+// M_{n-1} = (a M_n + e^{-a}) / n, stable for |a| < 1 (each step scales the error by |a| / n)
 __device__ __noinline__ void moments_f32(const MomentCoeffs& MC, float a, float* M) {
     if (fabsf(a) < 1.f) {
-#pragma unroll 1
-        for (int n = 0; n < 10; ++n) {
-            float s = MC.cf[n][23];
+        float s = MC.cf[9][23];
 #pragma unroll
-            for (int m = 22; m >= 0; --m) s = fmaf(a, s, MC.cf[n][m]);
-            M[n] = s;
-        }
+        for (int m = 22; m >= 0; --m) s = fmaf(a, s, MC.cf[9][m]);
+        M[9] = s;
+        const float e = expf(-a);
+#pragma unroll
+        for (int n = 9; n >= 1; --n) M[n - 1] = (a * M[n] + e) * (1.f / float(n));
     } else {
         float e = expf(-a);
         M[0] = (1.f - e) / a;
@@ -544,6 +587,126 @@ __device__ __forceinline__ void transfer_step(const MomentCoeffs& MC, const T j4
     step_operator(MC, al, rh, Dlen, O, Ej);
 #pragma unroll
     for (int i = 0; i < 4; ++i) E[i] = Ej[4 * i] * j4[0] + Ej[4 * i + 1] * j4[1] + Ej[4 * i + 2] * j4[2] + Ej[4 * i + 3] * j4[3];
+}
+
+// the coefficients (o_n, e_n) of the rescaled step at the scaled invariants; same branches and
+// thresholds as step_operator
+template <class TD>
+__device__ __forceinline__ void step_coefficients(const MomentCoeffs& MC, TD a, TD a2, TD r2, TD ar, scalar_t<TD> D, TD o[4], TD e[4]) {
+    using S = scalar_t<TD>;
+    if ((a2 + r2) * D * D < lin_thr<TD>()) {
+        const TD ex = exp(-a), ph = phi_fn(MC, a), m1 = moment_n(MC, a, 1);
+        o[0] = ex; o[1] = -D * ex; o[2] = TD(S(0)); o[3] = TD(S(0));
+        e[0] = D * ph; e[1] = -(D * D) * m1; e[2] = TD(S(0)); e[3] = TD(S(0));
+        return;
+    }
+    const TD h = (a2 - r2) / S(2);
+    const TD rt2 = h * h + ar * ar;
+    const TD root = rt2 > S(0) ? sqrt(rt2) : TD(S(0));
+    TD L1sq, L2sq;
+    if (h >= S(0)) { L1sq = h + root; L2sq = L1sq > S(0) ? ar * ar / L1sq : TD(S(0)); }
+    else { L2sq = root - h; L1sq = L2sq > S(0) ? ar * ar / L2sq : TD(S(0)); }
+    const TD L1 = L1sq > S(0) ? sqrt(L1sq) : TD(S(0)), L2 = L2sq > S(0) ? sqrt(L2sq) : TD(S(0));
+    const TD b1 = L1 * D, b2 = L2 * D;
+    const TD Th = L1sq + L2sq;
+    const TD ex = exp(-a);
+    TD M[10];
+    moments(MC, a, M);
+    if (Th * D * D * ((a2 + r2) * D * D + S(1)) < cub_thr<TD>()) {
+        o[0] = ex; o[1] = -D * ex; o[2] = (D * D / S(2)) * ex; o[3] = -(D * D * D / S(6)) * ex;
+        e[0] = D * M[0]; e[1] = -(D * D) * M[1]; e[2] = (D * D * D / S(2)) * M[2]; e[3] = -(D * D * D * D / S(6)) * M[3];
+        return;
+    }
+    TD ecosh, esinhb, ecoshm1;
+    if (b1 < S(1)) {
+        const TD sh = sinh(b1 / S(2));
+        ecosh = ex * cosh(b1);
+        esinhb = ex * (fabs(b1) < S(0.1) ? sinhc_excess(b1) + S(1) : sinh(b1) / b1);
+        ecoshm1 = ex * S(2) * sh * sh;
+    } else {
+        const TD em = exp(-(a - b1)), ep = exp(-(a + b1));
+        ecosh = (em + ep) / S(2); esinhb = (em - ep) / (S(2) * b1); ecoshm1 = (em - S(2) * ex + ep) / S(2);
+    }
+    const TD sb2 = sin(b2), cb2 = cos(b2), sh2 = sin(b2 / S(2));
+    const TD c0 = (L2sq * ecosh + L1sq * ex * cb2) / Th;
+    const TD c2 = (ecoshm1 + ex * S(2) * sh2 * sh2) / Th;
+    const TD sincb2 = fabs(b2) < S(0.1) ? S(1) - sinc_deficit(b2) : sb2 / b2;
+    const TD so = D * esinhb, sn = D * ex * sincb2;
+    const TD ph_a = fabs(a) < S(1) ? M[0] : -expm1(-a) / a;
+    const TD icoshm1 = b1 < S(0.1) ? b1 * b1 * (M[2] / S(2) + b1 * b1 * (M[4] / S(24) + b1 * b1 * (M[6] / S(720) + b1 * b1 * M[8] / S(40320))))
+                                   : (phi_fn(MC, a - b1) + phi_fn(MC, a + b1)) / S(2) - ph_a;
+    const TD vser = b2 * b2 * (M[2] / S(2) - b2 * b2 * (M[4] / S(24) - b2 * b2 * (M[6] / S(720) - b2 * b2 * M[8] / S(40320))));
+    const TD icos_closed = (a - ex * (a * cb2 - b2 * sb2)) / (a * a + b2 * b2);
+    const TD iversin = b2 < S(0.1) ? vser : ph_a - icos_closed;
+    const TD icos = b2 < S(0.1) ? ph_a - vser : icos_closed;
+    const TD sdser = b2 * b2 * (M[3] / S(6) - b2 * b2 * (M[5] / S(120) - b2 * b2 * (M[7] / S(5040) - b2 * b2 * M[9] / S(362880))));
+    const TD isinc = b2 < S(0.1) ? M[1] - sdser : (S(1) - ex * (a * sb2 / b2 + cb2)) / (a * a + b2 * b2);
+    const TD ishx = b1 < S(0.1) ? b1 * b1 * (M[3] / S(6) + b1 * b1 * (M[5] / S(120) + b1 * b1 * (M[7] / S(5040) + b1 * b1 * M[9] / S(362880))))
+                                : (phi_fn(MC, a - b1) - phi_fn(MC, a + b1)) / (S(2) * b1) - M[1];
+    const TD Ich = D * (ph_a + icoshm1);
+    const TD Ic = D * icos;
+    const TD Ish = D * D * (M[1] + ishx);
+    const TD Is = D * D * isinc;
+    const TD C0 = (L2sq * Ich + L1sq * Ic) / Th;
+    const TD C2 = D * (icoshm1 + iversin) / Th;
+    o[0] = c0; o[1] = -(so * L2sq + sn * L1sq) / Th; o[2] = c2; o[3] = (sn - so) / Th;
+    e[0] = C0; e[1] = -(Ish * L2sq + Is * L1sq) / Th; e[2] = C2; e[3] = (Is - Ish) / Th;
+}
+
+// <x, G_theta y> for the six sparse generators G = dK/dtheta, theta = aQ, aU, aV, rQ, rU, rV
+template <class T>
+__device__ __forceinline__ void kgen_forms(const T x[4], const T y[4], T out[6]) {
+    out[0] = x[0] * y[1] + x[1] * y[0];
+    out[1] = x[0] * y[2] + x[2] * y[0];
+    out[2] = x[0] * y[3] + x[3] * y[0];
+    out[3] = x[2] * y[3] - x[3] * y[2];
+    out[4] = x[3] * y[1] - x[1] * y[3];
+    out[5] = x[1] * y[2] - x[2] * y[1];
+}
+
+template <class T>
+__device__ __forceinline__ void kmul(const T K[16], const T v[4], T out[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = K[4 * i] * v[0] + K[4 * i + 1] * v[1] + K[4 * i + 2] * v[2] + K[4 * i + 3] * v[3];
+}
+template <class T>
+__device__ __forceinline__ void kmul_t(const T K[16], const T v[4], T out[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = K[i] * v[0] + K[4 + i] * v[1] + K[8 + i] * v[2] + K[12 + i] * v[3];
+}
+template <class T>
+__device__ __forceinline__ T dot4(const T x[4], const T y[4]) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2] + x[3] * y[3]; }
+
+// The exact step in its structured form: O = sum_n o_n K^n, E = s sum_n e_n K^n j with the
+// coefficients of step_coefficients, K the rescaled matrix and s the power-of-two rescaling: the same
+// operator as transfer_step (the same branches and thresholds), with one assembly for all branches.
+template <class T>
+__device__ __forceinline__ void transfer_step_structured(const MomentCoeffs& MC, const T j4[4], const T al[4], const T rh[3], T Dl, T O[16],
+                                                         T E[4]) {
+    const T s = pow2_below(Dl);
+    const T D = Dl / s;
+    const T aI = al[0] * s, aQ = al[1] * s, aU = al[2] * s, aV = al[3] * s, rQ = rh[0] * s, rU = rh[1] * s, rV = rh[2] * s;
+    T o[4], e[4];
+    step_coefficients(MC, aI * D, aQ * aQ + aU * aU + aV * aV, rQ * rQ + rU * rU + rV * rV, aQ * rQ + aU * rU + aV * rV, D, o, e);
+    T K[16];
+    K[0] = 0; K[1] = aQ; K[2] = aU; K[3] = aV; K[4] = aQ; K[5] = 0; K[6] = rV; K[7] = -rU;
+    K[8] = aU; K[9] = -rV; K[10] = 0; K[11] = rQ; K[12] = aV; K[13] = rU; K[14] = -rQ; K[15] = 0;
+    T K2[16];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) K2[4 * i + jj] = K[4 * i] * K[jj] + K[4 * i + 1] * K[4 + jj] + K[4 * i + 2] * K[8 + jj] + K[4 * i + 3] * K[12 + jj];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const T k3 = K2[4 * i] * K[jj] + K2[4 * i + 1] * K[4 + jj] + K2[4 * i + 2] * K[8 + jj] + K2[4 * i + 3] * K[12 + jj];
+            O[4 * i + jj] = ((i == jj) ? o[0] : T(0)) + o[1] * K[4 * i + jj] + o[2] * K2[4 * i + jj] + o[3] * k3;
+        }
+    T Kj[4], K2j[4], K3j[4];
+    kmul(K, j4, Kj); kmul(K, Kj, K2j); kmul(K, K2j, K3j);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) E[i] = s * (e[0] * j4[i] + e[1] * Kj[i] + e[2] * K2j[i] + e[3] * K3j[i]);
 }
 
 // ---- splats -------------------------------------------------------------------------------------
