@@ -129,6 +129,9 @@ def run_ours(args):
     cache = ks.GeodesicCache(c["camera"], c["N"], device=local)
     ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
     dev = torch.device("cuda", local)
+    tuned = None
+    if args.autotune and prec != ks.KS_FP64:
+        tuned = ks.autotune(cache, ks.PolarizedSplats(c["params"]), [c["t_obs"]], c["nus"], c["L"], trials=1)
     model_dev = ks.PolarizedSplats(torch.tensor(c["params"], device=dev))
     times_dev = torch.tensor([c["t_obs"]], dtype=torch.float64, device=dev)
     nus_dev = torch.tensor(c["nus"], dtype=torch.float64, device=dev)
@@ -206,6 +209,7 @@ def run_ours(args):
                      "kernel": "k_polarized", "flops_per_launch": flops_per_launch, "sfu_ops_per_launch": sfu / max(launches_per_step, 1),
                      "events": counts},
         "gpu_launches": int(all_launches),
+        "autotune": None if tuned is None else {"block": tuned[0], "units_per_warp": tuned[1], "ms": tuned[2]},
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -473,6 +477,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gradient", action="store_true", help="skip the chi^2 + gradient measurement")
+    ap.add_argument("--autotune", action=argparse.BooleanOptionalAction, default=True,
+                    help="time the consumer's launch shapes before the timed steps (ks_autotune)")
     ap.add_argument("--res", type=int, default=None, help="screen resolution (default: the workload's; smaller cases for profiling)")
     ap.add_argument("--nsamples", type=int, default=None, help="samples per ray (default: the workload's)")
     ap.add_argument("--workload", default="polarized", choices=["polarized", "movie", "fit"],

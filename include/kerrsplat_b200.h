@@ -226,6 +226,14 @@ int ks_kernel_stats(ks_context* ctx, double* render_ms, long long* render_launch
  * and the launch count of their reverse-pass kernels. */
 int ks_adjoint_stats(ks_context* ctx, double* adjoint_ms, long long* launches, int reset);
 
+/* The autotuner of the mixed forward pass: renders the scene (mixed precision) with every block size
+ * (384, 256, 128 threads of the persistent consumer, where it fits) and work-unit density (2, 4, 8 or 16
+ * work units per resident warp, which sets how finely rays are split into sample segments), `trials`
+ * timed renders each after one warm-up, and keeps the fastest for this context's later calls; block,
+ * units and best_ms (the render kernels' time) report the choice. */
+int ks_autotune(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+                int32_t nfreq, double L, int32_t nmax, double slab, int32_t trials, int32_t* block, int32_t* units, double* best_ms);
+
 /* Count work events during ks_render (samples, valid samples, splat tests, weights evaluated,
  * coefficient evaluations, local frames, transfer steps); ks_event_counts reads the 7 counters of
  * the last counted render. */

@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -531,6 +531,18 @@ def spacetime_derivatives(cache, model, times, nus, L, h_a=1e-5, h_theta=1e-5, n
                                                      int(nmax), float(slab), float(h_a), float(h_theta), _ptr(out),
                                                      _ptr(img) if img is not None else None))
     return (out, img) if return_image else out
+
+
+def autotune(cache, model, times, nus, L, nmax=-1, slab=0.0, trials=2):
+    """Pick the mixed forward pass's block size and work-unit density for this scene by timing every
+    candidate on the GPU; later renders of the cache use the choice. Returns (block, units, ms)."""
+    times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+    nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+    arr, nsets, _keep = _set_array(model)
+    b, u, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+    cache._check(cache._lib.ks_autotune(cache._ctx, arr, nsets, _ptr(times), int(times.shape[0]), _ptr(nus), int(nus.shape[0]), float(L),
+                                        int(nmax), float(slab), int(trials), ctypes.byref(b), ctypes.byref(u), ctypes.byref(ms)))
+    return b.value, u.value, ms.value
 
 
 def normal_matrix(cache, J, precision=KS_FP64):

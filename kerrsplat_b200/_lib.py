@@ -89,6 +89,9 @@ EXTRA_SIGNATURES = [
     ("ks_set_event_counting", ctypes.c_int, [_VP, ctypes.c_int]),
     ("ks_event_counts", ctypes.c_int, [_VP, _VP]),
     ("ks_adjoint_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+    ("ks_autotune", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32, ctypes.c_double,
+                                   ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.POINTER(ctypes.c_int32), _D]),
     ("ks_thin_image_noalloc", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _VP, ctypes.c_int32]),
 ]
 

@@ -668,6 +668,7 @@ struct ks_context {
     DevBuf gtab, samples, kstop, tails, slots, dgrad, seeds, chi_part, chi_val, dstage;
     DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part, jvp_tab, jvp_in, jvp_out, st_buf;
     bool samples_ready = false;
+    int tune_nt = 0, tune_units = 0;        // the autotuner's choice for the mixed forward (0: the default)
     int nkv = 0;                            // knot values after the splat table in `tab`
     MixedJob last_job{};                    // the segmentation of the last mixed forward pass
     float* fwd_gstate = nullptr;            // set during the adjoint's forward pass only
@@ -862,7 +863,8 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     const long long resident = (long long)nsm * per_sm * W;
     const long long base_units = job.nchunks * job.nframes * job.nvc;
     int nseg = 1;
-    while (job.nmax < 0 && base_units * nseg < 8 * resident && (nseg * 2) * 16 <= N) nseg *= 2;
+    const int units_per_warp = c->tune_units > 0 ? c->tune_units : 8;
+    while (job.nmax < 0 && base_units * nseg < units_per_warp * resident && (nseg * 2) * 16 <= N) nseg *= 2;
     job.seg_len = (N + nseg - 1) / nseg;
     job.nseg = (N + job.seg_len - 1) / job.seg_len;
     job.total = base_units * job.nseg;
@@ -930,6 +932,10 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
               w128 = consume_blocks<CH, 128, KM>(c, ntot) * 4;
     const int best = std::max(w384, std::max(w256, w128));
     if (best <= 0) return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
+    // the autotuner's block size when it fits
+    if (c->tune_nt == 384 && w384 > 0) return launch_consume<CH, 384, KM>(c, job, ntot, nsm, w384 / 12);
+    if (c->tune_nt == 256 && w256 > 0) return launch_consume<CH, 256, KM>(c, job, ntot, nsm, w256 / 8);
+    if (c->tune_nt == 128 && w128 > 0) return launch_consume<CH, 128, KM>(c, job, ntot, nsm, w128 / 4);
     if (w384 == best) return launch_consume<CH, 384, KM>(c, job, ntot, nsm, w384 / 12);
     if (w256 == best) return launch_consume<CH, 256, KM>(c, job, ntot, nsm, w256 / 8);
     if (w128 > 0) return launch_consume<CH, 128, KM>(c, job, ntot, nsm, w128 / 4);
@@ -2000,6 +2006,38 @@ int ks_vis_chi2_gradient(ks_context* c, const ks_splat_set* sets, int32_t nsets,
     const VisData vd{nuv, u, v, tap, g, vis, sigma, psize, scale};
     return adjoint_run(c, sets, nsets, &t_obs, 1, &nu, 1, L, precision, nmax, slab, nullptr, KS_ORDER_SCREEN, nullptr, nullptr, 0.0,
                        nullptr, chi2, dparams, accumulate, image, &vd);
+}
+
+int ks_autotune(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
+                int32_t nfreq, double L, int32_t nmax, double slab, int32_t trials, int32_t* block, int32_t* units, double* best_ms) {
+    if (!c || trials < 1) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    const long long n4 = c->npix * (long long)nframes * nfreq * 4;
+    if (nframes < 1 || nfreq < 1) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    KS_CUDA(c, c->st_buf.ensure(size_t(n4) * sizeof(double)));
+    const int cand_nt[3] = {384, 256, 128}, cand_u[4] = {2, 4, 8, 16};
+    double best = 1e300;
+    int bnt = 0, bu = 0;
+    const int save_nt = c->tune_nt, save_u = c->tune_units;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 4; ++b) {
+            c->tune_nt = cand_nt[a]; c->tune_units = cand_u[b];
+            int s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L, KS_MIXED, nmax, slab, c->st_buf.as<double>(), KS_ORDER_SORTED);
+            if (s) { c->tune_nt = save_nt; c->tune_units = save_u; return s; }
+            const double before = c->kernel_ms;
+            for (int t = 0; t < trials; ++t) {
+                s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L, KS_MIXED, nmax, slab, c->st_buf.as<double>(), KS_ORDER_SORTED);
+                if (s) { c->tune_nt = save_nt; c->tune_units = save_u; return s; }
+            }
+            const double ms = (c->kernel_ms - before) / trials;
+            if (ms < best) { best = ms; bnt = cand_nt[a]; bu = cand_u[b]; }
+        }
+    c->tune_nt = bnt; c->tune_units = bu;
+    if (block) *block = bnt;
+    if (units) *units = bu;
+    if (best_ms) *best_ms = best;
+    return KS_OK;
 }
 
 int ks_adjoint_stats(ks_context* c, double* adjoint_ms, long long* launches, int reset) {

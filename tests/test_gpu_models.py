@@ -131,3 +131,18 @@ def test_uneven_sample_counts_match_oracle(oracle, prec, tol):
     print("uneven", prec, counts, errs, ev["samples"], int(nsorted.sum()) * len(nus))
     assert max(errs.values()) < tol, errs
     assert ev["samples"] == int(nsorted.sum()) * len(nus)
+
+
+def test_autotune_keeps_results(oracle):
+    # ks_autotune picks a launch shape by timing; the image stays within the mixed tolerance
+    c = scenes.config2(res=24, N=128)
+    rng = np.random.Generator(np.random.PCG64(34))
+    p = scenes.thermal_params(rng, 8, c["a"])
+    cache = ks.GeodesicCache(c["camera"], c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    m = ks.PolarizedSplats(p)
+    block, units, ms = ks.autotune(cache, m, [0.0], c["nus"], c["L"], trials=1)
+    assert block in (128, 256, 384) and units in (2, 4, 8, 16) and ms > 0
+    out = np.asarray(ks.render(cache, m, [0.0], c["nus"], c["L"], precision=ks.KS_MIXED))
+    ref = np.asarray(ks.render(cache, m, [0.0], c["nus"], c["L"], precision=ks.KS_FP64))
+    assert rel_l2(out, ref) < 1e-4
