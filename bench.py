@@ -36,6 +36,10 @@ UNIT = "ray-samples/s"
 FLOPS = {"samples": 330, "valid_samples": 95, "splat_tests": 22, "weights": 32, "coefficients": 170,
          "frames": 115, "steps": 1150}
 SFU = {"samples": 12, "valid_samples": 9, "splat_tests": 2, "weights": 1, "coefficients": 22, "frames": 4, "steps": 12}
+# k_consume's DRAM traffic per ray-sample: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch
+# at 192x192, N = 1024, 3 frequencies (1.3315e9 + 0.1376e9 B over 36864 x 1024 ray-samples; reads = the
+# FP32 sample stream, 32 B per ray-sample, + the plan; writes = segment states), scaled by ray-samples
+CONSUME_TRAFFIC_PER_RAY_SAMPLE = (1.3315e9 + 0.1376e9) / (36864 * 1024)
 
 
 def rank_info():
@@ -154,6 +158,7 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     cache.kernel_stats(reset=True)
+    cache.consume_stats(reset=True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize(dev)
@@ -164,6 +169,7 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
     ms_total = e0.elapsed_time(e1)
     render_ms, render_launches, all_launches = cache.kernel_stats(reset=True)
+    consume_ms, consume_launches = cache.consume_stats(reset=True)
     ms_total = max_over_ranks(ms_total, dev)
     ms_step = ms_total / args.steps
     value = units_per_step * world / (ms_step / 1e3)
@@ -185,11 +191,23 @@ def run_ours(args):
     e2e_ms = max_over_ranks(e2e_ms, dev)
     e2e_value = units_per_step * world / (e2e_ms / 1e3)
 
-    # roofline of the dominant kernel (k_polarized): algorithmic FP32 work per launch / its time
-    flops = sum(FLOPS[k] * counts[k] for k in FLOPS)
-    sfu = sum(SFU[k] * counts[k] for k in SFU)
-    launch_ms = render_ms / max(render_launches, 1)
-    launches_per_step = render_launches / args.steps
+    # roofline of the dominant kernel: k_consume on the mixed path (the march runs before it in
+    # k_stream, so its per-sample flops are left out), k_polarized<double> on the FP64 plain path;
+    # algorithmic FP32 (FP64) work per launch / its CUDA-event time
+    if prec != ks.KS_FP64 and consume_launches > 0:
+        kname = "k_consume"
+        flops = sum(FLOPS[k] * counts[k] for k in FLOPS if k != "samples")
+        sfu = sum(SFU[k] * counts[k] for k in SFU if k != "samples")
+        launch_ms = consume_ms / consume_launches
+        launches_per_step = consume_launches / args.steps
+        traffic = CONSUME_TRAFFIC_PER_RAY_SAMPLE * cache.npix * c["N"]
+    else:
+        kname = "k_polarized<double,1>"
+        flops = sum(FLOPS[k] * counts[k] for k in FLOPS)
+        sfu = sum(SFU[k] * counts[k] for k in SFU)
+        launch_ms = render_ms / max(render_launches, 1)
+        launches_per_step = render_launches / args.steps
+        traffic = None
     flops_per_launch = flops / max(launches_per_step, 1)
     achieved = flops_per_launch / (launch_ms / 1e3) / 1e12
     pk = peaks()
@@ -205,9 +223,12 @@ def run_ours(args):
                    "l2": "no flush: the per-ray FP64 plan + anchor table (~150 MB) exceeds the 126 MB L2"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "traffic": None, "peak_source": "nominal FP32 pipe (148 SMs x 128 lanes x 2 x max SM clock); MEASURED_PEAKS.json has no FP32 figure",
-                     "kernel": "k_polarized", "flops_per_launch": flops_per_launch, "sfu_ops_per_launch": sfu / max(launches_per_step, 1),
-                     "events": counts},
+                     "traffic": traffic, "traffic_source": "ncu DRAM bytes of one k_consume launch at 192x192 N=1024, scaled by ray-samples"
+                     if traffic else None,
+                     "peak_source": "nominal FP32 pipe (148 SMs x 128 lanes x 2 x max SM clock); MEASURED_PEAKS.json has no FP32 figure",
+                     "kernel": kname, "kernel_ms": launch_ms, "flops_per_launch": flops_per_launch,
+                     "sfu_ops_per_launch": sfu / max(launches_per_step, 1), "events": counts,
+                     "hbm_frac": (traffic / (launch_ms / 1e3) / 1e9) / pk["hbm_gbs"] if traffic and pk.get("hbm_gbs") else None},
         "gpu_launches": int(all_launches),
         "autotune": None if tuned is None else {"block": tuned[0], "units_per_warp": tuned[1], "ms": tuned[2]},
         "clocks": {k: clocks[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")},

@@ -192,13 +192,14 @@ int ks_jvp(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const doubl
 
 /* The image's derivatives with respect to the spacetime block (a, theta_o, ln L) that
  * spacetime_valgrad (src/Fit/joint.jl:74-82) takes with three-partial duals through regenerate! and the
- * transport: dimage (3 x nfreq x nframes x npix x 4, screen order) = d/da, d/dtheta_o by central
- * differences of the render with steps h_a, h_theta (four regenerates, the context regenerated back at
- * (a, theta_o) before the call returns), and d/d(ln L) exactly (a dual on the step length, through the
- * J v pass) for thermal scenes, by central differences otherwise. image (optional): the image. */
+ * transport: dimage (3 x nfreq x nframes x npix x 4, screen order) = d/da, d/dtheta_o, d/d(ln L) of the
+ * observed Stokes images, exact forward-mode duals through the ray constants, the Mino step, the anchors,
+ * the recurrence march and the polarized consumer (all splat kinds, knot splats included) at the
+ * context's sample counts, anchor spacing and sorted order. The pass runs in FP64 duals for either
+ * precision. image (optional, screen order): the image of the same pass. The context is not changed. */
 int ks_spacetime_derivatives(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes,
-                             const double* nus, int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, double h_a,
-                             double h_theta, double* dimage, double* image);
+                             const double* nus, int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, double* dimage,
+                             double* image);
 
 /* normal_matrix(J) (src/Fit/gauss_newton.jl:486-494): A = J^T J of a row-major m x n Jacobian (FP64),
  * A n x n. KS_FP64: FP64 tiles; KS_MIXED: the 3xTF32 tensor-core GEMM with FP32 accumulation. */
@@ -221,6 +222,10 @@ int ks_context_stream(ks_context* ctx, void** stream);
 /* Device time (CUDA events on the context stream) of the render kernels since the last reset,
  * their launch count, and the launch count of every kernel of this library. */
 int ks_kernel_stats(ks_context* ctx, double* render_ms, long long* render_launches, long long* all_launches, int reset);
+
+/* Device time (CUDA events on the context stream) of the persistent consumer k_consume alone in the
+ * mixed ks_render calls since the last reset, and its launch count (one per mixed render). */
+int ks_consume_stats(ks_context* ctx, double* consume_ms, long long* launches, int reset);
 
 /* Device time (CUDA events) of the adjoint calls (ks_adjoint, ks_chi2_gradient) since the last reset
  * and the launch count of their reverse-pass kernels. */

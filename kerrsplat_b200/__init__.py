@@ -217,6 +217,13 @@ class GeodesicCache:
         self._check(self._lib.ks_kernel_stats(self._ctx, ctypes.byref(ms), ctypes.byref(kl), ctypes.byref(al), int(reset)))
         return ms.value, kl.value, al.value
 
+    def consume_stats(self, reset=False):
+        """(ms, launches) of k_consume alone in the mixed renders since the last reset."""
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        self._check(self._lib.ks_consume_stats(self._ctx, ctypes.byref(ms), ctypes.byref(n), int(reset)))
+        return ms.value, n.value
+
     def count_events(self, on=True):
         self._check(self._lib.ks_set_event_counting(self._ctx, int(on)))
 
@@ -517,10 +524,10 @@ def jvp(cache, model, times, nus, L, dirs, nmax=-1, slab=0.0, precision=KS_FP64,
     return (out, img) if return_image else out
 
 
-def spacetime_derivatives(cache, model, times, nus, L, h_a=1e-5, h_theta=1e-5, nmax=-1, slab=0.0, precision=KS_FP64, return_image=False):
+def spacetime_derivatives(cache, model, times, nus, L, nmax=-1, slab=0.0, precision=KS_FP64, return_image=False):
     """d(image)/d(a, theta_o, ln L) (the spacetime block of spacetime_valgrad, joint.jl:74-82): array
-    (3, nfreq, nframes, npix, 4) in screen order; a and theta_o by central differences with steps
-    h_a, h_theta, ln L exactly for thermal scenes."""
+    (3, nfreq, nframes, npix, 4) in screen order, by three-partial FP64 duals through the ray
+    constants, the anchors, the march and the transport at the cache's sample counts."""
     times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
     nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
     nt, nf = int(times.shape[0]), int(nus.shape[0])
@@ -528,7 +535,7 @@ def spacetime_derivatives(cache, model, times, nus, L, h_a=1e-5, h_theta=1e-5, n
     out = np.empty((3, nf, nt, cache.npix, 4))
     img = np.empty((nf, nt, cache.npix, 4)) if return_image else None
     cache._check(cache._lib.ks_spacetime_derivatives(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision),
-                                                     int(nmax), float(slab), float(h_a), float(h_theta), _ptr(out),
+                                                     int(nmax), float(slab), _ptr(out),
                                                      _ptr(img) if img is not None else None))
     return (out, img) if return_image else out
 

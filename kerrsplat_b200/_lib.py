@@ -74,8 +74,7 @@ SIGNATURES = [
                                             ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int64, _VP, _VP, _VP,
                                             _VP, _VP, _VP, ctypes.c_double, ctypes.c_double, _VP, _VP, ctypes.c_int32, _VP]),
     ("ks_spacetime_derivatives", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
-                                                ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
-                                                ctypes.c_double, _VP, _VP]),
+                                                ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _VP, _VP]),
     ("ks_normal_matrix", ctypes.c_int, [_VP, _VP, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, _VP]),
     ("ks_sample_adjoint", ctypes.c_int, [_VP, ctypes.c_int64, _VP, _VP, _VP, _VP, ctypes.c_int32, _VP]),
     ("ks_chi2_gradient", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
@@ -89,6 +88,7 @@ EXTRA_SIGNATURES = [
     ("ks_set_event_counting", ctypes.c_int, [_VP, ctypes.c_int]),
     ("ks_event_counts", ctypes.c_int, [_VP, _VP]),
     ("ks_adjoint_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+    ("ks_consume_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     ("ks_autotune", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32, ctypes.c_double,
                                    ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                    ctypes.POINTER(ctypes.c_int32), _D]),

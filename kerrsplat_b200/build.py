@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libkerrsplat_b200.so")
 SOURCES = ["ks_lib.cu"]
-HEADERS = ["ks_elliptic.cuh", "ks_plan.cuh", "ks_march.cuh", "ks_dual.cuh", "ks_transfer.cuh", "ks_mixed.cuh", "ks_adjoint.cuh", "ks_dft.cuh"]
+HEADERS = ["ks_elliptic.cuh", "ks_plan.cuh", "ks_march.cuh", "ks_dual.cuh", "ks_transfer.cuh", "ks_mixed.cuh", "ks_adjoint.cuh", "ks_spacetime.cuh", "ks_dft.cuh"]
 
 
 def nvcc_command(out=LIB, extra=()):

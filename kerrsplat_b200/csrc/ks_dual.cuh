@@ -117,7 +117,11 @@ __device__ __forceinline__ ks::Dual<T, N> dchain(const ks::Dual<T, N>& x, T f, T
     return r;
 }
 
-template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> sqrt(const ks::Dual<T, N>& x) { T s = sqrt(x.v); return dchain(x, s, T(0.5) / s); }
+// sqrt with a zero derivative at 0 (a clamped argument: sqrt(fmax(x, 0)), R_F's sqrt(0) of a constant)
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> sqrt(const ks::Dual<T, N>& x) {
+    const T s = sqrt(x.v);
+    return dchain(x, s, s > T(0) ? T(0.5) / s : T(0));
+}
 template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> exp(const ks::Dual<T, N>& x) { T e = exp(x.v); return dchain(x, e, e); }
 template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> expm1(const ks::Dual<T, N>& x) { return dchain(x, expm1(x.v), exp(x.v)); }
 template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> log(const ks::Dual<T, N>& x) { return dchain(x, log(x.v), T(1) / x.v); }
@@ -141,6 +145,28 @@ __device__ __forceinline__ ks::Dual<T, N> atan2(const ks::Dual<T, N>& y, const k
     for (int i = 0; i < N; ++i) r.d[i] = fy * y.d[i] + fx * x.d[i];
     return r;
 }
+// asin with a zero derivative where the argument reaches +-1 (a clamped argument)
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> asin(const ks::Dual<T, N>& x) {
+    const T s = T(1) - x.v * x.v;
+    return dchain(x, asin(x.v), s > T(0) ? T(1) / sqrt(s) : T(0));
+}
+// acos with a zero derivative where the argument reaches +-1 (safe_acos, step.jl:157-172)
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> acos(const ks::Dual<T, N>& x) {
+    const T s = T(1) - x.v * x.v;
+    return dchain(x, acos(x.v), s > T(0) ? -T(1) / sqrt(s) : T(0));
+}
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> atan(const ks::Dual<T, N>& x) { return dchain(x, atan(x.v), T(1) / (T(1) + x.v * x.v)); }
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> cbrt(const ks::Dual<T, N>& x) {
+    const T c = cbrt(x.v);
+    return dchain(x, c, c != T(0) ? T(1) / (T(3) * c * c) : T(0));
+}
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> hypot(const ks::Dual<T, N>& x, const ks::Dual<T, N>& y) { return sqrt(x * x + y * y); }
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> copysign(const ks::Dual<T, N>& x, const ks::Dual<T, N>& y) {
+    return (signbit(x.v) != signbit(y.v)) ? -x : x;
+}
+// piecewise constant: the value's floor, no partials
+template <class T, int N> __device__ __forceinline__ ks::Dual<T, N> floor(const ks::Dual<T, N>& x) { return ks::Dual<T, N>(floor(x.v)); }
+
 // x^y; the log term only when the exponent carries partials (a constant exponent at x <= 0 stays finite)
 template <class T, int N>
 __device__ __forceinline__ ks::Dual<T, N> pow(const ks::Dual<T, N>& x, const ks::Dual<T, N>& y) {

@@ -43,8 +43,9 @@ __global__ void k_root_case(Spacetime st, const double* __restrict__ alpha, cons
     idx[i] = i;
 }
 
-__device__ __forceinline__ MarchRay<double> march_ray_of(const RayC& R, const Spacetime& st, double dtau) {
-    MarchRay<double> M;
+template <class T>
+__device__ __forceinline__ MarchRay<T> march_ray_of(const RayCT<T>& R, const SpacetimeT<T>& st, TimeT<T> dtau) {
+    MarchRay<T> M;
     M.rcase = R.rcase; M.k = R.k; M.c = R.c; M.fo = R.fo; M.fo_d = R.fo;
     M.m0 = R.map[0]; M.m1 = R.map[1]; M.m2 = R.map[2]; M.m3 = R.map[3];
     M.tau_valid = R.tau_valid; M.dtau = dtau;
@@ -57,8 +58,10 @@ __device__ __forceinline__ MarchRay<double> march_ray_of(const RayC& R, const Sp
     return M;
 }
 
-__device__ __forceinline__ JS<double> xr_at(const RayC& R, double tau) { return jstate(R.c * (R.fo - tau), R.k); }
-__device__ __forceinline__ JS<double> xt_at(const RayC& R, double tau) { return jstate(R.pscale * (tau + R.poffset) / R.tempfac, R.pmu); }
+template <class T>
+__device__ __forceinline__ JS<T> xr_at(const RayCT<T>& R, TimeT<T> tau) { return jstate(R.c * (R.fo - tau), R.k); }
+template <class T>
+__device__ __forceinline__ JS<T> xt_at(const RayCT<T>& R, TimeT<T> tau) { return jstate(R.pscale * (tau + R.poffset) / R.tempfac, R.pmu); }
 
 __global__ void k_build_plan(Spacetime st, const double* __restrict__ alpha, const double* __restrict__ beta,
                              const long long* __restrict__ perm, long long npix, long long npad, double* __restrict__ f,
@@ -123,20 +126,21 @@ __global__ void k_build_plan(Spacetime st, const double* __restrict__ alpha, con
 }
 
 // The smooth integrands at tau from direct Jacobi states, the t part in its large-r form past r = 64.
-__device__ __forceinline__ void anchor_integrand(const RayC& R, const MarchRay<double>& M, double tau, double& gt, double& gp) {
-    JS<double> xr = xr_at(R, tau), xt = xt_at(R, tau);
-    Point<double> p = ray_point(M, xr, xt, tau);
+template <class T>
+__device__ __forceinline__ void anchor_integrand(const RayCT<T>& R, const MarchRay<T>& M, TimeT<T> tau, T& gt, T& gp) {
+    JS<T> xr = xr_at(R, tau), xt = xt_at(R, tau);
+    Point<T> p = ray_point(M, xr, xt, tau);
     gt = p.gt; gp = p.gphi;
-    double r = p.r, a = M.a, lam = M.lam;
-    double P = r * r + a * a - a * lam;
+    T r = p.r, a = M.a, lam = M.lam;
+    T P = r * r + a * a - a * lam;
     if (r > 64.0 && P > 0.0) {
-        double D = r * r - 2.0 * r + a * a;
-        double Qv = M.eta + (lam - a) * (lam - a);
-        double as = fabs(p.s);
-        double diff = D * Qv / (P + as) * (1.0 + 2.0 / r) + 2.0 * (2.0 * r - a * a) * P / (r * D);
-        double s2 = 1.0 - p.cth * p.cth;
-        double wp = p.s * M.rp / (r * (r - M.rp)) / M.sp;
-        double wm = p.s * M.rmn / (r * (r - M.rmn)) / M.sm;
+        T D = r * r - 2.0 * r + a * a;
+        T Qv = M.eta + (lam - a) * (lam - a);
+        T as = fabs(p.s);
+        T diff = D * Qv / (P + as) * (1.0 + 2.0 / r) + 2.0 * (2.0 * r - a * a) * P / (r * D);
+        T s2 = 1.0 - p.cth * p.cth;
+        T wp = p.s * M.rp / (r * (r - M.rp)) / M.sp;
+        T wm = p.s * M.rmn / (r * (r - M.rmn)) / M.sm;
         gt = diff + a * (lam - a * s2) - M.Qt * wp - M.Qtm * wm;
     }
 }
@@ -144,11 +148,12 @@ __device__ __forceinline__ void anchor_integrand(const RayC& R, const MarchRay<d
 __constant__ double c_gl_x[16];
 __constant__ double c_gl_w[16];
 
-__device__ void gl_panel(const RayC& R, const MarchRay<double>& M, double ta, double tb, double& It, double& Ip) {
-    double mid = 0.5 * (ta + tb), half = 0.5 * (tb - ta);
-    double st = 0.0, sp = 0.0;
+template <class T>
+__device__ void gl_panel(const RayCT<T>& R, const MarchRay<T>& M, TimeT<T> ta, TimeT<T> tb, T& It, T& Ip) {
+    const TimeT<T> mid = 0.5 * (ta + tb), half = 0.5 * (tb - ta);
+    T st = T(0.0), sp = T(0.0);
     for (int i = 0; i < 16; ++i) {
-        double gt, gp;
+        T gt, gp;
         anchor_integrand(R, M, mid + half * c_gl_x[i], gt, gp);
         st += c_gl_w[i] * gt; sp += c_gl_w[i] * gp;
     }
@@ -614,6 +619,7 @@ __global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, 
 }  // namespace
 
 #include "ks_adjoint.cuh"
+#include "ks_spacetime.cuh"
 
 namespace {
 
@@ -682,6 +688,10 @@ struct ks_context {
     long long ranges[6] = {0, 0, 0, 0, 0, 0};
     // timing of the render kernels (CUDA events on the context stream)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t evc0 = nullptr, evc1 = nullptr;   // around k_consume (the mixed path's dominant kernel)
+    bool consume_timed = false;
+    double consume_ms = 0.0;
+    long long consume_launches = 0;
     double kernel_ms = 0.0;
     long long kernel_launches = 0;
     long long launches = 0;
@@ -878,9 +888,12 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
     KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
     const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
+    cudaEventRecord(c->evc0, c->stream);
     k_consume<CH, NT, KM><<<unsigned(grid), NT, smem, c->stream>>>(
         plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
         c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr);
+    cudaEventRecord(c->evc1, c->stream);
+    c->consume_timed = true;
     c->launches++;
     c->kernel_launches++;
     KS_CUDA(c, cudaGetLastError());
@@ -993,6 +1006,8 @@ int ks_context_create(int device, int flags, ks_context** out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return KS_ERR_DEVICE; }
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
+    cudaEventCreate(&c->evc0);
+    cudaEventCreate(&c->evc1);
     init_constants();
     if (cudaGetLastError() != cudaSuccess) { delete c; return KS_ERR_DEVICE; }
     *out = c;
@@ -1008,6 +1023,8 @@ int ks_context_destroy(ks_context* c) {
         b->release();
     for (DevBuf& b : c->dft_in) b.release();
     if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->evc0) cudaEventDestroy(c->evc0);
+    if (c->evc1) cudaEventDestroy(c->evc1);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1030,6 +1047,15 @@ int ks_kernel_stats(ks_context* c, double* render_ms, long long* render_launches
     if (render_launches) *render_launches = c->kernel_launches;
     if (all_launches) *all_launches = c->launches;
     if (reset) { c->kernel_ms = 0.0; c->kernel_launches = 0; c->launches = 0; }
+    return KS_OK;
+}
+
+// Device time of k_consume alone in the mixed ks_render calls since the last reset, and its launches.
+int ks_consume_stats(ks_context* c, double* consume_ms, long long* launches, int reset) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (consume_ms) *consume_ms = c->consume_ms;
+    if (launches) *launches = c->consume_launches;
+    if (reset) { c->consume_ms = 0.0; c->consume_launches = 0; }
     return KS_OK;
 }
 
@@ -1359,6 +1385,13 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->kernel_ms += ms;
+    if (precision != KS_FP64 && c->consume_timed) {
+        float mc = 0.f;
+        cudaEventElapsedTime(&mc, c->evc0, c->evc1);
+        c->consume_ms += mc;
+        c->consume_launches++;
+        c->consume_timed = false;
+    }
     return KS_OK;
 }
 
@@ -1860,12 +1893,6 @@ int jvp_impl(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doubl
     return KS_OK;
 }
 
-__global__ void k_central_diff(long long n, const double* __restrict__ plus, const double* __restrict__ minus, double inv2h,
-                               double* __restrict__ out) {
-    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (q < n) out[q] = (plus[q] - minus[q]) * inv2h;
-}
-
 }  // namespace
 
 extern "C" {
@@ -1877,64 +1904,78 @@ int ks_jvp(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double*
 }
 
 int ks_spacetime_derivatives(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes, const double* nus,
-                             int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, double h_a, double h_theta,
-                             double* dimage, double* image) {
+                             int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab, double* dimage, double* image) {
     if (!c || !dimage || !sets || nsets < 1) return KS_ERR_ARGUMENT;
     if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
-    if (!(h_a > 0 && h_theta > 0 && std::isfinite(h_a) && std::isfinite(h_theta))) return fail(c, KS_ERR_ARGUMENT, "steps must be positive");
-    if (nframes < 1 || nfreq < 1) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
-    const Spacetime st0 = c->st;
-    if (!(st0.a - h_a > 0.0 && st0.a + h_a < 1.0)) return fail(c, KS_ERR_ARGUMENT, "a +- h_a must stay in (0, 1)");
+    if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
     KS_CUDA(c, cudaSetDevice(c->device));
-    const long long n4 = c->npix * (long long)nframes * nfreq * 4;
-    KS_CUDA(c, c->st_buf.ensure(size_t(n4) * 3 * sizeof(double)));
-    double* bp = c->st_buf.as<double>();
-    double* bm = bp + n4;
-    double* b3 = bm + n4;
-    const bool dev = is_device_ptr(dimage);
-    double* dd = dev ? dimage : nullptr;
-    std::vector<double> host;
-    if (!dev) { KS_CUDA(c, c->stage_out.ensure(size_t(n4) * 3 * sizeof(double))); dd = c->stage_out.as<double>(); }
-    const double steps[2] = {h_a, h_theta};
-    int status = KS_OK;
-    for (int q = 0; q < 2 && status == KS_OK; ++q) {
-        for (int sgn = 0; sgn < 2 && status == KS_OK; ++sgn) {
-            const double d = (sgn == 0 ? 1.0 : -1.0) * steps[q];
-            status = regenerate_impl(c, st0.a + (q == 0 ? d : 0.0), st0.thetao + (q == 1 ? d : 0.0), st0.N, st0.M, st0.density, st0.nmin);
-            if (status == KS_OK)
-                status = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, sgn == 0 ? bp : bm, KS_ORDER_SCREEN);
-        }
-        if (status == KS_OK) {
-            k_central_diff<<<nblocks(n4, 256), 256, 0, c->stream>>>(n4, bp, bm, 0.5 / steps[q], dd + q * n4);
-            c->launches++;
-        }
-    }
-    // back at (a, theta_o)
+    std::vector<double> ht(nframes), hnu(nfreq);
+    KS_CUDA(c, cudaMemcpy(ht.data(), times, nframes * sizeof(double), cudaMemcpyDefault));
+    KS_CUDA(c, cudaMemcpy(hnu.data(), nus, nfreq * sizeof(double), cudaMemcpyDefault));
+    for (double v : ht) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite observation time");
+    for (double v : hnu) if (!(std::isfinite(v) && v > 0)) return fail(c, KS_ERR_NONFINITE, "frequencies must be finite and positive");
+    int ntot = 0;
     {
-        int s2 = regenerate_impl(c, st0.a, st0.thetao, st0.N, st0.M, st0.density, st0.nmin);
-        if (status == KS_OK) status = s2;
+        int s = build_tables(c, sets, nsets, &ntot, false);
+        if (s) return s;
     }
-    if (status) return status;
-    // d/d(ln L): exact through a dual step length for thermal scenes, else central differences in ln L
-    bool thermal = true;
-    for (int s = 0; s < nsets; ++s) thermal = thermal && sets[s].kind == KS_THERMAL21;
-    if (thermal) {
-        int s = jvp_impl(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, nullptr, 1, dd + 2 * n4, KS_ORDER_SCREEN,
-                         image ? b3 : nullptr, true);
-        if (s) return s;
-    } else {
-        const double h = 1e-5;
-        int s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L * std::exp(h), precision, nmax, slab, bp, KS_ORDER_SCREEN);
-        if (!s) s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L * std::exp(-h), precision, nmax, slab, bm, KS_ORDER_SCREEN);
-        if (!s && image) s = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, b3, KS_ORDER_SCREEN);
-        if (s) return s;
-        k_central_diff<<<nblocks(n4, 256), 256, 0, c->stream>>>(n4, bp, bm, 0.5 / h, dd + 2 * n4);
+    const int ncombo = nframes * nfreq;
+    std::vector<double> hc(2 * size_t(ncombo));
+    for (int fv = 0; fv < nfreq; ++fv)
+        for (int ft = 0; ft < nframes; ++ft) {
+            hc[size_t(fv) * nframes + ft] = ht[ft];
+            hc[ncombo + size_t(fv) * nframes + ft] = hnu[fv];
+        }
+    KS_CUDA(c, c->combos.ensure(hc.size() * sizeof(double)));
+    KS_CUDA(c, cudaMemcpyAsync(c->combos.p, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const double* dct = c->combos.as<double>();
+    const long long n = c->npix;
+    const long long nrc = n * ncombo;
+    // the dual table, the dual anchor records, then the per-(ray, combination) value + 3 partials
+    const long long ntab = (long long)ntot * ST_COUNT + c->nkv;
+    const size_t tab_bytes = (size_t(std::max<long long>(ntab, 1)) * sizeof(D3) + 255) / 256 * 256;
+    const size_t rec_bytes = size_t(c->total_anchors) * SA_COUNT * sizeof(D3);
+    KS_CUDA(c, c->jvp_tab.ensure(tab_bytes + rec_bytes));
+    D3* dtab = c->jvp_tab.as<D3>();
+    D3* rec = reinterpret_cast<D3*>(static_cast<unsigned char*>(c->jvp_tab.p) + tab_bytes);
+    KS_CUDA(c, c->st_buf.ensure(size_t(nrc) * 16 * sizeof(double)));
+    cudaEventRecord(c->ev0, c->stream);
+    if (ntab > 0) {
+        k_lift_table<<<nblocks(ntab, 256), 256, 0, c->stream>>>(ntab, c->tab.as<double>(), dtab);
         c->launches++;
+        KS_CUDA(c, cudaGetLastError());
     }
+    const PlanView P = plan_view(c);
+    k_st_anchors<<<dim3(nblocks(n, 64), c->max_nanch), 64, 0, c->stream>>>(P, c->st, n, rec);
+    c->launches++;
     KS_CUDA(c, cudaGetLastError());
-    if (!dev) KS_CUDA(c, cudaMemcpyAsync(dimage, dd, size_t(n4) * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (image) KS_CUDA(c, cudaMemcpyAsync(image, b3, size_t(n4) * sizeof(double), cudaMemcpyDefault, c->stream));
+    k_st_prefix<<<nblocks(n, 64), 64, 0, c->stream>>>(P, n, rec);
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    k_spacetime_dual<<<nblocks(nrc, 64), 64, 0, c->stream>>>(P, c->st, n, rec, dtab, ntot, dct, dct + ncombo, ncombo, L, nmax, slab,
+                                                             c->st_buf.as<double>());
+    c->launches++;
+    c->adjoint_launches++;
+    KS_CUDA(c, cudaGetLastError());
+    // screen order: dimage (3 x ncombo x npix x 4) and the image
+    const bool dev = is_device_ptr(dimage);
+    const bool idev = image && is_device_ptr(image);
+    const size_t n4 = size_t(nrc) * 4;
+    KS_CUDA(c, c->stage_out.ensure(n4 * 4 * sizeof(double)));
+    double* dd = dev ? dimage : c->stage_out.as<double>();
+    double* di = image ? (idev ? image : c->stage_out.as<double>() + 3 * n4) : nullptr;
+    k_spacetime_unpack<<<nblocks(nrc, 256), 256, 0, c->stream>>>(c->st_buf.as<double>(), c->perm.as<long long>(), n, ncombo, dd, di);
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    cudaEventRecord(c->ev1, c->stream);
+    if (!dev) KS_CUDA(c, cudaMemcpyAsync(dimage, dd, n4 * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (image && !idev) KS_CUDA(c, cudaMemcpyAsync(image, di, n4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->adjoint_ms += ms;
     return KS_OK;
 }
 

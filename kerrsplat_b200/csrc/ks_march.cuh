@@ -16,11 +16,17 @@ struct Sample {
     bool nur, nutheta, ok;
 };
 
+// The type of Mino times: FP64 for the FP32 and FP64 marches (sample times compared in FP64), the
+// dual itself when the times carry derivatives (the spacetime duals: tau_k = k tau_total / (N + 1)).
+template <class T> struct TimeOf { using type = double; };
+template <class S, int N> struct TimeOf<Dual<S, N>> { using type = Dual<S, N>; };
+template <class T> using TimeT = typename TimeOf<T>::type;
+
 template <class T>
 struct MarchRay {
     int rcase;
     T k, c, fo, m0, m1, m2, m3;
-    double tau_valid, dtau, fo_d;  // compared against sample times in FP64
+    TimeT<T> tau_valid, dtau, fo_d;  // compared against sample times in FP64
     T pmu, pscale, tempfac, poffset, sqrt_up, um, up_m_um, psign;
     bool vortical, scattering;
     T a, lam, eta, rp, rmn, sp, sm, Qt, Qtm, Qphi, Qphim, r4, qC, qn, sqrt_eps, gc, mp, K2;
@@ -129,7 +135,7 @@ __device__ __forceinline__ void smooth(const MarchRay<T>& R, Point<T>& p, T dn) 
     T wp = s * R.rp / (r * (r - R.rp)) / R.sp;
     T wm = s * R.rmn / (r * (r - R.rmn)) / R.sm;
     T P = r * r + a * a - a * lam;
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (is_f32<T>) {
         if (r > T(64) && P > T(0)) {
             // dt/dtau - |s|(1 + 2/r) without cancellation (see the anchor integrand)
             T Qv = R.eta + (lam - a) * (lam - a);
@@ -157,7 +163,7 @@ __device__ __forceinline__ T r_pot(const MarchRay<T>& R, T r) {
 }
 
 template <class T>
-__device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<T>& xr, const JS<T>& xt, double tau) {
+__device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<T>& xr, const JS<T>& xt, TimeT<T> tau) {
     Point<T> p;
     p.r = radius(R, xr);
     polar_cos(R, xt, p.theta, p.cth, p.nuth);
@@ -183,7 +189,7 @@ __device__ __forceinline__ Point<T> turning_point(const MarchRay<T>& R, const JS
 }
 
 template <class T>
-__device__ __forceinline__ T polar_closed(const MarchRay<T>& R, double tau, T sn, T cn) {
+__device__ __forceinline__ T polar_closed(const MarchRay<T>& R, TimeT<T> tau, T sn, T cn) {
     T X = (T(tau) + R.poffset) / R.tempfac;
     T nw = floor((X + R.K2 / T(2)) / R.K2);
     T A = (atan(R.sqrt_eps * sn / cn) + nw * kpi<T>()) / R.sqrt_eps;
@@ -196,7 +202,7 @@ __device__ __forceinline__ T polar_closed(const MarchRay<T>& R, double tau, T sn
 // from the previous interval (the same inputs, hence the same value).
 template <class T>
 __device__ __forceinline__ void increment(const MarchRay<T>& R, const Point<T>& pa, const Point<T>& pm, const Point<T>& pb,
-                                          double ta, double tb, T pca, T pcb, T& It, T& Iphi) {
+                                          TimeT<T> ta, TimeT<T> tb, T pca, T pcb, T& It, T& Iphi) {
     T h = T(tb - ta);
     T ra = pa.r, rb = pb.r;
     T dFr = (rb - ra) + T(2) * log(rb / ra);

@@ -17,13 +17,15 @@
 
 namespace ks {
 
-struct Spacetime {
-    double a, thetao, rp, rmn, rh, abscos, cos2;
+template <class T>
+struct SpacetimeT {
+    T a, thetao, rp, rmn, rh, abscos, cos2;
     int N, M;        // N: samples per ray (with uneven counts, the largest)
     // uneven counts: N_j = clamp(64 ceil(density tau_total_j / 64), nmin, N); density 0 = uniform N
     double density;
     int nmin;
 };
+using Spacetime = SpacetimeT<double>;
 
 enum PlanField {
     PF_ALPHA, PF_BETA, PF_ETA, PF_LAM, PF_NUMREALS, PF_CASE,
@@ -48,56 +50,60 @@ enum PlanField {
 enum AnchorField { AF_XR_SN, AF_XR_CN, AF_XR_DN, AF_XT_SN, AF_XT_CN, AF_XT_DN, AF_T, AF_PHI, AF_OK,
                    AF_SEG_T, AF_SEG_PHI, AF_PAD, AF_COUNT };
 
-struct Cplx { double re, im; };
+template <class T> struct CplxT { T re, im; };
 
-KS_HD Cplx cx(double r, double i) { return {r, i}; }
-KS_HD Cplx cadd(Cplx a, Cplx b) { return {a.re + b.re, a.im + b.im}; }
-KS_HD Cplx cmul(Cplx a, Cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
-KS_HD Cplx cdiv(Cplx a, Cplx b) {
-    double d = b.re * b.re + b.im * b.im;
+template <class T> KS_HD CplxT<T> cx(T r, T i) { return {r, i}; }
+template <class T> KS_HD CplxT<T> cadd(CplxT<T> a, CplxT<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <class T> KS_HD CplxT<T> cmul(CplxT<T> a, CplxT<T> b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+template <class T> KS_HD CplxT<T> cdiv(CplxT<T> a, CplxT<T> b) {
+    T d = b.re * b.re + b.im * b.im;
     return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
 }
-KS_HD double cabs_(Cplx a) { return hypot(a.re, a.im); }
+template <class T> KS_HD T cabs_(CplxT<T> a) { return hypot(a.re, a.im); }
 // principal square root of a real number as a complex number
-KS_HD Cplx csqrt_real(double x) { return x >= 0 ? Cplx{sqrt(x), 0.0} : Cplx{0.0, sqrt(-x)}; }
+template <class T> KS_HD CplxT<T> csqrt_real(T x) { return val(x) >= 0 ? CplxT<T>{sqrt(x), T(0.0)} : CplxT<T>{T(0.0), sqrt(-x)}; }
 // principal cube root of a complex number
-KS_HD Cplx ccbrt(Cplx z) {
-    double r = cabs_(z);
-    if (r == 0.0) return {0.0, 0.0};
-    double th = atan2(z.im, z.re) / 3.0;
-    double m = cbrt(r);
+template <class T> KS_HD CplxT<T> ccbrt(CplxT<T> z) {
+    T r = cabs_(z);
+    if (val(r) == 0.0) return {T(0.0), T(0.0)};
+    T th = atan2(z.im, z.re) / 3.0;
+    T m = cbrt(r);
     return {m * cos(th), m * sin(th)};
 }
 
-// All the FP64 constants of one ray (sorted slot), built from the screen point.
-struct RayC {
-    double alpha, beta, eta, lam;
-    double rre[4], rim[4];
+// All the constants of one ray (sorted slot), built from the screen point; T = double for the
+// geodesics, a dual number for their derivatives in (a, theta_o).
+template <class T>
+struct RayCT {
+    T alpha, beta, eta, lam;
+    T rre[4], rim[4];
     int numreals, rcase;
-    double k, c, fo, map[4], tau_valid, tau_total;
-    double pmu, pscale, tempfac, poffset, sqrt_up, um, up_m_um, psign; bool vortical; double gtho;
-    double sp, sm, Qt, Qtm, Qphi, Qphim, r4, qC, qn, sqrt_eps, gc, mp, K2; bool scattering;
-    double vabsalpha, valpha2, vabsbeta;
+    T k, c, fo, map[4], tau_valid, tau_total;
+    T pmu, pscale, tempfac, poffset, sqrt_up, um, up_m_um, psign; bool vortical; T gtho;
+    T sp, sm, Qt, Qtm, Qphi, Qphim, r4, qC, qn, sqrt_eps, gc, mp, K2; bool scattering;
+    T vabsalpha, valpha2, vabsbeta;
 };
+using RayC = RayCT<double>;
 
 KS_HD double sgn(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
 
 // Mino time at which the inbound radial closed form reaches radius r (inverse of the r(X) maps,
 // recurrence.jl:169-177): tau = fo - X / c.
-KS_HD double mino_time_at(const RayC& R, double r) {
-    double X;
+template <class T>
+KS_HD T mino_time_at(const RayCT<T>& R, T r) {
+    T X;
     if (R.rcase == 2) {
-        double r1 = R.rre[0], r3 = R.rre[2], r4 = R.rre[3];
-        double s2 = (r3 - r1) * (r4 - r) / ((r4 - r1) * (r3 - r));
-        X = ellip_f(asin(sqrt(fmax(0.0, fmin(1.0, s2)))), R.k);
+        T r1 = R.rre[0], r3 = R.rre[2], r4 = R.rre[3];
+        T s2 = (r3 - r1) * (r4 - r) / ((r4 - r1) * (r3 - r));
+        X = ellip_f(asin(sqrt(fmax(T(0.0), fmin(T(1.0), s2)))), R.k);
     } else if (R.rcase == 3) {
-        double cn = (R.map[0] - r * R.map[2]) / (r * R.map[3] - R.map[1]);
-        X = ellip_f(acos(fmax(-1.0, fmin(1.0, cn))), R.k);
+        T cn = (R.map[0] - r * R.map[2]) / (r * R.map[3] - R.map[1]);
+        X = ellip_f(acos(fmax(T(-1.0), fmin(T(1.0), cn))), R.k);
     } else {
-        double w = -(r + R.map[1]) / R.map[0];
-        double sc = (R.map[2] - w) / (1.0 + w * R.map[2]);
-        double ph = atan(sc);
-        if (ph < 0.0) ph += kPi;
+        T w = -(r + R.map[1]) / R.map[0];
+        T sc = (R.map[2] - w) / (1.0 + w * R.map[2]);
+        T ph = atan(sc);
+        if (val(ph) < 0.0) ph += kPi;
         X = ellip_f(ph, R.k);
     }
     return R.fo - X / R.c;
@@ -106,51 +112,52 @@ KS_HD double mino_time_at(const RayC& R, double r) {
 // Roots of the radial potential by the resolvent cubic (Gralla & Lupsasca 2020), the radial and
 // polar closed-form constants (test/highprec_reference.jl:65-122, recurrence.jl:64-109, 207-237),
 // the quadrature constants (quadrature.jl:68-97) and the visibility constants (recurrence.jl:293-298).
-KS_HD RayC build_ray(const Spacetime& st, double alpha, double beta) {
-    RayC R;
-    const double a = st.a, th = st.thetao;
-    double ct = cos(th);
+template <class T>
+KS_HD RayCT<T> build_ray(const SpacetimeT<T>& st, T alpha, T beta) {
+    RayCT<T> R;
+    const T a = st.a, th = st.thetao;
+    T ct = cos(th);
     R.alpha = alpha; R.beta = beta;
     R.eta = (alpha * alpha - a * a) * ct * ct + beta * beta;
     R.lam = -alpha * sin(th);
-    const double eta = R.eta, lam = R.lam;
+    const T eta = R.eta, lam = R.lam;
     // radial roots
-    double A = a * a - eta - lam * lam;
-    double B = 2.0 * (eta + (lam - a) * (lam - a));
-    double Cc = -a * a * eta;
-    double P = -A * A / 12.0 - Cc;
-    double Q = -A / 3.0 * ((A / 6.0) * (A / 6.0) - Cc) - B * B / 8.0;
-    double disc = (P / 3.0) * (P / 3.0) * (P / 3.0) + (Q / 2.0) * (Q / 2.0);
-    Cplx sq = csqrt_real(disc);
-    Cplx wp = ccbrt(cadd(cx(-Q / 2.0, 0.0), sq));
-    Cplx wm = cabs_(wp) > 0.0 ? cdiv(cx(-P / 3.0, 0.0), wp) : ccbrt(cadd(cx(-Q / 2.0, 0.0), cx(-sq.re, -sq.im)));
-    double xi0 = (wp.re + wm.re) - A / 3.0;
-    double z = sqrt(fmax(xi0 / 2.0, 0.0));
-    double arg12 = -A / 2.0 - z * z + B / (4.0 * z);
-    double arg34 = -A / 2.0 - z * z - B / (4.0 * z);
-    if (arg12 >= 0.0) { double s = sqrt(arg12); R.rre[0] = -z - s; R.rim[0] = 0; R.rre[1] = -z + s; R.rim[1] = 0; }
-    else { double s = sqrt(-arg12); R.rre[0] = -z; R.rim[0] = -s; R.rre[1] = -z; R.rim[1] = s; }
-    if (arg34 >= 0.0) { double s = sqrt(arg34); R.rre[2] = z - s; R.rim[2] = 0; R.rre[3] = z + s; R.rim[3] = 0; }
-    else { double s = sqrt(-arg34); R.rre[2] = z; R.rim[2] = -s; R.rre[3] = z; R.rim[3] = s; }
-    R.numreals = (arg12 >= 0.0 ? 2 : 0) + (arg34 >= 0.0 ? 2 : 0);
+    T A = a * a - eta - lam * lam;
+    T B = 2.0 * (eta + (lam - a) * (lam - a));
+    T Cc = -a * a * eta;
+    T P = -A * A / 12.0 - Cc;
+    T Q = -A / 3.0 * ((A / 6.0) * (A / 6.0) - Cc) - B * B / 8.0;
+    T disc = (P / 3.0) * (P / 3.0) * (P / 3.0) + (Q / 2.0) * (Q / 2.0);
+    CplxT<T> sq = csqrt_real(disc);
+    CplxT<T> wp = ccbrt(cadd(cx(-Q / 2.0, T(0.0)), sq));
+    CplxT<T> wm = val(cabs_(wp)) > 0.0 ? cdiv(cx(-P / 3.0, T(0.0)), wp) : ccbrt(cadd(cx(-Q / 2.0, T(0.0)), cx(-sq.re, -sq.im)));
+    T xi0 = (wp.re + wm.re) - A / 3.0;
+    T z = sqrt(fmax(xi0 / 2.0, T(0.0)));
+    T arg12 = -A / 2.0 - z * z + B / (4.0 * z);
+    T arg34 = -A / 2.0 - z * z - B / (4.0 * z);
+    if (val(arg12) >= 0.0) { T s = sqrt(arg12); R.rre[0] = -z - s; R.rim[0] = T(0.0); R.rre[1] = -z + s; R.rim[1] = T(0.0); }
+    else { T s = sqrt(-arg12); R.rre[0] = -z; R.rim[0] = -s; R.rre[1] = -z; R.rim[1] = s; }
+    if (val(arg34) >= 0.0) { T s = sqrt(arg34); R.rre[2] = z - s; R.rim[2] = T(0.0); R.rre[3] = z + s; R.rim[3] = T(0.0); }
+    else { T s = sqrt(-arg34); R.rre[2] = z; R.rim[2] = -s; R.rre[3] = z; R.rim[3] = s; }
+    R.numreals = (val(arg12) >= 0.0 ? 2 : 0) + (val(arg34) >= 0.0 ? 2 : 0);
     R.rcase = R.numreals == 4 ? 2 : (R.numreals == 2 ? 3 : 4);
-    const double inf = double(INFINITY);
+    const T inf = T(double(INFINITY));
     if (R.rcase == 2) {
-        double r1 = R.rre[0], r2 = R.rre[1], r3 = R.rre[2], r4 = R.rre[3];
-        double r31 = r3 - r1, r32 = r3 - r2, r41 = r4 - r1, r42 = r4 - r2;
+        T r1 = R.rre[0], r2 = R.rre[1], r3 = R.rre[2], r4 = R.rre[3];
+        T r31 = r3 - r1, r32 = r3 - r2, r41 = r4 - r1, r42 = r4 - r2;
         R.k = r32 * r41 / (r31 * r42);
         R.c = sqrt(r31 * r42) / 2.0;
         R.fo = 2.0 / sqrt(r31 * r42) * ellip_f(asin(sqrt(r31 / r41)), R.k);
         R.map[0] = r1; R.map[1] = r3; R.map[2] = r41; R.map[3] = r4 - r3;
         R.tau_total = 2.0 * R.fo;
-        R.tau_valid = r4 < st.rh ? mino_time_at(R, st.rh) : inf;
+        R.tau_valid = val(r4) < val(st.rh) ? mino_time_at(R, st.rh) : inf;
     } else if (R.rcase == 3) {
-        double r1 = R.rre[0], r2 = R.rre[1];
-        double r21 = r2 - r1;
-        double dr32 = R.rre[2] - R.rre[1], di32 = R.rim[2] - R.rim[1];
-        double dr31 = R.rre[2] - R.rre[0], di31 = R.rim[2] - R.rim[0];
-        double Aa = sqrt(dr32 * dr32 + di32 * di32);
-        double Bb = sqrt(dr31 * dr31 + di31 * di31);
+        T r1 = R.rre[0], r2 = R.rre[1];
+        T r21 = r2 - r1;
+        T dr32 = R.rre[2] - R.rre[1], di32 = R.rim[2] - R.rim[1];
+        T dr31 = R.rre[2] - R.rre[0], di31 = R.rim[2] - R.rim[0];
+        T Aa = sqrt(dr32 * dr32 + di32 * di32);
+        T Bb = sqrt(dr31 * dr31 + di31 * di31);
         R.k = ((Aa + Bb) * (Aa + Bb) - r21 * r21) / (4.0 * Aa * Bb);
         R.c = sqrt(Aa * Bb);
         R.fo = ellip_f(acos((Aa - Bb) / (Aa + Bb)), R.k) / sqrt(Aa * Bb);
@@ -158,59 +165,59 @@ KS_HD RayC build_ray(const Spacetime& st, double alpha, double beta) {
         R.tau_valid = inf;
         R.tau_total = mino_time_at(R, st.rh);
     } else {
-        double a1 = fabs(R.rim[3]), a2 = fabs(R.rim[1]);
-        double b1 = R.rre[3], b2 = R.rre[1];
-        double C = sqrt((a1 - a2) * (a1 - a2) + (b1 - b2) * (b1 - b2));
-        double D = sqrt((a1 + a2) * (a1 + a2) + (b1 - b2) * (b1 - b2));
+        T a1 = fabs(R.rim[3]), a2 = fabs(R.rim[1]);
+        T b1 = R.rre[3], b2 = R.rre[1];
+        T C = sqrt((a1 - a2) * (a1 - a2) + (b1 - b2) * (b1 - b2));
+        T D = sqrt((a1 + a2) * (a1 + a2) + (b1 - b2) * (b1 - b2));
         R.k = 4.0 * C * D / ((C + D) * (C + D));
         R.c = (C + D) / 2.0;
-        double g0 = sqrt(fmax((4.0 * a2 * a2 - (C - D) * (C - D)) / ((C + D) * (C + D) - 4.0 * a2 * a2), 0.0));
+        T g0 = sqrt(fmax((4.0 * a2 * a2 - (C - D) * (C - D)) / ((C + D) * (C + D) - 4.0 * a2 * a2), T(0.0)));
         R.fo = 2.0 / (C + D) * ellip_f(kPi / 2.0 + atan(g0), R.k);
-        R.map[0] = a2; R.map[1] = b1; R.map[2] = g0; R.map[3] = 0.0;
+        R.map[0] = a2; R.map[1] = b1; R.map[2] = g0; R.map[3] = T(0.0);
         R.tau_valid = inf;
         R.tau_total = mino_time_at(R, st.rh);
     }
     // polar constants, Krang's rounding (recurrence.jl:218-236)
-    double Dth = (1.0 - (eta + lam * lam) / (a * a)) / 2.0;
-    double dsc = sqrt(Dth * Dth + eta / (a * a));
-    double up = Dth + dsc, um = Dth - dsc;
-    double m = up / um;
+    T Dth = (1.0 - (eta + lam * lam) / (a * a)) / 2.0;
+    T dsc = sqrt(Dth * Dth + eta / (a * a));
+    T up = Dth + dsc, um = Dth - dsc;
+    T m = up / um;
     R.tempfac = 1.0 / sqrt(fabs(um * a * a));
-    R.vortical = eta < 0.0;
-    double sb = sgn(beta);
-    double kq;
+    R.vortical = val(eta) < 0.0;
+    double sb = sgn(val(beta));
+    T kq;
     if (R.vortical) {
         kq = 1.0 - m;
-        double arg = fmax(0.0, fmin(1.0, (ct * ct - um) / (up - um)));
+        T arg = fmax(T(0.0), fmin(T(1.0), (ct * ct - um) / (up - um)));
         R.gtho = R.tempfac * ellip_f(asin(sqrt(arg)), kq);
-        double sigma = th > kPi / 2.0 ? -1.0 : 1.0;
+        double sigma = val(th) > kPi / 2.0 ? -1.0 : 1.0;
         R.poffset = sigma * sb * R.gtho;
-        R.psign = sigma;
+        R.psign = T(sigma);
     } else {
         kq = m;
-        double arg = fmax(-1.0, fmin(1.0, ct / sqrt(up)));
+        T arg = fmax(T(-1.0), fmin(T(1.0), ct / sqrt(up)));
         R.gtho = R.tempfac * ellip_f(asin(arg), kq);
         R.poffset = sb * R.gtho;
-        R.psign = sb;
+        R.psign = T(sb);
     }
     R.pmu = -kq / (1.0 - kq);
     R.pscale = sqrt(1.0 - kq);
     R.sqrt_up = sqrt(up); R.um = um; R.up_m_um = up - um;
     // quadrature constants
-    double E = st.rp * st.rp + a * a - a * lam;
-    double Em = st.rmn * st.rmn + a * a - a * lam;
+    T E = st.rp * st.rp + a * a - a * lam;
+    T Em = st.rmn * st.rmn + a * a - a * lam;
     R.sp = -fabs(E); R.sm = -fabs(Em);
     R.Qt = (st.rp * st.rp + a * a) * E / (st.rp - st.rmn);
     R.Qtm = -(st.rmn * st.rmn + a * a) * Em / (st.rp - st.rmn);
     R.Qphi = a * (2.0 * st.rp - a * lam) / (st.rp - st.rmn);
     R.Qphim = -a * (2.0 * st.rmn - a * lam) / (st.rp - st.rmn);
-    R.scattering = (R.rcase == 2) && !(R.tau_valid < inf);
-    R.r4 = R.rcase == 2 ? R.rre[3] : double(NAN);
-    double mu_neg = -R.pmu / (1.0 - R.pmu);
-    double upq = R.sqrt_up * R.sqrt_up;
+    R.scattering = (R.rcase == 2) && !(val(R.tau_valid) < val(inf));
+    R.r4 = R.rcase == 2 ? R.rre[3] : T(double(NAN));
+    T mu_neg = -R.pmu / (1.0 - R.pmu);
+    T upq = R.sqrt_up * R.sqrt_up;
     if (R.vortical) { R.qC = 1.0 / (1.0 - R.um); R.qn = (upq - R.um) / (1.0 - R.um); }
-    else { R.qC = 1.0; R.qn = upq; }
-    R.sqrt_eps = sqrt(fmax(1.0 - R.qn, 0.0));
+    else { R.qC = T(1.0); R.qn = upq; }
+    R.sqrt_eps = sqrt(fmax(1.0 - R.qn, T(0.0)));
     R.gc = 1.0 / sqrt(1.0 - mu_neg);
     R.mp = mu_neg / (1.0 - mu_neg);
     R.K2 = 2.0 * ellip_k(R.pmu) / R.pscale;

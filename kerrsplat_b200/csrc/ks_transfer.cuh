@@ -752,7 +752,7 @@ __device__ __forceinline__ void knot_centre(const T* kn, int nk, T t, T& cx, T& 
 template <class T>
 __device__ __forceinline__ void knot_exponent(const T* p, const T* knots, T t, T x, T y, T z, T& q) {
     T cx, cy, cz;
-    knot_centre(knots + int(p[ST_KOFF]), int(p[ST_NK]), t, cx, cy, cz);
+    knot_centre(knots + int(value_of(p[ST_KOFF])), int(value_of(p[ST_NK])), t, cx, cy, cz);
     const T d0 = x - cx, d1 = y - cy, d2 = z - cz;
     const T u0 = p[ST_R0] * d0 + p[ST_R3] * d1 + p[ST_R6] * d2;
     const T u1 = p[ST_R1] * d0 + p[ST_R4] * d1 + p[ST_R7] * d2;
@@ -765,7 +765,7 @@ __device__ __forceinline__ void knot_exponent(const T* p, const T* knots, T t, T
 // The exponent of any splat of a polarized scene: false when the support sphere culls it.
 template <class T>
 __device__ __forceinline__ bool any_exponent(const T* p, const T* knots, T t, T x, T y, T z, T& q) {
-    if (int(p[ST_KIND]) == KS_KNOT21) {
+    if (int(value_of(p[ST_KIND])) == KS_KNOT21) {
         const T dx = x - p[ST_CX], dy = y - p[ST_CY], dz = z - p[ST_CZ];
         if (dx * dx + dy * dy + dz * dz > p[ST_RHO]) return false;   // outside the knots' bounding sphere
         knot_exponent(p, knots, t, x, y, z, q);

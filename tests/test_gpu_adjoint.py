@@ -242,16 +242,15 @@ def test_normal_matrix(prec, tol):
 
 
 def test_spacetime_derivatives_match_oracle(scene, oracle):
-    """The spacetime block (a, theta_o, ln L) of spacetime_valgrad (joint.jl:74-82): d/da and
-    d/dtheta_o against the oracle's central differences with the same steps (the same discretised
-    function, FP64: 1e-6), d/d(ln L) (a dual step length) against the oracle's central difference in
-    ln L (1e-6)."""
+    """The spacetime block (a, theta_o, ln L) of spacetime_valgrad (joint.jl:74-82), three-partial
+    duals through the ray constants, anchors, march and transport, against the oracle's central
+    differences (step 1e-5, the same discretised function: 1e-6)."""
     s = scene
     c, cam = s["c"], s["cam"]
     m = ks.PolarizedSplats(s["p"])
     h = 1e-5
     nu, t = s["nus"][:1], s["times"][:1]
-    d, img = ks.spacetime_derivatives(s["cache"], m, t, nu, c["L"], h_a=h, h_theta=h, precision=ks.KS_FP64, return_image=True)
+    d, img = ks.spacetime_derivatives(s["cache"], m, t, nu, c["L"], precision=ks.KS_FP64, return_image=True)
 
     def orc(a, th, L):
         return oracle.polarized_image(a, th, cam.alpha, cam.beta, N, c["M"], [("thermal", s["p"], None)], t[0], nu[0], L)
@@ -263,9 +262,61 @@ def test_spacetime_derivatives_match_oracle(scene, oracle):
     print("spacetime derivatives rel L2 (a, theta_o, ln L):", errs)
     assert max(errs) < 1e-6, errs
     assert rel_l2(img[0, 0], orc(a, th, L)) < 1e-10
-    # the context is back at (a, theta_o)
+    # the context is unchanged
     again = np.asarray(ks.render(s["cache"], m, t, nu, L, precision=ks.KS_FP64))[0, 0]
     assert rel_l2(again, orc(a, th, L)) < 1e-10
+
+
+def test_spacetime_derivatives_all_kinds():
+    """The dual spacetime pass over thermal, power-law, kappa and knot splats, two frames and two
+    frequencies, against central differences of the FP64 render (regenerated at a +- h, theta_o +- h;
+    L e^(+-h)); its image equals the FP64 render (1e-12). A regenerate at a shifted spin or inclination
+    can move a ray's anchor spacing (an integer of k) or carry a sample across the weight cutoff: the
+    discretised function jumps there by ~1e-10 relative, which a central difference with one step turns
+    into errors up to ~1e-4 at some pixels, while the duals keep those choices at the values. So each
+    element is compared with the closest of the central differences at h = 1e-4, 1e-5, 1e-6: a jump
+    spoils a step, not all three (rel L2 1e-6)."""
+    a, tho = 0.94, np.deg2rad(163.0)
+    rng = np.random.Generator(np.random.PCG64(41))
+    pt = scenes.thermal_params(rng, 3, a)
+    pp = scenes.powerlaw_params(rng, 3, a)
+    pk = scenes.kappa_params(rng, 3, a)
+    pn = scenes.thermal_params(rng, 2, a, rlo=3.0, rhi=7.0)
+    pn[3:6] = np.log(rng.uniform(0.8, 2.0, (3, 2)))
+    ktimes = np.array([-80.0, -30.0, 20.0, 60.0])
+    model = ks.CompositeModel(ks.PolarizedSplats(pt), ks.PowerLawSplats(pp), ks.KappaSplats(pk),
+                              ks.KnotSplats(pn, scenes.trajectory_knots(pn, a, ktimes), ktimes))
+    cam = ks.Camera((-12.0, 12.0), (-12.0, 12.0), 12)
+    cache = ks.GeodesicCache(cam, 96)
+    L = ks.gravitational_radius(4e6)
+    times, nus = [0.0, 20.0], [230e9, 690e9]
+    ks.regenerate(cache, a, tho)
+    d, img = ks.spacetime_derivatives(cache, model, times, nus, L, return_image=True)
+    base = np.asarray(ks.render(cache, model, times, nus, L, precision=ks.KS_FP64))
+    assert rel_l2(img, base) < 1e-12
+
+    def rend(aa, th, LL):
+        ks.regenerate(cache, aa, th)
+        return np.asarray(ks.render(cache, model, times, nus, LL, precision=ks.KS_FP64))
+
+    errs = []
+    for q in range(3):
+        fds = []
+        for h in (1e-4, 1e-5, 1e-6):
+            if q == 0:
+                fds.append((rend(a + h, tho, L) - rend(a - h, tho, L)) / (2 * h))
+            elif q == 1:
+                fds.append((rend(a, tho + h, L) - rend(a, tho - h, L)) / (2 * h))
+            else:
+                fds.append((rend(a, tho, L * np.exp(h)) - rend(a, tho, L * np.exp(-h))) / (2 * h))
+        fds = np.stack(fds)
+        pick = np.argmin(np.abs(fds - d[q][None]), axis=0)
+        best = np.take_along_axis(fds, pick[None], axis=0)[0]
+        assert np.abs(best).max() > 0
+        errs.append(rel_l2(d[q], best))
+    ks.regenerate(cache, a, tho)
+    print("spacetime derivatives, all kinds, rel L2 (a, theta_o, ln L):", errs)
+    assert max(errs) < 1e-6, errs
 
 
 def test_vis_chi2_gradient(scene, oracle):
