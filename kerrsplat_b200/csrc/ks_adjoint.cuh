@@ -683,15 +683,22 @@ struct AdjSmem {
 struct AdjUnit {
     long long ur, jbase, j;
     int seg, f, v0, k0, k1, nc;
-    bool live;
+    bool live, dead;
 };
+// The unit of warp `warp` in block work unit ub: the block's W warps take W consecutive chunks of
+// 32 rays with the same segment, frame and frequencies (k_consume's block units, last rays first) and
+// step through the samples together. U.ur is the warp unit's index in the numbering of the per-unit
+// partial sums; a warp whose chunk lies past the last ray is dead (no rays, no partial sums).
 template <int CH>
-__device__ __forceinline__ AdjUnit adj_unit(const MixedJob& job, unsigned long long u, int lane, int N) {
+__device__ __forceinline__ AdjUnit adj_block_unit(const MixedJob& job, long long btotal, unsigned long long ub, int warp, int W, int lane,
+                                                  int N) {
     AdjUnit U;
-    U.ur = job.total - 1 - (long long)u;
     const long long per_chunk = (long long)job.nseg * job.nframes * job.nvc;
-    const long long wg = U.ur / per_chunk;
-    const long long rem = U.ur % per_chunk;
+    const long long br = btotal - 1 - (long long)ub;
+    const long long wg = (br / per_chunk) * W + warp;
+    const long long rem = br % per_chunk;
+    U.dead = wg >= job.nchunks;
+    U.ur = wg * per_chunk + rem;
     U.seg = int(rem / (job.nframes * job.nvc));
     const int y = int(rem % (job.nframes * job.nvc));
     U.f = y / job.nvc;
@@ -725,12 +732,17 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
     const int N = st.N;
     const long long npad = job.npad, npix = job.npix;
     const float a = float(st.a);
+    // block work units, one barrier per sample (the phase alignment of k_consume)
+    __shared__ unsigned long long s_unit;
+    constexpr int W = NT / 32;
+    const long long btotal = (job.nchunks + W - 1) / W * job.nseg * job.nframes * job.nvc;
     for (;;) {
-        unsigned long long u = 0;
-        if (lane == 0) u = atomicAdd(work, 1ull);
-        u = __shfl_sync(full, u, 0);
-        if (u >= (unsigned long long)job.total) break;
-        const AdjUnit U = adj_unit<CH>(job, u, lane, N);
+        __syncthreads();
+        if (threadIdx.x == 0) s_unit = atomicAdd(work, 1ull);
+        __syncthreads();
+        const unsigned long long u = s_unit;
+        if (u >= (unsigned long long)btotal) break;
+        const AdjUnit U = adj_block_unit<CH>(job, btotal, u, warp, W, lane, N);
         float Lnu[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c) Lnu[c] = float(job.L / (cnu[min(U.v0 + c, job.nfreq - 1)] / kNU0));
@@ -762,7 +774,7 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
                 if (lane >= d) incl2 += v;
             }
             const int total2 = __shfl_sync(full, incl2, 31);
-            if (total2 == 0) continue;
+            if (total2 == 0) { __syncthreads(); continue; }
             // Sigma dtau of this lane's sample, for the worker that takes its steps
             const float rr = sp[SM_R * npad], cth = sp[SM_CTH * npad];
             const float sgd = (rr * rr + a * a * cth * cth) * dtau_o;
@@ -810,6 +822,7 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
                 }
             }
             __syncwarp();
+            __syncthreads();
         }
     }
 }
@@ -842,12 +855,17 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
     const long long npad = job.npad;
     const float a = float(st.a), a_sin_tho = float(st.a * sin(st.thetao));
     const long long gsz = (long long)ntot * GR_COUNT;
+    // block work units, one barrier per sample (the phase alignment of k_consume)
+    __shared__ unsigned long long s_unit;
+    constexpr int W = NT / 32;
+    const long long btotal = (job.nchunks + W - 1) / W * job.nseg * job.nframes * job.nvc;
     for (;;) {
-        unsigned long long u = 0;
-        if (lane == 0) u = atomicAdd(work, 1ull);
-        u = __shfl_sync(full, u, 0);
-        if (u >= (unsigned long long)job.total) break;
-        const AdjUnit U = adj_unit<CH>(job, u, lane, N);
+        __syncthreads();
+        if (threadIdx.x == 0) s_unit = atomicAdd(work, 1ull);
+        __syncthreads();
+        const unsigned long long u = s_unit;
+        if (u >= (unsigned long long)btotal) break;
+        const AdjUnit U = adj_block_unit<CH>(job, btotal, u, warp, W, lane, N);
         const float t_obs = float(ct[U.f]);
         float nu[CH];
 #pragma unroll
@@ -855,8 +873,10 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
         const float dtau = float(plan_f[(long long)PF_DTAU * npad + U.j]);
         const float alpha = float(plan_f[(long long)PF_ALPHA * npad + U.j]), beta = float(plan_f[(long long)PF_BETA * npad + U.j]);
         const float eta = float(plan_f[(long long)PF_ETA * npad + U.j]), lam = float(plan_f[(long long)PF_LAM * npad + U.j]);
-        float* gacc = global_acc ? gunit + U.ur * gsz : gacc_smem;
-        for (long long q = lane; q < gsz; q += 32) gacc[q] = 0.f;
+        // a dead warp has no active sample: it neither zeroes nor adds to an accumulator
+        float* gacc = global_acc ? gunit + (U.dead ? 0 : U.ur) * gsz : gacc_smem;
+        if (!U.dead)
+            for (long long q = lane; q < gsz; q += 32) gacc[q] = 0.f;
         {
             // the unit's bounds and candidate splats (as the forward pass)
             UnitBox b{3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f};
@@ -886,7 +906,7 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
                     if (gact[(combo * N + (k - 1)) * npad + U.j]) actbits |= 1u << c;
                 }
             }
-            if (__ballot_sync(full, actbits != 0u) == 0u) continue;
+            if (__ballot_sync(full, actbits != 0u) == 0u) { __syncthreads(); continue; }
             float x = 0.f, yy = 0.f, z = 0.f, ts = 0.f, rho = 0.f;
             if (actbits) {
                 x = sp[SM_X * npad]; yy = sp[SM_Y * npad]; z = sp[SM_Z * npad]; ts = sp[SM_T * npad];
@@ -975,8 +995,9 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
                     __syncwarp();
                 }
             }
+            __syncthreads();
         }
-        if (!global_acc) {
+        if (!global_acc && !U.dead) {
             float* gu = gunit + U.ur * gsz;
             for (long long q = lane; q < gsz; q += 32) gu[q] = gacc[q];
         }
