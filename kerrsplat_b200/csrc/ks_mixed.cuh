@@ -234,23 +234,16 @@ struct MixedSink {
         bool valid = live && inrange && usable;
         if (valid) ev[1]++;
         if (valid && nmax >= 0) valid = wind_ok(r * cth);
-        unsigned vmask = __ballot_sync(full, valid);
-        // the block's warps run each sample's phases together (two barriers per sample, see k_consume)
-        if (vmask == 0u) { __syncthreads(); __syncthreads(); return; }
+        // no early return when no lane has a valid sample: the block's warps take every barrier of
+        // the sample together (the tests/evaluation groups, the steps; see k_consume)
         float* mys = sf + lane;
         float t = 0.f, rho = 0.f;
         if (valid) {
             rho = sqrtf(x * x + y * y);
             t = t_obs - ts;
-            SampleFrame<float> F = sample_frame(a, r, 0.f, sth, cth, eta, lam, nur, nuth);
             mys[SF_X * 32] = x; mys[SF_Y * 32] = y; mys[SF_Z * 32] = z; mys[SF_T * 32] = ts;
-            mys[SF_PU0 * 32] = F.pu[0]; mys[SF_PU1 * 32] = F.pu[1]; mys[SF_PU2 * 32] = F.pu[2]; mys[SF_PU3 * 32] = F.pu[3];
-            mys[SF_PZ0 * 32] = F.pz[0]; mys[SF_PZ1 * 32] = F.pz[1]; mys[SF_PZ2 * 32] = F.pz[2]; mys[SF_PZ3 * 32] = F.pz[3];
-            mys[SF_LI * 32] = F.lapse_inv; mys[SF_OL * 32] = F.om_lapse; mys[SF_SDS * 32] = F.sDS; mys[SF_MIS * 32] = F.misS; mys[SF_IVP * 32] = F.ivarpi;
-            mys[SF_R * 32] = r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
-            mys[SF_SG * 32] = (r * r + a * a * cth * cth) * dtau;   // Sigma dtau of this lane's ray
-            mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
         }
+        bool framed = false;   // the sample's frame data is computed at its first passing pair
         float acc[CH][11];
         unsigned actbits = 0u;
 #pragma unroll
@@ -308,7 +301,21 @@ struct MixedSink {
             }
             const int off = incl - n;
             const int total = __shfl_sync(full, incl, 31);
-            if (total > kItemCap) { single_end = g1; continue; }   // redo this group chunk by chunk
+            // the block redoes the group chunk by chunk when a warp's list would overflow (a barrier:
+            // every warp takes the same groups)
+            if (__syncthreads_or(total > kItemCap)) { single_end = g1; continue; }
+            if (n > 0 && !framed) {
+                // what the evaluations of this lane's pairs read: the sample's frame, position, Sigma dtau
+                const SampleFrame<float> F = sample_frame(a, r, 0.f, sth, cth, eta, lam, nur, nuth);
+                mys[SF_PU0 * 32] = F.pu[0]; mys[SF_PU1 * 32] = F.pu[1]; mys[SF_PU2 * 32] = F.pu[2]; mys[SF_PU3 * 32] = F.pu[3];
+                mys[SF_PZ0 * 32] = F.pz[0]; mys[SF_PZ1 * 32] = F.pz[1]; mys[SF_PZ2 * 32] = F.pz[2]; mys[SF_PZ3 * 32] = F.pz[3];
+                mys[SF_LI * 32] = F.lapse_inv; mys[SF_OL * 32] = F.om_lapse; mys[SF_SDS * 32] = F.sDS; mys[SF_MIS * 32] = F.misS;
+                mys[SF_IVP * 32] = F.ivarpi;
+                mys[SF_R * 32] = r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
+                mys[SF_SG * 32] = (r * r + a * a * cth * cth) * dtau;   // Sigma dtau of this lane's ray
+                mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
+                framed = true;
+            }
             if (total > 0) {
                 // the list: this lane's pairs at [off, off + n), in splat order
                 int k = off;
@@ -520,8 +527,8 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
     const int N = st.N;
     const long long npad = job.npad;
     // Block work units: the block's W warps take W consecutive chunks of 32 rays with the same segment,
-    // frame and frequencies, and step through the samples together: each sample's tests and
-    // evaluations, then its steps, end at a block barrier. Warps in the same phase share the
+    // frame and frequencies, and step through the samples together: within a sample, each group's
+    // tests, its evaluations and the steps are separated by block barriers. Warps in the same phase share the
     // instruction cache lines of that phase (free-running warps in different phases thrashed it:
     // ncu "no instruction" stalls; 24% faster at 256x256, N = 1024, 3 frequencies, same results).
     __shared__ unsigned long long s_unit;
