@@ -1,21 +1,21 @@
-// ks_mixed.cuh -- the mixed-precision march-and-transfer kernel with warp-cooperative compaction.
+// ks_mixed.cuh -- the mixed-precision transfer consumer with block-cooperative compaction.
 //
-// One thread owns one ray (sorted slot) and marches it in FP32 (the recurrence and the quadrature,
-// re-anchored to the FP64 table every M samples). What the reference does per sample
-// (transport.jl:190-198: every element's coefficients, their sum, one exact step, compositing)
-// is split across the 32 lanes of the warp so that the expensive parts run on full warps:
-//   1. every lane with a valid sample tests a chunk of 32 splats against the support sphere and the
-//      weight cutoff (cheap, uniform work) and records the passing (lane, splat) pairs in a per-warp
-//      list in shared memory, in lane order and splat order;
-//   2. the warp evaluates the listed pairs 32 at a time (weight, local frame, synchrotron
-//      coefficients at every frequency, cap, invariants, rotation into the screen basis), each lane
-//      taking one pair whatever ray it belongs to; the owner lane then adds the results of its own
-//      pairs in splat order (the same order as the reference's sum over elements, so the result is
-//      deterministic);
-//   3. the (lane, frequency) pairs with an active sample are again spread over the warp for the
+// k_stream marches every ray once in FP32 (the recurrence and the quadrature, re-anchored to the FP64
+// table every M samples) into a sample stream; k_consume walks the stream with one thread per ray
+// (sorted slot) in blocks that step through the samples together. What the reference does per sample
+// (transport.jl:190-198: every element's coefficients, their sum, one exact step, compositing) is
+// spread over the block so that the expensive parts run on full warps (MixedSink):
+//   1. every thread with a valid sample tests the candidate splats against the support sphere and
+//      the weight cutoff and records the passing (thread, splat) pairs in one block list, in thread
+//      order and splat order;
+//   2. the block evaluates the listed pairs NT at a time (weight, local frame, synchrotron
+//      coefficients at every frequency, cap, invariants, rotation into the screen basis), each thread
+//      taking one pair whatever ray it belongs to; the owner then adds the results of its own pairs in
+//      splat order (the order of the reference's sum over elements, so the result is deterministic);
+//   3. the (thread, frequency) pairs with an active sample are again spread over the block for the
 //      exact 4x4 step (O, E), and each owner composes its own steps front to back (S += P E,
 //      P = P O; step.jl:347).
-// The per-lane Stokes states live in shared memory, the splat table too.
+// The per-thread Stokes states live in shared memory, the splat table too.
 #pragma once
 #include "ks_transfer.cuh"
 
@@ -29,7 +29,6 @@ enum SampleField { SF_X, SF_Y, SF_Z, SF_T, SF_PU0, SF_PU1, SF_PU2, SF_PU3, SF_PZ
 constexpr int kSF = SF_COUNT;                   // floats per lane of sample data
 constexpr int kMaxSplatWords = 16;              // candidate masks cover up to 512 splats
 constexpr int kGroupWords = 8;                  // candidate words tested before one evaluation list
-constexpr int kItemCap = 1024;                  // pairs in one evaluation list (the per-warp item buffer)
 
 // The bounds of a work unit's samples (quasi-Cartesian KS box, cylindrical radius and height) and the
 // splats whose support can reach them: a pattern-rotating splat's support lies within its support
@@ -75,14 +74,14 @@ __device__ __forceinline__ void unit_candidates(const float* tab, int ntot, cons
 
 template <int CH>
 struct MixedSmem {
-    // bytes of the per-warp regions (the splat table comes first), all [field][32 lanes]
+    // per-warp shares of the block's regions (the splat table comes first); the block pools them:
+    // sample data [kSF][NT], pair list | step results, pair results [CH * 12][NT], meta, states
     static constexpr int kSampleBytes = 32 * kSF * 4;
-    static constexpr int kItemBytes = 32 * 32 * 2 > 32 * 20 * 4 ? 32 * 32 * 2 : 32 * 20 * 4;   // item list | step results
-    static constexpr int kResBytes = 32 * CH * 12 * 4;                                          // pair results | step inputs
-    static constexpr int kMetaBytes = 32 * 4 * 2 + kMaxSplatWords * 4;                           // step offsets, bits; candidate mask
-    static constexpr int kStateBytes = 32 * CH * 20 * 4;                                        // P (16) and S (4) per lane and frequency
+    static constexpr int kItemBytes = 32 * 20 * 4;                                              // pair list (4 B items) | step results [20][NT]
+    static constexpr int kResBytes = 32 * CH * 12 * 4;                                          // pair results | step inputs | pass masks
+    static constexpr int kMetaBytes = 32 * 4 * 2 + kMaxSplatWords * 4 + 2 * 4;                   // step offsets, bits; candidate mask; scan sums
+    static constexpr int kStateBytes = 32 * CH * 20 * 4;                                        // P (16) and S (4) per thread and frequency
     static constexpr int kWarpBytes = kSampleBytes + kItemBytes + kResBytes + kMetaBytes + kStateBytes;
-    static_assert(kItemCap * 2 <= kItemBytes, "the item list holds kItemCap pairs");
     static_assert(kGroupWords * 32 * 4 <= kResBytes, "a group's pass masks fit in the pair-results buffer");
     static_assert(32 * kMaxSplatWords <= 512, "items carry 9-bit splat indices");
     // the splat table and the knot array (nkv floats) come first
@@ -92,22 +91,23 @@ struct MixedSmem {
 
 // Out-of-line pieces of the consumer: one copy of each in the instruction cache (inlined into the
 // per-frequency loop and the three populations they overflowed it; ncu: "no instruction" stalls).
-// s: the owner lane's column of the warp's sample data ([field][32] layout)
+// s: the owner's column of the block's sample data ([field][NT] layout)
+template <int NT>
 __device__ __noinline__ LFrame<float> local_frame_ool(const float* s, const float* p, float a, float a_sin_tho) {
     SampleFrame<float> F;
-    F.pu[0] = s[SF_PU0 * 32]; F.pu[1] = s[SF_PU1 * 32]; F.pu[2] = s[SF_PU2 * 32]; F.pu[3] = s[SF_PU3 * 32];
-    F.pz[0] = s[SF_PZ0 * 32]; F.pz[1] = s[SF_PZ1 * 32]; F.pz[2] = s[SF_PZ2 * 32]; F.pz[3] = s[SF_PZ3 * 32];
-    F.lapse_inv = s[SF_LI * 32]; F.om_lapse = s[SF_OL * 32]; F.sDS = s[SF_SDS * 32]; F.misS = s[SF_MIS * 32]; F.ivarpi = s[SF_IVP * 32];
-    F.r = s[SF_R * 32]; F.sth = s[SF_STH * 32]; F.cth = s[SF_CTH * 32]; F.a = a;
+    F.pu[0] = s[SF_PU0 * NT]; F.pu[1] = s[SF_PU1 * NT]; F.pu[2] = s[SF_PU2 * NT]; F.pu[3] = s[SF_PU3 * NT];
+    F.pz[0] = s[SF_PZ0 * NT]; F.pz[1] = s[SF_PZ1 * NT]; F.pz[2] = s[SF_PZ2 * NT]; F.pz[3] = s[SF_PZ3 * NT];
+    F.lapse_inv = s[SF_LI * NT]; F.om_lapse = s[SF_OL * NT]; F.sDS = s[SF_SDS * NT]; F.misS = s[SF_MIS * NT]; F.ivarpi = s[SF_IVP * NT];
+    F.r = s[SF_R * NT]; F.sth = s[SF_STH * NT]; F.cth = s[SF_CTH * NT]; F.a = a;
     return local_frame(F, p[ST_U1], p[ST_U2], p[ST_U3], p[ST_BHX], p[ST_BHY], p[ST_BHZ], p[ST_BZERO] != 0.f,
-                       s[SF_ALPHA * 32], s[SF_BETA * 32], a_sin_tho);
+                       s[SF_ALPHA * NT], s[SF_BETA * NT], a_sin_tho);
 }
 
 // Screen-basis coefficients of one splat at one frequency (transport.jl:265-270), written with a
-// stride of 32 floats: j (4), alpha (4), rho (3), active flag.
+// stride of NT floats: j (4), alpha (4), rho (3), active flag.
 // KM: the populations the scene contains (bit 0 thermal, 1 power law, 2 kappa); the kernel for a
 // thermal-only scene carries none of the other fits' code.
-template <int KM>
+template <int KM, int NT>
 __device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, float ne, float nuf, float sb, float cb, float s2c, float c2c,
                                                      float* r) {
     Coef<float> cf;
@@ -118,16 +118,16 @@ __device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, f
     else
         cf = thermal_cs(ne, p[ST_TE], p[ST_F0], p[ST_KR], p[ST_BMAG], nuf, sb, cb);
     bool on = cf.jI > 0.f || cf.aI > 0.f || cf.rQ != 0.f || cf.rV != 0.f;
-    if (!on) { r[352] = 0.f; return; }
+    if (!on) { r[11 * NT] = 0.f; return; }
     float fe = cap_factor(cf.jI, cf.jQ, cf.jV, 0.99f);
     float fa = cap_factor(cf.aI, cf.aQ, cf.aV, 0.99f);
     float nh = nuf / float(kNU0);
     float i2 = 1.f / (nh * nh);
     float jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
-    r[0] = cf.jI * i2; r[32] = jQ * c2c; r[64] = jQ * s2c; r[96] = cf.jV * fe * i2;
-    r[128] = nh * cf.aI; r[160] = aQ * c2c; r[192] = aQ * s2c; r[224] = cf.aV * fa * nh;
-    r[256] = rQ * c2c; r[288] = rQ * s2c; r[320] = nh * cf.rV;
-    r[352] = 1.f;
+    r[0] = cf.jI * i2; r[NT] = jQ * c2c; r[2 * NT] = jQ * s2c; r[3 * NT] = cf.jV * fe * i2;
+    r[4 * NT] = nh * cf.aI; r[5 * NT] = aQ * c2c; r[6 * NT] = aQ * s2c; r[7 * NT] = cf.aV * fa * nh;
+    r[8 * NT] = rQ * c2c; r[9 * NT] = rQ * s2c; r[10 * NT] = nh * cf.rV;
+    r[11 * NT] = 1.f;
 }
 
 __device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float* O, float* E) {
@@ -139,8 +139,25 @@ __device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float*
     for (int q = 0; q < 4; ++q) E[q] = e[q];
 }
 
-template <int CH, int KM>
+// The consumer of one thread (one ray) of a block work unit: all NT threads of the block call
+// consume() for the same sample together. What the reference does per sample (transport.jl:190-198:
+// every element's coefficients, their sum, one exact step, compositing) is spread over the block:
+//   1. every thread with a valid sample tests the unit's candidate splats against the support and
+//      the weight cutoff, and the passing (thread, splat) pairs of up to kGroupWords candidate words
+//      go into one block list (thread order, splat order within a thread);
+//   2. the block evaluates the list NT pairs at a time (weight, local frame, synchrotron
+//      coefficients at every frequency, cap, invariants, rotation into the screen basis), each thread
+//      taking one pair whatever ray it belongs to, and every owner adds the results of its own pairs
+//      in list order (the reference's order of the sum over elements: deterministic);
+//   3. the (thread, frequency) pairs with an active sample are spread over the block for the exact
+//      4x4 step (O, E), and each owner composes its steps front to back (S += P E, P = P O;
+//      step.jl:347).
+// Block lists keep every round full across warps: with per-warp lists the warps of a block waited at
+// the phase barriers for the one with the most pairs.
+template <int CH, int KM, int NT>
 struct MixedSink {
+    static constexpr int W = NT / 32;
+    static_assert(NT <= 512, "items carry 9-bit owner indices");
     const float* tab; int ntot;
     const float* knots;   // the knot array of knot splats (after the table)
     float t_obs;
@@ -148,32 +165,35 @@ struct MixedSink {
     int nc;
     float a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
     int nmax;
-    int lane;
-    bool live;        // false for the padding lanes past the last ray
-    float* sf;        // this warp's sample data [kSF][32]
-    uint16_t* items;  // this warp's pair list [1024]
-    float* sres;      // step results [20][32] (aliases the pair list)
-    float* res;       // pair results [CH * 12][32] | step inputs
-    float* state;     // this lane's P/S column of the warp's [CH * 20][32] array
-    int* meta_off;    // this warp's first step item per lane [32]
-    unsigned* meta_bits;   // and active-frequency bits [32]
-    const unsigned* cand;  // the unit's candidate splats (unit_candidates)
+    int tid;
+    bool live;        // false for the padding threads past the last ray
+    float* sf;        // the block's sample data [kSF][NT]
+    unsigned* items;  // the block's pair list (item_cap entries: owner << 9 | splat)
+    float* sres;      // step results [20][NT] (aliases the pair list)
+    float* res;       // pair results [CH * 12][NT] | step inputs | a group's pass masks [kGroupWords][NT]
+    float* state;     // this thread's P/S column of the block's [CH * 20][NT] array
+    int* meta_off;    // the block's first step item per thread [NT]
+    unsigned* meta_bits;   // and active-frequency bits [NT]
+    int* wsum;        // warp sums of the block scans, double-buffered [2][W]
+    int scan_par;
+    int item_cap;
+    const unsigned* cand;  // this warp's candidate splats (unit_candidates)
     float zprev; int wn; bool inside, crossed, zset;
     unsigned int ev[7];
-    // the adjoint's forward pass (null otherwise): at every active (sample, lane, frequency) the state
-    // P before the sample (16) and the summed coefficients (11) into gstate[((combo N + k - 1) 27 +
-    // field) npad + ray], and gact[(combo N + k - 1) npad + ray] = 1
+    // the adjoint's forward pass (null otherwise): at every active (sample, thread, frequency) the
+    // state P before the sample (16) and the summed coefficients (11) into gstate[((combo N + k - 1)
+    // 27 + field) npad + ray], and gact[(combo N + k - 1) npad + ray] = 1; jbase = the block's first ray
     float* gstate;
     unsigned char* gact;
     long long gnpad, jbase;
     int gN, kcur, gframes, gf, gv0;
-    int nsamp;        // this lane's samples
+    int nsamp;        // this thread's samples
 
     __device__ void init() {
         for (int c = 0; c < CH; ++c) {
-            float* st = state + c * 20 * 32;
-            for (int q = 0; q < 16; ++q) st[q * 32] = (q % 5 == 0) ? 1.f : 0.f;
-            for (int q = 16; q < 20; ++q) st[q * 32] = 0.f;
+            float* st = state + c * 20 * NT;
+            for (int q = 0; q < 16; ++q) st[q * NT] = (q % 5 == 0) ? 1.f : 0.f;
+            for (int q = 16; q < 20; ++q) st[q * NT] = 0.f;
         }
         for (int q = 0; q < 7; ++q) ev[q] = 0;
         wn = 0; inside = false; crossed = false; zset = false; zprev = 0.f;
@@ -195,17 +215,42 @@ struct MixedSink {
         return wn <= nmax;
     }
 
-    // pair (owner lane o, splat i): weight, frame, coefficients at every frequency -> res slot
+    // Exclusive block scan of v (one barrier; the warp sums alternate between two buffers, so the
+    // next scan does not overwrite sums a slower warp is still reading); total = the block sum.
+    __device__ int scan(int v, int& total) {
+        const int lane = tid & 31, warp = tid >> 5;
+        int* ws = wsum + scan_par * W;
+        scan_par ^= 1;
+        int incl = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        if (lane == 31) ws[warp] = incl;
+        __syncthreads();
+        int pre = 0, tot = 0;
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            const int sv = ws[q];
+            pre += (q < warp) ? sv : 0;
+            tot += sv;
+        }
+        total = tot;
+        return pre + incl - v;
+    }
+
+    // pair (owner o, splat i): weight, frame, coefficients at every frequency -> res slot
     __device__ void evaluate(int o, int i, float* out) {
-        // this warp's sample data is stored field-major ([field][lane]) so that lanes hit distinct banks
+        // the block's sample data is stored field-major ([field][thread]) so that threads hit distinct banks
         const float* s = sf + o;
         const float* p = tab + i * ST_COUNT;
         const int kind = int(p[ST_KIND]);
         float q;
-        if (kind == KS_KNOT21) knot_exponent(p, knots, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], q);
-        else splat_exponent(p, t_obs - s[SF_T * 32], s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], false, q);
+        if (kind == KS_KNOT21) knot_exponent(p, knots, t_obs - s[SF_T * NT], s[SF_X * NT], s[SF_Y * NT], s[SF_Z * NT], q);
+        else splat_exponent(p, t_obs - s[SF_T * NT], s[SF_X * NT], s[SF_Y * NT], s[SF_Z * NT], false, q);
         float G = __expf(-q);
-        LFrame<float> lf = local_frame_ool(s, p, a, a_sin_tho);
+        LFrame<float> lf = local_frame_ool<NT>(s, p, a, a_sin_tho);
         float sb, cb;
         pitch_sc(lf.cosB, sb, cb);
         float ne = p[ST_NE] * G;
@@ -213,64 +258,60 @@ struct MixedSink {
         int act = 0;
 #pragma unroll 1
         for (int c = 0; c < CH; ++c) {
-            float* r = out + c * 12 * 32;   // out = res + slot; fields are 32 apart
-            if (c >= nc) { r[352] = 0.f; continue; }
+            float* r = out + c * 12 * NT;   // out = res + slot; fields are NT apart
+            if (c >= nc) { r[11 * NT] = 0.f; continue; }
             float nuc = nu[0];
 #pragma unroll
             for (int cc = 1; cc < CH; ++cc) nuc = (cc == c) ? nu[cc] : nuc;
-            screen_coefficients_ool<KM>(kind, p, ne, nuc / lf.g, sb, cb, s2c, c2c, r);
-            act |= r[352] != 0.f;
+            screen_coefficients_ool<KM, NT>(kind, p, ne, nuc / lf.g, sb, cb, s2c, c2c, r);
+            act |= r[11 * NT] != 0.f;
         }
         ev[4] += act ? 1 : 0;
     }
 
-    // The consumer for one sample of every lane of the warp (all 32 lanes call it together):
+    // The consumer for one sample of every thread of the block (all NT threads call it together):
     // `usable` = Krang's validity and outside r_h (1 + 1e-3) (transport.jl:171-173); x, y, z the
     // quasi-Cartesian Kerr-Schild position, ts the regularized lookback time t~.
     __device__ void consume(bool usable, float x, float y, float z, float ts, float r, float sth, float cth, bool nur, bool nuth) {
-        const unsigned full = 0xffffffffu;
         const bool inrange = kcur <= nsamp;   // a ray with fewer samples than the unit's segment
         if (inrange) ev[0]++;
         bool valid = live && inrange && usable;
         if (valid) ev[1]++;
         if (valid && nmax >= 0) valid = wind_ok(r * cth);
-        // no early return when no lane has a valid sample: the block's warps take every barrier of
-        // the sample together (the tests/evaluation groups, the steps; see k_consume)
-        float* mys = sf + lane;
+        float* mys = sf + tid;
         float t = 0.f, rho = 0.f;
         if (valid) {
             rho = sqrtf(x * x + y * y);
             t = t_obs - ts;
-            mys[SF_X * 32] = x; mys[SF_Y * 32] = y; mys[SF_Z * 32] = z; mys[SF_T * 32] = ts;
+            mys[SF_X * NT] = x; mys[SF_Y * NT] = y; mys[SF_Z * NT] = z; mys[SF_T * NT] = ts;
         }
-        bool framed = false;   // the sample's frame data is computed at its first passing pair
+        bool framed = false;   // the sample's frame data is formed at its first passing pair
         float acc[CH][11];
         unsigned actbits = 0u;
 #pragma unroll
         for (int c = 0; c < CH; ++c)
 #pragma unroll
             for (int q = 0; q < 11; ++q) acc[c][q] = 0.f;
-        __syncwarp();
-        // Tests over groups of up to kGroupWords candidate words (256 splats): every passing (lane,
-        // splat) pair of a group goes into one list, so that the evaluation rounds run on full warps
-        // whatever the chunk a splat belongs to. The group's pass masks are kept in the pair-results
-        // buffer until the list is written (it is free until the evaluations). A group whose list
-        // would overflow is redone one chunk (32 splats, at most 1024 pairs) at a time.
+        // Tests over groups of up to kGroupWords candidate words (256 splats), one block list per
+        // group. The group's pass masks are kept in the pair-results buffer until the list is written
+        // (it is free until the evaluations). A group whose list would overflow is redone one chunk
+        // (32 splats, the mask in a register) at a time, in windows of item_cap pairs.
         const int nw = (ntot + 31) >> 5;
-        unsigned* gmask = reinterpret_cast<unsigned*>(res) + lane;   // [kGroupWords][32]
+        unsigned* gmask = reinterpret_cast<unsigned*>(res) + tid;   // [kGroupWords][NT]
         int single_end = -1;   // chunks below this index go one at a time
         for (int g0 = 0; g0 < nw;) {
-            const int g1 = (g0 < single_end) ? g0 + 1 : min(nw, g0 + kGroupWords);
-            // 1. tests of the unit's candidates: support sphere, then the weight cutoff
+            const bool single = g0 < single_end;
+            const int g1 = single ? g0 + 1 : min(nw, g0 + kGroupWords);
             int n = 0;
+            unsigned m1 = 0u;
             for (int wd = g0; wd < g1; ++wd) {
                 const unsigned cm = cand[wd];
                 unsigned mask = 0u;
                 if (valid && cm) {
-                    unsigned cb = cm;
-                    while (cb) {
-                        const int b = __ffs(cb) - 1;
-                        cb &= cb - 1;
+                    unsigned cbits = cm;
+                    while (cbits) {
+                        const int b = __ffs(cbits) - 1;
+                        cbits &= cbits - 1;
                         const float* p = tab + (wd * 32 + b) * ST_COUNT;
                         float q;
                         ev[2]++;
@@ -290,111 +331,99 @@ struct MixedSink {
                         if (q < kQCUT) mask |= 1u << b;
                     }
                 }
-                gmask[(wd - g0) * 32] = mask;
+                if (single) m1 = mask;
+                else gmask[(wd - g0) * NT] = mask;
                 n += __popc(mask);
             }
-            int incl = n;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                int v = __shfl_up_sync(full, incl, d);
-                if (lane >= d) incl += v;
-            }
-            const int off = incl - n;
-            const int total = __shfl_sync(full, incl, 31);
-            // the block redoes the group chunk by chunk when a warp's list would overflow (a barrier:
-            // every warp takes the same groups)
-            if (__syncthreads_or(total > kItemCap)) { single_end = g1; continue; }
+            int total;
+            const int off = scan(n, total);   // block-uniform total: every thread takes the same branches
+            if (!single && total > item_cap) { single_end = g1; continue; }
             if (n > 0 && !framed) {
-                // what the evaluations of this lane's pairs read: the sample's frame, position, Sigma dtau
+                // what the evaluations of this thread's pairs read: the sample's frame, position, Sigma dtau
                 const SampleFrame<float> F = sample_frame(a, r, 0.f, sth, cth, eta, lam, nur, nuth);
-                mys[SF_PU0 * 32] = F.pu[0]; mys[SF_PU1 * 32] = F.pu[1]; mys[SF_PU2 * 32] = F.pu[2]; mys[SF_PU3 * 32] = F.pu[3];
-                mys[SF_PZ0 * 32] = F.pz[0]; mys[SF_PZ1 * 32] = F.pz[1]; mys[SF_PZ2 * 32] = F.pz[2]; mys[SF_PZ3 * 32] = F.pz[3];
-                mys[SF_LI * 32] = F.lapse_inv; mys[SF_OL * 32] = F.om_lapse; mys[SF_SDS * 32] = F.sDS; mys[SF_MIS * 32] = F.misS;
-                mys[SF_IVP * 32] = F.ivarpi;
-                mys[SF_R * 32] = r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
-                mys[SF_SG * 32] = (r * r + a * a * cth * cth) * dtau;   // Sigma dtau of this lane's ray
-                mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
+                mys[SF_PU0 * NT] = F.pu[0]; mys[SF_PU1 * NT] = F.pu[1]; mys[SF_PU2 * NT] = F.pu[2]; mys[SF_PU3 * NT] = F.pu[3];
+                mys[SF_PZ0 * NT] = F.pz[0]; mys[SF_PZ1 * NT] = F.pz[1]; mys[SF_PZ2 * NT] = F.pz[2]; mys[SF_PZ3 * NT] = F.pz[3];
+                mys[SF_LI * NT] = F.lapse_inv; mys[SF_OL * NT] = F.om_lapse; mys[SF_SDS * NT] = F.sDS; mys[SF_MIS * NT] = F.misS;
+                mys[SF_IVP * NT] = F.ivarpi;
+                mys[SF_R * NT] = r; mys[SF_STH * NT] = sth; mys[SF_CTH * NT] = cth;
+                mys[SF_SG * NT] = (r * r + a * a * cth * cth) * dtau;   // Sigma dtau of this thread's ray
+                mys[SF_ALPHA * NT] = alpha; mys[SF_BETA * NT] = beta;
                 framed = true;
             }
-            if (total > 0) {
-                // the list: this lane's pairs at [off, off + n), in splat order
-                int k = off;
-                for (int wd = g0; wd < g1; ++wd) {
-                    unsigned m = gmask[(wd - g0) * 32];
-                    while (m) {
-                        const int b = __ffs(m) - 1;
-                        m &= m - 1;
-                        items[k++] = uint16_t((lane << 9) | (wd * 32 + b));
+            for (int wb = 0; wb < total; wb += item_cap) {
+                // this thread's pairs with list index in [wb, wb + item_cap)
+                if (n > 0 && off + n > wb && off < wb + item_cap) {
+                    int k = off;
+                    for (int wd = g0; wd < g1; ++wd) {
+                        unsigned m = single ? m1 : gmask[(wd - g0) * NT];
+                        while (m) {
+                            const int b = __ffs(m) - 1;
+                            m &= m - 1;
+                            if (k >= wb && k < wb + item_cap) items[k - wb] = (unsigned(tid) << 9) | unsigned(wd * 32 + b);
+                            ++k;
+                        }
                     }
                 }
-                __syncwarp();
-                // 2. evaluation rounds over the warp, then owner accumulation in list order
-                for (int base = 0; base < total; base += 32) {
-                    const int kk0 = base + lane;
-                    if (kk0 < total) {
-                        const int it = items[kk0];
-                        evaluate(it >> 9, it & 511, res + lane);
+                __syncthreads();
+                // 2. evaluation rounds over the block, then owner accumulation in list order
+                const int wt = min(item_cap, total - wb);
+                for (int base = 0; base < wt; base += NT) {
+                    const int kk0 = base + tid;
+                    if (kk0 < wt) {
+                        const unsigned it = items[kk0];
+                        evaluate(int(it >> 9), int(it & 511u), res + tid);
                     }
-                    __syncwarp();
-                    const int lo = max(off, base), hi = min(off + n, base + 32);
+                    __syncthreads();
+                    const int lo = max(off, wb + base), hi = min(off + n, wb + base + NT);
                     for (int kk = lo; kk < hi; ++kk) {
-                        const float* r = res + (kk - base);
+                        const float* rr = res + (kk - wb - base);
 #pragma unroll
                         for (int c = 0; c < CH; ++c) {
-                            if (r[(c * 12 + 11) * 32] != 0.f) {
+                            if (rr[(c * 12 + 11) * NT] != 0.f) {
 #pragma unroll
-                                for (int q = 0; q < 11; ++q) acc[c][q] += r[(c * 12 + q) * 32];
+                                for (int q = 0; q < 11; ++q) acc[c][q] += rr[(c * 12 + q) * NT];
                                 actbits |= 1u << c;
                             }
                         }
                     }
-                    __syncwarp();
+                    __syncthreads();
                 }
             }
             g0 = g1;
         }
-        // 3. steps: (lane, frequency) pairs with active coefficients, spread over the warp
-        __syncthreads();
+        // 3. steps: (thread, frequency) pairs with active coefficients, spread over the block
         const int n2 = __popc(actbits);
-        int incl2 = n2;
+        int total2;
+        const int off2 = scan(n2, total2);
+        if (total2 == 0) return;
+        // publish this thread's sums (step inputs) in the results buffer: [c][12][NT]
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            int v = __shfl_up_sync(full, incl2, d);
-            if (lane >= d) incl2 += v;
-        }
-        const int off2 = incl2 - n2;
-        const int total2 = __shfl_sync(full, incl2, 31);
-        if (total2 == 0) { __syncthreads(); return; }
-        // publish this lane's sums (step inputs) in the results buffer: [lane][c][12]
-        {
+        for (int c = 0; c < CH; ++c)
 #pragma unroll
-            for (int c = 0; c < CH; ++c)
-#pragma unroll
-                for (int q = 0; q < 11; ++q) res[(c * 12 + q) * 32 + lane] = acc[c][q];
-        }
-        meta_off[lane] = off2;
-        meta_bits[lane] = actbits;
-        __syncwarp();
-        for (int base = 0; base < total2; base += 32) {
-            const int g = base + lane;
+            for (int q = 0; q < 11; ++q) res[(c * 12 + q) * NT + tid] = acc[c][q];
+        meta_off[tid] = off2;
+        meta_bits[tid] = actbits;
+        __syncthreads();
+        for (int base = 0; base < total2; base += NT) {
+            const int g = base + tid;
             if (g < total2) {
-                // owner: the last lane whose first item is <= g (offsets are non-decreasing)
+                // owner: the last thread whose first item is <= g (offsets are non-decreasing)
                 int o = 0;
 #pragma unroll
-                for (int d = 16; d >= 1; d >>= 1)
-                    if (o + d < 32 && meta_off[o + d] <= g) o += d;
+                for (int d = 256; d >= 1; d >>= 1)
+                    if (o + d < NT && meta_off[o + d] <= g) o += d;
                 // its (g - off)-th active frequency
                 unsigned bits = meta_bits[o];
-                int j = g - meta_off[o];
+                const int j = g - meta_off[o];
                 for (int q = 0; q < j; ++q) bits &= bits - 1;
                 const int c = __ffs(bits) - 1;
                 float in[11];
 #pragma unroll
-                for (int q = 0; q < 11; ++q) in[q] = res[(c * 12 + q) * 32 + o];
+                for (int q = 0; q < 11; ++q) in[q] = res[(c * 12 + q) * NT + o];
                 float Lc = Lnu[0];
 #pragma unroll
                 for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;   // no dynamic register indexing
-                float Dl = Lc * sf[SF_SG * 32 + o];   // the owner's Sigma dtau
+                const float Dl = Lc * sf[SF_SG * NT + o];   // the owner's Sigma dtau
                 float O[16], E[4];
                 transfer_step_ool(in, Dl, O, E);
                 if (gstate) {
@@ -404,13 +433,13 @@ struct MixedSink {
                     for (int q = 0; q < 11; ++q) gs[q * gnpad] = in[q];
                 }
 #pragma unroll
-                for (int q = 0; q < 16; ++q) sres[q * 32 + lane] = O[q];
+                for (int q = 0; q < 16; ++q) sres[q * NT + tid] = O[q];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) sres[(16 + q) * 32 + lane] = E[q];
+                for (int q = 0; q < 4; ++q) sres[(16 + q) * NT + tid] = E[q];
             }
-            __syncwarp();
+            __syncthreads();
             // owners compose their steps front to back (frequency order)
-            const int lo = max(off2, base), hi = min(off2 + n2, base + 32);
+            const int lo = max(off2, base), hi = min(off2 + n2, base + NT);
             if (lo < hi) {
                 unsigned bits = actbits;
                 for (int q = off2; q < lo; ++q) bits &= bits - 1;
@@ -419,36 +448,35 @@ struct MixedSink {
                     bits &= bits - 1;
                     float OE[20];
 #pragma unroll
-                    for (int q = 0; q < 20; ++q) OE[q] = sres[q * 32 + (g2 - base)];
-                    float* st = state + c * 20 * 32;   // this lane's column, fields 32 apart
+                    for (int q = 0; q < 20; ++q) OE[q] = sres[q * NT + (g2 - base)];
+                    float* st = state + c * 20 * NT;   // this thread's column, fields NT apart
                     float P[16], S4[4];
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) P[q] = st[q * 32];
+                    for (int q = 0; q < 16; ++q) P[q] = st[q * NT];
                     if (gstate) {
                         const long long combo = (long long)(gv0 + c) * gframes + gf;
                         const long long row = combo * gN + (kcur - 1);
-                        float* gs = gstate + row * 27 * gnpad + jbase + lane;
+                        float* gs = gstate + row * 27 * gnpad + jbase + tid;
 #pragma unroll
                         for (int q = 0; q < 16; ++q) gs[q * gnpad] = P[q];
-                        gact[row * gnpad + jbase + lane] = 1;
+                        gact[row * gnpad + jbase + tid] = 1;
                     }
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) S4[q] = st[(16 + q) * 32];
+                    for (int q = 0; q < 4; ++q) S4[q] = st[(16 + q) * NT];
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        S4[r] += P[4 * r] * OE[16] + P[4 * r + 1] * OE[17] + P[4 * r + 2] * OE[18] + P[4 * r + 3] * OE[19];
+                    for (int r4 = 0; r4 < 4; ++r4) {
+                        S4[r4] += P[4 * r4] * OE[16] + P[4 * r4 + 1] * OE[17] + P[4 * r4 + 2] * OE[18] + P[4 * r4 + 3] * OE[19];
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
-                            st[(4 * r + q) * 32] = P[4 * r] * OE[q] + P[4 * r + 1] * OE[4 + q] + P[4 * r + 2] * OE[8 + q] + P[4 * r + 3] * OE[12 + q];
+                            st[(4 * r4 + q) * NT] = P[4 * r4] * OE[q] + P[4 * r4 + 1] * OE[4 + q] + P[4 * r4 + 2] * OE[8 + q] + P[4 * r4 + 3] * OE[12 + q];
                     }
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) st[(16 + q) * 32] = S4[q];
+                    for (int q = 0; q < 4; ++q) st[(16 + q) * NT] = S4[q];
                     ev[6]++;
                 }
             }
-            __syncwarp();
+            __syncthreads();
         }
-        __syncthreads();
     }
 };
 
@@ -518,9 +546,20 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
     extern __shared__ __align__(16) unsigned char smem[];
     float* tab = reinterpret_cast<float*>(smem);
     for (int q = threadIdx.x; q < ntot * ST_COUNT + job.nkv; q += blockDim.x) tab[q] = float(tab64[q]);
-    unsigned char* wbase = smem + MixedSmem<CH>::tab_bytes(ntot, job.nkv);
+    // the block's regions after the table (each the sum of the warps' shares, MixedSmem)
+    using MS = MixedSmem<CH>;
+    constexpr int W = NT / 32;
+    unsigned char* bb = smem + MS::tab_bytes(ntot, job.nkv);
+    float* sf_b = reinterpret_cast<float*>(bb);
+    unsigned char* items_b = bb + W * MS::kSampleBytes;
+    float* res_b = reinterpret_cast<float*>(items_b + W * MS::kItemBytes);
+    int* meta_off_b = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(res_b) + W * MS::kResBytes);
+    unsigned* meta_bits_b = reinterpret_cast<unsigned*>(meta_off_b + NT);
+    unsigned* cand_b = meta_bits_b + NT;                                   // [W][kMaxSplatWords]
+    int* wsum_b = reinterpret_cast<int*>(cand_b + W * kMaxSplatWords);     // [2][W]
+    float* state_b = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(meta_off_b) + W * MS::kMetaBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wb = wbase + size_t(warp) * MixedSmem<CH>::kWarpBytes;
+    unsigned* cand = cand_b + warp * kMaxSplatWords;
     __syncthreads();
     unsigned int ev[7] = {0, 0, 0, 0, 0, 0, 0};
     unsigned int samples_c = 0;
@@ -533,7 +572,6 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
     // ncu "no instruction" stalls; 24% faster at 256x256, N = 1024, 3 frequencies, same results).
     __shared__ unsigned long long s_unit;
     __shared__ int s_kmax;
-    constexpr int W = NT / 32;
     const long long nbchunks = (job.nchunks + W - 1) / W;
     const long long btotal = nbchunks * job.nseg * job.nframes * job.nvc;
     for (;;) {
@@ -559,7 +597,7 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         __syncthreads();
         const int kmax = s_kmax;
         const int k1 = min(min(N + 1, k0 + job.seg_len), kmax + 1);
-        MixedSink<CH, KM> sink;
+        MixedSink<CH, KM, NT> sink;
         sink.tab = tab; sink.ntot = ntot; sink.knots = tab + ntot * ST_COUNT;
         sink.t_obs = float(ct[f]);
         sink.nc = min(CH, job.nfreq - v0);
@@ -573,20 +611,21 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         sink.alpha = float(P.get(PF_ALPHA, j)); sink.beta = float(P.get(PF_BETA, j));
         sink.eta = float(P.get(PF_ETA, j)); sink.lam = float(P.get(PF_LAM, j));
         sink.a_sin_tho = float(st.a * sin(st.thetao)); sink.slab = job.slab; sink.nmax = job.nmax;
-        sink.lane = lane; sink.live = live;
+        sink.tid = threadIdx.x; sink.live = live;
         sink.nsamp = int(P.get(PF_NSAMP, j));
-        sink.gstate = job.gstate; sink.gact = job.gact; sink.gnpad = npad; sink.jbase = w * 32;
+        sink.gstate = job.gstate; sink.gact = job.gact; sink.gnpad = npad; sink.jbase = (ur / per_chunk) * NT;
         sink.gN = N; sink.gframes = job.nframes; sink.gf = f; sink.gv0 = v0;
-        sink.sf = reinterpret_cast<float*>(wb);
-        sink.items = reinterpret_cast<uint16_t*>(wb + MixedSmem<CH>::kSampleBytes);
-        sink.sres = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes);
-        sink.res = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes);
-        sink.meta_off = reinterpret_cast<int*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes + MixedSmem<CH>::kResBytes);
-        sink.meta_bits = reinterpret_cast<unsigned*>(sink.meta_off + 32);
-        unsigned* cand = sink.meta_bits + 32;
+        sink.sf = sf_b;
+        sink.items = reinterpret_cast<unsigned*>(items_b);
+        sink.sres = reinterpret_cast<float*>(items_b);
+        sink.res = res_b;
+        sink.meta_off = meta_off_b;
+        sink.meta_bits = meta_bits_b;
+        sink.wsum = wsum_b;
+        sink.scan_par = 0;
+        sink.item_cap = W * MS::kItemBytes / 4;
         sink.cand = cand;
-        sink.state = reinterpret_cast<float*>(wb + MixedSmem<CH>::kSampleBytes + MixedSmem<CH>::kItemBytes + MixedSmem<CH>::kResBytes +
-                                              MixedSmem<CH>::kMetaBytes) + lane;
+        sink.state = state_b + threadIdx.x;
         sink.init();
         {
             // the unit's bounds and candidate splats
@@ -610,13 +649,12 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
             sink.consume((flags & 8u) != 0u, sp[SM_X * npad], sp[SM_Y * npad], sp[SM_Z * npad], sp[SM_T * npad], sp[SM_R * npad],
                          sp[SM_STH * npad], sp[SM_CTH * npad], (flags & 2u) != 0u, (flags & 4u) != 0u);
         }
-        __syncwarp();
         if (live) {
             for (int c = 0; c < sink.nc; ++c) {
-                const float* S = sink.state + c * 20 * 32;
+                const float* S = sink.state + c * 20 * NT;
                 float* o = seg_out + (((long long)((v0 + c) * job.nframes + f) * job.nseg + seg) * job.npix + j) * 20;
 #pragma unroll
-                for (int q = 0; q < 20; ++q) o[q] = S[q * 32];
+                for (int q = 0; q < 20; ++q) o[q] = S[q * NT];
             }
             for (int q = 0; q < 7; ++q) ev[q] += sink.ev[q];
             samples_c += sink.ev[0] * sink.nc;
