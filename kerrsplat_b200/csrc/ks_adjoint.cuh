@@ -604,21 +604,21 @@ namespace {
 
 using namespace ks;
 
-// s: the owner lane's column of the warp's sample data ([field][32]); cb: the owner's c-bar column of
-// [CH][11][32]; nu: the unit's frequencies
-template <int CH>
+// s: the owner's column of the block's sample data ([field][NT]); cb: the owner's c-bar column of
+// [CH][11][NT]; nu: the unit's frequencies
+template <int CH, int NT>
 __device__ __noinline__ void element_adjoint_ool(const float* p, const double* gt, const float* s, float t_obs, float a, float a_sin_tho,
                                                  const float* nu, int nc, unsigned act, const float* cb, float* g) {
     SampleFrame<float> F;
-    F.pu[0] = s[SF_PU0 * 32]; F.pu[1] = s[SF_PU1 * 32]; F.pu[2] = s[SF_PU2 * 32]; F.pu[3] = s[SF_PU3 * 32];
-    F.pz[0] = s[SF_PZ0 * 32]; F.pz[1] = s[SF_PZ1 * 32]; F.pz[2] = s[SF_PZ2 * 32]; F.pz[3] = s[SF_PZ3 * 32];
-    F.lapse_inv = s[SF_LI * 32]; F.om_lapse = s[SF_OL * 32]; F.sDS = s[SF_SDS * 32]; F.misS = s[SF_MIS * 32]; F.ivarpi = s[SF_IVP * 32];
-    F.r = s[SF_R * 32]; F.sth = s[SF_STH * 32]; F.cth = s[SF_CTH * 32]; F.a = a;
+    F.pu[0] = s[SF_PU0 * NT]; F.pu[1] = s[SF_PU1 * NT]; F.pu[2] = s[SF_PU2 * NT]; F.pu[3] = s[SF_PU3 * NT];
+    F.pz[0] = s[SF_PZ0 * NT]; F.pz[1] = s[SF_PZ1 * NT]; F.pz[2] = s[SF_PZ2 * NT]; F.pz[3] = s[SF_PZ3 * NT];
+    F.lapse_inv = s[SF_LI * NT]; F.om_lapse = s[SF_OL * NT]; F.sDS = s[SF_SDS * NT]; F.misS = s[SF_MIS * NT]; F.ivarpi = s[SF_IVP * NT];
+    F.r = s[SF_R * NT]; F.sth = s[SF_STH * NT]; F.cth = s[SF_CTH * NT]; F.a = a;
     float gl[GR_COUNT];
 #pragma unroll
     for (int r = 0; r < GR_COUNT; ++r) gl[r] = 0.f;
-    element_adjoint<float, CH>(p, gt, F, s[SF_X * 32], s[SF_Y * 32], s[SF_Z * 32], t_obs - s[SF_T * 32], s[SF_ALPHA * 32], s[SF_BETA * 32],
-                               a_sin_tho, nu, nc, act, cb, 11 * 32, 32, gl);
+    element_adjoint<float, CH>(p, gt, F, s[SF_X * NT], s[SF_Y * NT], s[SF_Z * NT], t_obs - s[SF_T * NT], s[SF_ALPHA * NT], s[SF_BETA * NT],
+                               a_sin_tho, nu, nc, act, cb, 11 * NT, NT, gl);
 #pragma unroll
     for (int r = 0; r < GR_COUNT; ++r) g[r] = gl[r];
 }
@@ -661,10 +661,12 @@ struct AdjSmem {
     static constexpr int kTwBytes = 32 * CH * 8 * 4;
     static constexpr int kMetaBytes = 32 * 4 * 2;
     static constexpr int kStepWarp = kTwBytes + kMetaBytes;
-    // element phase: sample data, pair list, c-bar per lane and frequency, the rows of each evaluated
-    // pair, then the warp's gradient accumulator [splat][21]
+    // element phase, per-warp shares of the block's regions: sample data, pair list (4 B items), c-bar
+    // per thread and frequency, the rows of each evaluated pair (or a group's pass masks), meta (active
+    // bits, scan sums), candidate masks; then the warps' gradient accumulators [splat][21]
     static constexpr int kSampleBytes = 32 * kSF * 4;
     static constexpr int kItemBytes = 32 * 32 * 2;
+    static_assert(kGroupWords * 32 * 4 <= 32 * GR_COUNT * 4, "a group's pass masks fit in the pair-rows buffer");
     static constexpr int kCbBytes = 32 * CH * 11 * 4;
     static constexpr int kGitemBytes = 32 * GR_COUNT * 4;
     static constexpr int kCandBytes = kMaxSplatWords * 4;
@@ -827,10 +829,13 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
     }
 }
 
-// The element phase: every work unit visits its samples (in order); the lanes with an active sample
-// test the splats against the support, the passing (lane, splat) pairs are evaluated 32 at a time
-// with the sample's c-bar (read back from gstate), and their 21 rows are summed per splat in list
-// order into the warp's accumulator; the unit writes its partial sums to gunit.
+// The element phase: every block work unit visits its samples (in order, all threads together); the
+// threads with an active sample test the splats against the support, the passing (thread, splat)
+// pairs of up to kGroupWords candidate words go into one block list and are evaluated NT at a time
+// with the sample's c-bar (read back from gstate), and every warp sums the 21 rows of its own
+// threads' pairs per splat, in list order, into its accumulator (the same pairs in the same order as
+// a warp-private list: the per-unit partial sums do not depend on the pooling); each warp unit writes
+// its partial sums to gunit.
 template <int CH, int NT>
 __global__ void __launch_bounds__(NT, 1)
 k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
@@ -838,26 +843,33 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
                const float* __restrict__ gstate, const unsigned char* __restrict__ gact, unsigned long long* __restrict__ work,
                float* __restrict__ gunit, int global_acc) {
     extern __shared__ __align__(16) unsigned char smem[];
+    using AS = AdjSmem<CH>;
+    constexpr int W = NT / 32;
     float* tab = reinterpret_cast<float*>(smem);
     for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wb = smem + AdjSmem<CH>::tab_bytes(ntot) + size_t(warp) * AdjSmem<CH>::warp_bytes(ntot, global_acc != 0);
-    float* sf = reinterpret_cast<float*>(wb);
-    uint16_t* items = reinterpret_cast<uint16_t*>(wb + AdjSmem<CH>::kSampleBytes);
-    float* cbs = reinterpret_cast<float*>(wb + AdjSmem<CH>::kSampleBytes + AdjSmem<CH>::kItemBytes);
-    float* gitem = cbs + 32 * CH * 11;                  // [item][21]
-    unsigned* meta_bits = reinterpret_cast<unsigned*>(gitem + 32 * GR_COUNT);
-    unsigned* cand = meta_bits + 64;                    // the unit's candidate splats
-    float* gacc_smem = reinterpret_cast<float*>(wb + AdjSmem<CH>::kFixed);   // [splat][21]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // the block's regions (each the sum of the warps' shares), then the warps' accumulators
+    unsigned char* bb = smem + AS::tab_bytes(ntot);
+    float* sf = reinterpret_cast<float*>(bb);                                            // [kSF][NT]
+    unsigned* items = reinterpret_cast<unsigned*>(bb + W * AS::kSampleBytes);           // owner << 9 | splat
+    float* cbs = reinterpret_cast<float*>(bb + W * (AS::kSampleBytes + AS::kItemBytes)); // [CH][11][NT]
+    float* gitem = cbs + NT * CH * 11;                                                  // [item][21] | pass masks
+    unsigned* meta_bits = reinterpret_cast<unsigned*>(gitem + NT * GR_COUNT);           // [NT]
+    int* wsum = reinterpret_cast<int*>(meta_bits + NT);                                 // [2][W]
+    unsigned* cand = reinterpret_cast<unsigned*>(reinterpret_cast<unsigned char*>(meta_bits) + W * AS::kMetaBytes) +
+                     warp * kMaxSplatWords;                                             // this warp's candidates
+    float* gacc_smem = reinterpret_cast<float*>(bb + W * AS::kFixed + size_t(warp) * AS::acc_bytes(ntot));   // [splat][21]
+    const int item_cap = W * AS::kItemBytes / 4;
     __syncthreads();
     const unsigned full = 0xffffffffu;
     const int N = st.N;
     const long long npad = job.npad;
     const float a = float(st.a), a_sin_tho = float(st.a * sin(st.thetao));
     const long long gsz = (long long)ntot * GR_COUNT;
-    // block work units, one barrier per sample (the phase alignment of k_consume)
+    const int nw = (ntot + 31) >> 5;
+    int scan_par = 0;
+    // block work units (the phase alignment of k_consume)
     __shared__ unsigned long long s_unit;
-    constexpr int W = NT / 32;
     const long long btotal = (job.nchunks + W - 1) / W * job.nseg * job.nframes * job.nvc;
     for (;;) {
         __syncthreads();
@@ -893,7 +905,6 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
             b.zlo = warp_min(b.zlo); b.zhi = warp_max(b.zhi); b.rlo = warp_min(b.rlo); b.rhi = warp_max(b.rhi);
             unit_candidates(tab, ntot, b, lane, cand);
         }
-        __syncwarp();
         for (int k = U.k0; k < U.k1; ++k) {
             const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
             const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
@@ -906,96 +917,108 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
                     if (gact[(combo * N + (k - 1)) * npad + U.j]) actbits |= 1u << c;
                 }
             }
-            if (__ballot_sync(full, actbits != 0u) == 0u) { __syncthreads(); continue; }
+            // the sample is skipped by the whole block when no thread has an active step (a barrier)
+            if (!__syncthreads_or(actbits != 0u)) continue;
             float x = 0.f, yy = 0.f, z = 0.f, ts = 0.f, rho = 0.f;
             if (actbits) {
                 x = sp[SM_X * npad]; yy = sp[SM_Y * npad]; z = sp[SM_Z * npad]; ts = sp[SM_T * npad];
                 const float r = sp[SM_R * npad], sth = sp[SM_STH * npad], cth = sp[SM_CTH * npad];
                 rho = sqrtf(x * x + yy * yy);
                 SampleFrame<float> F = sample_frame(a, r, 0.f, sth, cth, eta, lam, (flags & 2u) != 0u, (flags & 4u) != 0u);
-                float* mys = sf + lane;
-                mys[SF_X * 32] = x; mys[SF_Y * 32] = yy; mys[SF_Z * 32] = z; mys[SF_T * 32] = ts;
-                mys[SF_PU0 * 32] = F.pu[0]; mys[SF_PU1 * 32] = F.pu[1]; mys[SF_PU2 * 32] = F.pu[2]; mys[SF_PU3 * 32] = F.pu[3];
-                mys[SF_PZ0 * 32] = F.pz[0]; mys[SF_PZ1 * 32] = F.pz[1]; mys[SF_PZ2 * 32] = F.pz[2]; mys[SF_PZ3 * 32] = F.pz[3];
-                mys[SF_LI * 32] = F.lapse_inv; mys[SF_OL * 32] = F.om_lapse; mys[SF_SDS * 32] = F.sDS; mys[SF_MIS * 32] = F.misS;
-                mys[SF_IVP * 32] = F.ivarpi;
-                mys[SF_R * 32] = r; mys[SF_STH * 32] = sth; mys[SF_CTH * 32] = cth;
-                mys[SF_SG * 32] = (r * r + a * a * cth * cth) * dtau;
-                mys[SF_ALPHA * 32] = alpha; mys[SF_BETA * 32] = beta;
+                float* mys = sf + tid;
+                mys[SF_X * NT] = x; mys[SF_Y * NT] = yy; mys[SF_Z * NT] = z; mys[SF_T * NT] = ts;
+                mys[SF_PU0 * NT] = F.pu[0]; mys[SF_PU1 * NT] = F.pu[1]; mys[SF_PU2 * NT] = F.pu[2]; mys[SF_PU3 * NT] = F.pu[3];
+                mys[SF_PZ0 * NT] = F.pz[0]; mys[SF_PZ1 * NT] = F.pz[1]; mys[SF_PZ2 * NT] = F.pz[2]; mys[SF_PZ3 * NT] = F.pz[3];
+                mys[SF_LI * NT] = F.lapse_inv; mys[SF_OL * NT] = F.om_lapse; mys[SF_SDS * NT] = F.sDS; mys[SF_MIS * NT] = F.misS;
+                mys[SF_IVP * NT] = F.ivarpi;
+                mys[SF_R * NT] = r; mys[SF_STH * NT] = sth; mys[SF_CTH * NT] = cth;
+                mys[SF_SG * NT] = (r * r + a * a * cth * cth) * dtau;
+                mys[SF_ALPHA * NT] = alpha; mys[SF_BETA * NT] = beta;
 #pragma unroll
                 for (int c = 0; c < CH; ++c) {
                     if (!((actbits >> c) & 1u)) continue;
                     const long long combo = (long long)(U.v0 + c) * job.nframes + U.f;
                     const float* gs = gstate + ((combo * N + (k - 1)) * 27 + 16) * npad + U.j;
 #pragma unroll
-                    for (int q = 0; q < 11; ++q) cbs[(c * 11 + q) * 32 + lane] = gs[q * npad];
+                    for (int q = 0; q < 11; ++q) cbs[(c * 11 + q) * NT + tid] = gs[q * npad];
                 }
             }
-            meta_bits[lane] = actbits;
-            __syncwarp();
+            meta_bits[tid] = actbits;
             const float t = t_obs - ts;
-            for (int s0 = 0; s0 < ntot; s0 += 32) {
-                const unsigned cm = cand[s0 >> 5];
-                if (cm == 0u) continue;
-                unsigned mask = 0u;
-                if (actbits) {
-                    unsigned cb2 = cm;
-                    while (cb2) {
-                        const int b = __ffs(cb2) - 1;
-                        cb2 &= cb2 - 1;
-                        const float* p = tab + (s0 + b) * ST_COUNT;
-                        const float dr = rho - p[ST_RHO], dz = z - p[ST_CZ];
-                        if (dr * dr + dz * dz > p[ST_SUPP]) continue;
-                        float q;
-                        if (!splat_exponent(p, t, x, yy, z, true, q)) continue;
-                        if (q < kQCUT) mask |= 1u << b;
-                    }
-                }
-                const int n = __popc(mask);
-                int incl = n;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    int v = __shfl_up_sync(full, incl, d);
-                    if (lane >= d) incl += v;
-                }
-                const int off = incl - n;
-                const int total = __shfl_sync(full, incl, 31);
-                if (total == 0) continue;
-                {
-                    unsigned m = mask;
-                    int kk = off;
-                    while (m) {
-                        const int b = __ffs(m) - 1;
-                        m &= m - 1;
-                        items[kk++] = uint16_t((lane << 5) | b);
-                    }
-                }
-                __syncwarp();
-                for (int base = 0; base < total; base += 32) {
-                    const int kk = base + lane;
-                    float g[GR_COUNT];
-#pragma unroll
-                    for (int r = 0; r < GR_COUNT; ++r) g[r] = 0.f;
-                    if (kk < total) {
-                        const int it = items[kk];
-                        const int o = it >> 5, i = s0 + (it & 31);
-                        element_adjoint_ool<CH>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, sf + o, t_obs, a, a_sin_tho, nu, U.nc,
-                                                meta_bits[o], cbs + o, g);
-                    }
-#pragma unroll
-                    for (int r = 0; r < GR_COUNT; ++r) gitem[lane * GR_COUNT + r] = g[r];
-                    __syncwarp();
-                    if (lane < GR_COUNT) {
-                        const int m = min(32, total - base);
-                        for (int q = 0; q < m; ++q) {
-                            const int i = s0 + (items[base + q] & 31);
-                            gacc[i * GR_COUNT + lane] += gitem[q * GR_COUNT + lane];
+            unsigned* gmask = reinterpret_cast<unsigned*>(gitem) + tid;   // [kGroupWords][NT]
+            int single_end = -1;
+            for (int g0 = 0; g0 < nw;) {
+                const bool single = g0 < single_end;
+                const int g1 = single ? g0 + 1 : min(nw, g0 + kGroupWords);
+                int n = 0;
+                unsigned m1 = 0u;
+                for (int wd = g0; wd < g1; ++wd) {
+                    const unsigned cm = cand[wd];
+                    unsigned mask = 0u;
+                    if (actbits && cm) {
+                        unsigned cb2 = cm;
+                        while (cb2) {
+                            const int b = __ffs(cb2) - 1;
+                            cb2 &= cb2 - 1;
+                            const float* p = tab + (wd * 32 + b) * ST_COUNT;
+                            const float dr = rho - p[ST_RHO], dz = z - p[ST_CZ];
+                            if (dr * dr + dz * dz > p[ST_SUPP]) continue;
+                            float q;
+                            if (!splat_exponent(p, t, x, yy, z, true, q)) continue;
+                            if (q < kQCUT) mask |= 1u << b;
                         }
                     }
-                    __syncwarp();
+                    if (single) m1 = mask;
+                    else gmask[(wd - g0) * NT] = mask;
+                    n += __popc(mask);
                 }
+                int total;
+                const int off = block_exscan<NT>(n, total, wsum, scan_par);
+                if (!single && total > item_cap) { single_end = g1; continue; }
+                // this warp's pairs: [wlo, whi) of the list (its threads' ranges are consecutive)
+                const int wlo = __shfl_sync(full, off, 0), whi = __shfl_sync(full, off + n, 31);
+                for (int wb = 0; wb < total; wb += item_cap) {
+                    if (n > 0 && off + n > wb && off < wb + item_cap) {
+                        int kk = off;
+                        for (int wd = g0; wd < g1; ++wd) {
+                            unsigned m = single ? m1 : gmask[(wd - g0) * NT];
+                            while (m) {
+                                const int b = __ffs(m) - 1;
+                                m &= m - 1;
+                                if (kk >= wb && kk < wb + item_cap) items[kk - wb] = (unsigned(tid) << 9) | unsigned(wd * 32 + b);
+                                ++kk;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                    const int wt = min(item_cap, total - wb);
+                    for (int base = 0; base < wt; base += NT) {
+                        const int kk0 = base + tid;
+                        float g[GR_COUNT];
+#pragma unroll
+                        for (int r = 0; r < GR_COUNT; ++r) g[r] = 0.f;
+                        if (kk0 < wt) {
+                            const unsigned it = items[kk0];
+                            const int o = int(it >> 9), i = int(it & 511u);
+                            element_adjoint_ool<CH, NT>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, sf + o, t_obs, a, a_sin_tho, nu, U.nc,
+                                                        meta_bits[o], cbs + o, g);
+                        }
+#pragma unroll
+                        for (int r = 0; r < GR_COUNT; ++r) gitem[tid * GR_COUNT + r] = g[r];
+                        __syncthreads();
+                        // this warp's pairs of the round, per splat in list order
+                        const int lo = max(wlo, wb + base), hi = min(whi, wb + base + NT);
+                        if (lane < GR_COUNT) {
+                            for (int q = lo; q < hi; ++q) {
+                                const int i = int(items[q - wb] & 511u);
+                                gacc[i * GR_COUNT + lane] += gitem[(q - wb - base) * GR_COUNT + lane];
+                            }
+                        }
+                        __syncthreads();
+                    }
+                }
+                g0 = g1;
             }
-            __syncthreads();
         }
         if (!global_acc && !U.dead) {
             float* gu = gunit + U.ur * gsz;

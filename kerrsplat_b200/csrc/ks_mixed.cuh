@@ -72,6 +72,35 @@ __device__ __forceinline__ void unit_candidates(const float* tab, int ntot, cons
     __syncwarp();
 }
 
+// Exclusive scan of v over the NT threads of a block, total = the block sum. One barrier: the warp
+// sums alternate between the two halves of ws2 ([2][NT / 32], `par` toggles on every call, the same
+// sequence in every thread), so a scan never overwrites sums a slower warp of the previous scan is
+// still reading.
+template <int NT>
+__device__ __forceinline__ int block_exscan(int v, int& total, int* ws2, int& par) {
+    constexpr int W = NT / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int* ws = ws2 + par * W;
+    par ^= 1;
+    int incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += u;
+    }
+    if (lane == 31) ws[warp] = incl;
+    __syncthreads();
+    int pre = 0, tot = 0;
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        const int sv = ws[q];
+        pre += (q < warp) ? sv : 0;
+        tot += sv;
+    }
+    total = tot;
+    return pre + incl - v;
+}
+
 template <int CH>
 struct MixedSmem {
     // per-warp shares of the block's regions (the splat table comes first); the block pools them:
@@ -215,30 +244,7 @@ struct MixedSink {
         return wn <= nmax;
     }
 
-    // Exclusive block scan of v (one barrier; the warp sums alternate between two buffers, so the
-    // next scan does not overwrite sums a slower warp is still reading); total = the block sum.
-    __device__ int scan(int v, int& total) {
-        const int lane = tid & 31, warp = tid >> 5;
-        int* ws = wsum + scan_par * W;
-        scan_par ^= 1;
-        int incl = v;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, incl, d);
-            if (lane >= d) incl += u;
-        }
-        if (lane == 31) ws[warp] = incl;
-        __syncthreads();
-        int pre = 0, tot = 0;
-#pragma unroll
-        for (int q = 0; q < W; ++q) {
-            const int sv = ws[q];
-            pre += (q < warp) ? sv : 0;
-            tot += sv;
-        }
-        total = tot;
-        return pre + incl - v;
-    }
+    __device__ int scan(int v, int& total) { return block_exscan<NT>(v, total, wsum, scan_par); }
 
     // pair (owner o, splat i): weight, frame, coefficients at every frequency -> res slot
     __device__ void evaluate(int o, int i, float* out) {
