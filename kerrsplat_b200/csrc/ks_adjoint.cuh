@@ -657,10 +657,12 @@ __global__ void k_adj_bounds(MixedJob job, const double* __restrict__ cnu, const
 // The per-lane state of the step phase (T and w per frequency) and of the element phase.
 template <int CH>
 struct AdjSmem {
-    // step phase: T (4) and w (4) per lane and frequency, meta
+    // step phase, per-warp shares of the block's regions: T (4) and w (4) per thread and frequency;
+    // step offsets, active bits, Sigma dtau per thread, scan sums
     static constexpr int kTwBytes = 32 * CH * 8 * 4;
     static constexpr int kMetaBytes = 32 * 4 * 2;
-    static constexpr int kStepWarp = kTwBytes + kMetaBytes;
+    static constexpr int kStepMetaBytes = 32 * 4 * 3 + 2 * 4;
+    static constexpr int kStepWarp = kTwBytes + kStepMetaBytes;
     // element phase, per-warp shares of the block's regions: sample data, pair list (4 B items), c-bar
     // per thread and frequency, the rows of each evaluated pair (or a group's pass masks), meta (active
     // bits, scan sums), candidate masks; then the warps' gradient accumulators [splat][21]
@@ -715,28 +717,30 @@ __device__ __forceinline__ AdjUnit adj_block_unit(const MixedJob& job, long long
     return U;
 }
 
-// The step phase: every work unit walks its segment from the last sample to the first, carrying T
-// per (lane, frequency); the (lane, frequency) pairs with an active sample are spread over the warp,
-// each computes w_k = P_k^T w_s and the step adjoint, writes c-bar over the stored coefficients
-// (fields 16..26 of its gstate row) and advances T <- E + O T.
+// The step phase: every block work unit walks its segment from the last sample to the first (all
+// threads together), carrying T per (thread, frequency); the (thread, frequency) pairs with an active
+// sample are spread over the block, each computes w_k = P_k^T w_s and the step adjoint, writes c-bar
+// over the stored coefficients (fields 16..26 of its gstate row) and advances T <- E + O T.
 template <int CH, int NT>
 __global__ void __launch_bounds__(NT)
 k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const double* __restrict__ plan_f, const float* __restrict__ stream,
             float* __restrict__ gstate, const unsigned char* __restrict__ gact, const float* __restrict__ bnd,
             unsigned long long* __restrict__ work) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wb = smem + size_t(warp) * AdjSmem<CH>::kStepWarp;
-    float* tw = reinterpret_cast<float*>(wb);                        // [c][8][32]: w 0..3, T 4..7
-    int* meta_off = reinterpret_cast<int*>(wb + AdjSmem<CH>::kTwBytes);
-    unsigned* meta_bits = reinterpret_cast<unsigned*>(meta_off + 32);
-    const unsigned full = 0xffffffffu;
+    using AS = AdjSmem<CH>;
+    constexpr int W = NT / 32;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float* tw = reinterpret_cast<float*>(smem);                              // [c][8][NT]: w 0..3, T 4..7
+    int* meta_off = reinterpret_cast<int*>(smem + W * AS::kTwBytes);         // [NT]
+    unsigned* meta_bits = reinterpret_cast<unsigned*>(meta_off + NT);        // [NT]
+    float* sgd_s = reinterpret_cast<float*>(meta_bits + NT);                 // [NT]: Sigma dtau of each thread's sample
+    int* wsum = reinterpret_cast<int*>(sgd_s + NT);                          // [2][W]
+    int scan_par = 0;
     const int N = st.N;
     const long long npad = job.npad, npix = job.npix;
     const float a = float(st.a);
-    // block work units, one barrier per sample (the phase alignment of k_consume)
+    // block work units (the phase alignment of k_consume)
     __shared__ unsigned long long s_unit;
-    constexpr int W = NT / 32;
     const long long btotal = (job.nchunks + W - 1) / W * job.nseg * job.nframes * job.nvc;
     for (;;) {
         __syncthreads();
@@ -745,6 +749,7 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
         const unsigned long long u = s_unit;
         if (u >= (unsigned long long)btotal) break;
         const AdjUnit U = adj_block_unit<CH>(job, btotal, u, warp, W, lane, N);
+        const long long jb = U.jbase - warp * 32;   // the block's first ray: thread o owns ray jb + o
         float Lnu[CH];
 #pragma unroll
         for (int c = 0; c < CH; ++c) Lnu[c] = float(job.L / (cnu[min(U.v0 + c, job.nfreq - 1)] / kNU0));
@@ -754,9 +759,8 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
             const long long combo = (long long)min(U.v0 + c, job.nfreq - 1) * job.nframes + U.f;
             const float* b = bnd + (combo * job.nseg + U.seg) * 8 * npix + U.j;
 #pragma unroll
-            for (int q = 0; q < 8; ++q) tw[(c * 8 + q) * 32 + lane] = (U.live && c < U.nc) ? b[(long long)q * npix] : 0.f;
+            for (int q = 0; q < 8; ++q) tw[(c * 8 + q) * NT + tid] = (U.live && c < U.nc) ? b[(long long)q * npix] : 0.f;
         }
-        __syncwarp();
         for (int k = U.k1 - 1; k >= U.k0; --k) {
             const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
             unsigned actbits = 0u;
@@ -769,62 +773,56 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
                 }
             }
             const int n2 = __popc(actbits);
-            int incl2 = n2;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                int v = __shfl_up_sync(full, incl2, d);
-                if (lane >= d) incl2 += v;
+            int total2;
+            const int off2 = block_exscan<NT>(n2, total2, wsum, scan_par);   // a barrier: the last sample's steps are done
+            if (total2 == 0) continue;
+            if (actbits) {
+                // Sigma dtau of this thread's sample, for the worker that takes its steps
+                const float rr = sp[SM_R * npad], cth = sp[SM_CTH * npad];
+                sgd_s[tid] = (rr * rr + a * a * cth * cth) * dtau_o;
             }
-            const int total2 = __shfl_sync(full, incl2, 31);
-            if (total2 == 0) { __syncthreads(); continue; }
-            // Sigma dtau of this lane's sample, for the worker that takes its steps
-            const float rr = sp[SM_R * npad], cth = sp[SM_CTH * npad];
-            const float sgd = (rr * rr + a * a * cth * cth) * dtau_o;
-            meta_off[lane] = incl2 - n2;
-            meta_bits[lane] = actbits;
-            __syncwarp();
-            for (int base = 0; base < total2; base += 32) {
-                const int g = base + lane;
-                int o = 0;
+            meta_off[tid] = off2;
+            meta_bits[tid] = actbits;
+            __syncthreads();
+            for (int base = 0; base < total2; base += NT) {
+                const int g = base + tid;
                 if (g < total2) {
+                    // owner: the last thread whose first item is <= g (offsets are non-decreasing)
+                    int o = 0;
 #pragma unroll
-                    for (int d = 16; d >= 1; d >>= 1)
-                        if (o + d < 32 && meta_off[o + d] <= g) o += d;
-                }
-                const float sg_o = __shfl_sync(full, sgd, o);
-                if (g < total2) {
+                    for (int d = 256; d >= 1; d >>= 1)
+                        if (o + d < NT && meta_off[o + d] <= g) o += d;
                     unsigned bits = meta_bits[o];
                     const int jj = g - meta_off[o];
                     for (int q = 0; q < jj; ++q) bits &= bits - 1;
                     const int c = __ffs(bits) - 1;
                     const long long combo = (long long)(U.v0 + c) * job.nframes + U.f;
-                    float* gs = gstate + ((combo * N + (k - 1)) * 27) * npad + U.jbase + o;
+                    float* gs = gstate + ((combo * N + (k - 1)) * 27) * npad + jb + o;
                     float Pm[16], in[11];
 #pragma unroll
                     for (int q = 0; q < 16; ++q) Pm[q] = gs[q * npad];
 #pragma unroll
                     for (int q = 0; q < 11; ++q) in[q] = gs[(16 + q) * npad];
-                    float* twc = tw + c * 8 * 32 + o;
+                    float* twc = tw + c * 8 * NT + o;
                     float wk[4], R[4];
 #pragma unroll
                     for (int s4 = 0; s4 < 4; ++s4)
-                        wk[s4] = Pm[s4] * twc[0] + Pm[4 + s4] * twc[32] + Pm[8 + s4] * twc[64] + Pm[12 + s4] * twc[96];
+                        wk[s4] = Pm[s4] * twc[0] + Pm[4 + s4] * twc[NT] + Pm[8 + s4] * twc[2 * NT] + Pm[12 + s4] * twc[3 * NT];
 #pragma unroll
-                    for (int s4 = 0; s4 < 4; ++s4) R[s4] = twc[(4 + s4) * 32];
+                    for (int s4 = 0; s4 < 4; ++s4) R[s4] = twc[(4 + s4) * NT];
                     float Lc = Lnu[0];
 #pragma unroll
                     for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;
                     float O[16], E[4], cb[11];
-                    sample_adjoint_structured(c_moments, in, Lc * sg_o, wk, R, O, E, cb);
+                    sample_adjoint_structured(c_moments, in, Lc * sgd_s[o], wk, R, O, E, cb);
 #pragma unroll
                     for (int q = 0; q < 11; ++q) gs[(16 + q) * npad] = cb[q];
+                    // (owner, frequency) pairs are distinct within a sample: no other worker touches this column
 #pragma unroll
                     for (int r = 0; r < 4; ++r)
-                        twc[(4 + r) * 32] = E[r] + O[4 * r] * R[0] + O[4 * r + 1] * R[1] + O[4 * r + 2] * R[2] + O[4 * r + 3] * R[3];
+                        twc[(4 + r) * NT] = E[r] + O[4 * r] * R[0] + O[4 * r + 1] * R[1] + O[4 * r + 2] * R[2] + O[4 * r + 3] * R[3];
                 }
             }
-            __syncwarp();
-            __syncthreads();
         }
     }
 }
