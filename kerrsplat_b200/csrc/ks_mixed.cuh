@@ -513,9 +513,11 @@ struct StreamSink {
     }
 };
 
-// One thread per (ray, segment of seg_len samples starting at an anchor multiple).
+// One thread per (ray, segment of seg_len samples starting at an anchor multiple). At most 128
+// registers (four blocks per SM): the FP64 march held 252 and ran 8 warps per SM; capped, 16 warps
+// per SM hide more of the FP64 latency (4% of the configuration-2 render, same stream).
 template <class T>
-__global__ void __launch_bounds__(128) k_stream(PlanView P, Spacetime st, long long npix, int seg_len, int nseg, float* __restrict__ out) {
+__global__ void __launch_bounds__(128, 4) k_stream(PlanView P, Spacetime st, long long npix, int seg_len, int nseg, float* __restrict__ out) {
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= npix * nseg) return;
     const long long j = q % npix;
