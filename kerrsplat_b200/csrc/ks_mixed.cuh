@@ -159,13 +159,20 @@ __device__ __noinline__ void screen_coefficients_ool(int kind, const float* p, f
     r[11 * NT] = 1.f;
 }
 
-__device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float* O, float* E) {
+// The exact step of one (owner, frequency): reads the owner's summed coefficients from shared memory
+// (11 values NT apart) and writes O (16) and E (4) to shared memory (NT apart): no arrays cross the
+// call (passed through the stack they cost a local store per element, most of them L1 misses).
+template <int NT>
+__device__ __noinline__ void transfer_step_ool(const float* in, float Dl, float* out) {
+    float v[11];
+#pragma unroll
+    for (int q = 0; q < 11; ++q) v[q] = in[q * NT];
     float o[16], e[4];
-    transfer_step_structured(c_moments, in, in + 4, in + 8, Dl, o, e);
+    transfer_step_structured(c_moments, v, v + 4, v + 8, Dl, o, e);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) O[q] = o[q];
+    for (int q = 0; q < 16; ++q) out[q * NT] = o[q];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) E[q] = e[q];
+    for (int q = 0; q < 4; ++q) out[(16 + q) * NT] = e[q];
 }
 
 // The consumer of one thread (one ray) of a block work unit: all NT threads of the block call
@@ -423,25 +430,18 @@ struct MixedSink {
                 const int j = g - meta_off[o];
                 for (int q = 0; q < j; ++q) bits &= bits - 1;
                 const int c = __ffs(bits) - 1;
-                float in[11];
-#pragma unroll
-                for (int q = 0; q < 11; ++q) in[q] = res[(c * 12 + q) * NT + o];
+                const float* in = res + (c * 12) * NT + o;   // the owner's sums, NT apart
                 float Lc = Lnu[0];
 #pragma unroll
                 for (int cc = 1; cc < CH; ++cc) Lc = (cc == c) ? Lnu[cc] : Lc;   // no dynamic register indexing
                 const float Dl = Lc * sf[SF_SG * NT + o];   // the owner's Sigma dtau
-                float O[16], E[4];
-                transfer_step_ool(in, Dl, O, E);
+                transfer_step_ool<NT>(in, Dl, sres + tid);
                 if (gstate) {
                     const long long combo = (long long)(gv0 + c) * gframes + gf;
                     float* gs = gstate + ((combo * gN + (kcur - 1)) * 27 + 16) * gnpad + jbase + o;
 #pragma unroll
-                    for (int q = 0; q < 11; ++q) gs[q * gnpad] = in[q];
+                    for (int q = 0; q < 11; ++q) gs[q * gnpad] = in[q * NT];
                 }
-#pragma unroll
-                for (int q = 0; q < 16; ++q) sres[q * NT + tid] = O[q];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) sres[(16 + q) * NT + tid] = E[q];
             }
             __syncthreads();
             // owners compose their steps front to back (frequency order)
