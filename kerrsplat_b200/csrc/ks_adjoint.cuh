@@ -605,7 +605,8 @@ namespace {
 using namespace ks;
 
 // s: the owner's column of the block's sample data ([field][NT]); cb: the owner's c-bar column of
-// [CH][11][NT]; nu: the unit's frequencies
+// [CH][11][NT]; nu: the unit's frequencies; g: the pair's 21 rows. All four in shared memory: an
+// array whose address crosses the call would live on the stack.
 template <int CH, int NT>
 __device__ __noinline__ void element_adjoint_ool(const float* p, const double* gt, const float* s, float t_obs, float a, float a_sin_tho,
                                                  const float* nu, int nc, unsigned act, const float* cb, float* g) {
@@ -869,6 +870,7 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
     // block work units (the phase alignment of k_consume)
     __shared__ unsigned long long s_unit;
     const long long btotal = (job.nchunks + W - 1) / W * job.nseg * job.nframes * job.nvc;
+    __shared__ float nu[CH];   // the block unit's frequencies
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_unit = atomicAdd(work, 1ull);
@@ -877,9 +879,7 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
         if (u >= (unsigned long long)btotal) break;
         const AdjUnit U = adj_block_unit<CH>(job, btotal, u, warp, W, lane, N);
         const float t_obs = float(ct[U.f]);
-        float nu[CH];
-#pragma unroll
-        for (int c = 0; c < CH; ++c) nu[c] = float(cnu[min(U.v0 + c, job.nfreq - 1)]);
+        if (tid < CH) nu[tid] = float(cnu[min(U.v0 + tid, job.nfreq - 1)]);   // read after the next barrier
         const float dtau = float(plan_f[(long long)PF_DTAU * npad + U.j]);
         const float alpha = float(plan_f[(long long)PF_ALPHA * npad + U.j]), beta = float(plan_f[(long long)PF_BETA * npad + U.j]);
         const float eta = float(plan_f[(long long)PF_ETA * npad + U.j]), lam = float(plan_f[(long long)PF_LAM * npad + U.j]);
@@ -992,17 +992,12 @@ k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, con
                     const int wt = min(item_cap, total - wb);
                     for (int base = 0; base < wt; base += NT) {
                         const int kk0 = base + tid;
-                        float g[GR_COUNT];
-#pragma unroll
-                        for (int r = 0; r < GR_COUNT; ++r) g[r] = 0.f;
                         if (kk0 < wt) {
                             const unsigned it = items[kk0];
                             const int o = int(it >> 9), i = int(it & 511u);
                             element_adjoint_ool<CH, NT>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, sf + o, t_obs, a, a_sin_tho, nu, U.nc,
-                                                        meta_bits[o], cbs + o, g);
+                                                        meta_bits[o], cbs + o, gitem + tid * GR_COUNT);
                         }
-#pragma unroll
-                        for (int r = 0; r < GR_COUNT; ++r) gitem[tid * GR_COUNT + r] = g[r];
                         __syncthreads();
                         // this warp's pairs of the round, per splat in list order
                         const int lo = max(wlo, wb + base), hi = min(whi, wb + base + NT);

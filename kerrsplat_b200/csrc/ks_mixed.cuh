@@ -501,14 +501,33 @@ struct StreamSink {
     float* out;
     long long npad, j;
     T a, rh_lo;
+    T rp, rm;       // the horizons
+    float afac;     // a / (2 sqrt(1 - a^2))
+    // The quasi-Cartesian Kerr-Schild position of ks_coords in the precision of the stream: the sample
+    // is FP64 (T = double) but x, y, z are stored in FP32, so the angles go to FP32 trigonometry once
+    // phi_KS is reduced into [-pi, pi] in T; sin theta comes from cos theta (sqrt((1 - c)(1 + c)),
+    // as accurate as sin(acos c)); r - r_+ and r - r_- are formed in T before the FP32 logarithm.
     __device__ void operator()(int k, const Sample<T>& s) {
         float* o = out + (long long)(k - 1) * SM_COUNT * npad + j;
         const bool usable = s.ok && s.r > rh_lo;
         unsigned flags = (s.ok ? 1u : 0u) | (s.nur ? 2u : 0u) | (s.nutheta ? 4u : 0u) | (usable ? 8u : 0u);
-        T x = 0, y = 0, z = 0, sth = 0, cth = 0;
-        if (usable) ks_coords(a, s.r, s.theta, s.phi, x, y, z, sth, cth);
-        o[SM_X * npad] = float(x); o[SM_Y * npad] = float(y); o[SM_Z * npad] = float(z); o[SM_T * npad] = float(s.t);
-        o[SM_R * npad] = float(s.r); o[SM_STH * npad] = float(sth); o[SM_CTH * npad] = float(cth);
+        float x = 0.f, y = 0.f, z = 0.f, sth = 0.f, cth = 0.f;
+        if (usable) {
+            const T c = s.cos_theta;
+            const T st2 = (T(1) - c) * (T(1) + c);
+            cth = float(c);
+            sth = float(sqrt(st2 > T(0) ? st2 : T(0)));
+            const float lg = logf(fabsf(float(s.r - rp + keps<T>()) / float(s.r - rm + keps<T>())));
+            const T phks = s.phi + T(afac * lg - atan2f(float(a), float(s.r)));
+            const T turns = rint(phks * T(0.15915494309189535));   // 1 / (2 pi)
+            const float phr = float(phks - turns * T(6.283185307179586));
+            float sp, cp;
+            sincosf(phr, &sp, &cp);
+            const float r = float(s.r);
+            x = r * sth * cp; y = r * sth * sp; z = r * cth;
+        }
+        o[SM_X * npad] = x; o[SM_Y * npad] = y; o[SM_Z * npad] = z; o[SM_T * npad] = float(s.t);
+        o[SM_R * npad] = float(s.r); o[SM_STH * npad] = sth; o[SM_CTH * npad] = cth;
         o[SM_FLAGS * npad] = __uint_as_float(flags);
     }
 };
@@ -524,7 +543,8 @@ __global__ void __launch_bounds__(128, 4) k_stream(PlanView P, Spacetime st, lon
     const int seg = int(q / npix);
     const int k0 = 1 + seg * seg_len, k1 = min(st.N + 1, k0 + seg_len);
     MarchRay<T> R = load_ray<T>(P, st, j);
-    StreamSink<T> sink{out, P.npad, j, T(st.a), T(st.rh * (1 + 1e-3))};
+    const double temp = sqrt(1.0 - st.a * st.a);
+    StreamSink<T> sink{out, P.npad, j, T(st.a), T(st.rh * (1 + 1e-3)), T(1.0 + temp), T(1.0 - temp), float(st.a / (2.0 * temp))};
     march_range(P, j, R, sink, k0, k1);
 }
 

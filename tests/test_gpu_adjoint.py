@@ -376,3 +376,42 @@ def test_mixed_adjoint_large_splat_table():
     g32 = ks.adjoint(cache, m, [0.0], [230e9], c["L"], ds, precision=ks.KS_MIXED)
     print("320 splats: mixed vs fp64", rel_l2(g32, g64))
     assert np.abs(g64).max() > 0 and rel_l2(g32, g64) < 1e-3
+
+
+def _crowded_scene():
+    """480 wide splats (6 M) stacked on one spot (the FP64 plain adjoint stages at most 501): every
+    sample near it passes every splat, so a block of the mixed kernels collects 384 x 256 pairs for a
+    group of candidate words (past its pair list: the group is redone chunk by chunk) and 384 x 32 for
+    one chunk (past it again: the chunk's list goes in two windows). The second block unit of the
+    24 x 24 screen has dead warps."""
+    c = scenes.config2(res=24, N=64)
+    rng = np.random.Generator(np.random.PCG64(33))
+    p = scenes.thermal_params(rng, 480, c["a"], rlo=5.5, rhi=6.5)
+    p[0:3] = np.array([[6.0], [0.0], [0.5]]) + 0.2 * rng.standard_normal((3, 480))
+    p[3:6] = np.log(6.0)
+    p[12] = np.log(3e3)
+    cam = ks.Camera((-12.0, 12.0), (-12.0, 12.0), 24)
+    cache = ks.GeodesicCache(cam, 64)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    return c, p, cache
+
+
+def test_crowded_pair_lists():
+    """The mixed forward pass and chi^2 gradient on the crowded scene: the chunk-by-chunk and windowed
+    pair lists give the FP64 plain results (image 1e-4, chi^2 1e-3, gradient 1e-3 rel L2)."""
+    c, p, cache = _crowded_scene()
+    m = ks.PolarizedSplats(p)
+    nus = [230e9]
+    img = np.asarray(ks.render(cache, m, [0.0], nus, c["L"], precision=ks.KS_FP64))
+    mix = np.asarray(ks.render(cache, m, [0.0], nus, c["L"], precision=ks.KS_MIXED))
+    assert np.abs(img).max() > 0
+    e = rel_l2(mix, img)
+    rng = np.random.Generator(np.random.PCG64(34))
+    data = img * (1 + 0.05 * rng.standard_normal(img.shape))
+    sigma = 0.01 * np.abs(img).max()
+    chi64, g64 = ks.chi2_gradient(cache, m, [0.0], nus, c["L"], data, sigma, precision=ks.KS_FP64)
+    chi32, g32 = ks.chi2_gradient(cache, m, [0.0], nus, c["L"], data, sigma, precision=ks.KS_MIXED)
+    print("crowded: image rel L2", e, "chi2", chi64, chi32, "grad rel L2", rel_l2(g32, g64))
+    assert e < 1e-4
+    assert abs(chi32 - chi64) <= 1e-3 * chi64
+    assert rel_l2(g32, g64) < 1e-3
