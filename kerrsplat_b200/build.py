@@ -11,9 +11,14 @@ HEADERS = ["ks_elliptic.cuh", "ks_plan.cuh", "ks_march.cuh", "ks_dual.cuh", "ks_
 
 
 def nvcc_command(out=LIB, extra=()):
+    """FP32 division and square root take the hardware approximations (-prec-div=false,
+    -prec-sqrt=false: a few ulp, inside the mixed path's 1e-4 budget; the coefficient fits divide
+    often and the IEEE sequences cost them a quarter of their time). FP64 arithmetic is unaffected,
+    denormals are kept."""
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
     return [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
             "--use_fast_math" if os.environ.get("KS_FAST_MATH") else "-Xptxas=-O3",
+            "-prec-div=false", "-prec-sqrt=false",
             "-shared", "-Xcompiler", "-fPIC", "-o", out] + list(extra) + [os.path.join(CSRC, s) for s in SOURCES]
 
 

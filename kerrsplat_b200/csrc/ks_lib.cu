@@ -956,12 +956,24 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     (void)M;
 }
 
-// The frequencies of a work unit: all of them (up to four) share the march and the splat tests. (Two
-// frequencies per unit, which doubles the resident warps of a 256-splat table, measured 8% slower on
-// the movie: the tests it repeats cost more than the occupancy it gains.)
+// The most warps of k_consume<CH, *, KM> resident per SM for an ntot-splat table.
+template <int CH, int KM>
+int resident_warps(ks_context* c, int ntot) {
+    return std::max(consume_blocks<CH, 384, KM>(c, ntot) * 12, std::max(consume_blocks<CH, 256, KM>(c, ntot) * 8,
+                                                                        consume_blocks<CH, 128, KM>(c, ntot) * 4));
+}
+
+// The frequencies of a work unit: all of them (up to four) share the march and the splat tests,
+// unless the per-thread states of four frequencies and a large splat table leave room for half as
+// many warps as two frequencies per unit would: then two (every sample is tested twice, but with the
+// block-cooperative consumer occupancy pays more: the 256-splat movie ran 4 warps per SM with four).
 template <int KM>
 int launch_mixed_km(ks_context* c, int ntot, int nframes, int nfreq, double L, int nmax, double slab) {
-    if (nfreq >= 4) return launch_mixed_ch<4, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
+    if (nfreq >= 4) {
+        if (resident_warps<2, KM>(c, ntot) >= 2 * resident_warps<4, KM>(c, ntot))
+            return launch_mixed_ch<2, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
+        return launch_mixed_ch<4, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
+    }
     if (nfreq == 3) return launch_mixed_ch<3, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
     if (nfreq == 2) return launch_mixed_ch<2, KM>(c, ntot, nframes, nfreq, L, nmax, slab);
     return launch_mixed_ch<1, KM>(c, ntot, nframes, nfreq, L, nmax, slab);

@@ -108,7 +108,7 @@ struct MixedSmem {
     static constexpr int kSampleBytes = 32 * kSF * 4;
     static constexpr int kItemBytes = 32 * 20 * 4;                                              // pair list (4 B items) | step results [20][NT]
     static constexpr int kResBytes = 32 * CH * 12 * 4;                                          // pair results | step inputs | pass masks
-    static constexpr int kMetaBytes = 32 * 4 * 2 + kMaxSplatWords * 4 + 2 * 4;                   // step offsets, bits; candidate mask; scan sums
+    static constexpr int kMetaBytes = 32 * 4 * 2 + kMaxSplatWords * 4 + 2 * 4 + 4 * 4;           // step offsets, bits; candidate mask; scan sums; class counts
     static constexpr int kStateBytes = 32 * CH * 20 * 4;                                        // P (16) and S (4) per thread and frequency
     static constexpr int kWarpBytes = kSampleBytes + kItemBytes + kResBytes + kMetaBytes + kStateBytes;
     static_assert(kGroupWords * 32 * 4 <= kResBytes, "a group's pass masks fit in the pair-results buffer");
@@ -213,6 +213,8 @@ struct MixedSink {
     int* wsum;        // warp sums of the block scans, double-buffered [2][W]
     int scan_par;
     int item_cap;
+    bool sort_kinds;       // the scene mixes populations or has knot splats: evaluate each round grouped by class
+    int* kcnt;             // per-warp class counts of a round [W][4]
     const unsigned* cand;  // this warp's candidate splats (unit_candidates)
     float zprev; int wn; bool inside, crossed, zset;
     unsigned int ev[7];
@@ -252,6 +254,42 @@ struct MixedSink {
     }
 
     __device__ int scan(int v, int& total) { return block_exscan<NT>(v, total, wsum, scan_par); }
+
+    // The evaluation class of a pair: 0 thermal, 1 knot (thermal coefficients, knot centre), 2 power
+    // law, 3 kappa; 4 for a thread without a pair this round.
+    __device__ int pair_class(int kk, int wt) const {
+        if (kk >= wt) return 4;
+        const int kind = int(tab[int(items[kk] & 511u) * ST_COUNT + ST_KIND]);
+        return kind == KS_KNOT21 ? 1 : kind == KS_POWERLAW22 ? 2 : kind == KS_KAPPA22 ? 3 : 0;
+    }
+
+    // The round's pairs [base, base + NT) of the list re-dealt to the threads grouped by class (a
+    // counting sort over warp ballots; two barriers), so that a warp runs one population's fit instead
+    // of all of them in turn. The results still go to each pair's own slot, so the owners' sums keep
+    // list order. Returns the list index this thread evaluates (>= wt: none).
+    __device__ int kind_sorted(int kk0, int wt, int base) {
+        const int lane = tid & 31, warp = tid >> 5;
+        const int cls = pair_class(kk0, wt);
+        unsigned mine = 0u;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const unsigned m = __ballot_sync(0xffffffffu, cls == k);
+            if (lane == 0) kcnt[warp * 4 + k] = __popc(m);
+            if (cls == k) mine = m;
+        }
+        __syncthreads();
+        int dst = NT;   // no pair: nothing to place
+        if (cls < 4) {
+            dst = __popc(mine & ((1u << lane) - 1u));
+            for (int w = 0; w < W; ++w)
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    dst += (k < cls || (k == cls && w < warp)) ? kcnt[w * 4 + k] : 0;
+            meta_off[dst] = kk0;   // the step offsets are free during the evaluations
+        }
+        __syncthreads();
+        return (tid < min(NT, wt - base)) ? meta_off[tid] : wt;
+    }
 
     // pair (owner o, splat i): weight, frame, coefficients at every frequency -> res slot
     __device__ void evaluate(int o, int i, float* out) {
@@ -381,10 +419,11 @@ struct MixedSink {
                 // 2. evaluation rounds over the block, then owner accumulation in list order
                 const int wt = min(item_cap, total - wb);
                 for (int base = 0; base < wt; base += NT) {
-                    const int kk0 = base + tid;
+                    int kk0 = base + tid;
+                    if (sort_kinds) kk0 = kind_sorted(kk0, wt, base);
                     if (kk0 < wt) {
                         const unsigned it = items[kk0];
-                        evaluate(int(it >> 9), int(it & 511u), res + tid);
+                        evaluate(int(it >> 9), int(it & 511u), res + (kk0 - base));
                     }
                     __syncthreads();
                     const int lo = max(off, wb + base), hi = min(off + n, wb + base + NT);
@@ -585,6 +624,7 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
     unsigned* meta_bits_b = reinterpret_cast<unsigned*>(meta_off_b + NT);
     unsigned* cand_b = meta_bits_b + NT;                                   // [W][kMaxSplatWords]
     int* wsum_b = reinterpret_cast<int*>(cand_b + W * kMaxSplatWords);     // [2][W]
+    int* kcnt_b = wsum_b + 2 * W;                                          // [W][4]
     float* state_b = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(meta_off_b) + W * MS::kMetaBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned* cand = cand_b + warp * kMaxSplatWords;
@@ -652,6 +692,8 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab
         sink.wsum = wsum_b;
         sink.scan_par = 0;
         sink.item_cap = W * MS::kItemBytes / 4;
+        sink.sort_kinds = (KM != 1) || (job.nkv > 0);
+        sink.kcnt = kcnt_b;
         sink.cand = cand;
         sink.state = state_b + threadIdx.x;
         sink.init();
