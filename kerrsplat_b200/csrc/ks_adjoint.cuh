@@ -837,15 +837,21 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
 // its partial sums to gunit.
 template <int CH, int NT>
 __global__ void __launch_bounds__(NT, 1)
-k_adj_elements(Spacetime st, MixedJob job, const double* __restrict__ tab64, const double* __restrict__ gtab, int ntot,
+k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, const double* __restrict__ gtab, int ntot,
                const double* __restrict__ ct, const double* __restrict__ cnu, const double* __restrict__ plan_f, const float* __restrict__ stream,
                const float* __restrict__ gstate, const unsigned char* __restrict__ gact, unsigned long long* __restrict__ work,
-               float* __restrict__ gunit, int global_acc) {
+               float* __restrict__ gunit, int global_acc, unsigned* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem[];
     using AS = AdjSmem<CH>;
     constexpr int W = NT / 32;
     float* tab = reinterpret_cast<float*>(smem);
-    for (int q = threadIdx.x; q < ntot * ST_COUNT; q += blockDim.x) tab[q] = float(tab64[q]);
+    // the FP32 splat table into shared memory by one bulk copy (k_consume's staging)
+    __shared__ __align__(8) unsigned long long tab_bar;
+    const unsigned tab_bytes = unsigned(AS::tab_bytes(ntot));
+    if (tab_bytes > 0 && !stage_bulk(tab, tab32, tab_bytes, &tab_bar)) {
+        if (threadIdx.x == 0) atomicOr(err, 1u);
+        return;
+    }
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // the block's regions (each the sum of the warps' shares), then the warps' accumulators
     unsigned char* bb = smem + AS::tab_bytes(ntot);

@@ -235,6 +235,12 @@ __global__ void k_anchor_prefix(long long npix, long long npad, const double* __
 
 // ---- kernels: splat tables ---------------------------------------------------------------------------
 
+// the table (and knot array) in FP32 for the mixed kernels' staging copy, zero-padded to np4 floats
+__global__ void k_tab_f32(long long n, long long np4, const double* __restrict__ src, float* __restrict__ dst) {
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q < np4) dst[q] = q < n ? float(src[q]) : 0.f;
+}
+
 // K0 and K1 from K_nu(x) = int_0^inf exp(-x cosh t) cosh(nu t) dt by the trapezoidal rule.
 __host__ __device__ void besselk01(double x, double& k0, double& k1) {
     // trapezoid in t on exp(-x (cosh t - 1)) (the factor exp(-x) applied at the end); the step
@@ -673,6 +679,8 @@ struct ks_context {
     // seeds, chi^2 partials; mixed path: per-sample states, activity, segment bounds, unit partials
     DevBuf gtab, samples, kstop, tails, slots, dgrad, seeds, chi_part, chi_val, dstage;
     DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part, jvp_tab, jvp_in, jvp_out, st_buf;
+    DevBuf tab32;     // the splat table and knot array in FP32, padded to 16 bytes (the TMA staging source)
+    DevBuf errflag;   // set by a kernel whose bounded wait gave up
     bool samples_ready = false;
     int tune_nt = 0, tune_units = 0;        // the autotuner's choice for the mixed forward (0: the default)
     int nkv = 0;                            // knot values after the splat table in `tab`
@@ -858,7 +866,27 @@ int build_tables(ks_context* c, const ks_splat_set* sets, int nsets, int* ntot_o
         tmp.release();
         first += S.nsplat;
     }
+    // the FP32 copy the mixed kernels stage into shared memory (a multiple of 16 bytes)
+    {
+        const long long nv = (long long)ntot * ST_COUNT + c->nkv;
+        const long long np4 = std::max<long long>(4, (nv + 3) / 4 * 4);
+        KS_CUDA(c, c->tab32.ensure(size_t(np4) * sizeof(float)));
+        k_tab_f32<<<nblocks(np4, 256), 256, 0, c->stream>>>(nv, np4, c->tab.as<double>(), c->tab32.as<float>());
+        c->launches++;
+        KS_CUDA(c, cudaGetLastError());
+    }
     *ntot_out = ntot;
+    return KS_OK;
+}
+
+// A kernel's bounded wait that gave up (the device flag, cleared): KS_ERR_TIMEOUT.
+int check_device_flag(ks_context* c, const char* what) {
+    unsigned f = 0;
+    KS_CUDA(c, cudaMemcpy(&f, c->errflag.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (f) {
+        KS_CUDA(c, cudaMemset(c->errflag.p, 0, sizeof(unsigned)));
+        return fail(c, KS_ERR_TIMEOUT, "%s: a shared-memory staging copy did not complete", what);
+    }
     return KS_OK;
 }
 
@@ -890,8 +918,8 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
     cudaEventRecord(c->evc0, c->stream);
     k_consume<CH, NT, KM><<<unsigned(grid), NT, smem, c->stream>>>(
-        plan_view(c), c->st, job, c->tab.as<double>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
-        c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr);
+        plan_view(c), c->st, job, c->tab32.as<float>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
+        c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr, c->errflag.as<unsigned>());
     cudaEventRecord(c->evc1, c->stream);
     c->consume_timed = true;
     c->launches++;
@@ -1020,6 +1048,10 @@ int ks_context_create(int device, int flags, ks_context** out) {
     cudaEventCreate(&c->ev1);
     cudaEventCreate(&c->evc0);
     cudaEventCreate(&c->evc1);
+    if (c->errflag.ensure(sizeof(unsigned)) != cudaSuccess || cudaMemset(c->errflag.p, 0, sizeof(unsigned)) != cudaSuccess) {
+        delete c;
+        return KS_ERR_DEVICE;
+    }
     init_constants();
     if (cudaGetLastError() != cudaSuccess) { delete c; return KS_ERR_DEVICE; }
     *out = c;
@@ -1404,6 +1436,7 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
         c->consume_launches++;
         c->consume_timed = false;
     }
+    if (precision != KS_FP64) return check_device_flag(c, "ks_render");
     return KS_OK;
 }
 
@@ -1512,10 +1545,10 @@ int launch_adjoint_mixed_nt(ks_context* c, int ntot, int per_sm, const double* d
         constexpr int W = NT / 32;
         const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
         const size_t smem = AdjSmem<CH>::bytes(ntot, W, global_acc);
-        k_adj_elements<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(c->st, job, c->tab.as<double>(), c->gtab.as<double>(), ntot, dt, dn,
+        k_adj_elements<CH, NT><<<unsigned(grid), NT, smem, c->stream>>>(c->st, job, c->tab32.as<float>(), c->gtab.as<double>(), ntot, dt, dn,
                                                                        c->plan.as<double>(), c->stream_buf.as<float>(), job.gstate, job.gact,
                                                                        c->work.as<unsigned long long>() + 1, c->adj_unit.as<float>(),
-                                                                       global_acc ? 1 : 0);
+                                                                       global_acc ? 1 : 0, c->errflag.as<unsigned>());
         c->launches++;
         c->adjoint_launches++;
         KS_CUDA(c, cudaGetLastError());
@@ -1764,6 +1797,7 @@ int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->adjoint_ms += ms;
+    if (precision != KS_FP64) return check_device_flag(c, "adjoint");
     return KS_OK;
 }
 

@@ -72,6 +72,38 @@ __device__ __forceinline__ void unit_candidates(const float* tab, int ntot, cons
     __syncwarp();
 }
 
+// ---- TMA bulk staging ----------------------------------------------------------------------------
+
+constexpr int kStageWaitLimit = 1 << 22;   // mbarrier polls before a staging copy is declared lost
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return unsigned(__cvta_generic_to_shared(p)); }
+
+// Stage `bytes` (a multiple of 16; both addresses 16-byte aligned) from global memory into this CTA's
+// shared memory with one TMA bulk copy (cp.async.bulk, no multicast) completing on the mbarrier `bar`.
+// Every thread of the block calls it; thread 0 initialises the barrier and issues the copy, all
+// threads wait for the barrier's phase 0 with a bounded number of polls. Returns false (the same in
+// every thread) when the copy did not land within the limit: the caller records an error and returns.
+__device__ __forceinline__ bool stage_bulk(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    const unsigned b = smem_u32(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // the barrier, visible to the copy engine
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long state;
+        asm volatile("mbarrier.arrive.expect_tx.shared.b64 %0, [%1], %2;" : "=l"(state) : "r"(b), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(b) : "memory");
+        (void)state;
+    }
+    unsigned done = 0;
+    for (int it = 0; it < kStageWaitLimit && !done; ++it)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(b) : "memory");
+    return __syncthreads_and(done != 0) != 0;
+}
+
 // Exclusive scan of v over the NT threads of a block, total = the block sum. One barrier: the warp
 // sums alternate between the two halves of ws2 ([2][NT / 32], `par` toggles on every call, the same
 // sequence in every thread), so a scan never overwrites sums a slower warp of the previous scan is
@@ -607,12 +639,18 @@ struct MixedJob {
 
 template <int CH, int NT, int KM>
 __global__ void __launch_bounds__(NT, 1)
-k_consume(PlanView P, Spacetime st, MixedJob job, const double* __restrict__ tab64, int ntot, const double* __restrict__ ct,
+k_consume(PlanView P, Spacetime st, MixedJob job, const float* __restrict__ tab32, int ntot, const double* __restrict__ ct,
           const double* __restrict__ cnu, const float* __restrict__ stream, unsigned long long* __restrict__ work,
-          float* __restrict__ seg_out, unsigned long long* __restrict__ counters) {
+          float* __restrict__ seg_out, unsigned long long* __restrict__ counters, unsigned* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem[];
     float* tab = reinterpret_cast<float*>(smem);
-    for (int q = threadIdx.x; q < ntot * ST_COUNT + job.nkv; q += blockDim.x) tab[q] = float(tab64[q]);
+    // the FP32 splat table and knot array (padded to 16 bytes) into shared memory by one bulk copy
+    __shared__ __align__(8) unsigned long long tab_bar;
+    const unsigned tab_bytes = unsigned(MixedSmem<CH>::tab_bytes(ntot, job.nkv));
+    if (tab_bytes > 0 && !stage_bulk(tab, tab32, tab_bytes, &tab_bar)) {
+        if (threadIdx.x == 0) atomicOr(err, 1u);
+        return;
+    }
     // the block's regions after the table (each the sum of the warps' shares, MixedSmem)
     using MS = MixedSmem<CH>;
     constexpr int W = NT / 32;
