@@ -1140,6 +1140,18 @@ struct JvpSink {
         }
         S x, y, z, sth, cth;
         ks_coords(a, r, th, ph, x, y, z, sth, cth);
+        emit(x, y, z, ts, r, sth, cth, s64.nur, s64.nutheta);
+    }
+    // one sample of the FP32 stream (k_stream: position, lookback time, r, sin/cos theta, flags)
+    __device__ void stream_sample(bool usable, S x, S y, S z, S ts, S r, S sth, S cth, bool nur, bool nuth) {
+        if (!usable) return;
+        if (nmax >= 0) {
+            wind(r * cth);
+            if (wn > nmax) return;
+        }
+        emit(x, y, z, ts, r, sth, cth, nur, nuth);
+    }
+    __device__ void emit(S x, S y, S z, S ts, S r, S sth, S cth, bool nur, bool nuth) {
         const S t = t_obs - ts;
         D in[11];
         for (int q = 0; q < 11; ++q) in[q] = D(S(0));
@@ -1156,7 +1168,7 @@ struct JvpSink {
             const D G = exp(-q);
             if (!(G > S(kWEIGHT_CUTOFF))) continue;
             if (!have_frame) {
-                const SampleFrame<S> F0 = sample_frame(a, r, th, sth, cth, eta, lam, s64.nur, s64.nutheta);
+                const SampleFrame<S> F0 = sample_frame(a, r, S(0), sth, cth, eta, lam, nur, nuth);
                 for (int k = 0; k < 4; ++k) { F.pu[k] = D(F0.pu[k]); F.pz[k] = D(F0.pz[k]); }
                 F.lapse_inv = D(F0.lapse_inv); F.om_lapse = D(F0.om_lapse); F.sDS = D(F0.sDS); F.misS = D(F0.misS); F.ivarpi = D(F0.ivarpi);
                 F.r = D(F0.r); F.sth = D(F0.sth); F.cth = D(F0.cth); F.a = D(F0.a);
@@ -1182,7 +1194,7 @@ struct JvpSink {
             active = true;
         }
         if (!active) return;
-        const S Sg = r * r + a * a * cos(th) * cos(th);
+        const S Sg = r * r + a * a * cth * cth;
         D Dl(Lnu * Sg * dtau);
         if (lnL_dir >= 0) Dl.d[lnL_dir] = Dl.v;
         D O[16], E[4];
@@ -1220,6 +1232,44 @@ __global__ void __launch_bounds__(64) k_jvp(PlanView P, Spacetime st, long long 
     sink.init();
     double rt, rp;
     march(P, st, j, R, sink, rt, rp);
+    const double n3 = nh * nh * nh;
+    for (int s = 0; s < 4; ++s) {
+        img[(c * npix + j) * 4 + s] = double(sink.Sv[s].v) * n3;
+        for (int d = 0; d < K; ++d) out[(((long long)d * ncombo + c) * npix + j) * 4 + s] = double(sink.Sv[s].d[d]) * n3;
+    }
+}
+
+// The mixed J v over the FP32 sample stream of k_stream (the FP64 march rounded to FP32, the
+// Kerr-Schild position formed there: the samples k_jvp<float, K> would round its own march to) instead
+// of a march per thread; one thread per (ray, combination), outputs as k_jvp.
+template <int K>
+__global__ void __launch_bounds__(64) k_jvp_stream(PlanView P, Spacetime st, long long npix, const Dual<float, K>* __restrict__ dtab, int ntot,
+                                                   const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L, int nmax,
+                                                   double slab, const float* __restrict__ stream, double* __restrict__ img, double* __restrict__ out,
+                                                   int lnL_dir) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= npix * ncombo) return;
+    const long long j = idx % npix;
+    const int c = int(idx / npix);
+    const long long npad = P.npad;
+    JvpSink<float, K> sink;
+    sink.tab = dtab; sink.ntot = ntot;
+    sink.t_obs = float(ct[c]); sink.nu = float(cnu[c]);
+    const double nh = cnu[c] / kNU0;
+    sink.Lnu = float(L / nh);
+    sink.a = float(st.a); sink.rh_lo = float(st.rh * (1 + 1e-3)); sink.dtau = float(P.get(PF_DTAU, j));
+    sink.alpha = float(P.get(PF_ALPHA, j)); sink.beta = float(P.get(PF_BETA, j));
+    sink.eta = float(P.get(PF_ETA, j)); sink.lam = float(P.get(PF_LAM, j));
+    sink.a_sin_tho = float(st.a * sin(st.thetao)); sink.slab = float(slab); sink.nmax = nmax;
+    sink.lnL_dir = lnL_dir;
+    sink.init();
+    const int Nj = int(P.get(PF_NSAMP, j));
+    const float* sp = stream + j;
+    for (int k = 1; k <= Nj; ++k, sp += SM_COUNT * npad) {
+        const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
+        sink.stream_sample((flags & 8u) != 0u, sp[SM_X * npad], sp[SM_Y * npad], sp[SM_Z * npad], sp[SM_T * npad], sp[SM_R * npad],
+                           sp[SM_STH * npad], sp[SM_CTH * npad], (flags & 2u) != 0u, (flags & 4u) != 0u);
+    }
     const double n3 = nh * nh * nh;
     for (int s = 0; s < 4; ++s) {
         img[(c * npix + j) * 4 + s] = double(sink.Sv[s].v) * n3;

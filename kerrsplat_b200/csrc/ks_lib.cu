@@ -890,6 +890,21 @@ int check_device_flag(ks_context* c, const char* what) {
     return KS_OK;
 }
 
+// The FP32 sample stream of every ray (k_stream; FP64 march unless c->geo64 is off), [k][field][npad].
+int launch_stream(ks_context* c) {
+    const int M = c->st.M, N = c->st.N;
+    const int sseg = std::max(M, (N / 4 + M - 1) / M * M);
+    const int nsseg = (N + sseg - 1) / sseg;
+    KS_CUDA(c, c->stream_buf.ensure(size_t(N) * SM_COUNT * c->npad * sizeof(float)));
+    if (c->geo64)
+        k_stream<double><<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
+    else
+        k_stream<float><<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
+    c->launches++;
+    KS_CUDA(c, cudaGetLastError());
+    return KS_OK;
+}
+
 template <int CH, int NT, int KM>
 int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int per_sm) {
     MixedJob job = job0;
@@ -952,15 +967,10 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
     const int M = c->st.M, N = c->st.N;
     // 1. the FP32 sample stream (one march per ray, shared by every frame and frequency)
-    const int sseg = std::max(M, (N / 4 + M - 1) / M * M);
-    const int nsseg = (N + sseg - 1) / sseg;
-    KS_CUDA(c, c->stream_buf.ensure(size_t(N) * SM_COUNT * c->npad * sizeof(float)));
-    if (c->geo64)
-        k_stream<double><<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
-    else
-        k_stream<float><<<nblocks(c->npix * nsseg, 128), 128, 0, c->stream>>>(plan_view(c), c->st, c->npix, sseg, nsseg, c->stream_buf.as<float>());
-    c->launches++;
-    KS_CUDA(c, cudaGetLastError());
+    {
+        int s = launch_stream(c);
+        if (s) return s;
+    }
     MixedJob job;
     job.npix = c->npix; job.npad = c->npad; job.nframes = nframes; job.nfreq = nfreq;
     job.nvc = (nfreq + CH - 1) / CH;
@@ -1838,8 +1848,12 @@ int jvp_chunk(ks_context* c, int ntot, const double* dparams_dev, const double* 
         KS_CUDA(c, cudaGetLastError());
     }
     const long long nrc = c->npix * ncombo;
-    k_jvp<S, K><<<nblocks(nrc, 64), 64, 0, c->stream>>>(plan_view(c), c->st, c->npix, dt, ntot, dct, dcn, ncombo, L, nmax, slab, img_sorted,
-                                                        out_sorted, lnL_dir);
+    if constexpr (std::is_same<S, float>::value)
+        k_jvp_stream<K><<<nblocks(nrc, 64), 64, 0, c->stream>>>(plan_view(c), c->st, c->npix, dt, ntot, dct, dcn, ncombo, L, nmax, slab,
+                                                                c->stream_buf.as<float>(), img_sorted, out_sorted, lnL_dir);
+    else
+        k_jvp<S, K><<<nblocks(nrc, 64), 64, 0, c->stream>>>(plan_view(c), c->st, c->npix, dt, ntot, dct, dcn, ncombo, L, nmax, slab, img_sorted,
+                                                            out_sorted, lnL_dir);
     c->launches++;
     c->adjoint_launches++;
     KS_CUDA(c, cudaGetLastError());
@@ -1912,6 +1926,12 @@ int jvp_impl(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doubl
     KS_CUDA(c, c->out_sorted.ensure(size_t(nrc) * 4 * sizeof(double)));
     KS_CUDA(c, c->jvp_out.ensure(size_t(K) * nrc * 4 * sizeof(double)));
     cudaEventRecord(c->ev0, c->stream);
+    if (precision == KS_MIXED) {
+        // the mixed J v reads the samples of the FP32 stream (the FP64 march, once for every chunk)
+        c->geo64 = true;
+        int s = launch_stream(c);
+        if (s) return s;
+    }
     for (int ch = 0; ch < nchunk; ++ch) {
         const double* dd = dp + np + (long long)ch * K * np;
         int s;
