@@ -223,6 +223,24 @@ int ks_context_stream(ks_context* ctx, void** stream);
  * their launch count, and the launch count of every kernel of this library. */
 int ks_kernel_stats(ks_context* ctx, double* render_ms, long long* render_launches, long long* all_launches, int reset);
 
+/* CUDA graph of one mixed render (the fit loop's forward pass with no host work): records the device
+ * work of ks_render(..., KS_MIXED, ...) for device-resident splat sets (params, and hyp of kappa sets,
+ * in device memory) and a device `out`: the splat tables built from the parameters, their FP32 copy,
+ * the sample stream, the consumer, the segment composition and the output in `order`. The call first
+ * renders once the ordinary way (validation, buffers, launch shape). Frames, frequencies, L, nmax,
+ * slab, the knot array, the splat counts and all pointers are fixed at capture; every replay re-reads
+ * the parameter values, so updating them in place on the device and replaying re-renders. One graph
+ * per context; a new capture or ks_graph_destroy releases the previous one. */
+int ks_render_graph_capture(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes,
+                            const double* nus, int32_t nfreq, double L, int32_t nmax, double slab, double* out, int32_t order);
+
+/* Replay the captured render on the context stream; wait != 0 synchronises (and reports a kernel whose
+ * bounded wait gave up, KS_ERR_TIMEOUT). */
+int ks_graph_launch(ks_context* ctx, int32_t wait);
+
+/* Release the captured graph. */
+int ks_graph_destroy(ks_context* ctx);
+
 /* Device time (CUDA events on the context stream) of the persistent consumer k_consume alone in the
  * mixed ks_render calls since the last reset, and its launch count (one per mixed render). */
 int ks_consume_stats(ks_context* ctx, double* consume_ms, long long* launches, int reset);

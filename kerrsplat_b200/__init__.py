@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "capture_render", "RenderGraph", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -415,6 +415,40 @@ def render(cache, model, times, nus, L, nmax=-1, slab=0.0, precision=KS_FP64, or
     cache._check(cache._lib.ks_render(cache._ctx, arr, nsets, _ptr(times), nt, _ptr(nus), nf, float(L), _precision(precision),
                                       int(nmax), float(slab), _ptr(out), o))
     return out
+
+
+class RenderGraph:
+    """A mixed render captured as a CUDA graph (ks_render_graph_capture): replay() re-renders into
+    `out` from the current values of the model's device parameter buffers, model.sets()[i].params
+    (column-major copies the model made of the matrices it was given; update those in place, e.g.
+    model.sets()[0].params[:, 12] += 0.1 for the log density of a thermal set). Frames, frequencies,
+    L, the splat counts and the knots are fixed at capture."""
+
+    def __init__(self, cache, model, times, nus, L, out, nmax, slab, order):
+        self.cache, self.model, self.out = cache, model, out
+        times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+        nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+        arr, nsets, self._keep = _set_array(model)
+        o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+        cache._check(cache._lib.ks_render_graph_capture(cache._ctx, arr, nsets, _ptr(times), int(times.shape[0]), _ptr(nus),
+                                                        int(nus.shape[0]), float(L), int(nmax), float(slab), _ptr(out), o))
+
+    def replay(self, wait=True):
+        self.cache._check(self.cache._lib.ks_graph_launch(self.cache._ctx, int(bool(wait))))
+        return self.out
+
+    def close(self):
+        self.cache._check(self.cache._lib.ks_graph_destroy(self.cache._ctx))
+
+
+def capture_render(cache, model, times, nus, L, out=None, nmax=-1, slab=0.0, order="screen"):
+    """Capture one mixed render of a device-resident model (torch CUDA tensors) as a CUDA graph; the
+    returned RenderGraph replays it with no host work (the forward pass of a fit iteration)."""
+    nt = len(np.atleast_1d(times)) if not hasattr(times, "data_ptr") else int(times.shape[0])
+    nf = len(np.atleast_1d(nus)) if not hasattr(nus, "data_ptr") else int(nus.shape[0])
+    if out is None:
+        out = _out_like(model.sets()[0].params, (nf, nt, cache.npix, 4))
+    return RenderGraph(cache, model, times, nus, L, out, nmax, slab, order)
 
 
 def _grad_like(model):

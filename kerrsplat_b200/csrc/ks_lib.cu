@@ -652,6 +652,10 @@ __global__ void k_unsort(const double* __restrict__ src, const long long* __rest
 struct DevBuf {
     void* p = nullptr;
     size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;   // one owner per allocation
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
     cudaError_t ensure(size_t bytes) {
         if (bytes <= n) return cudaSuccess;
         if (p) cudaFree(p);
@@ -681,6 +685,10 @@ struct ks_context {
     DevBuf adj_state, adj_act, adj_bnd, adj_unit, adj_part, jvp_tab, jvp_in, jvp_out, st_buf;
     DevBuf tab32;     // the splat table and knot array in FP32, padded to 16 bytes (the TMA staging source)
     DevBuf errflag;   // set by a kernel whose bounded wait gave up
+    cudaGraph_t graph = nullptr;          // ks_render_graph_capture: one mixed render of device-resident sets
+    cudaGraphExec_t graph_exec = nullptr;
+    bool capturing = false;               // inside that capture: no timing events
+    std::vector<void*> graph_bufs;        // the buffers the graph uses, as captured (a replay checks them)
     bool samples_ready = false;
     int tune_nt = 0, tune_units = 0;        // the autotuner's choice for the mixed forward (0: the default)
     int nkv = 0;                            // knot values after the splat table in `tab`
@@ -931,12 +939,14 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
     KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
     const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
-    cudaEventRecord(c->evc0, c->stream);
+    if (!c->capturing) cudaEventRecord(c->evc0, c->stream);
     k_consume<CH, NT, KM><<<unsigned(grid), NT, smem, c->stream>>>(
         plan_view(c), c->st, job, c->tab32.as<float>(), ntot, dt, dn, c->stream_buf.as<float>(), c->work.as<unsigned long long>(),
         c->seg_out.as<float>(), c->count_events ? c->counters.as<unsigned long long>() : nullptr, c->errflag.as<unsigned>());
-    cudaEventRecord(c->evc1, c->stream);
-    c->consume_timed = true;
+    if (!c->capturing) {
+        cudaEventRecord(c->evc1, c->stream);
+        c->consume_timed = true;
+    }
     c->launches++;
     c->kernel_launches++;
     KS_CUDA(c, cudaGetLastError());
@@ -1080,6 +1090,8 @@ int ks_context_destroy(ks_context* c) {
     if (c->evc0) cudaEventDestroy(c->evc0);
     if (c->evc1) cudaEventDestroy(c->evc1);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return KS_OK;
@@ -1181,6 +1193,7 @@ namespace {
 int regenerate_impl(ks_context* c, double a, double theta_o, int32_t nsamples, int32_t anchor_M, double density, int32_t nmin) {
     if (!c) return KS_ERR_ARGUMENT;
     if (c->npix <= 0) return fail(c, KS_ERR_ARGUMENT, "set a camera before regenerate");
+    ks_graph_destroy(c);   // a captured render holds the old geometry's launch shape
     if (!std::isfinite(a) || !std::isfinite(theta_o)) return fail(c, KS_ERR_NONFINITE, "non-finite spin or inclination");
     if (!(a > 0.0 && a < 1.0)) return fail(c, KS_ERR_ARGUMENT, "spin must lie in (0, 1) (the analytic polar solution divides by a)");
     if (nsamples < 1) return fail(c, KS_ERR_ARGUMENT, "need at least one sample per ray");
@@ -1447,6 +1460,107 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
         c->consume_timed = false;
     }
     if (precision != KS_FP64) return check_device_flag(c, "ks_render");
+    return KS_OK;
+}
+
+// The device buffers a captured render reads or writes (a replay requires them unmoved).
+std::vector<void*> graph_buffers(const ks_context* c) {
+    return {c->tab.p, c->tab32.p, c->stream_buf.p, c->seg_out.p, c->work.p, c->out_sorted.p, c->combos.p, c->errflag.p,
+            c->perm.p, c->plan.p, c->anchors.p, c->aoff.p};
+}
+
+// One mixed render of device-resident splat sets recorded into a CUDA graph: the splat tables built
+// from the parameters (in place on the device), their FP32 copy, the sample stream, the consumer, the
+// segment composition and the output in `order`. Frames, frequencies, L, the knot array, the splat
+// counts and the pointers are fixed at capture; a replay re-reads the parameter values.
+int ks_render_graph_capture(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes,
+                            const double* nus, int32_t nfreq, double L, int32_t nmax, double slab, double* out, int32_t order) {
+    if (!c || !out || !sets || nsets < 1) return KS_ERR_ARGUMENT;
+    if (!is_device_ptr(out)) return fail(c, KS_ERR_ARGUMENT, "the graph's output must be device memory");
+    for (int s = 0; s < nsets; ++s) {
+        if (sets[s].nsplat > 0 && !is_device_ptr(sets[s].params))
+            return fail(c, KS_ERR_ARGUMENT, "set %d: a graph reads device-resident parameters", s);
+        if (sets[s].kind == KS_KAPPA22 && sets[s].nsplat > 0 && !is_device_ptr(sets[s].hyp))
+            return fail(c, KS_ERR_ARGUMENT, "set %d: a graph reads device-resident hyp", s);
+    }
+    ks_graph_destroy(c);
+    const bool counting = c->count_events;
+    c->count_events = false;
+    // one ordinary render: validation, tables and knots, buffers, the launch shape
+    int status = ks_render(c, sets, nsets, times, nframes, nus, nfreq, L, KS_MIXED, nmax, slab, out, order);
+    c->count_events = counting;
+    if (status) return status;
+    int ntot = 0;
+    bool thermal_only = true;
+    for (int s = 0; s < nsets; ++s) {
+        ntot += sets[s].nsplat;
+        thermal_only = thermal_only && (sets[s].kind == KS_THERMAL21 || sets[s].nsplat == 0);
+    }
+    KS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    c->capturing = true;
+    int first = 0, koff = 0;
+    for (int s = 0; s < nsets && status == KS_OK; ++s) {
+        const ks_splat_set& S = sets[s];
+        if (S.nsplat == 0) continue;
+        const int nk = S.kind == KS_KNOT21 ? S.nknots : 0;
+        SetDesc d{S.kind, nrows_of(S.kind), S.nsplat, first, static_cast<const double*>(S.params),
+                  S.kind == KS_KAPPA22 ? static_cast<const double*>(S.hyp) : nullptr, S.gamma_max > 0 ? S.gamma_max : 1e5,
+                  S.kind == KS_KNOT21 ? koff : 0, nk,
+                  c->tab.as<const double>() + size_t(ntot) * ST_COUNT};
+        k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
+        if (cudaGetLastError() != cudaSuccess) status = fail(c, KS_ERR_DEVICE, "graph capture: splat table of set %d", s);
+        first += S.nsplat;
+        koff += S.nsplat * 4 * nk;   // per knot splat: its nk times and 3 nk centres
+    }
+    if (status == KS_OK) {
+        const long long nv = (long long)ntot * ST_COUNT + c->nkv;
+        const long long np4 = std::max<long long>(4, (nv + 3) / 4 * 4);
+        k_tab_f32<<<nblocks(np4, 256), 256, 0, c->stream>>>(nv, np4, c->tab.as<double>(), c->tab32.as<float>());
+        if (cudaGetLastError() != cudaSuccess) status = fail(c, KS_ERR_DEVICE, "graph capture: FP32 table");
+    }
+    if (status == KS_OK) status = launch_mixed(c, ntot, nullptr, nframes, nfreq, L, nmax, slab, thermal_only);
+    if (status == KS_OK) status = emit(c, c->out_sorted.as<double>(), 4, nframes * nfreq, order, out);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    c->capturing = false;
+    if (status != KS_OK || ec != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return status != KS_OK ? status : fail(c, KS_ERR_DEVICE, "graph capture: %s", cudaGetErrorString(ec));
+    }
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        return fail(c, KS_ERR_DEVICE, "graph instantiation: %s", cudaGetErrorString(ei));
+    }
+    c->graph = g;
+    c->graph_exec = ex;
+    c->graph_bufs = graph_buffers(c);
+    return KS_OK;
+}
+
+// Replay the captured render on the context stream; with wait, synchronise and report a kernel whose
+// bounded wait gave up.
+int ks_graph_launch(ks_context* c, int32_t wait) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (!c->graph_exec) return fail(c, KS_ERR_ARGUMENT, "no captured graph");
+    if (graph_buffers(c) != c->graph_bufs)
+        return fail(c, KS_ERR_ARGUMENT, "a later call reallocated buffers the graph uses: capture again");
+    KS_CUDA(c, cudaGraphLaunch(c->graph_exec, c->stream));
+    c->launches++;
+    if (!wait) return KS_OK;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_device_flag(c, "graph replay");
+}
+
+int ks_graph_destroy(ks_context* c) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    c->graph_exec = nullptr;
+    c->graph = nullptr;
     return KS_OK;
 }
 

@@ -146,3 +146,32 @@ def test_autotune_keeps_results(oracle):
     out = np.asarray(ks.render(cache, m, [0.0], c["nus"], c["L"], precision=ks.KS_MIXED))
     ref = np.asarray(ks.render(cache, m, [0.0], c["nus"], c["L"], precision=ks.KS_FP64))
     assert rel_l2(out, ref) < 1e-4
+
+
+def test_render_graph_replays_and_follows_parameters():
+    """ks_render_graph_capture / ks_graph_launch: a mixed render of device-resident thermal and
+    power-law sets captured as a CUDA graph replays to the image of ks_render bit for bit, and after
+    an in-place change of the model's parameter buffer the replay equals the re-render; a regenerate
+    drops the graph."""
+    import torch
+    a, tho = 0.94, np.deg2rad(163.0)
+    rng = np.random.Generator(np.random.PCG64(35))
+    pt = scenes.thermal_params(rng, 6, a)
+    pp = scenes.powerlaw_params(rng, 4, a)
+    model = ks.CompositeModel(ks.PolarizedSplats(torch.tensor(pt, device="cuda")), ks.PowerLawSplats(torch.tensor(pp, device="cuda")))
+    cam = ks.Camera((-12.0, 12.0), (-12.0, 12.0), 16)
+    cache = ks.GeodesicCache(cam, 96)
+    ks.regenerate(cache, a, tho)
+    L = ks.gravitational_radius(4e6)
+    times, nus = [0.0, 10.0], [230e9, 345e9]
+    g = ks.capture_render(cache, model, times, nus, L)
+    ref = ks.render(cache, model, times, nus, L, precision=ks.KS_MIXED).cpu().numpy()
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(g.replay().cpu().numpy(), ref)
+    model.sets()[0].params[:, 12] += np.log(1.5)   # the thermal log densities, in place
+    ref2 = ks.render(cache, model, times, nus, L, precision=ks.KS_MIXED).cpu().numpy()
+    assert not np.array_equal(ref2, ref)
+    assert np.array_equal(g.replay().cpu().numpy(), ref2)
+    ks.regenerate(cache, a, tho)
+    with pytest.raises(ValueError, match="no captured graph"):
+        g.replay()
