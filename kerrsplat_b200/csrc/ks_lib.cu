@@ -975,7 +975,6 @@ template <int CH, int KM>
 int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, int nmax, double slab) {
     int nsm = 0;
     KS_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
-    const int M = c->st.M, N = c->st.N;
     // 1. the FP32 sample stream (one march per ray, shared by every frame and frequency)
     {
         int s = launch_stream(c);
@@ -1001,7 +1000,6 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     if (w256 == best) return launch_consume<CH, 256, KM>(c, job, ntot, nsm, w256 / 8);
     if (w128 > 0) return launch_consume<CH, 128, KM>(c, job, ntot, nsm, w128 / 4);
     return fail(c, KS_ERR_ARGUMENT, "too many splats for one launch (%d)", ntot);
-    (void)M;
 }
 
 // The most warps of k_consume<CH, *, KM> resident per SM for an ntot-splat table.

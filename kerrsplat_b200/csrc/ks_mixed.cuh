@@ -91,11 +91,9 @@ __device__ __forceinline__ bool stage_bulk(void* dst, const void* src, unsigned 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned long long state;
-        asm volatile("mbarrier.arrive.expect_tx.shared.b64 %0, [%1], %2;" : "=l"(state) : "r"(b), "r"(bytes) : "memory");
+        asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared.b64 st, [%0], %1;\n\t}" ::"r"(b), "r"(bytes) : "memory");
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(b) : "memory");
-        (void)state;
     }
     unsigned done = 0;
     for (int it = 0; it < kStageWaitLimit && !done; ++it)
