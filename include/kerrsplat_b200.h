@@ -241,6 +241,12 @@ int ks_graph_launch(ks_context* ctx, int32_t wait);
 /* Release the captured graph. */
 int ks_graph_destroy(ks_context* ctx);
 
+/* Test hook for the bounded waits (no reference counterpart): while on != 0, the mixed kernels arm
+ * the shared-memory barrier of their splat-table staging without issuing the copy and poll it only
+ * 4096 times, so every block's wait runs out; the kernels record it and return (no fault, no hang) and
+ * the call fails with KS_ERR_TIMEOUT. The context stays usable; turn the hook off to render again. */
+int ks_set_stage_test(ks_context* ctx, int32_t on);
+
 /* Device time (CUDA events on the context stream) of the persistent consumer k_consume alone in the
  * mixed ks_render calls since the last reset, and its launch count (one per mixed render). */
 int ks_consume_stats(ks_context* ctx, double* consume_ms, long long* launches, int reset);

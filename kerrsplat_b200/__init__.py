@@ -217,6 +217,10 @@ class GeodesicCache:
         self._check(self._lib.ks_kernel_stats(self._ctx, ctypes.byref(ms), ctypes.byref(kl), ctypes.byref(al), int(reset)))
         return ms.value, kl.value, al.value
 
+    def set_stage_test(self, on):
+        """Test hook: while on, mixed calls fail with a timeout of the table-staging wait (no fault)."""
+        self._check(self._lib.ks_set_stage_test(self._ctx, int(bool(on))))
+
     def consume_stats(self, reset=False):
         """(ms, launches) of k_consume alone in the mixed renders since the last reset."""
         ms = ctypes.c_double()

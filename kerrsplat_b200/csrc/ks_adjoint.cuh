@@ -848,7 +848,7 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
     // the FP32 splat table into shared memory by one bulk copy (k_consume's staging)
     __shared__ __align__(8) unsigned long long tab_bar;
     const unsigned tab_bytes = unsigned(AS::tab_bytes(ntot));
-    if (tab_bytes > 0 && !stage_bulk(tab, tab32, tab_bytes, &tab_bar)) {
+    if (tab_bytes > 0 && !stage_bulk(tab, tab32, tab_bytes, &tab_bar, job.stage_test == 0, job.stage_test ? 4096 : kStageWaitLimit)) {
         if (threadIdx.x == 0) atomicOr(err, 1u);
         return;
     }

@@ -688,6 +688,7 @@ struct ks_context {
     cudaGraph_t graph = nullptr;          // ks_render_graph_capture: one mixed render of device-resident sets
     cudaGraphExec_t graph_exec = nullptr;
     bool capturing = false;               // inside that capture: no timing events
+    int stage_test = 0;                   // ks_set_stage_test
     std::vector<void*> graph_bufs;        // the buffers the graph uses, as captured (a replay checks them)
     bool samples_ready = false;
     int tune_nt = 0, tune_units = 0;        // the autotuner's choice for the mixed forward (0: the default)
@@ -987,6 +988,7 @@ int launch_mixed_ch(ks_context* c, int ntot, int nframes, int nfreq, double L, i
     job.nmax = nmax; job.slab = float(slab); job.L = L;
     job.nkv = c->nkv;
     job.ch = CH;
+    job.stage_test = c->stage_test;
     // the block size with the most resident warps (the per-warp shared memory sets the limit)
     const int w384 = consume_blocks<CH, 384, KM>(c, ntot) * 12, w256 = consume_blocks<CH, 256, KM>(c, ntot) * 8,
               w128 = consume_blocks<CH, 128, KM>(c, ntot) * 4;
@@ -1111,6 +1113,14 @@ int ks_kernel_stats(ks_context* c, double* render_ms, long long* render_launches
     if (render_launches) *render_launches = c->kernel_launches;
     if (all_launches) *all_launches = c->launches;
     if (reset) { c->kernel_ms = 0.0; c->kernel_launches = 0; c->launches = 0; }
+    return KS_OK;
+}
+
+// Test hook of the staging error path: while on, the mixed kernels arm their table-staging barrier
+// without issuing the copy, so the bounded wait runs out and the call fails with KS_ERR_TIMEOUT.
+int ks_set_stage_test(ks_context* c, int32_t on) {
+    if (!c) return KS_ERR_ARGUMENT;
+    c->stage_test = on ? 1 : 0;
     return KS_OK;
 }
 

@@ -83,7 +83,10 @@ __device__ __forceinline__ unsigned smem_u32(const void* p) { return unsigned(__
 // Every thread of the block calls it; thread 0 initialises the barrier and issues the copy, all
 // threads wait for the barrier's phase 0 with a bounded number of polls. Returns false (the same in
 // every thread) when the copy did not land within the limit: the caller records an error and returns.
-__device__ __forceinline__ bool stage_bulk(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+// With issue == false (a test of the error path) the barrier is armed but no copy is issued, so every
+// thread's wait runs out after `limit` polls and the function returns false.
+__device__ __forceinline__ bool stage_bulk(void* dst, const void* src, unsigned bytes, unsigned long long* bar, bool issue = true,
+                                           int limit = kStageWaitLimit) {
     const unsigned b = smem_u32(bar);
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared.b64 [%0], 1;" ::"r"(b) : "memory");
@@ -92,11 +95,12 @@ __device__ __forceinline__ bool stage_bulk(void* dst, const void* src, unsigned 
     __syncthreads();
     if (threadIdx.x == 0) {
         asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared.b64 st, [%0], %1;\n\t}" ::"r"(b), "r"(bytes) : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                     ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(b) : "memory");
+        if (issue)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(b) : "memory");
     }
     unsigned done = 0;
-    for (int it = 0; it < kStageWaitLimit && !done; ++it)
+    for (int it = 0; it < limit && !done; ++it)
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared.b64 p, [%1], 0;\n\tselp.u32 %0, 1, 0, p;\n\t}"
                      : "=r"(done) : "r"(b) : "memory");
     return __syncthreads_and(done != 0) != 0;
@@ -633,6 +637,7 @@ struct MixedJob {
     unsigned char* gact = nullptr;
     int nkv = 0;                      // knot values after the splat table
     int ch = 1;                       // frequencies per work unit
+    int stage_test = 0;               // test hook: arm the table-staging barrier without the copy
 };
 
 template <int CH, int NT, int KM>
@@ -645,7 +650,7 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const float* __restrict__ tab3
     // the FP32 splat table and knot array (padded to 16 bytes) into shared memory by one bulk copy
     __shared__ __align__(8) unsigned long long tab_bar;
     const unsigned tab_bytes = unsigned(MixedSmem<CH>::tab_bytes(ntot, job.nkv));
-    if (tab_bytes > 0 && !stage_bulk(tab, tab32, tab_bytes, &tab_bar)) {
+    if (tab_bytes > 0 && !stage_bulk(tab, tab32, tab_bytes, &tab_bar, job.stage_test == 0, job.stage_test ? 4096 : kStageWaitLimit)) {
         if (threadIdx.x == 0) atomicOr(err, 1u);
         return;
     }

@@ -175,3 +175,23 @@ def test_render_graph_replays_and_follows_parameters():
     ks.regenerate(cache, a, tho)
     with pytest.raises(ValueError, match="no captured graph"):
         g.replay()
+
+
+def test_staging_wait_runs_out_cleanly():
+    """The bounded wait of the splat-table staging: with the test hook the barrier is armed but no
+    copy is issued, so every block's wait runs out; the kernels record it and return, the call fails
+    with KS_ERR_TIMEOUT, and the same context then renders the same image as before (no GPU fault)."""
+    c = scenes.config2(res=16, N=64)
+    rng = np.random.Generator(np.random.PCG64(36))
+    p = scenes.thermal_params(rng, 5, c["a"])
+    cache = ks.GeodesicCache(c["camera"], c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    m = ks.PolarizedSplats(p)
+    ref = np.asarray(ks.render(cache, m, [0.0], [230e9], c["L"], precision=ks.KS_MIXED))
+    cache.set_stage_test(True)
+    with pytest.raises(ks.KsError) as err:
+        ks.render(cache, m, [0.0], [230e9], c["L"], precision=ks.KS_MIXED)
+    assert err.value.status == ks._lib.KS_ERR_TIMEOUT
+    cache.set_stage_test(False)
+    again = np.asarray(ks.render(cache, m, [0.0], [230e9], c["L"], precision=ks.KS_MIXED))
+    assert np.array_equal(again, ref)
