@@ -281,7 +281,12 @@ int ks_event_counts(ks_context* ctx, unsigned long long out[7]);
  * loads the library until the process exits). The first call on a device looks up that array's device
  * address (cudaGetSymbolAddress, once per device); make that first call before any stream capture.
  * Every call shares the array: calls that overlap on the GPU race. More than KS_NOALLOC_MAX_SPLATS
- * splats, or host pointers, return KS_ERR_ARGUMENT. */
+ * splats, or host pointers, return KS_ERR_ARGUMENT.
+ * Ordering: the call runs on the context stream (ks_context_stream), a non-blocking stream that does
+ * not wait for the caller's streams. Whatever writes `params`, or still uses `out`, must be complete
+ * before the call: synchronise the stream that does it, or make the context stream wait for it (an
+ * event recorded on the caller's stream and cudaStreamWaitEvent on the context stream). Neither
+ * allocates. The call is synchronous: it returns after its kernels have finished. */
 #define KS_NOALLOC_MAX_SPLATS 256
 int ks_thin_image_noalloc(ks_context* ctx, const double* params, int32_t nsplat, double t_obs, int32_t precision,
                           double* out, int32_t order);

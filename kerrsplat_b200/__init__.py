@@ -106,12 +106,18 @@ def _as_f64(x):
 
 
 def _colmajor(p, nrows):
-    """(nrows, nsplat) parameter matrix -> contiguous buffer in column-major order."""
+    """(nrows, nsplat) parameter matrix -> contiguous buffer in column-major order.
+
+    For a CUDA tensor the transposed copy runs on torch's current stream; the library reads it on
+    its own non-blocking stream, so the copy is waited for here before the buffer is handed over."""
     if hasattr(p, "data_ptr"):
         import torch
         if p.dim() != 2 or p.shape[0] != nrows:
             raise ValueError(f"parameter matrix must be {nrows} x nsplat, got {tuple(p.shape)}")
-        return p.to(torch.float64).t().contiguous(), int(p.shape[1])
+        buf = p.to(torch.float64).t().contiguous()
+        if buf.is_cuda:
+            torch.cuda.current_stream(buf.device).synchronize()
+        return buf, int(p.shape[1])
     p = np.asarray(p, dtype=np.float64)
     if p.ndim != 2 or p.shape[0] != nrows:
         raise ValueError(f"parameter matrix must be {nrows} x nsplat, got {p.shape}")
@@ -302,10 +308,14 @@ def thin_image(cache, params, t_obs, precision=KS_FP64):
 
 def thin_image_noalloc(cache, params, t_obs, out, precision=KS_FP64, order="sorted"):
     """ks_thin_image_noalloc: the thin image with no device allocation inside the call, for callers
-    whose device memory is owned by their own allocator. `params` (14, nsplat) and `out` (npix) must
-    be CUDA tensors (params in column-major order: pass `p.t().contiguous()` of a (nsplat, 14) view or
-    use `_colmajor`); at most KS_NOALLOC_MAX_SPLATS splats; see include/kerrsplat_b200.h."""
+    whose device memory is owned by their own allocator. `params` is a (14, nsplat) CUDA tensor, as
+    for thin_image_sorted, and `out` an (npix,) float64 CUDA tensor; at most KS_NOALLOC_MAX_SPLATS
+    splats. The library runs on its own stream, so pending work on torch's current stream (the
+    writers of `params` and `out`) is waited for before the call."""
     buf, ns = _colmajor(params, 14)
+    if hasattr(out, "is_cuda") and out.is_cuda:
+        import torch
+        torch.cuda.current_stream(out.device).synchronize()
     o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
     cache._check(cache._lib.ks_thin_image_noalloc(cache._ctx, _ptr(buf), ns, float(t_obs), _precision(precision), _ptr(out), o))
     return out

@@ -109,6 +109,20 @@ void kso_polarized_image(double a, double thetao, const double* alpha, const dou
     }
 }
 
+// ipole's RIAF (test/riaf_model.jl) through the RadiativeTransport consumer at one frequency
+// (stokes_image, test/test_polarized.jl:54-61): out npix x 4 (I, Q, U, V in cgs), screen order.
+// mirror_chi != 0 plants a sign error in the screen angle (for the tests of the comparison itself).
+void kso_riaf_image(double a, double thetao, const double* alpha, const double* beta, long npix, int N, int M, int pandya,
+                    double nu, double L, int mirror_chi, double* out) {
+    RIAF m = riaf_example(a, pandya != 0);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long i = 0; i < npix; ++i) {
+        Ray R = make_ray(a, thetao, alpha[i], beta[i]);
+        PolarizedResult res = riaf_ray(R, N, M, m, nu, L, mirror_chi != 0);
+        out[4 * i] = res.I; out[4 * i + 1] = res.Q; out[4 * i + 2] = res.U; out[4 * i + 3] = res.V;
+    }
+}
+
 // The exact step (step.jl:27-54): O (4x4 row-major) and E = Ej j.
 void kso_transfer_step(const double* j, const double* alpha, const double* rho, double D, double* O, double* E) {
     V4 jj = {j[0], j[1], j[2], j[3]}, al = {alpha[0], alpha[1], alpha[2], alpha[3]};
@@ -119,9 +133,10 @@ void kso_transfer_step(const double* j, const double* alpha, const double* rho, 
 }
 
 // Coefficient fits on vectors (coefficients.jl, kappa.jl): out is n x 8 (jI jQ jV aI aQ aV rQ rV).
-void kso_thermal(long n, const double* ne, const double* Te, const double* B, const double* nu, const double* th, int dexter_rhoV, double* out) {
+void kso_thermal(long n, const double* ne, const double* Te, const double* B, const double* nu, const double* th, int dexter_rhoV, int pandya,
+                 double* out) {
     for (long i = 0; i < n; ++i) {
-        Coeffs c = thermal_synchrotron(ne[i], Te[i], B[i], nu[i], th[i], dexter_rhoV != 0);
+        Coeffs c = thermal_synchrotron(ne[i], Te[i], B[i], nu[i], th[i], dexter_rhoV != 0, pandya != 0);
         double v[8] = {c.jI, c.jQ, c.jV, c.aI, c.aQ, c.aV, c.rQ, c.rV};
         std::memcpy(out + 8 * i, v, sizeof v);
     }

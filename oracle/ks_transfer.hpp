@@ -65,8 +65,32 @@ inline double dexter_II(double x) { return 2.5651 * (1 + 1.92 * std::pow(x, -1.0
 inline double dexter_IQ(double x) { return 2.5651 * (1 + 0.93193 * std::pow(x, -1.0 / 3) + 0.499873 * std::pow(x, -2.0 / 3)) * std::exp(-1.8899 * std::pow(x, 1.0 / 3)); }
 inline double dexter_IV(double x) { return (1.81384 / x + 3.42319 * std::pow(x, -2.0 / 3) + 0.0292545 * std::pow(x, -0.5) + 2.03773 * std::pow(x, -1.0 / 3)) * std::exp(-1.8899 * std::pow(x, 1.0 / 3)); }
 
-// coefficients.jl:101-145 (default prescription: Dexter emissivities, Shcherbakov rho_V)
-inline Coeffs thermal_synchrotron(double ne, double Te, double B, double nu, double th, bool dexter_rhoV = false) {
+// coefficients.jl:147-169: Pandya et al. (2016) thermal emissivities (symphony maxwell_juettner_I/Q/V,
+// ipole's signs), ipole's `emission_type 1`.
+inline void thermal_synchrotron_pandya(double ne, double Te, double B, double nu, double th, double& jI, double& jQ, double& jV) {
+    double st = std::sin(th);
+    double nuc = EE * B / (2 * PI * ME * CL);
+    double nus = (2.0 / 9.0) * nuc * st * Te * Te;
+    double X = nu / nus;
+    double pref = ne * EE * EE * nuc / CL;
+    double term1 = std::sqrt(2.0) * PI / 27 * st;
+    double x13 = std::pow(X, 1.0 / 3), x16 = std::pow(X, 1.0 / 6), x12 = std::pow(X, 0.5);
+    double c1112 = std::pow(2.0, 11.0 / 12);
+    double ex = std::exp(-x13);
+    double bi = x12 + c1112 * x16;
+    jI = pref * term1 * bi * bi * ex;
+    double te = std::pow(Te, 24.0 / 25);
+    double t2 = (7 * te + 35) / (10 * te + 75);
+    double bq = x12 + t2 * c1112 * x16;
+    jQ = pref * term1 * bq * bq * ex;
+    double tv1 = (37 - 87 * std::sin(th - 28.0 / 25)) / (100 * (Te + 1));
+    double tv2 = std::pow(1 + (std::pow(Te, 3.0 / 5) / 25 + 7.0 / 10) * std::pow(X, 9.0 / 25), 5.0 / 3);
+    jV = pref * tv1 * tv2 * ex;
+}
+
+// coefficients.jl:101-145 (default prescription: Dexter emissivities, Shcherbakov rho_V; `pandya`
+// switches the emissivities to the Pandya fits, coefficients.jl:134-135)
+inline Coeffs thermal_synchrotron(double ne, double Te, double B, double nu, double th, bool dexter_rhoV = false, bool pandya = false) {
     double st = std::sin(th), ct = std::cos(th);
     double w0 = EE * B / (ME * CL);
     double wp2 = 4 * PI * ne * EE * EE / ME;
@@ -90,12 +114,17 @@ inline Coeffs thermal_synchrotron(double ne, double Te, double B, double nu, dou
     if (dexter_rhoV && k2 > 0) ff = (k0 - 0.43793091 * std::log(1 + 0.00185777 * std::pow(x, 1.50316886))) / k2;
     else ff = (k2 > 0 ? k0 / k2 : 1.0) * (1 - 0.11 * std::log(1 + 0.035 * x));
     double rV = w / CL * (wp2w2 * w0w * ff * ct);
-    double nus = 3 * EE * B * st / (4 * PI * ME * CL) * Te * Te + 1;
-    double xs = nu / nus;
-    double pref = ne * EE * EE * nu / (2 * std::sqrt(3.0) * CL * Te * Te);
-    double jI = pref * dexter_II(xs);
-    double jQ = pref * dexter_IQ(xs);
-    double jV = 2 * ne * EE * EE * nu * ct / st / (3 * std::sqrt(3.0) * CL * Te * Te * Te) * dexter_IV(xs);
+    double jI, jQ, jV;
+    if (pandya) {
+        thermal_synchrotron_pandya(ne, Te, B, nu, th, jI, jQ, jV);
+    } else {
+        double nus = 3 * EE * B * st / (4 * PI * ME * CL) * Te * Te + 1;
+        double xs = nu / nus;
+        double pref = ne * EE * EE * nu / (2 * std::sqrt(3.0) * CL * Te * Te);
+        jI = pref * dexter_II(xs);
+        jQ = pref * dexter_IQ(xs);
+        jV = 2 * ne * EE * EE * nu * ct / st / (3 * std::sqrt(3.0) * CL * Te * Te * Te) * dexter_IV(xs);
+    }
     double Bn = planck(nu, Te);
     double invB = Bn > 0 ? 1.0 / Bn : 0.0;
     return {jI, jQ, jV, jI * invB, jQ * invB, jV * invB, rQ, rV};
@@ -266,6 +295,18 @@ inline M4 metric_uu(double a, double r, double th) {
     g[5] = D / S;
     g[10] = 1.0 / S;
     g[15] = (D - a * a * s * s) / (S * D * s * s);
+    return g;
+}
+// Krang's metric_dd: the Boyer-Lindquist metric, (t, r, theta, phi).
+inline M4 metric_dd(double a, double r, double th) {
+    double s = std::sin(th), c = std::cos(th);
+    double S = r * r + a * a * c * c, D = r * r - 2 * r + a * a;
+    M4 g{};
+    g[0] = -(1 - 2 * r / S);
+    g[3] = g[12] = -2 * a * r * s * s / S;
+    g[5] = S / D;
+    g[10] = S;
+    g[15] = (r * r + a * a + 2 * a * a * r * s * s / S) * s * s;
     return g;
 }
 // ZAMO components (t, r, phi, -theta) of a BL contravariant vector (Krang's jac_zamo_u_bl_d).
@@ -678,10 +719,13 @@ inline bool accumulate_elements(const std::vector<SplatSet>& sets, const Ray& R,
     return active;
 }
 
-// RadiativeTransport consumer (transport.jl:171-198); nmax >= 0 selects the winding consumer.
+// RadiativeTransport consumer (transport.jl:171-198) over any element sum: `accum(s, j4, a4, r3)`
+// fills the summed screen coefficients of a sample and says whether any element is active there.
+// nmax >= 0 selects the winding consumer.
 struct PolarizedResult { double I, Q, U, V; };
-inline PolarizedResult polarized_ray(const Ray& R, int N, int M, const std::vector<SplatSet>& sets, double t_obs, double nu, double L,
-                                     int nmax, double slab, double* resid_t = nullptr, double* resid_phi = nullptr) {
+template <class Accum>
+inline PolarizedResult polarized_ray_model(const Ray& R, int N, int M, double nu, double L, int nmax, double slab, Accum&& accum,
+                                           double* resid_t = nullptr, double* resid_phi = nullptr) {
     RadState st = rad_zero();
     Winding w = winding_zero();
     double rh = horizon(R.a);
@@ -693,7 +737,7 @@ inline PolarizedResult polarized_ray(const Ray& R, int N, int M, const std::vect
             if (w.n > nmax) return;
         }
         V4 j4, a4; double r3[3];
-        if (!accumulate_elements(sets, R, s, t_obs, nu, j4, a4, r3)) return;
+        if (!accum(s, j4, a4, r3)) return;
         double ct = std::cos(s.theta);
         double Sg = s.r * s.r + R.a * R.a * ct * ct;
         double D = L / nuhat(nu) * Sg * dtau;
@@ -703,6 +747,102 @@ inline PolarizedResult polarized_ray(const Ray& R, int N, int M, const std::vect
     }, resid_t, resid_phi);
     double n3 = nuhat(nu) * nuhat(nu) * nuhat(nu);
     return {st.S[0] * n3, st.S[1] * n3, st.S[2] * n3, st.S[3] * n3};
+}
+
+// The splat sets of a scene as the model (polarized.jl:121-130, transport.jl:306-316).
+inline PolarizedResult polarized_ray(const Ray& R, int N, int M, const std::vector<SplatSet>& sets, double t_obs, double nu, double L,
+                                     int nmax, double slab, double* resid_t = nullptr, double* resid_phi = nullptr) {
+    return polarized_ray_model(R, N, M, nu, L, nmax, slab, [&](const Sample& s, V4& j4, V4& a4, double r3[3]) {
+        return accumulate_elements(sets, R, s, t_obs, nu, j4, a4, r3);
+    }, resid_t, resid_phi);
+}
+
+// ---- ipole's RIAF as a one-element fluid model (test/riaf_model.jl) ----------------------------
+// A thick disk with power-law density and temperature, a toroidal field of equipartition-like
+// strength, Keplerian rotation outside the ISCO and the conserved-quantity plunge inside it, thermal
+// synchrotron with Pandya emissivities (ipole's emission_type 1).
+struct RIAF { double nth0, Te0, disk_h, pow_nth, pow_T, Ne_unit, Te_unit, eps, r_isco, rout; bool pandya; };
+
+// riaf_model.jl:25-29 (Bardeen, Press & Teukolsky 1972, prograde)
+inline double isco_radius(double a) {
+    double z1 = 1 + std::cbrt(1 - a * a) * (std::cbrt(1 + a) + std::cbrt(1 - a));
+    double z2 = std::sqrt(3 * a * a + z1 * z1);
+    return 3 + z2 - std::copysign(std::sqrt((3 - z1) * (3 + z1 + 2 * z2)), a);
+}
+// riaf_model.jl:31-34 (ipole's model/riaf/example.par)
+inline RIAF riaf_example(double a, bool pandya = true) {
+    return {1.0, 1.0, 0.1, -1.1, -0.84, 3e7, 3e11, 0.1, isco_radius(a), 100.0, pandya};
+}
+inline double quad(const M4& g, const V4& x, const V4& y) {
+    double s = 0;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) s += x[i] * g[4 * i + j] * y[j];
+    return s;
+}
+// riaf_model.jl:38-93: the coefficients and the local frame of the RIAF at one sample; false where
+// the model is empty (inside r_h + 0.1 or beyond rout).
+inline bool riaf_element(const RIAF& m, const Ray& R, const Sample& s, double nu, Coeffs& cf, Frame& fr) {
+    const double a = R.a, r = s.r, th = s.theta;
+    const double rh = horizon(a);
+    if (!(r > rh + 0.1 && r < m.rout)) return false;
+    double sth = std::sin(th), cth = std::cos(th);
+    double zc = r * cth, rc = r * sth;
+    double n = m.nth0 * std::exp(-zc * zc / 2 / rc / rc / m.disk_h / m.disk_h) * std::pow(r, m.pow_nth) * m.Ne_unit;
+    double Te = m.Te0 * std::pow(r, m.pow_T) * m.Te_unit * KBOL / (ME * CL * CL);
+    double bmag = std::sqrt(8 * PI * m.eps * n * MP * CL * CL / 6 / r);
+    if (bmag == 0) bmag = 1e-6;
+    M4 gdd = metric_dd(a, r, th), guu = metric_uu(a, r, th);
+    double om, ur;
+    if (r < m.r_isco) {
+        double wisco = 1 / (std::pow(m.r_isco, 1.5) + a);
+        M4 gi = metric_dd(a, m.r_isco, th);
+        V4 ui = {1.0, 0.0, 0.0, wisco};
+        double nrm = std::sqrt(-quad(gi, ui, ui));
+        for (double& x : ui) x /= nrm;
+        V4 ud = mv(gi, ui);
+        double e = ud[0], l = ud[3];
+        double Kcon = guu[0] * e * e + 2 * guu[3] * e * l + guu[15] * l * l;
+        double urk = -std::sqrt(std::max(0.0, -(1 + Kcon) / guu[5]));
+        V4 ut = mv(guu, V4{e, urk, 0.0, l});
+        om = ut[3] / ut[0];
+        ur = ut[1];
+    } else {
+        om = 1 / (std::pow(r, 1.5) + a);
+        ur = 0.0;
+    }
+    double K = gdd[0] + 2 * om * gdd[3] + om * om * gdd[15];
+    double ut = std::sqrt(std::max(0.0, -(1 + ur * ur * gdd[5]) / K));
+    V4 u = {ut, ur, 0.0, om * ut};
+    // toroidal field projected orthogonal to u, normalised to bmag
+    V4 Bc = {0.0, 0.0, 0.0, 1.0};
+    double BdotU = quad(gdd, Bc, u);
+    V4 b;
+    for (int i = 0; i < 4; ++i) b[i] = Bc[i] + BdotU * u[i];
+    double bn = bmag / std::sqrt(quad(gdd, b, b));
+    for (double& x : b) x *= bn;
+    // ZAMO velocity and the fluid-frame field
+    M4 J = jac_zamo_u_bl_d(a, r, th);
+    V4 uz = mv(J, u);
+    double ut3[3] = {uz[1], uz[2], uz[3]};
+    V4 bz = mv(boost_zamo_to_fluid(ut3[0], ut3[1], ut3[2]), mv(J, b));
+    double Bf[3] = {bz[1], bz[2], bz[3]};
+    fr = local_frame(a, r, th, R.eta, R.lam, s.nur, s.nutheta, R.alpha, R.beta, R.thetao, ut3, Bf);
+    double nuf = nu / fr.g;
+    double thB = std::acos(std::max(-1.0, std::min(1.0, fr.cosB)));
+    cf = thermal_synchrotron(n, Te, bmag, nuf, thB, false, m.pandya);
+    return true;
+}
+
+// The RIAF through the RadiativeTransport consumer (stokes_image of test/test_polarized.jl:54-61).
+// `mirror_chi` negates the screen angle (a planted convention error for the tests: it must fail the
+// comparison with ipole's images).
+inline PolarizedResult riaf_ray(const Ray& R, int N, int M, const RIAF& m, double nu, double L, bool mirror_chi = false) {
+    return polarized_ray_model(R, N, M, nu, L, -1, 0.0, [&](const Sample& s, V4& j4, V4& a4, double r3[3]) {
+        Coeffs cf; Frame fr;
+        if (!riaf_element(m, R, s, nu, cf, fr)) return false;
+        if (mirror_chi) fr.chi = -fr.chi;
+        return screen_coefficients(cf, fr, nu, j4, a4, r3);
+    });
 }
 
 // ThinRenderer (Splats.jl:113-128); params THIN14, column-major

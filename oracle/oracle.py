@@ -121,11 +121,22 @@ def transfer_step(j, alpha, rho, D):
     return O.reshape(4, 4), E
 
 
-def thermal(ne, Te, B, nu, th, dexter_rhoV=False):
+def thermal(ne, Te, B, nu, th, dexter_rhoV=False, pandya=False):
     args = [_d(np.atleast_1d(x)) for x in (ne, Te, B, nu, th)]
     n = args[0].size
     out = np.empty((n, 8))
-    load().kso_thermal(ctypes.c_long(n), *[_p(x) for x in args], int(dexter_rhoV), _p(out))
+    load().kso_thermal(ctypes.c_long(n), *[_p(x) for x in args], int(dexter_rhoV), int(pandya), _p(out))
+    return out
+
+
+def riaf_image(a, theta_o, alpha, beta, N, M, nu, L, pandya=True, mirror_chi=False):
+    """ipole's example RIAF (test/riaf_model.jl) through the polarized consumer: (npix, 4) cgs,
+    screen order. `mirror_chi` plants a sign error in the screen angle (tests of the comparison)."""
+    alpha, beta = _d(alpha), _d(beta)
+    n = alpha.size
+    out = np.empty((n, 4))
+    load().kso_riaf_image(ctypes.c_double(a), ctypes.c_double(theta_o), _p(alpha), _p(beta), ctypes.c_long(n), int(N), int(M),
+                          int(pandya), ctypes.c_double(nu), ctypes.c_double(L), int(mirror_chi), _p(out))
     return out
 
 

@@ -2,10 +2,14 @@
 
 Two kinds of fixtures:
 
-1. Extracts of the reference's own committed golden data (validation/symphony/*.csv, the
-   symphony-generated coefficient tables that test/test_coefficients.jl compares against at 1e-12):
-   every 4th row, the columns the tests use. Needs the reference checkout (REFERENCE_ROOT,
-   default /root/reference).
+1. Extracts of the reference's own committed golden data. Needs the reference checkout, named by
+   the REFERENCE_ROOT environment variable or the `--reference <dir>` argument (no default):
+   * validation/symphony/*.csv, the symphony-generated coefficient tables that
+     test/test_coefficients.jl compares against at 1e-12: every 4th row, the columns the tests use;
+   * validation/ipole_riaf/riaf_{fine,2thz}_{I,Q,U,V}.csv, ipole's full-Stokes images of its
+     example RIAF at 230 GHz and 2 THz (100 x 100, row = x index, column = y index), which
+     test/test_polarized.jl:156-178 compares KerrSplat's images against: all eight arrays as float64
+     in one compressed file, ipole_riaf.npz (keys "fine_I" ... "2thz_V").
 2. High-precision references restated in mpmath (the reference's own BigFloat references are
    Julia, test/highprec_reference.jl and test/test_transfer_step.jl):
    * r(tau), theta(tau) from the closed forms with Newton-polished roots (highprec_reference.jl:22-156);
@@ -32,13 +36,20 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle  # noqa: E402
 
-REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("REFERENCE_ROOT")
+
+
+def reference_root():
+    if not REFERENCE_ROOT:
+        raise SystemExit("name the reference checkout: REFERENCE_ROOT=<dir> or --reference <dir>")
+    return REFERENCE_ROOT
 mp.mp.dps = 40
 
 
 # ---- 1. symphony tables --------------------------------------------------------------------------
 SYMPHONY = {
-    "thermal_table.csv": ["nu", "Thetae", "B", "ne", "theta", "jI", "jQ", "jV", "aI", "aQ", "aV", "rhoQ", "rhoV", "rhoV_dexter"],
+    "thermal_table.csv": ["nu", "Thetae", "B", "ne", "theta", "jI", "jQ", "jV", "aI", "aQ", "aV", "rhoQ", "rhoV", "rhoV_dexter",
+                          "jI_pandya", "jQ_pandya", "jV_pandya"],
     "powerlaw_table.csv": ["nu", "p", "gamma_min", "gamma_max", "B", "ne", "theta", "jI", "jQ", "jV", "aI", "aQ", "aV"],
     "kappa_table.csv": ["nu", "kappa", "w", "B", "ne", "theta", "jI", "jQ", "jV", "aI", "aQ", "aV", "rhoQ", "rhoV"],
     "powerlaw_rho_table.csv": ["nu", "B", "theta", "p", "gamma_min", "gamma_max", "ne", "rhoQ", "rhoV"],
@@ -46,7 +57,7 @@ SYMPHONY = {
 
 
 def extract_symphony():
-    src = os.path.join(REFERENCE_ROOT, "validation", "symphony")
+    src = os.path.join(reference_root(), "validation", "symphony")
     for name, cols in SYMPHONY.items():
         with open(os.path.join(src, name)) as f:
             rows = list(csv.DictReader(f))
@@ -56,6 +67,15 @@ def extract_symphony():
             w.writerow(cols)
             for r in keep:
                 w.writerow([r[c] for c in cols])
+
+
+def extract_ipole_riaf():
+    src = os.path.join(reference_root(), "validation", "ipole_riaf")
+    arrays = {}
+    for tag in ("fine", "2thz"):
+        for st in "IQUV":
+            arrays[f"{tag}_{st}"] = np.loadtxt(os.path.join(src, f"riaf_{tag}_{st}.csv"), delimiter=",", dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "ipole_riaf.npz"), **arrays)
 
 
 # ---- 2. geodesics in mpmath -----------------------------------------------------------------------
@@ -309,9 +329,16 @@ def special_fixtures():
 
 if __name__ == "__main__":
     oracle.build()
-    what = sys.argv[1:] or ["symphony", "special", "step", "geodesic", "anchor"]
+    args = sys.argv[1:]
+    if "--reference" in args:
+        i = args.index("--reference")
+        REFERENCE_ROOT = args[i + 1]
+        del args[i:i + 2]
+    what = args or ["symphony", "ipole", "special", "step", "geodesic", "anchor"]
     if "symphony" in what:
         extract_symphony()
+    if "ipole" in what:
+        extract_ipole_riaf()
     if "special" in what:
         special_fixtures()
     if "step" in what:

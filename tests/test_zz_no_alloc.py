@@ -61,3 +61,32 @@ def test_noalloc_thin_image_matches_existing_entry_point():
                                    ctypes.c_void_p(host_out.ctypes.data), _lib.KS_ORDER_SORTED)
     assert st == _lib.KS_ERR_ARGUMENT
     cache.close()
+
+
+def test_noalloc_wrapper_on_torch_tensors_allocates_no_device_memory():
+    """The Python wrapper on CUDA tensors (the transposed parameter copy is made on torch's stream and
+    waited for) gives ks_thin_image's image, and a call after the first one leaves the device's free
+    memory unchanged (cudaMemGetInfo): the table lives in the static array, the plan and anchors were
+    allocated by regenerate."""
+    import torch
+    c = scenes.config1(res=20, N=80)
+    cache = ks.GeodesicCache(c["camera"], c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    dev = torch.device("cuda", 0)
+    p = torch.tensor(c["params"], device=dev)
+    out = torch.zeros(cache.npix, dtype=torch.float64, device=dev)
+    for prec, tol in ((ks.KS_FP64, 1e-10), (ks.KS_MIXED, 1e-4)):
+        ref = np.asarray(ks.thin_image_sorted(cache, c["params"], 0.0, precision=prec))
+        ks.thin_image_noalloc(cache, p, 0.0, out, precision=prec)       # first call: symbol lookup
+        buf = p.t().contiguous()                                           # made before the measurement
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info(dev)
+        lib = _lib.load()
+        st = lib.ks_thin_image_noalloc(cache._ctx, ctypes.c_void_p(buf.data_ptr()), p.shape[1], 0.0, prec,
+                                       ctypes.c_void_p(out.data_ptr()), _lib.KS_ORDER_SORTED)
+        assert st == _lib.KS_OK, lib.ks_last_error(cache._ctx)
+        free1, _ = torch.cuda.mem_get_info(dev)
+        assert free1 == free0, (free0, free1)
+        got = out.cpu().numpy()
+        assert rel_l2(got, ref) < tol, (prec, rel_l2(got, ref))
+    cache.close()
