@@ -32,7 +32,7 @@ UNIT = "ray-samples/s"
 # Algorithmic FP32-pipe work per event of the polarized consumer and the march (flops: add, mul =
 # 1, fma = 2, div = 1) and special-function-unit operations (sqrt, exp, log, sin, cos, atan, acos,
 # pow count 1 each), counted from the kernel source (kerrsplat_b200/csrc/ks_march.cuh,
-# ks_transfer.cuh, ks_lib.cu PolSink): see DESIGN.md "Roofline".
+# ks_transfer.cuh, ks_lib.cu PolSink).
 FLOPS = {"samples": 330, "valid_samples": 95, "splat_tests": 22, "weights": 32, "coefficients": 170,
          "frames": 115, "steps": 1150}
 SFU = {"samples": 12, "valid_samples": 9, "splat_tests": 2, "weights": 1, "coefficients": 22, "frames": 4, "steps": 12}
@@ -485,7 +485,8 @@ def cpu_baseline(c, nrays):
     dt = time.perf_counter() - t0
     units = idx.size * c["N"] * len(c["nus"])
     return {"value": units / dt, "unit": UNIT, "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"{idx.size} random rays of the 256x256 workload x {c['N']} samples x {len(c['nus'])} frequencies ({dt:.1f} s)"}
+            "sample": f"{idx.size} random rays of the 256x256 workload x {c['N']} samples x {len(c['nus'])} frequencies ({dt:.1f} s)",
+            "seconds": dt, "units": units, "rays": int(idx.size)}
 
 
 def run_reference(args):
@@ -493,18 +494,19 @@ def run_reference(args):
     if rank != 0:
         return
     c = workload()
-    samples = []
+    units, secs = 0, 0.0
     for k in range(args.warmup + args.steps):
         b = cpu_baseline(c, args.cpu_rays)
         if k >= args.warmup:
-            samples.append(b["value"])
-    v = float(np.mean(samples))
-    units_per_step = c["camera"].npix * c["N"] * len(c["nus"])
+            units += b["units"]
+            secs += b["seconds"]
+    v = units / secs
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": units_per_step / v * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded PCG64 scene, cfg 2 distributions)",
-            "config": {"workload": "polarized image 256x256 +-20M, a=0.5, theta_o=60deg, N=1024, M=64, 64 thermal splats, 86/230/345 GHz",
-                       "note": "each step renders a bounded random sample of the rays; ms_per_step extrapolates to the full screen"},
+            "config": {"workload": f"{b['rays']} seeded random rays of the polarized image 256x256 +-20M, a=0.5, theta_o=60deg, N=1024, M=64, "
+                                   "64 thermal splats, 86/230/345 GHz",
+                       "note": "one step renders the ray sample at every frequency; ms_per_step is that sample's time"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": b["cores"], "kind": "port", "sample": b["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

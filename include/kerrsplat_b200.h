@@ -127,6 +127,17 @@ int ks_render(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const do
               const double* nus, int32_t nfreq, double L, int32_t precision, int32_t nmax, double slab,
               double* out, int32_t order);
 
+/* ipole's RIAF through the polarized consumer: the fluid model of test/riaf_model.jl:11-93 (the reference's
+ * RIAFModel, rendered by stokes_image = fused_march!(RadiativeTransport(model, nu, L), out, cache),
+ * test/test_polarized.jl:54-61) at nfreq frequencies. model = {nth0, Te0, disk_h, pow_nth, pow_T, Ne_unit,
+ * Te_unit, eps, r_isco, rout} (riaf_example, riaf_model.jl:31-34); pandya != 0 selects the Pandya
+ * emissivities (ipole's emission_type 1). out has npix x 4 x nfreq doubles, index (f_nu * npix + pixel) * 4
+ * + stokes, in cgs, pixels in `order`. KS_FP64 runs the element and the step in FP64, KS_MIXED in FP32
+ * (the march stays FP64 in both). */
+#define KS_RIAF_PARAMS 10
+int ks_riaf_image(ks_context* ctx, const double* model, int32_t pandya, const double* nus, int32_t nfreq, double L, int32_t precision,
+                  double* out, int32_t order);
+
 /* Visibilities of an image (vis_kernel!, src/Fit/device_visibilities.jl:61-73): `image` npix x 4
  * (Stokes I, Q, U, V per pixel, in `order`), V nuv x 4 complex as (re, im) doubles,
  * V_k = tap_k scale sum_j I_j exp(2 pi i (u_k l_j + v_k m_j)) with l = -(i - (nalpha + 1)/2) psize

@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "capture_render", "RenderGraph", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "capture_render", "RenderGraph", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "RIAFModel", "riaf_image", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
 ]
@@ -660,6 +660,40 @@ def sweep_passes(cache, model, L, nmax=-1, slab=0.0, precision=KS_FP64):
         return adjoint(cache, model, np.atleast_1d(t), [nu], L, ds, nmax=nmax, slab=slab, precision=precision)
 
     return forward, reverse
+
+
+class RIAFModel:
+    """ipole's RIAF as a fluid model (the reference's test/riaf_model.jl:11-23): density and
+    temperature power laws in r with a Gaussian thick-disk profile, a toroidal field of
+    equipartition-like strength, Keplerian rotation outside r_isco and the plunge inside it,
+    thermal synchrotron with Pandya emissivities when `pandya`."""
+
+    def __init__(self, nth0, Te0, disk_h, pow_nth, pow_T, Ne_unit, Te_unit, eps, r_isco, rout, pandya=True):
+        self.values = np.array([nth0, Te0, disk_h, pow_nth, pow_T, Ne_unit, Te_unit, eps, r_isco, rout], dtype=np.float64)
+        self.pandya = bool(pandya)
+
+    @staticmethod
+    def isco_radius(a):
+        """The prograde ISCO (Bardeen, Press & Teukolsky 1972; riaf_model.jl:25-29)."""
+        z1 = 1 + np.cbrt(1 - a * a) * (np.cbrt(1 + a) + np.cbrt(1 - a))
+        z2 = np.sqrt(3 * a * a + z1 * z1)
+        return 3 + z2 - np.copysign(np.sqrt((3 - z1) * (3 + z1 + 2 * z2)), a)
+
+    @classmethod
+    def example(cls, a=0.9375, pandya=True):
+        """ipole's model/riaf/example.par (riaf_example, riaf_model.jl:31-34)."""
+        return cls(1.0, 1.0, 0.1, -1.1, -0.84, 3e7, 3e11, 0.1, cls.isco_radius(a), 100.0, pandya)
+
+
+def riaf_image(cache, riaf, nus, L, precision=KS_FP64, order="screen"):
+    """Stokes images of a RIAFModel through the polarized consumer (stokes_image,
+    test/test_polarized.jl:54-61): (nfreq, npix, 4) cgs, screen order unless order="sorted"."""
+    nus = np.ascontiguousarray(np.atleast_1d(nus), dtype=np.float64)
+    out = np.empty((nus.size, cache.npix, 4))
+    o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
+    cache._check(cache._lib.ks_riaf_image(cache._ctx, _ptr(riaf.values), int(riaf.pandya), _ptr(nus), nus.size, float(L),
+                                          _precision(precision), _ptr(out), o))
+    return out
 
 
 def polarized_image(cache, model, t_obs, nu, L, nmax=-1, slab=0.0, precision=KS_FP64):

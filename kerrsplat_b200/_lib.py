@@ -30,6 +30,7 @@ KS_KAPPA22 = 3
 KS_KNOT21 = 4
 
 KS_NOALLOC_MAX_SPLATS = 256
+KS_RIAF_PARAMS = 10
 
 NROWS = {KS_THIN14: 14, KS_THERMAL21: 21, KS_POWERLAW22: 22, KS_KAPPA22: 22, KS_KNOT21: 21}
 
@@ -80,6 +81,7 @@ SIGNATURES = [
     ("ks_chi2_gradient", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
                                         ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _VP, _VP, ctypes.c_double, _VP,
                                         _VP, _VP, ctypes.c_int32, _VP]),
+    ("ks_riaf_image", ctypes.c_int, [_VP, _VP, ctypes.c_int32, _VP, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _VP, ctypes.c_int32]),
 ]
 # library extensions outside include/kerrsplat_b200.h's reference-facing set
 EXTRA_SIGNATURES = [

@@ -622,6 +622,193 @@ __global__ void __launch_bounds__(kBlock) k_polarized(PlanView P, Spacetime st, 
     }
 }
 
+// ---- ipole's RIAF as a fluid model of the polarized consumer ------------------------------------
+// The reference's test/riaf_model.jl: a thick disk with power-law density and temperature, a
+// toroidal field of equipartition-like strength, Keplerian rotation outside the ISCO and the plunge
+// with the ISCO's conserved energy and angular momentum inside it, thermal synchrotron (Pandya
+// emissivities when `pandya`, ipole's emission_type 1). One element, evaluated at every sample.
+struct RiafModel { double nth0, Te0, disk_h, pow_nth, pow_T, Ne_unit, Te_unit, eps, r_isco, rout; int pandya; };
+
+constexpr double kMP = 1.67262171e-24, kKBOL = 1.3806505e-16;   // constants.jl:3-12
+
+// The coefficients and the local frame of the RIAF at the BL point (r, theta) of a sample, for the
+// photon of the sample's frame F; false where the model is empty (r <= r_h + 0.1 or r >= rout).
+template <class T>
+__device__ __forceinline__ bool riaf_element(const RiafModel& m, T a, T r, T th, T sth, T cth, const SampleFrame<T>& F, T alpha, T beta,
+                                             T a_sin_tho, T nu, Coef<T>& cf, LFrame<T>& lf) {
+    const T rh = T(1) + sqrt(T(1) - a * a);
+    if (!(r > rh + T(0.1) && r < T(m.rout))) return false;
+    // density, temperature, field strength (ipole's get_model_ne / thetae / b)
+    const T zc = r * cth, rc = r * sth;
+    const T hh = T(m.disk_h);
+    const T n = T(m.nth0) * exp(-zc * zc / T(2) / rc / rc / hh / hh) * pow(r, T(m.pow_nth)) * T(m.Ne_unit);
+    const T Te = T(m.Te0) * pow(r, T(m.pow_T)) * T(m.Te_unit) * T(kKBOL) / (T(kME) * T(kCL) * T(kCL));
+    T bmag = sqrt(T(8) * kpi<T>() * T(m.eps) * n * T(kMP) * T(kCL) * T(kCL) / T(6) / r);
+    if (bmag == T(0)) bmag = T(1e-6);
+    // the Boyer-Lindquist metric at (r, theta) and at (r_isco, theta)
+    const T s2 = sth * sth;
+    auto gdd = [&](T rr, T& gtt, T& gtp, T& grr, T& gpp) {
+        const T S = rr * rr + a * a * cth * cth, D = rr * rr - T(2) * rr + a * a;
+        gtt = -(T(1) - T(2) * rr / S); gtp = -T(2) * a * rr * s2 / S; grr = S / D;
+        gpp = (rr * rr + a * a + T(2) * a * a * rr * s2 / S) * s2;
+    };
+    T gtt, gtp, grr, gpp;
+    gdd(r, gtt, gtp, grr, gpp);
+    T om, ur;
+    const T risco = T(m.r_isco);
+    if (r < risco) {
+        // the plunge: the ISCO's conserved e, l (ipole get_model_fourv)
+        T itt, itp, irr, ipp;
+        gdd(risco, itt, itp, irr, ipp);
+        const T wis = T(1) / (pow(risco, T(1.5)) + a);
+        const T nrm = sqrt(-(itt + T(2) * wis * itp + wis * wis * ipp));
+        const T u0 = T(1) / nrm, u3 = wis / nrm;
+        const T e = itt * u0 + itp * u3, l = itp * u0 + ipp * u3;
+        // the inverse metric at (r, theta)
+        const T S = r * r + a * a * cth * cth, D = r * r - T(2) * r + a * a;
+        const T A = (r * r + a * a) * (r * r + a * a) - a * a * D * s2;
+        const T utt = -A / (S * D), utp = -T(2) * a * r / (S * D), urr = D / S, upp = (D - a * a * s2) / (S * D * s2);
+        const T Kcon = utt * e * e + T(2) * utp * e * l + upp * l * l;
+        const T q = -(T(1) + Kcon) / urr;
+        const T urk = -(q > T(0) ? sqrt(q) : T(0));
+        const T c0 = utt * e + utp * l, c3 = utp * e + upp * l;
+        om = c3 / c0;
+        ur = urr * urk;
+    } else {
+        om = T(1) / (pow(r, T(1.5)) + a);
+        ur = T(0);
+    }
+    const T K = gtt + T(2) * om * gtp + om * om * gpp;
+    const T q2 = -(T(1) + ur * ur * grr) / K;
+    const T ut = q2 > T(0) ? sqrt(q2) : T(0);
+    const T u[4] = {ut, ur, T(0), om * ut};
+    // toroidal field projected orthogonal to u, normalised to bmag
+    const T BdotU = gtp * u[0] + gpp * u[3];
+    T b[4] = {BdotU * u[0], BdotU * u[1], T(0), T(1) + BdotU * u[3]};
+    const T bb = gtt * b[0] * b[0] + T(2) * gtp * b[0] * b[3] + grr * b[1] * b[1] + gpp * b[3] * b[3];
+    const T bs = bmag / sqrt(bb);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) b[k] *= bs;
+    // ZAMO components (t, r, phi, -theta): lapse, sqrt(S/D), varpi (. - omega_frame t), -sqrt(S)
+    const T S = r * r + a * a * cth * cth, D = r * r - T(2) * r + a * a;
+    const T A = (r * r + a * a) * (r * r + a * a) - a * a * D * s2;
+    const T lapse = sqrt(S * D / A), omf = T(2) * a * r / A, varpi = sqrt(A / S) * sth, sSD = sqrt(S / D);
+    const T u1 = sSD * u[1], u2 = varpi * (u[3] - omf * u[0]), u3 = T(0);
+    const T bz0 = lapse * b[0], bz1 = sSD * b[1], bz2 = varpi * (b[3] - omf * b[0]), bz3 = T(0);
+    // the field in the fluid frame: boost_zamo_to_fluid(u) (frames.jl:31-41)
+    const T gam = sqrt(T(1) + u1 * u1 + u2 * u2 + u3 * u3), qf = T(1) / (gam + T(1));
+    const T ub = u1 * bz1 + u2 * bz2 + u3 * bz3;
+    const T f1 = -u1 * bz0 + bz1 + u1 * ub * qf, f2 = -u2 * bz0 + bz2 + u2 * ub * qf, f3 = -u3 * bz0 + bz3 + u3 * ub * qf;
+    const T fn = sqrt(f1 * f1 + f2 * f2 + f3 * f3);
+    const bool bzero = !(fn > T(0));
+    lf = local_frame(F, u1, u2, u3, bzero ? T(0) : f1 / fn, bzero ? T(0) : f2 / fn, bzero ? T(1) : f3 / fn, bzero, alpha, beta, a_sin_tho);
+    const T nuf = nu / lf.g;
+    T sb, cb;
+    if constexpr (is_f32<T>) {
+        pitch_sc(lf.cosB, sb, cb);
+    } else {
+        const T thb = acos(fmin(T(1), fmax(T(-1), lf.cosB)));
+        sb = sin(thb); cb = cos(thb);
+    }
+    // Bessel ratios at 1/Theta_e (K2 = K0 + 2 K1 / x), FP64
+    double k0, k1;
+    const double xb = 1.0 / double(Te);
+    besselk01(xb, k0, k1);
+    const double k2 = k0 + 2.0 * k1 / xb;
+    const T f0 = k2 > 0 ? T(k0 / k2) : T(1), kr = k2 > 0 ? T(k1 / k2) : T(1);
+    cf = thermal_cs(n, Te, f0, kr, bmag, nuf, sb, cb);
+    if (m.pandya && sb > T(0)) {
+        T jI, jQ, jV;
+        pandya_emissivities(n, Te, bmag, nuf, sb, cb, jI, jQ, jV);
+        const T Bn = planck(nuf, Te);
+        const T invB = Bn > T(0) ? T(1) / Bn : T(0);
+        cf.jI = jI; cf.jQ = jQ; cf.jV = jV; cf.aI = jI * invB; cf.aQ = jQ * invB; cf.aV = jV * invB;
+    }
+    return true;
+}
+
+// RadiativeTransport of the RIAF at one frequency (stokes_image, test/test_polarized.jl:54-61): the
+// FP64 march, the element and the step in T.
+template <class T>
+struct RiafSink {
+    RiafModel m;
+    T nu, Lnu;
+    T a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho;
+    T P[16], S[4];
+    unsigned int ev[7];
+
+    __device__ void init() {
+        for (int q = 0; q < 16; ++q) P[q] = (q % 5 == 0) ? T(1) : T(0);
+        for (int q = 0; q < 4; ++q) S[q] = T(0);
+        for (int q = 0; q < 7; ++q) ev[q] = 0;
+    }
+
+    __device__ void operator()(int, const Sample<double>& s) {
+        ev[0]++;
+        if (!(s.ok && T(s.r) > rh_lo)) return;
+        ev[1]++;
+        const T r = T(s.r), th = T(s.theta);
+        const T sth = sin(th), cth = cos(th);
+        const SampleFrame<T> F = sample_frame(a, r, th, sth, cth, eta, lam, s.nur, s.nutheta);
+        Coef<T> cf;
+        LFrame<T> lf;
+        ev[2]++;
+        if (!riaf_element(m, a, r, th, sth, cth, F, alpha, beta, a_sin_tho, nu, cf, lf)) return;
+        ev[3]++; ev[4]++; ev[5]++;
+        // screen_coefficients (transport.jl:265-270): cap, invariants at nu/g, rotate by 2 chi
+        if (!(cf.jI > T(0) || cf.aI > T(0) || cf.rQ != T(0) || cf.rV != T(0))) return;
+        const T fe = cap_factor(cf.jI, cf.jQ, cf.jV, T(0.99));
+        const T fa = cap_factor(cf.aI, cf.aQ, cf.aV, T(0.99));
+        const T nh = nu / lf.g / T(kNU0);
+        const T i2 = T(1) / (nh * nh);
+        const T jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+        const T j4[4] = {cf.jI * i2, jQ * lf.c2c, jQ * lf.s2c, cf.jV * fe * i2};
+        const T a4[4] = {nh * cf.aI, aQ * lf.c2c, aQ * lf.s2c, cf.aV * fa * nh};
+        const T r3[3] = {rQ * lf.c2c, rQ * lf.s2c, nh * cf.rV};
+        const T Dl = Lnu * (r * r + a * a * cth * cth) * dtau;
+        ev[6]++;
+        T O[16], E[4];
+        transfer_step(c_moments, j4, a4, r3, Dl, O, E);
+        T Pn[16];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            S[i] += P[4 * i] * E[0] + P[4 * i + 1] * E[1] + P[4 * i + 2] * E[2] + P[4 * i + 3] * E[3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                Pn[4 * i + q] = P[4 * i] * O[q] + P[4 * i + 1] * O[4 + q] + P[4 * i + 2] * O[8 + q] + P[4 * i + 3] * O[12 + q];
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) P[q] = Pn[q];
+    }
+};
+
+// One thread per ray, one frequency per grid row: out[(f npix + j) 4 + stokes] in sorted order.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_riaf(PlanView P, Spacetime st, long long npix, RiafModel m, const double* __restrict__ nus,
+                                                 double L, double* __restrict__ out, unsigned long long* __restrict__ counters) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= npix) return;
+    const int f = blockIdx.y;
+    MarchRay<double> R = load_ray<double>(P, st, j);
+    RiafSink<T> sink;
+    sink.m = m;
+    const double nh = nus[f] / kNU0;
+    sink.nu = T(nus[f]); sink.Lnu = T(L / nh);
+    sink.a = T(st.a); sink.rh_lo = T(st.rh * (1 + 1e-3)); sink.dtau = T(R.dtau);
+    sink.alpha = T(P.get(PF_ALPHA, j)); sink.beta = T(P.get(PF_BETA, j)); sink.eta = T(R.eta); sink.lam = T(R.lam);
+    sink.a_sin_tho = T(st.a * sin(st.thetao));
+    sink.init();
+    double rt, rp;
+    march(P, st, j, R, sink, rt, rp);
+    double* o = out + ((long long)f * npix + j) * 4;
+    const double n3 = nh * nh * nh;
+    o[0] = double(sink.S[0]) * n3; o[1] = double(sink.S[1]) * n3; o[2] = double(sink.S[2]) * n3; o[3] = double(sink.S[3]) * n3;
+    if (counters) {
+        atomicAdd(&counters[0], (unsigned long long)sink.ev[0]);
+        for (int q = 1; q < 7; ++q) atomicAdd(&counters[q], (unsigned long long)sink.ev[q]);
+    }
+}
+
 }  // namespace
 
 #include "ks_adjoint.cuh"
@@ -1468,6 +1655,51 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
         c->consume_timed = false;
     }
     if (precision != KS_FP64) return check_device_flag(c, "ks_render");
+    return KS_OK;
+}
+
+int ks_riaf_image(ks_context* c, const double* model, int32_t pandya, const double* nus, int32_t nfreq, double L, int32_t precision,
+                  double* out, int32_t order) {
+    if (!c || !out || !model || !nus) return KS_ERR_ARGUMENT;
+    if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
+    if (nfreq < 1) return fail(c, KS_ERR_ARGUMENT, "need at least one frequency");
+    if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
+    if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
+    if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
+    KS_CUDA(c, cudaSetDevice(c->device));
+    double hm[KS_RIAF_PARAMS];
+    KS_CUDA(c, cudaMemcpy(hm, model, sizeof hm, cudaMemcpyDefault));
+    for (double v : hm) if (!std::isfinite(v)) return fail(c, KS_ERR_NONFINITE, "non-finite RIAF parameter");
+    if (!(hm[9] > 0 && hm[8] > 0 && hm[2] > 0)) return fail(c, KS_ERR_ARGUMENT, "RIAF needs positive disk_h, r_isco and rout");
+    std::vector<double> hnu(nfreq);
+    KS_CUDA(c, cudaMemcpy(hnu.data(), nus, nfreq * sizeof(double), cudaMemcpyDefault));
+    for (double v : hnu) if (!(std::isfinite(v) && v > 0)) return fail(c, KS_ERR_NONFINITE, "frequencies must be finite and positive");
+    const RiafModel m{hm[0], hm[1], hm[2], hm[3], hm[4], hm[5], hm[6], hm[7], hm[8], hm[9], pandya != 0};
+    const long long n = c->npix;
+    KS_CUDA(c, c->combos.ensure(hnu.size() * sizeof(double)));
+    KS_CUDA(c, cudaMemcpyAsync(c->combos.p, hnu.data(), hnu.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    KS_CUDA(c, c->out_sorted.ensure(size_t(n) * 4 * nfreq * sizeof(double)));
+    if (c->count_events) {
+        KS_CUDA(c, c->counters.ensure(8 * sizeof(unsigned long long)));
+        KS_CUDA(c, cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(unsigned long long), c->stream));
+    }
+    unsigned long long* ctr = c->count_events ? c->counters.as<unsigned long long>() : nullptr;
+    cudaEventRecord(c->ev0, c->stream);
+    const dim3 grid(unsigned(nblocks(n)), unsigned(nfreq));
+    if (precision == KS_FP64)
+        k_riaf<double><<<grid, kBlock, 0, c->stream>>>(plan_view(c), c->st, n, m, c->combos.as<double>(), L, c->out_sorted.as<double>(), ctr);
+    else
+        k_riaf<float><<<grid, kBlock, 0, c->stream>>>(plan_view(c), c->st, n, m, c->combos.as<double>(), L, c->out_sorted.as<double>(), ctr);
+    cudaEventRecord(c->ev1, c->stream);
+    c->launches++;
+    c->kernel_launches++;
+    KS_CUDA(c, cudaGetLastError());
+    int s = emit(c, c->out_sorted.as<double>(), 4, nfreq, order, out);
+    if (s) return s;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->kernel_ms += ms;
     return KS_OK;
 }
 

@@ -340,7 +340,6 @@ struct MixedSink {
         pitch_sc(lf.cosB, sb, cb);
         float ne = p[ST_NE] * G;
         const float s2c = lf.s2c, c2c = lf.c2c;
-        int act = 0;
 #pragma unroll 1
         for (int c = 0; c < CH; ++c) {
             float* r = out + c * 12 * NT;   // out = res + slot; fields are NT apart
@@ -349,9 +348,11 @@ struct MixedSink {
 #pragma unroll
             for (int cc = 1; cc < CH; ++cc) nuc = (cc == c) ? nu[cc] : nuc;
             screen_coefficients_ool<KM, NT>(kind, p, ne, nuc / lf.g, sb, cb, s2c, c2c, r);
-            act |= r[11 * NT] != 0.f;
         }
-        ev[4] += act ? 1 : 0;
+        // the work events of the pair, counted as the FP64 consumer counts them: one local frame
+        // (shared by the frequencies) and one coefficient evaluation per frequency
+        ev[4] += nc;
+        ev[5] += 1;
     }
 
     // The consumer for one sample of every thread of the block (all NT threads call it together):

@@ -137,6 +137,31 @@ __device__ __forceinline__ Coef<T> thermal_cs(T ne, T Te, T f0, T kr, T B, T nu,
     return {jI, jQ, jV, jI * invB, jQ * invB, jV * invB, rQ, rV};
 }
 
+// coefficients.jl:147-169: the Pandya et al. (2016) thermal emissivities (ipole's emission_type 1) at
+// the pitch angle whose sine and cosine are st, ct; sin(theta - 28/25) by the angle-difference rule.
+template <class T>
+__device__ __forceinline__ void pandya_emissivities(T ne, T Te, T B, T nu, T st, T ct, T& jI, T& jQ, T& jV) {
+    const T PI = kpi<T>();
+    T nuc = T(kEE) * B / (T(2) * PI * T(kME) * T(kCL));
+    T nus = T(2.0 / 9.0) * nuc * st * Te * Te;
+    T X = nu / nus;
+    T pref = ne * T(kEE) * T(kEE) * nuc / T(kCL);
+    T term1 = T(1.4142135623730951) * PI / T(27) * st;
+    T x13 = fpow(X, T(1.0 / 3)), x16 = fpow(X, T(1.0 / 6)), x12 = sqrt(X);
+    const T c1112 = T(1.8877486253633868);   // 2^(11/12)
+    T ex = fexp(-x13);
+    T bi = x12 + c1112 * x16;
+    jI = pref * term1 * bi * bi * ex;
+    T te = fpow(Te, T(24.0 / 25));
+    T t2 = (T(7) * te + T(35)) / (T(10) * te + T(75));
+    T bq = x12 + t2 * c1112 * x16;
+    jQ = pref * term1 * bq * bq * ex;
+    T s28 = st * T(0.4356824462767121 /* cos(28/25) */) - ct * T(0.9001004421765051 /* sin(28/25) */);
+    T tv1 = (T(37) - T(87) * s28) / (T(100) * (Te + T(1)));
+    T tv2 = fpow(T(1) + (fpow(Te, T(3.0 / 5)) / T(25) + T(7.0 / 10)) * fpow(X, T(9.0 / 25)), T(5.0 / 3));
+    jV = pref * tv1 * tv2 * ex;
+}
+
 // coefficients.jl:208-256 (Pandya+ 2016 power-law fits, Jones & O'Dell rotativities); gamj, gama are
 // the splat's Gamma-function products, gspan = gmin^(1-p) - gmax^(1-p)
 template <class T>

@@ -1,0 +1,210 @@
+"""Parity at the five benchmark configurations' own sizes (GPU).
+
+* Configuration 1 in full (128 x 128, N = 512, 12 thin splats): the FP64 image within 1e-10 of the
+  oracle in relative L2 and per pixel, the mixed image within 1e-4.
+* Configuration 2 in full (256 x 256, N = 1024, 64 thermal splats, 86/230/345 GHz): the FP64 render
+  against the oracle on a seeded sample of 1024 rays, within 1e-10 relative Stokes L2 per pixel
+  (pixels brighter than 1e-6 of the sample's brightest; the rest within 1e-10 of that pixel's
+  scale), and the full mixed image within 1e-4 of the full FP64 image at every frequency.
+* Configuration 3: the gradient of the image-domain chi^2 (target rendered from parameters perturbed
+  by 5%, 1% pixel noise) against central finite differences with relative step 1e-6 on 200 seeded
+  parameters of the 64 x 21 scene, the FP64 renders on a 64 x 64 screen over the same field of view
+  (every splat projects onto it): the FP64 adjoint within 1e-4 per parameter (floor 1e-3 of the
+  largest component), the mixed adjoint within 1e-3 in relative L2 over the 200.
+* Configuration 4, a cut (128 x 128, two frames, the four frequencies, the uneven sample counts
+  128-2048, all 256 splats of the three populations with the knot trajectories): the mixed cube
+  within 1e-4 of the FP64 cube, and the FP64 cube against the oracle on a seeded sample of rays,
+  each at its own sample count, within 1e-10.
+* Configuration 5's transform at full size (the 1024 x 1024 image of the first parameter set, 2000
+  baselines): the FP64 direct DFT against a numpy direct sum on 64 seeded baselines within 1e-10
+  (and the adjoint transform on them), the 3xTF32 tensor-core DFT within 1e-5 of the FP64 one.
+"""
+import numpy as np
+import pytest
+
+import kerrsplat_b200 as ks
+from kerrsplat_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(x, y):
+    x, y = np.asarray(x), np.asarray(y)
+    return np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300)
+
+
+def per_pixel(got, ref):
+    """Relative Stokes L2 of every pixel (rows of (npix, 4) arrays)."""
+    nr = np.linalg.norm(ref, axis=1)
+    return np.linalg.norm(got - ref, axis=1) / np.maximum(nr, 1e-300), nr
+
+
+@pytest.fixture(scope="module")
+def threads(oracle):
+    oracle.set_threads(max(1, oracle.num_threads()))
+    return oracle
+
+
+def test_config1_full_thin_image(threads):
+    oracle = threads
+    c = scenes.config1()
+    cache = ks.GeodesicCache(c["camera"], c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
+    ref = oracle.thin_image(c["a"], c["theta_o"], c["camera"].alpha, c["camera"].beta, c["N"], c["M"], c["params"], c["t_obs"])
+    got64 = np.asarray(ks.thin_image(cache, c["params"], c["t_obs"], precision=ks.KS_FP64)).T.ravel()
+    got32 = np.asarray(ks.thin_image(cache, c["params"], c["t_obs"], precision=ks.KS_MIXED)).T.ravel()
+    lit = ref > 1e-6 * ref.max()
+    pix = np.abs(got64 - ref)[lit] / ref[lit]
+    print("config 1: FP64", rel_l2(got64, ref), "worst pixel", pix.max(), "mixed", rel_l2(got32, ref))
+    assert ref.max() > 0 and lit.sum() > 1000
+    assert rel_l2(got64, ref) < 1e-10
+    assert pix.max() < 1e-10
+    assert np.all(np.abs(got64 - ref)[~lit] < 1e-10 * ref.max())
+    assert rel_l2(got32, ref) < 1e-4
+    cache.close()
+
+
+@pytest.fixture(scope="module")
+def cfg2_full():
+    c = scenes.config2()
+    cache = ks.GeodesicCache(c["camera"], c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
+    model = ks.PolarizedSplats(c["params"])
+    out64 = np.asarray(ks.render(cache, model, [0.0], c["nus"], c["L"], precision=ks.KS_FP64))
+    out32 = np.asarray(ks.render(cache, model, [0.0], c["nus"], c["L"], precision=ks.KS_MIXED))
+    yield c, out64, out32
+    cache.close()
+
+
+def test_config2_fp64_per_pixel_on_sampled_rays(cfg2_full, threads):
+    oracle = threads
+    c, out64, _ = cfg2_full
+    cam = c["camera"]
+    rng = np.random.Generator(np.random.PCG64(1234))
+    idx = np.sort(rng.choice(cam.npix, 1024, replace=False))
+    for f, nu in enumerate(c["nus"]):
+        ref = oracle.polarized_image(c["a"], c["theta_o"], cam.alpha[idx], cam.beta[idx], c["N"], c["M"],
+                                     [("thermal", c["params"], None)], 0.0, nu, c["L"])
+        got = out64[f, 0, idx]
+        pix, nr = per_pixel(got, ref)
+        lit = nr > 1e-6 * nr.max()
+        print(f"config 2 FP64 at {nu / 1e9:.0f} GHz: {lit.sum()} lit of {idx.size}, worst lit pixel {pix[lit].max():.2e}, "
+              f"median {np.median(pix[lit]):.2e}, total {rel_l2(got, ref):.2e}")
+        assert lit.sum() > 300
+        assert pix[lit].max() < 1e-10, (nu, pix[lit].max())
+        assert np.all(np.linalg.norm(got - ref, axis=1)[~lit] < 1e-10 * nr.max())
+        assert rel_l2(got, ref) < 1e-10
+
+
+def test_config2_mixed_full_image_within_1e4_of_fp64(cfg2_full):
+    c, out64, out32 = cfg2_full
+    for f, nu in enumerate(c["nus"]):
+        tot = rel_l2(out32[f, 0], out64[f, 0])
+        per = [rel_l2(out32[f, 0, :, q], out64[f, 0, :, q]) for q in range(4)]
+        print(f"config 2 mixed vs FP64 at {nu / 1e9:.0f} GHz: total {tot:.2e}, per Stokes {np.array(per)}")
+        assert tot < 1e-4, (nu, tot)
+        assert per[0] < 1e-4, (nu, per)
+
+
+def test_config3_gradient_vs_central_differences():
+    c = scenes.config2(res=64)
+    cam, L, nus = c["camera"], c["L"], c["nus"]
+    p0 = c["params"]
+    cache = ks.GeodesicCache(cam, c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
+    # the target: every parameter moved by 5%, 1% Gaussian noise per Stokes on each pixel
+    pt, rng = scenes.config3_target(p0)
+    target = np.asarray(ks.render(cache, ks.PolarizedSplats(pt), [0.0], nus, L, precision=ks.KS_FP64))
+    sigma = 0.01 * target[..., 0].max()
+    data = target + sigma * rng.standard_normal(target.shape)
+
+    def chi2(p):
+        img = np.asarray(ks.render(cache, ks.PolarizedSplats(p), [0.0], nus, L, precision=ks.KS_FP64))
+        return float(np.sum(((img - data) / sigma) ** 2))
+
+    x64, g64 = ks.chi2_gradient(cache, ks.PolarizedSplats(p0), [0.0], nus, L, data, sigma, precision=ks.KS_FP64)
+    x32, g32 = ks.chi2_gradient(cache, ks.PolarizedSplats(p0), [0.0], nus, L, data, sigma, precision=ks.KS_MIXED)
+    g64, g32 = np.asarray(g64).reshape(p0.shape), np.asarray(g32).reshape(p0.shape)
+    assert abs(x64 - chi2(p0)) < 1e-10 * x64
+    sel = np.random.Generator(np.random.PCG64(3)).choice(p0.size, 200, replace=False)
+    rows, cols = np.unravel_index(sel, p0.shape)
+    fd = np.empty(200)
+    for k, (r, i) in enumerate(zip(rows, cols)):
+        h = 1e-6 * max(abs(p0[r, i]), 1.0)
+        pp, pm = p0.copy(), p0.copy()
+        pp[r, i] += h
+        pm[r, i] -= h
+        fd[k] = (chi2(pp) - chi2(pm)) / (2 * h)
+    a64, a32 = g64[rows, cols], g32[rows, cols]
+    floor = 1e-3 * np.abs(fd).max()
+    err64 = np.abs(a64 - fd) / (np.abs(fd) + floor)
+    print(f"config 3: chi2 {x64:.6e}, FP64 adjoint vs FD worst {err64.max():.2e} median {np.median(err64):.2e}; "
+          f"mixed vs FD rel L2 {rel_l2(a32, fd):.2e}; mixed vs FP64 over all 1344 {rel_l2(g32, g64):.2e}")
+    assert err64.max() < 1e-4, (err64.max(), rows[err64.argmax()], cols[err64.argmax()])
+    assert rel_l2(a32, fd) < 1e-3
+    assert rel_l2(g32, g64) < 1e-3
+    cache.close()
+
+
+def test_config4_cut_uneven_movie(threads):
+    oracle = threads
+    c = scenes.config4(res=128, nframes=2)
+    cam, L, nus, times = c["camera"], c["L"], c["nus"], c["times"]
+    cache = ks.GeodesicCache(cam, c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"], uneven=(c["density"], c["nmin"]))
+    kap = ks.KappaSplats(c["kappa"])
+    model = ks.CompositeModel(ks.KnotSplats(c["thermal"], c["knots"], c["knot_times"]), ks.PowerLawSplats(c["powerlaw"]), kap)
+    out64 = np.asarray(ks.render(cache, model, times, nus, L, precision=ks.KS_FP64))
+    out32 = np.asarray(ks.render(cache, model, times, nus, L, precision=ks.KS_MIXED))
+    errs = {(v, f): rel_l2(out32[v, f], out64[v, f]) for v in range(len(nus)) for f in range(len(times))}
+    print("config 4 cut, mixed vs FP64:", errs)
+    assert max(errs.values()) < 1e-4, errs
+    # FP64 against the oracle on sampled rays, each at its own sample count
+    nsorted = cache.nsamples_per_ray
+    nscreen = np.empty_like(nsorted)
+    nscreen[cache.perm] = nsorted
+    assert nscreen.min() >= 128 and nscreen.max() <= 2048 and np.unique(nscreen).size > 4
+    idx = np.sort(np.random.Generator(np.random.PCG64(44)).choice(cam.npix, 160, replace=False))
+    sets = [("knot", c["thermal"], None, c["knots"], c["knot_times"]), ("powerlaw", c["powerlaw"], None), ("kappa", c["kappa"], kap.hyp)]
+    for v in (0, 3):
+        ref = np.zeros((idx.size, 4))
+        for Nj in np.unique(nscreen[idx]):
+            m = nscreen[idx] == Nj
+            ref[m] = oracle.polarized_image(c["a"], c["theta_o"], cam.alpha[idx][m], cam.beta[idx][m], int(Nj), c["M"], sets,
+                                            times[1], nus[v], L)
+        got = out64[v, 1, idx]
+        pix, nr = per_pixel(got, ref)
+        lit = nr > 1e-6 * nr.max()
+        print(f"config 4 FP64 vs oracle at {nus[v] / 1e9:.0f} GHz: total {rel_l2(got, ref):.2e}, worst lit pixel {pix[lit].max():.2e}")
+        assert lit.sum() > 20
+        assert rel_l2(got, ref) < 1e-10
+        assert pix[lit].max() < 1e-10
+    cache.close()
+
+
+def test_config5_full_size_transform(threads):
+    c = scenes.config5()
+    cam = c["camera"]
+    cache = ks.GeodesicCache(cam, c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
+    img = np.asarray(ks.render(cache, ks.PolarizedSplats(c["sets"][0]), [c["t_obs"]], [c["nu"]], c["L"], precision=ks.KS_MIXED))[0, 0]
+    assert img[:, 0].max() > 0
+    u, v, psize, scale = c["u"], c["v"], c["psize"], c["scale"]
+    V64 = ks.visibilities(cache, img, u, v, psize, scale, precision=ks.KS_FP64)
+    V32 = ks.visibilities(cache, img, u, v, psize, scale, precision=ks.KS_MIXED)
+    sub = np.sort(np.random.Generator(np.random.PCG64(55)).choice(u.size, 64, replace=False))
+    ref = threads.visibilities(img, *cam.size, u[sub], v[sub], None, psize, scale)
+    print(f"config 5 DFT: FP64 vs numpy on 64 baselines {rel_l2(V64[sub], ref):.2e}; 3xTF32 vs FP64 {rel_l2(V32, V64):.2e}")
+    assert rel_l2(V64[sub], ref) < 1e-10
+    assert rel_l2(V32, V64) < 1e-5
+    # the adjoint transform, weights on the sampled baselines only
+    rng = np.random.Generator(np.random.PCG64(56))
+    w = np.zeros((u.size, 4), dtype=complex)
+    w[sub] = rng.standard_normal((64, 4)) + 1j * rng.standard_normal((64, 4))
+    s64 = ks.vis_seed(cache, w, u, v, psize, scale, precision=ks.KS_FP64)
+    sref = threads.vis_seed(w[sub], *cam.size, u[sub], v[sub], None, psize, scale)
+    s32 = ks.vis_seed(cache, w, u, v, psize, scale, precision=ks.KS_MIXED)
+    print(f"config 5 adjoint DFT: FP64 vs numpy {rel_l2(s64, sref):.2e}; 3xTF32 vs FP64 {rel_l2(s32, s64):.2e}")
+    assert rel_l2(s64, sref) < 1e-10
+    assert rel_l2(s32, s64) < 1e-5
+    cache.close()
