@@ -9,7 +9,11 @@ Two kinds of fixtures:
    * validation/ipole_riaf/riaf_{fine,2thz}_{I,Q,U,V}.csv, ipole's full-Stokes images of its
      example RIAF at 230 GHz and 2 THz (100 x 100, row = x index, column = y index), which
      test/test_polarized.jl:156-178 compares KerrSplat's images against: all eight arrays as float64
-     in one compressed file, ipole_riaf.npz (keys "fine_I" ... "2thz_V").
+     in one compressed file, ipole_riaf.npz (keys "fine_I" ... "2thz_V");
+   * test/data/synth_eht2017{,_noiseless}.uvfits, their parses by ehtim (*_ehtim.csv) and the source
+     image synth_eht2017_image.fits, which test/test_uvfits.jl pins the uvfits reader, the FITS
+     image reader and the sky conventions of the transform against: copied unchanged into
+     tests/golden/uvfits/.
 2. High-precision references restated in mpmath (the reference's own BigFloat references are
    Julia, test/highprec_reference.jl and test/test_transfer_step.jl):
    * r(tau), theta(tau) from the closed forms with Newton-polished roots (highprec_reference.jl:22-156);
@@ -76,6 +80,18 @@ def extract_ipole_riaf():
         for st in "IQUV":
             arrays[f"{tag}_{st}"] = np.loadtxt(os.path.join(src, f"riaf_{tag}_{st}.csv"), delimiter=",", dtype=np.float64)
     np.savez_compressed(os.path.join(HERE, "ipole_riaf.npz"), **arrays)
+
+
+UVFITS = ["synth_eht2017.uvfits", "synth_eht2017_noiseless.uvfits", "synth_eht2017_ehtim.csv", "synth_eht2017_noiseless_ehtim.csv",
+          "synth_eht2017_image.fits"]
+
+
+def copy_uvfits():
+    import shutil
+    dst = os.path.join(HERE, "uvfits")
+    os.makedirs(dst, exist_ok=True)
+    for name in UVFITS:
+        shutil.copyfile(os.path.join(reference_root(), "test", "data", name), os.path.join(dst, name))
 
 
 # ---- 2. geodesics in mpmath -----------------------------------------------------------------------
@@ -334,11 +350,13 @@ if __name__ == "__main__":
         i = args.index("--reference")
         REFERENCE_ROOT = args[i + 1]
         del args[i:i + 2]
-    what = args or ["symphony", "ipole", "special", "step", "geodesic", "anchor"]
+    what = args or ["symphony", "ipole", "uvfits", "special", "step", "geodesic", "anchor"]
     if "symphony" in what:
         extract_symphony()
     if "ipole" in what:
         extract_ipole_riaf()
+    if "uvfits" in what:
+        copy_uvfits()
     if "special" in what:
         special_fixtures()
     if "step" in what:

@@ -68,3 +68,24 @@ def test_seed_and_chi2_match_oracle(dft_case, oracle, prec, tol):
     x, s = ks.frame_chi2_seed(c["cache"], c["img"], c["u"], c["v"], Vt, sigma, c["psize"], c["scale"], tap=c["tap"], gains=gains, precision=prec)
     assert abs(x - x_ref) / x_ref < tol * 10
     assert rel(s, s_ref) < tol * 10
+
+
+@pytest.mark.parametrize("prec,tol", [(ks.KS_FP64, 5e-7), (ks.KS_MIXED, 2e-5)])
+def test_transform_of_ehtim_source_image_matches_its_observation(prec, tol):
+    """The GPU transform (FP64 direct and 3xTF32) of the ehtim observation's source image against the
+    observation's noiseless visibilities (the sky conventions, east = -alpha, pinned against an
+    independent code: test/test_uvfits.jl), in Jy with scale 1."""
+    import os
+    from kerrsplat_b200 import fitsio
+    d = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "uvfits")
+    img, hdr = fitsio.read_stokes_fits(os.path.join(d, "synth_eht2017_image.fits"))
+    psize = hdr["psize_deg"] * np.pi / 180
+    clean = fitsio.read_uvfits(os.path.join(d, "synth_eht2017_noiseless.uvfits"))
+    cam = ks.Camera((-16.0, 16.0), (-16.0, 16.0), 32)
+    cache = ks.GeodesicCache(cam, 8)
+    ks.regenerate(cache, 0.5, np.deg2rad(30.0))
+    V = ks.visibilities(cache, img.reshape(32 * 32, 4, order="F"), clean.u, clean.v, psize, 1.0, precision=prec)
+    err = np.max(np.abs(V - clean.vis))
+    print("GPU transform of the source image vs the noiseless observation", prec, err)
+    assert err < tol
+    cache.close()
