@@ -895,18 +895,14 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
             for (long long q = lane; q < gsz; q += 32) gacc[q] = 0.f;
         {
             // the unit's bounds and candidate splats (as the forward pass)
-            UnitBox b{3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f};
+            UnitBox b = unit_box_empty();
             const int nsamp = int(plan_f[(long long)PF_NSAMP * npad + U.j]);
             for (int k = U.k0; k < U.k1; ++k) {
                 const float* bp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
                 if (!U.live || k > nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
-                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
-                const float rho = sqrtf(x * x + y * y);
-                b.xlo = fminf(b.xlo, x); b.xhi = fmaxf(b.xhi, x); b.ylo = fminf(b.ylo, y); b.yhi = fmaxf(b.yhi, y);
-                b.zlo = fminf(b.zlo, z); b.zhi = fmaxf(b.zhi, z); b.rlo = fminf(b.rlo, rho); b.rhi = fmaxf(b.rhi, rho);
+                unit_box_add(b, bp[SM_X * npad], bp[SM_Y * npad], bp[SM_Z * npad], t_obs - bp[SM_T * npad]);
             }
-            b.xlo = warp_min(b.xlo); b.xhi = warp_max(b.xhi); b.ylo = warp_min(b.ylo); b.yhi = warp_max(b.yhi);
-            b.zlo = warp_min(b.zlo); b.zhi = warp_max(b.zhi); b.rlo = warp_min(b.rlo); b.rhi = warp_max(b.rhi);
+            unit_box_reduce(b);
             unit_candidates(tab, ntot, b, lane, cand);
         }
         for (int k = U.k0; k < U.k1; ++k) {

@@ -30,12 +30,23 @@ constexpr int kSF = SF_COUNT;                   // floats per lane of sample dat
 constexpr int kMaxSplatWords = 16;              // candidate masks cover up to 512 splats
 constexpr int kGroupWords = 8;                  // candidate words tested before one evaluation list
 
-// The bounds of a work unit's samples (quasi-Cartesian KS box, cylindrical radius and height) and the
-// splats whose support can reach them: a pattern-rotating splat's support lies within its support
-// radius of the circle its centre runs on (rho = ST_RHO, z = ST_CZ), a knot splat's within its
-// bounding sphere (centre ST_CX..CZ, radius^2 ST_RHO). Splats outside are below the weight cutoff at
-// every sample of the unit, so the per-sample tests skip them (the same result, fewer tests).
-struct UnitBox { float xlo, xhi, ylo, yhi, zlo, zhi, rlo, rhi; };
+// The bounds of a work unit's samples (quasi-Cartesian KS box, cylindrical radius and height, and the
+// range of their emission times t = t_obs - t~) and the splats whose support can reach them: a
+// pattern-rotating splat's support lies within its support radius of the circle its centre runs on
+// (rho = ST_RHO, z = ST_CZ), and within it of the arc its centre covers over the unit's emission times
+// (the centre's angle is phi_0 + omega (t - t0)); a knot splat's within its bounding sphere (centre
+// ST_CX..CZ, radius^2 ST_RHO). Splats outside are below the weight cutoff at every sample of the unit,
+// so the per-sample tests skip them (the same result, fewer tests).
+struct UnitBox { float xlo, xhi, ylo, yhi, zlo, zhi, rlo, rhi, tlo, thi; };
+
+// Widen the unit box with one sample (position, cylindrical radius, emission time).
+__device__ __forceinline__ void unit_box_add(UnitBox& b, float x, float y, float z, float t) {
+    const float rho = sqrtf(x * x + y * y);
+    b.xlo = fminf(b.xlo, x); b.xhi = fmaxf(b.xhi, x); b.ylo = fminf(b.ylo, y); b.yhi = fmaxf(b.yhi, y);
+    b.zlo = fminf(b.zlo, z); b.zhi = fmaxf(b.zhi, z); b.rlo = fminf(b.rlo, rho); b.rhi = fmaxf(b.rhi, rho);
+    b.tlo = fminf(b.tlo, t); b.thi = fmaxf(b.thi, t);
+}
+__device__ __forceinline__ UnitBox unit_box_empty() { return {3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f}; }
 
 __device__ __forceinline__ float warp_min(float v) {
 #pragma unroll
@@ -46,6 +57,34 @@ __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
     for (int d = 16; d >= 1; d >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, d));
     return v;
+}
+
+// The box of the arc a pattern-rotating splat's centre covers while its rotation angle runs over
+// [lo, hi] (relative to the centre's angle at t0), widened by `pad`: the end points and the axis
+// extremes the arc passes. False when the arc is not shorter than a turn (then only the circle bounds).
+__device__ __forceinline__ bool arc_box(const float* p, float lo, float hi, float pad, float& xlo, float& xhi, float& ylo, float& yhi) {
+    if (!(hi - lo < 6.0f)) return false;
+    const float rho = p[ST_RHO];
+    const float a0 = atan2f(p[ST_CY], p[ST_CX]);
+    const float A = a0 + lo, B = a0 + hi;
+    float sa, ca, sb, cb;
+    sincosf(A, &sa, &ca);
+    sincosf(B, &sb, &cb);
+    xlo = rho * fminf(ca, cb); xhi = rho * fmaxf(ca, cb); ylo = rho * fminf(sa, sb); yhi = rho * fmaxf(sa, sb);
+    // the axis directions 0, pi/2, pi, 3 pi/2 (+ 2 pi k) inside [A, B] (with a margin: conservative)
+    const float two_pi = 6.283185307179586f, m = 1e-3f;
+    for (int q = 0; q < 4; ++q) {
+        const float d = q * 1.5707963267948966f;
+        const float k = ceilf((A - m - d) / two_pi);
+        if (d + two_pi * k <= B + m) {
+            if (q == 0) xhi = rho;
+            else if (q == 1) yhi = rho;
+            else if (q == 2) xlo = -rho;
+            else ylo = -rho;
+        }
+    }
+    xlo -= pad; xhi += pad; ylo -= pad; yhi += pad;
+    return true;
 }
 
 // the candidate mask words of a unit (all lanes call it; cand gets ceil(ntot / 32) words)
@@ -64,12 +103,29 @@ __device__ __forceinline__ void unit_candidates(const float* tab, int ntot, cons
                 const float dr = fmaxf(fmaxf(b.rlo - p[ST_RHO], p[ST_RHO] - b.rhi), 0.f);
                 const float dz = fmaxf(fmaxf(b.zlo - p[ST_CZ], p[ST_CZ] - b.zhi), 0.f);
                 keep = dr * dr + dz * dz <= p[ST_SUPP] * 1.0001f;
+                float xlo, xhi, ylo, yhi;
+                const float om = p[ST_OMEGA];
+                const float pa = om * (b.tlo - p[ST_T0]), pb = om * (b.thi - p[ST_T0]);
+                // the pad covers the FP32 rounding of the angles (phases up to ~1e3 rad) and positions
+                const float pad = 1e-3f * p[ST_RHO] + 1e-4f * (fabsf(pa) + fabsf(pb)) * p[ST_RHO] + 1e-3f;
+                if (keep && b.tlo <= b.thi && arc_box(p, fminf(pa, pb), fmaxf(pa, pb), pad, xlo, xhi, ylo, yhi)) {
+                    const float dx = fmaxf(fmaxf(b.xlo - xhi, xlo - b.xhi), 0.f);
+                    const float dy = fmaxf(fmaxf(b.ylo - yhi, ylo - b.yhi), 0.f);
+                    keep = dx * dx + dy * dy + dz * dz <= p[ST_SUPP] * 1.0001f;
+                }
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) cand[s0 >> 5] = m;
     }
     __syncwarp();
+}
+
+// The warp's union of its lanes' boxes.
+__device__ __forceinline__ void unit_box_reduce(UnitBox& b) {
+    b.xlo = warp_min(b.xlo); b.xhi = warp_max(b.xhi); b.ylo = warp_min(b.ylo); b.yhi = warp_max(b.yhi);
+    b.zlo = warp_min(b.zlo); b.zhi = warp_max(b.zhi); b.rlo = warp_min(b.rlo); b.rhi = warp_max(b.rhi);
+    b.tlo = warp_min(b.tlo); b.thi = warp_max(b.thi);
 }
 
 // ---- TMA bulk staging ----------------------------------------------------------------------------
@@ -288,6 +344,7 @@ struct MixedSink {
     }
 
     __device__ int scan(int v, int& total) { return block_exscan<NT>(v, total, wsum, scan_par); }
+
 
     // The evaluation class of a pair: 0 thermal, 1 knot (thermal coefficients, knot centre), 2 power
     // law, 3 kappa; 4 for a thread without a pair this round.
@@ -741,17 +798,13 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const float* __restrict__ tab3
         sink.init();
         {
             // the unit's bounds and candidate splats
-            UnitBox b{3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f, 3e38f, -3e38f};
+            UnitBox b = unit_box_empty();
             const float* bp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
             for (int k = k0; k < k1; ++k, bp += SM_COUNT * npad) {
                 if (!live || k > sink.nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
-                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
-                const float rho = sqrtf(x * x + y * y);
-                b.xlo = fminf(b.xlo, x); b.xhi = fmaxf(b.xhi, x); b.ylo = fminf(b.ylo, y); b.yhi = fmaxf(b.yhi, y);
-                b.zlo = fminf(b.zlo, z); b.zhi = fmaxf(b.zhi, z); b.rlo = fminf(b.rlo, rho); b.rhi = fmaxf(b.rhi, rho);
+                unit_box_add(b, bp[SM_X * npad], bp[SM_Y * npad], bp[SM_Z * npad], sink.t_obs - bp[SM_T * npad]);
             }
-            b.xlo = warp_min(b.xlo); b.xhi = warp_max(b.xhi); b.ylo = warp_min(b.ylo); b.yhi = warp_max(b.yhi);
-            b.zlo = warp_min(b.zlo); b.zhi = warp_max(b.zhi); b.rlo = warp_min(b.rlo); b.rhi = warp_max(b.rhi);
+            unit_box_reduce(b);
             unit_candidates(tab, ntot, b, lane, cand);
         }
         const float* sp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;

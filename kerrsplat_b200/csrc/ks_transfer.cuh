@@ -58,6 +58,19 @@ __device__ __forceinline__ float fexp(float x) { return __expf(x); }
 __device__ __forceinline__ double fexp(double x) { return exp(x); }
 __device__ __forceinline__ float flog(float x) { return __logf(x); }
 __device__ __forceinline__ double flog(double x) { return log(x); }
+// Sine and cosine of a phase. FP32: the argument is reduced by 2 pi split in two floats (Cody & Waite
+// 1980; 2 pi = 6.2831854820251465 - 1.7484555314695172e-7 to FP32's precision twice) and the hardware
+// approximations run on [-pi, pi] (absolute error ~4e-7, below the FP32 rounding of the phases these
+// take, a few to a thousand radians). FP64 and dual numbers: the library functions.
+__device__ __forceinline__ float freduce(float x) {
+    const float k = rintf(x * 0.15915494309189535f);
+    const float r = fmaf(-k, 6.2831854820251465f, x);
+    return fmaf(-k, -1.7484555314695172e-7f, r);
+}
+__device__ __forceinline__ void fsincos(float x, float& s, float& c) { __sincosf(freduce(x), &s, &c); }
+__device__ __forceinline__ float fcos(float x) { return __cosf(freduce(x)); }
+template <class T> __device__ __forceinline__ void fsincos(const T& x, T& s, T& c) { s = sin(x); c = cos(x); }
+template <class T> __device__ __forceinline__ T fcos(const T& x) { return cos(x); }
 // the same for dual numbers (the adjoint's forward-mode derivatives)
 template <class T, int N> __device__ __forceinline__ Dual<T, N> fexp(const Dual<T, N>& x) { T e = fexp(x.v); return dchain(x, e, e); }
 template <class T, int N> __device__ __forceinline__ Dual<T, N> flog(const Dual<T, N>& x) { return dchain(x, flog(x.v), T(1) / x.v); }
@@ -118,7 +131,7 @@ __device__ __forceinline__ Coef<T> thermal_cs(T ne, T Te, T f0, T kr, T B, T nu,
     }
     T extraterm = (T(0.011) * fexp(-x / T(47.2)) - T(7.9370052598409974e-01 /* 2^(-1/3) */) / T(67.44733739010397 /* 3^(23/6) */) * PI * T(1e4) * fpow(x + T(1e-16), T(-8.0 / 3))) *
                   sw;
-    T jffunc = T(2.011) * fexp(-fpow(x, T(1.035)) / T(4.7)) - cos(x / T(2)) * fexp(-fpow(x, T(1.2)) / T(2.73)) - T(0.011) * fexp(-x / T(47.2)) + extraterm;
+    T jffunc = T(2.011) * fexp(-fpow(x, T(1.035)) / T(4.7)) - fcos(x / T(2)) * fexp(-fpow(x, T(1.2)) / T(2.73)) - T(0.011) * fexp(-x / T(47.2)) + extraterm;
     T eps11m22 = jffunc * wp2w2 * w0w * w0w * (kr + T(6) * Te) * st * st;
     T rQ = w / (T(2) * T(kCL)) * eps11m22;
     T ff = f0 * (T(1) - T(0.11) * flog(T(1) + T(0.035) * x));
@@ -742,7 +755,8 @@ __device__ __forceinline__ void transfer_step_structured(const MomentCoeffs& MC,
 template <class T>
 __device__ __forceinline__ bool splat_exponent(const T* p, T t, T x, T y, T z, bool cull, T& q) {
     T ph = p[ST_OMEGA] * (t - p[ST_T0]);
-    T sp = sin(ph), cp = cos(ph);
+    T sp, cp;
+    fsincos(ph, sp, cp);
     T cx = p[ST_CX] * cp - p[ST_CY] * sp, cy = p[ST_CX] * sp + p[ST_CY] * cp;
     T d0 = x - cx, d1 = y - cy, d2 = z - p[ST_CZ];
     if (cull && d0 * d0 + d1 * d1 + d2 * d2 > p[ST_SUPP]) return false;
