@@ -411,7 +411,8 @@ struct ThinSink {
 
 template <class T>
 __global__ void k_thin(PlanView P, Spacetime st, long long npix, const double* __restrict__ tab64, int nsplat, double t_obs,
-                       double* __restrict__ out, double* __restrict__ resid_t, double* __restrict__ resid_phi) {
+                       const long long* __restrict__ perm, double* __restrict__ out, double* __restrict__ resid_t,
+                       double* __restrict__ resid_phi) {
     extern __shared__ __align__(16) unsigned char smem[];
     T* tab = reinterpret_cast<T*>(smem);
     for (int q = threadIdx.x; q < nsplat * ST_COUNT; q += blockDim.x) tab[q] = T(tab64[q]);
@@ -422,34 +423,17 @@ __global__ void k_thin(PlanView P, Spacetime st, long long npix, const double* _
     ThinSink<T> sink{tab, nsplat, T(t_obs), T(st.a), T(st.rh * (1 + 1e-3)), T(R.dtau), T(0), R.eta, R.lam};
     double rt, rp;
     march(P, st, j, R, sink, rt, rp);
-    out[j] = double(sink.acc);
+    out[perm ? perm[j] : j] = double(sink.acc);   // sorted order, or screen order through the permutation
     if (resid_t) { resid_t[j] = rt; resid_phi[j] = rp; }
 }
 
 // The allocation-free thin-image variant (ks_thin_image_noalloc) keeps its splat table in this
-// file-scope device array instead of a context buffer. Every GPU that loads the library holds it until
-// the process exits; every call overwrites the first nsplat rows before reading them; calls that
-// overlap on the GPU (two streams, two host threads) share it and race.
+// file-scope device array instead of a context buffer and runs k_thin with the image written straight
+// into the caller's buffer. Every GPU that loads the library holds the array until the process exits;
+// every call overwrites the first nsplat rows before reading them; calls that overlap on the GPU (two
+// streams, two host threads) share it and race.
 constexpr int kNoAllocMaxSplats = 256;
 static __device__ __align__(256) double g_noalloc_tab[kNoAllocMaxSplats * ST_COUNT];
-
-// k_thin, with the image written straight into the caller's buffer (in sorted or screen order
-// through the permutation) so that no intermediate device buffer is needed.
-template <class T>
-__global__ void k_thin_noalloc(PlanView P, Spacetime st, long long npix, const double* __restrict__ tab64, int nsplat, double t_obs,
-                               const long long* __restrict__ perm, double* __restrict__ out) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    T* tab = reinterpret_cast<T*>(smem);
-    for (int q = threadIdx.x; q < nsplat * ST_COUNT; q += blockDim.x) tab[q] = T(tab64[q]);
-    __syncthreads();
-    long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (j >= npix) return;
-    MarchRay<T> R = load_ray<T>(P, st, j);
-    ThinSink<T> sink{tab, nsplat, T(t_obs), T(st.a), T(st.rh * (1 + 1e-3)), T(R.dtau), T(0), R.eta, R.lam};
-    double rt, rp;
-    march(P, st, j, R, sink, rt, rp);
-    out[perm ? perm[j] : j] = double(sink.acc);
-}
 
 // RadiativeTransport over a concatenated splat table (transport.jl:171-198, polarized.jl:121-150,
 // populations.jl:70-104), CH (t_obs, nu) combinations per thread sharing the march.
@@ -1553,11 +1537,11 @@ int ks_thin_image(ks_context* c, const double* params, int32_t nsplat, double t_
     cudaEventRecord(c->ev0, c->stream);
     if (precision == KS_FP64) {
         KS_CUDA(c, cudaFuncSetAttribute(k_thin<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_thin<double><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, c->tab.as<double>(), nsplat, t_obs,
+        k_thin<double><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, c->tab.as<double>(), nsplat, t_obs, nullptr,
                                                                  c->out_sorted.as<double>(), c->resid_t.as<double>(), c->resid_phi.as<double>());
     } else {
         KS_CUDA(c, cudaFuncSetAttribute(k_thin<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_thin<float><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, c->tab.as<double>(), nsplat, t_obs,
+        k_thin<float><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, c->tab.as<double>(), nsplat, t_obs, nullptr,
                                                                 c->out_sorted.as<double>(), nullptr, nullptr);
     }
     cudaEventRecord(c->ev1, c->stream);
@@ -2743,11 +2727,11 @@ int ks_thin_image_noalloc(ks_context* c, const double* params, int32_t nsplat, d
     const long long* perm = order == KS_ORDER_SCREEN ? c->perm.as<long long>() : nullptr;
     const size_t smem = size_t(nsplat) * ST_COUNT * (precision == KS_FP64 ? sizeof(double) : sizeof(float));
     if (precision == KS_FP64) {
-        KS_CUDA(c, cudaFuncSetAttribute(k_thin_noalloc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_thin_noalloc<double><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, tab, nsplat, t_obs, perm, out);
+        KS_CUDA(c, cudaFuncSetAttribute(k_thin<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_thin<double><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, tab, nsplat, t_obs, perm, out, nullptr, nullptr);
     } else {
-        KS_CUDA(c, cudaFuncSetAttribute(k_thin_noalloc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_thin_noalloc<float><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, tab, nsplat, t_obs, perm, out);
+        KS_CUDA(c, cudaFuncSetAttribute(k_thin<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_thin<float><<<nblocks(n), kBlock, smem, c->stream>>>(plan_view(c), c->st, n, tab, nsplat, t_obs, perm, out, nullptr, nullptr);
     }
     c->launches++;
     KS_CUDA(c, cudaGetLastError());

@@ -217,155 +217,107 @@ __device__ __forceinline__ JS<T> load_js(const double* rec, int off) {
     return {T(rec[off]), T(rec[off + 1]), T(rec[off + 2])};
 }
 
-// March ray j with its N samples and call f(k, sample) for k = 1..N; returns the largest anchor residuals.
-template <class T, class F>
-__device__ __forceinline__ void march(const PlanView& P, const Spacetime& st, long long j, const MarchRay<T>& R,
-                                      F& f, double& resid_t, double& resid_phi) {
-    const int N = R.nsamp;
-    (void)st;
-    const double dtau = R.dtau;
-    const double h = dtau / 2.0;
-    const double* A0 = P.anchors + R.anchor_off * AF_COUNT;
-    JS<T> xr = load_js<T>(A0, AF_XR_SN), xt = load_js<T>(A0, AF_XT_SN);
-    Point<T> pa = ray_point(R, xr, xt, dtau);
-    T pca = polar_closed(R, dtau, pa.sn, pa.cn);
-    T t = T(A0[AF_T]), phi = T(A0[AF_PHI]);
+// March samples [k_begin, k_end) of ray j and call f(k, sample) for each (quadrature.jl:231-296): the
+// march starts at the last anchor at or before k_begin (its Jacobi states, t~ and phi from the table)
+// and runs silently up to k_begin, so the lanes of a warp call f the same number of times whatever
+// their anchor spacing. At every anchor the quadrature's t~ and phi are replaced by the anchor's; with
+// RESID the largest |quadrature - anchor| of the ray (cache.residual_t / residual_phi) is tracked.
+template <bool RESID, class T, class F>
+__device__ __forceinline__ void march_impl(const PlanView& P, long long j, const MarchRay<T>& R, F& f, int k_begin, int k_end,
+                                           double& resid_t, double& resid_phi) {
     double rt = 0.0, rphi = 0.0;
-    {
-        Sample<T> s{t, pa.r, pa.theta, pa.cth, phi, pa.nur, pa.nuth, (dtau <= R.tau_valid) && visible(R, pa.cth)};
-        f(1, s);
-    }
-    int next_anchor = 1 + R.Manchor;   // sample index of the next anchor
-    int m = 1;
-    for (int k = 2; k <= N; ++k) {
-        double ta = (k - 1) * dtau, tb = k * dtau;
-        xr = jstep(xr, R.dr, R.k);
-        xt = jstep(xt, R.dth, R.pmu);
-        Point<T> pm = ray_point(R, xr, xt, ta + h);
-        const bool anchor = (k == next_anchor);
-        const double* Am = P.anchors + (R.anchor_off + m) * AF_COUNT;
-        if (anchor) {
-            xr = load_js<T>(Am, AF_XR_SN); xt = load_js<T>(Am, AF_XT_SN);
-        } else {
+    if (k_end > R.nsamp + 1) k_end = R.nsamp + 1;
+    if (k_begin < k_end) {
+        const double dtau = R.dtau;
+        const double h = dtau / 2.0;
+        int m = (k_begin - 1) / R.Manchor;
+        if (m > R.nanch - 1) m = R.nanch - 1;
+        const int ka = 1 + m * R.Manchor;
+        const double* A0 = P.anchors + (R.anchor_off + m) * AF_COUNT;
+        JS<T> xr = load_js<T>(A0, AF_XR_SN), xt = load_js<T>(A0, AF_XT_SN);
+        Point<T> pa = ray_point(R, xr, xt, ka * dtau);
+        T pca = polar_closed(R, ka * dtau, pa.sn, pa.cn);
+        T t = T(A0[AF_T]), phi = T(A0[AF_PHI]);
+        if (ka >= k_begin) {
+            Sample<T> s{t, pa.r, pa.theta, pa.cth, phi, pa.nur, pa.nuth, (ka * dtau <= R.tau_valid) && visible(R, pa.cth)};
+            f(ka, s);
+        }
+        int next_anchor = ka + R.Manchor;
+        ++m;
+        for (int k = ka + 1; k < k_end; ++k) {
+            double ta = (k - 1) * dtau, tb = k * dtau;
             xr = jstep(xr, R.dr, R.k);
             xt = jstep(xt, R.dth, R.pmu);
-        }
-        Point<T> pb = ray_point(R, xr, xt, tb);
-        T pcb = polar_closed(R, tb, pb.sn, pb.cn);
-        if (k == R.turn_k) {
-            const double* pf = P.f;
-            const long long np = P.npad;
-            JS<T> p1r = {T(pf[PF_P1R_SN * np + j]), T(pf[PF_P1R_CN * np + j]), T(pf[PF_P1R_DN * np + j])};
-            JS<T> p1t = {T(pf[PF_P1T_SN * np + j]), T(pf[PF_P1T_CN * np + j]), T(pf[PF_P1T_DN * np + j])};
-            JS<T> p2r = {T(pf[PF_P2R_SN * np + j]), T(pf[PF_P2R_CN * np + j]), T(pf[PF_P2R_DN * np + j])};
-            JS<T> p2t = {T(pf[PF_P2T_SN * np + j]), T(pf[PF_P2T_CN * np + j]), T(pf[PF_P2T_DN * np + j])};
-            JS<T> ptt = {T(pf[PF_PTT_SN * np + j]), T(pf[PF_PTT_CN * np + j]), T(pf[PF_PTT_DN * np + j])};
-            double fo = R.fo_d;
-            Point<T> pt = turning_point(R, ptt);
-            Point<T> p1 = ray_point(R, p1r, p1t, (ta + fo) / 2.0);
-            Point<T> p2 = ray_point(R, p2r, p2t, (fo + tb) / 2.0);
-            T pct = polar_closed(R, fo, pt.sn, pt.cn);
-            T It1, Ip1, It2, Ip2;
-            increment(R, pa, p1, pt, ta, fo, pca, pct, It1, Ip1);
-            increment(R, pt, p2, pb, fo, tb, pct, pcb, It2, Ip2);
-            t += It1 + It2; phi += Ip1 + Ip2;
-        } else {
-            T It, Ip;
-            increment(R, pa, pm, pb, ta, tb, pca, pcb, It, Ip);
-            t += It; phi += Ip;
-        }
-        if (anchor) {
-            if (Am[AF_OK] != 0.0) {
-                double at = Am[AF_T], ap = Am[AF_PHI];
-                rt = fmax(rt, fabs(double(t) - at));
-                rphi = fmax(rphi, fabs(double(phi) - ap));
-                t = T(at); phi = T(ap);
+            Point<T> pm = ray_point(R, xr, xt, ta + h);
+            const bool anchor = (k == next_anchor);
+            const double* Am = P.anchors + (R.anchor_off + m) * AF_COUNT;
+            if (anchor) {
+                xr = load_js<T>(Am, AF_XR_SN); xt = load_js<T>(Am, AF_XT_SN);
+            } else {
+                xr = jstep(xr, R.dr, R.k);
+                xt = jstep(xt, R.dth, R.pmu);
             }
-            ++m;
-            next_anchor += R.Manchor;
+            Point<T> pb = ray_point(R, xr, xt, tb);
+            T pcb = polar_closed(R, tb, pb.sn, pb.cn);
+            if (k == R.turn_k) {
+                const double* pf = P.f;
+                const long long np = P.npad;
+                JS<T> p1r = {T(pf[PF_P1R_SN * np + j]), T(pf[PF_P1R_CN * np + j]), T(pf[PF_P1R_DN * np + j])};
+                JS<T> p1t = {T(pf[PF_P1T_SN * np + j]), T(pf[PF_P1T_CN * np + j]), T(pf[PF_P1T_DN * np + j])};
+                JS<T> p2r = {T(pf[PF_P2R_SN * np + j]), T(pf[PF_P2R_CN * np + j]), T(pf[PF_P2R_DN * np + j])};
+                JS<T> p2t = {T(pf[PF_P2T_SN * np + j]), T(pf[PF_P2T_CN * np + j]), T(pf[PF_P2T_DN * np + j])};
+                JS<T> ptt = {T(pf[PF_PTT_SN * np + j]), T(pf[PF_PTT_CN * np + j]), T(pf[PF_PTT_DN * np + j])};
+                double fo = R.fo_d;
+                Point<T> pt = turning_point(R, ptt);
+                Point<T> p1 = ray_point(R, p1r, p1t, (ta + fo) / 2.0);
+                Point<T> p2 = ray_point(R, p2r, p2t, (fo + tb) / 2.0);
+                T pct = polar_closed(R, fo, pt.sn, pt.cn);
+                T It1, Ip1, It2, Ip2;
+                increment(R, pa, p1, pt, ta, fo, pca, pct, It1, Ip1);
+                increment(R, pt, p2, pb, fo, tb, pct, pcb, It2, Ip2);
+                t += It1 + It2; phi += Ip1 + Ip2;
+            } else {
+                T It, Ip;
+                increment(R, pa, pm, pb, ta, tb, pca, pcb, It, Ip);
+                t += It; phi += Ip;
+            }
+            if (anchor) {
+                if (Am[AF_OK] != 0.0) {
+                    const double at = Am[AF_T], ap = Am[AF_PHI];
+                    if constexpr (RESID) {
+                        rt = fmax(rt, fabs(double(t) - at));
+                        rphi = fmax(rphi, fabs(double(phi) - ap));
+                    }
+                    t = T(at); phi = T(ap);
+                }
+                ++m;
+                next_anchor += R.Manchor;
+            }
+            if (k >= k_begin) {
+                Sample<T> s{t, pb.r, pb.theta, pb.cth, phi, pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cth)};
+                f(k, s);
+            }
+            pa = pb;
+            pca = pcb;
         }
-        Sample<T> s{t, pb.r, pb.theta, pb.cth, phi, pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cth)};
-        f(k, s);
-        pa = pb;
-        pca = pcb;
     }
     resid_t = rt;
     resid_phi = rphi;
 }
 
-// March samples [k_begin, k_end) of ray j and call f(k, sample) for each (no residuals). The march
-// starts at the last anchor at or before k_begin (its Jacobi states, t~ and phi from the table) and
-// runs silently up to k_begin, so the lanes of a warp call f the same number of times whatever
-// their anchor spacing. With k_begin = 1 this is the stream of march() (quadrature.jl:231-296).
+// March ray j with its N samples and call f(k, sample) for k = 1..N; returns the largest anchor residuals.
+template <class T, class F>
+__device__ __forceinline__ void march(const PlanView& P, const Spacetime& st, long long j, const MarchRay<T>& R,
+                                      F& f, double& resid_t, double& resid_phi) {
+    (void)st;
+    march_impl<true>(P, j, R, f, 1, R.nsamp + 1, resid_t, resid_phi);
+}
+
+// March samples [k_begin, k_end) of ray j (no residuals): the work segments of the sample stream.
 template <class T, class F>
 __device__ __forceinline__ void march_range(const PlanView& P, long long j, const MarchRay<T>& R, F& f, int k_begin, int k_end) {
-    if (k_end > R.nsamp + 1) k_end = R.nsamp + 1;
-    if (k_begin >= k_end) return;
-    const double dtau = R.dtau;
-    const double h = dtau / 2.0;
-    int m = (k_begin - 1) / R.Manchor;
-    if (m > R.nanch - 1) m = R.nanch - 1;
-    const int ka = 1 + m * R.Manchor;
-    const double* A0 = P.anchors + (R.anchor_off + m) * AF_COUNT;
-    JS<T> xr = load_js<T>(A0, AF_XR_SN), xt = load_js<T>(A0, AF_XT_SN);
-    Point<T> pa = ray_point(R, xr, xt, ka * dtau);
-    T pca = polar_closed(R, ka * dtau, pa.sn, pa.cn);
-    T t = T(A0[AF_T]), phi = T(A0[AF_PHI]);
-    if (ka >= k_begin) {
-        Sample<T> s{t, pa.r, pa.theta, pa.cth, phi, pa.nur, pa.nuth, (ka * dtau <= R.tau_valid) && visible(R, pa.cth)};
-        f(ka, s);
-    }
-    int next_anchor = ka + R.Manchor;
-    ++m;
-    for (int k = ka + 1; k < k_end; ++k) {
-        double ta = (k - 1) * dtau, tb = k * dtau;
-        xr = jstep(xr, R.dr, R.k);
-        xt = jstep(xt, R.dth, R.pmu);
-        Point<T> pm = ray_point(R, xr, xt, ta + h);
-        const bool anchor = (k == next_anchor);
-        const double* Am = P.anchors + (R.anchor_off + m) * AF_COUNT;
-        if (anchor) {
-            xr = load_js<T>(Am, AF_XR_SN); xt = load_js<T>(Am, AF_XT_SN);
-        } else {
-            xr = jstep(xr, R.dr, R.k);
-            xt = jstep(xt, R.dth, R.pmu);
-        }
-        Point<T> pb = ray_point(R, xr, xt, tb);
-        T pcb = polar_closed(R, tb, pb.sn, pb.cn);
-        if (k == R.turn_k) {
-            const double* pf = P.f;
-            const long long np = P.npad;
-            JS<T> p1r = {T(pf[PF_P1R_SN * np + j]), T(pf[PF_P1R_CN * np + j]), T(pf[PF_P1R_DN * np + j])};
-            JS<T> p1t = {T(pf[PF_P1T_SN * np + j]), T(pf[PF_P1T_CN * np + j]), T(pf[PF_P1T_DN * np + j])};
-            JS<T> p2r = {T(pf[PF_P2R_SN * np + j]), T(pf[PF_P2R_CN * np + j]), T(pf[PF_P2R_DN * np + j])};
-            JS<T> p2t = {T(pf[PF_P2T_SN * np + j]), T(pf[PF_P2T_CN * np + j]), T(pf[PF_P2T_DN * np + j])};
-            JS<T> ptt = {T(pf[PF_PTT_SN * np + j]), T(pf[PF_PTT_CN * np + j]), T(pf[PF_PTT_DN * np + j])};
-            double fo = R.fo_d;
-            Point<T> pt = turning_point(R, ptt);
-            Point<T> p1 = ray_point(R, p1r, p1t, (ta + fo) / 2.0);
-            Point<T> p2 = ray_point(R, p2r, p2t, (fo + tb) / 2.0);
-            T pct = polar_closed(R, fo, pt.sn, pt.cn);
-            T It1, Ip1, It2, Ip2;
-            increment(R, pa, p1, pt, ta, fo, pca, pct, It1, Ip1);
-            increment(R, pt, p2, pb, fo, tb, pct, pcb, It2, Ip2);
-            t += It1 + It2; phi += Ip1 + Ip2;
-        } else {
-            T It, Ip;
-            increment(R, pa, pm, pb, ta, tb, pca, pcb, It, Ip);
-            t += It; phi += Ip;
-        }
-        if (anchor) {
-            if (Am[AF_OK] != 0.0) { t = T(Am[AF_T]); phi = T(Am[AF_PHI]); }
-            ++m;
-            next_anchor += R.Manchor;
-        }
-        if (k >= k_begin) {
-            Sample<T> s{t, pb.r, pb.theta, pb.cth, phi, pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cth)};
-            f(k, s);
-        }
-        pa = pb;
-        pca = pcb;
-    }
+    double rt, rp;
+    march_impl<false>(P, j, R, f, k_begin, k_end, rt, rp);
 }
 
 }  // namespace ks

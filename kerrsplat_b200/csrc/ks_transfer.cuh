@@ -456,11 +456,11 @@ __device__ __noinline__ void moments_f32(const MomentCoeffs& MC, float a, float*
 #pragma unroll
         for (int m = 22; m >= 0; --m) s = fmaf(a, s, MC.cf[9][m]);
         M[9] = s;
-        const float e = expf(-a);
+        const float e = __expf(-a);
 #pragma unroll
         for (int n = 9; n >= 1; --n) M[n - 1] = (a * M[n] + e) * (1.f / float(n));
     } else {
-        float e = expf(-a);
+        float e = __expf(-a);
         M[0] = (1.f - e) / a;
 #pragma unroll
         for (int n = 1; n < 10; ++n) M[n] = (float(n) * M[n - 1] - e) / a;
@@ -470,6 +470,7 @@ template <> __device__ __forceinline__ void moments<float>(const MomentCoeffs& M
 
 template <class T> __device__ __forceinline__ T phi_fn(const MomentCoeffs& MC, T a) {
     if (fabs(a) < T(1)) return moment_n(MC, a, 0);
+    if constexpr (is_f32<T>) return (T(1) - fexp(-a)) / a;   // |a| >= 1: no cancellation
     return -expm1(-a) / a;
 }
 
@@ -647,7 +648,7 @@ __device__ __forceinline__ void step_coefficients(const MomentCoeffs& MC, TD a, 
     const TD L1 = L1sq > S(0) ? sqrt(L1sq) : TD(S(0)), L2 = L2sq > S(0) ? sqrt(L2sq) : TD(S(0));
     const TD b1 = L1 * D, b2 = L2 * D;
     const TD Th = L1sq + L2sq;
-    const TD ex = exp(-a);
+    const TD ex = fexp(-a);
     TD M[10];
     moments(MC, a, M);
     if (Th * D * D * ((a2 + r2) * D * D + S(1)) < cub_thr<TD>()) {
@@ -662,15 +663,24 @@ __device__ __forceinline__ void step_coefficients(const MomentCoeffs& MC, TD a, 
         esinhb = ex * (fabs(b1) < S(0.1) ? sinhc_excess(b1) + S(1) : sinh(b1) / b1);
         ecoshm1 = ex * S(2) * sh * sh;
     } else {
-        const TD em = exp(-(a - b1)), ep = exp(-(a + b1));
+        const TD em = fexp(-(a - b1)), ep = fexp(-(a + b1));
         ecosh = (em + ep) / S(2); esinhb = (em - ep) / (S(2) * b1); ecoshm1 = (em - S(2) * ex + ep) / S(2);
     }
-    const TD sb2 = sin(b2), cb2 = cos(b2), sh2 = sin(b2 / S(2));
+    TD sb2, cb2, sh2;
+    if constexpr (is_f32<TD>) {
+        // one reduced hardware sine/cosine of the half angle: sin b2 = 2 s c, cos b2 = 1 - 2 s^2
+        TD ch2;
+        fsincos(b2 / S(2), sh2, ch2);
+        sb2 = S(2) * sh2 * ch2;
+        cb2 = S(1) - S(2) * sh2 * sh2;
+    } else {
+        sb2 = sin(b2); cb2 = cos(b2); sh2 = sin(b2 / S(2));
+    }
     const TD c0 = (L2sq * ecosh + L1sq * ex * cb2) / Th;
     const TD c2 = (ecoshm1 + ex * S(2) * sh2 * sh2) / Th;
     const TD sincb2 = fabs(b2) < S(0.1) ? S(1) - sinc_deficit(b2) : sb2 / b2;
     const TD so = D * esinhb, sn = D * ex * sincb2;
-    const TD ph_a = fabs(a) < S(1) ? M[0] : -expm1(-a) / a;
+    const TD ph_a = fabs(a) < S(1) ? M[0] : (S(1) - ex) / a;   // |a| >= 1: no cancellation
     const TD icoshm1 = b1 < S(0.1) ? b1 * b1 * (M[2] / S(2) + b1 * b1 * (M[4] / S(24) + b1 * b1 * (M[6] / S(720) + b1 * b1 * M[8] / S(40320))))
                                    : (phi_fn(MC, a - b1) + phi_fn(MC, a + b1)) / S(2) - ph_a;
     const TD vser = b2 * b2 * (M[2] / S(2) - b2 * b2 * (M[4] / S(24) - b2 * b2 * (M[6] / S(720) - b2 * b2 * M[8] / S(40320))));
