@@ -37,9 +37,9 @@ FLOPS = {"samples": 330, "valid_samples": 95, "splat_tests": 22, "weights": 32, 
          "frames": 115, "steps": 1150}
 SFU = {"samples": 12, "valid_samples": 9, "splat_tests": 2, "weights": 1, "coefficients": 22, "frames": 4, "steps": 12}
 # k_consume's DRAM traffic per ray-sample: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch
-# at 192x192, N = 1024, 3 frequencies (1.3315e9 + 0.1376e9 B over 36864 x 1024 ray-samples; reads = the
-# FP32 sample stream, 32 B per ray-sample, + the plan; writes = segment states), scaled by ray-samples
-CONSUME_TRAFFIC_PER_RAY_SAMPLE = (1.3315e9 + 0.1376e9) / (36864 * 1024)
+# of this workload at full size (256x256, N = 1024, 3 frequencies: 2.9926e9 + 0.1260e9 B over 65536 x 1024
+# ray-samples; reads = the FP32 sample stream, 32 B per ray-sample, + the plan; writes = segment states)
+CONSUME_TRAFFIC_PER_RAY_SAMPLE = (2.992645e9 + 0.126026e9) / (65536 * 1024)
 
 
 def rank_info():
@@ -245,7 +245,7 @@ def run_ours(args):
                    "l2": "no flush: the per-ray FP64 plan + anchor table (~150 MB) exceeds the 126 MB L2"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "traffic": traffic, "traffic_source": "ncu DRAM bytes of one k_consume launch at 192x192 N=1024, scaled by ray-samples"
+                     "traffic": traffic, "traffic_source": "ncu DRAM bytes of one k_consume launch of this workload (256x256, N=1024, 3 frequencies)"
                      if traffic else None,
                      "peak_source": "nominal FP32 pipe (148 SMs x 128 lanes x 2 x max SM clock); MEASURED_PEAKS.json has no FP32 figure",
                      "kernel": kname, "kernel_ms": launch_ms, "flops_per_launch": flops_per_launch,
@@ -360,6 +360,11 @@ def run_movie(args):
     units = float(nsamp.sum()) * nf * nt
     for _ in range(args.warmup):
         ks.render(cache, model, c["times"], c["nus"], c["L"], precision=ks.KS_MIXED, out=out, order="sorted")
+    # work-event counts of one movie (the consumer's samples, splat tests, weights, evaluations, steps)
+    cache.count_events(True)
+    ks.render(cache, model, c["times"], c["nus"], c["L"], precision=ks.KS_MIXED, out=out, order="sorted")
+    events = cache.event_counts()
+    cache.count_events(False)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize(dev)
@@ -375,7 +380,7 @@ def run_movie(args):
             "dtype": "f32", "data": "synthetic (seeded PCG64 scene, cfg 4 distributions)",
             "config": {"workload": f"batched movie {args.res}x{args.res} +-15M, a=0.94, theta_o=163deg, {nt} frames x 4 freqs, uneven N "
                                    f"(mean {nsamp.mean():.0f}, {nsamp.min()}-{nsamp.max()}), 85 knot + 85 power-law + 86 kappa splats",
-                       "ray_samples_per_step": units, "finite": finite},
+                       "ray_samples_per_step": units, "finite": finite, "events": events},
             "clocks": {k: clk.summary()[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")}}
     if args.fp64_steps > 0:
         # the FP64 plain path on the first frame only (one march per frame and frequency)

@@ -164,7 +164,7 @@ __device__ __forceinline__ bool element_adjoint(const T* p, const double* __rest
     // the weight and its geometric partials (Splats.jl:58-93, polarized.jl:22-29)
     const T ph = p[ST_OMEGA] * (t - p[ST_T0]);
     T sp, cp;
-    sincos(ph, &sp, &cp);
+    fsincos(ph, sp, cp);
     const T cx = p[ST_CX] * cp - p[ST_CY] * sp, cy = p[ST_CX] * sp + p[ST_CY] * cp;
     const T d0 = x - cx, d1 = y - cy, d2 = z - p[ST_CZ];
     if (d0 * d0 + d1 * d1 + d2 * d2 > p[ST_SUPP]) return false;   // outside_support (polarized.jl:110-120)
@@ -176,31 +176,37 @@ __device__ __forceinline__ bool element_adjoint(const T* p, const double* __rest
     e[0] = u[0] * p[ST_ES1]; e[1] = u[1] * p[ST_ES2]; e[2] = u[2] * p[ST_ES3];
     const T tt = (t - p[ST_T0]) * p[ST_INVW];
     const T q = (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] + tt * tt) / T(2);
-    const T G = exp(-q);
+    const T G = fexp(-q);
     if (!(G > T(kWEIGHT_CUTOFF))) return false;
 
-    // the fluid rows as seven forward-mode duals (splat_coefficients, polarized.jl:140-150)
-    using D = Dual<T, 7>;
-    D Te(p[ST_TE]), f0(p[ST_F0]), kr(p[ST_KR]), Bm(p[ST_BMAG]);
+    // The seven fluid rows (splat_coefficients, polarized.jl:140-150): ln Te, ln B, the field's two
+    // angles, the three velocity components. The frame depends on the last five only: it is formed
+    // once per pair on five duals. The fits at each frequency depend on the fluid rows through four
+    // scalars (ln Te with the Bessel ratios, ln B, nu_f = nu / g, cos theta_B), so they run on four
+    // duals; the frame's partials of g, cos theta_B and the 2 chi rotation carry them to the rows.
+    using D5 = Dual<T, 5>;
+    D5 bx(p[ST_BHX]), by(p[ST_BHY]), bz(p[ST_BHZ]);
+    bx.d[0] = T(gt[GT_DBT0]); by.d[0] = T(gt[GT_DBT1]); bz.d[0] = T(gt[GT_DBT2]);
+    bx.d[1] = T(gt[GT_DBP0]); by.d[1] = T(gt[GT_DBP1]); bz.d[1] = T(gt[GT_DBP2]);
+    const D5 u1 = D5::seed(p[ST_U1], 2), u2 = D5::seed(p[ST_U2], 3), u3 = D5::seed(p[ST_U3], 4);
+    SampleFrame<D5> Fd;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { Fd.pu[k] = D5(F.pu[k]); Fd.pz[k] = D5(F.pz[k]); }
+    Fd.lapse_inv = D5(F.lapse_inv); Fd.om_lapse = D5(F.om_lapse); Fd.sDS = D5(F.sDS); Fd.misS = D5(F.misS); Fd.ivarpi = D5(F.ivarpi);
+    Fd.r = D5(F.r); Fd.sth = D5(F.sth); Fd.cth = D5(F.cth); Fd.a = D5(F.a);
+    const LFrame<D5> lf = local_frame(Fd, u1, u2, u3, bx, by, bz, p[ST_BZERO] != T(0), D5(alpha), D5(beta), D5(a_sin_tho));
+    using D4 = Dual<T, 4>;
+    D4 Te(p[ST_TE]), f0(p[ST_F0]), kr(p[ST_KR]), Bm(p[ST_BMAG]);
     Te.d[0] = p[ST_TE]; f0.d[0] = T(gt[GT_DF0]); kr.d[0] = T(gt[GT_DKR]);
     Bm.d[1] = p[ST_BMAG];
-    D bx(p[ST_BHX]), by(p[ST_BHY]), bz(p[ST_BHZ]);
-    bx.d[2] = T(gt[GT_DBT0]); by.d[2] = T(gt[GT_DBT1]); bz.d[2] = T(gt[GT_DBT2]);
-    bx.d[3] = T(gt[GT_DBP0]); by.d[3] = T(gt[GT_DBP1]); bz.d[3] = T(gt[GT_DBP2]);
-    const D u1 = D::seed(p[ST_U1], 4), u2 = D::seed(p[ST_U2], 5), u3 = D::seed(p[ST_U3], 6);
-    SampleFrame<D> Fd;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) { Fd.pu[k] = D(F.pu[k]); Fd.pz[k] = D(F.pz[k]); }
-    Fd.lapse_inv = D(F.lapse_inv); Fd.om_lapse = D(F.om_lapse); Fd.sDS = D(F.sDS); Fd.misS = D(F.misS); Fd.ivarpi = D(F.ivarpi);
-    Fd.r = D(F.r); Fd.sth = D(F.sth); Fd.cth = D(F.cth); Fd.a = D(F.a);
-    const LFrame<D> lf = local_frame(Fd, u1, u2, u3, bx, by, bz, p[ST_BZERO] != T(0), D(alpha), D(beta), D(a_sin_tho));
     // the pitch angle's sine and cosine: FP32 from its cosine directly (no angle formed), FP64 through
     // safe_acos as the reference does
-    D sbv, cbv;
-    if constexpr (is_f32<T>) pitch_sc(lf.cosB, sbv, cbv);
-    else { const D thb = safe_acos(lf.cosB); sbv = sin(thb); cbv = cos(thb); }
-    const D s2c = lf.s2c, c2c = lf.c2c;
-    const D ne(p[ST_NE] * G);
+    const D4 cosB = D4::seed(lf.cosB.v, 3);
+    D4 sbv, cbv;
+    if constexpr (is_f32<T>) pitch_sc(cosB, sbv, cbv);
+    else { const D4 thb = safe_acos(cosB); sbv = sin(thb); cbv = cos(thb); }
+    const T s2c = lf.s2c.v, c2c = lf.c2c.v, gv = lf.g.v;
+    const D4 ne(p[ST_NE] * G);
     T sc = T(0);
     T fl[7] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
     bool any = false;
@@ -208,22 +214,32 @@ __device__ __forceinline__ bool element_adjoint(const T* p, const double* __rest
     for (int c = 0; c < CH; ++c) {
         if (c >= nc || !((act >> c) & 1u)) continue;
         const T* cbc = cb + c * cstride;
-        const D nuf = D(nu[c]) / lf.g;
-        const Coef<D> cf = thermal_cs(ne, Te, f0, kr, Bm, nuf, sbv, cbv);
+        const T nufv = nu[c] / gv;
+        const D4 nuf = D4::seed(nufv, 2);
+        const Coef<D4> cf = thermal_cs(ne, Te, f0, kr, Bm, nuf, sbv, cbv);
         // screen_coefficients (transport.jl:265-270)
         if (!(cf.jI > T(0) || cf.aI > T(0) || cf.rQ != T(0) || cf.rV != T(0))) continue;
-        const D fe = cap_factor(cf.jI, cf.jQ, cf.jV, D(T(0.99)));
-        const D fa = cap_factor(cf.aI, cf.aQ, cf.aV, D(T(0.99)));
-        const D nh = nuf / T(kNU0);
-        const D i2 = D(T(1)) / (nh * nh);
-        const D jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
-        const D qd = (cf.jI * i2) * cbc[0] + (jQ * c2c) * cbc[qstride] + (jQ * s2c) * cbc[2 * qstride] + (cf.jV * fe * i2) * cbc[3 * qstride] +
-                     (nh * cf.aI) * cbc[4 * qstride] + (aQ * c2c) * cbc[5 * qstride] + (aQ * s2c) * cbc[6 * qstride] +
-                     (cf.aV * fa * nh) * cbc[7 * qstride] + (rQ * c2c) * cbc[8 * qstride] + (rQ * s2c) * cbc[9 * qstride] +
-                     (nh * cf.rV) * cbc[10 * qstride];
-        sc += qd.v;
+        const D4 fe = cap_factor(cf.jI, cf.jQ, cf.jV, D4(T(0.99)));
+        const D4 fa = cap_factor(cf.aI, cf.aQ, cf.aV, D4(T(0.99)));
+        const D4 nh = nuf / T(kNU0);
+        const D4 i2 = D4(T(1)) / (nh * nh);
+        const D4 jQ = cf.jQ * fe * i2, aQ = cf.aQ * fa * nh, rQ = cf.rQ * nh;
+        // c-bar . c = A + cos(2 chi) Bq + sin(2 chi) Cq
+        const D4 A = (cf.jI * i2) * cbc[0] + (cf.jV * fe * i2) * cbc[3 * qstride] + (nh * cf.aI) * cbc[4 * qstride] +
+                     (cf.aV * fa * nh) * cbc[7 * qstride] + (nh * cf.rV) * cbc[10 * qstride];
+        const D4 Bq = jQ * cbc[qstride] + aQ * cbc[5 * qstride] + rQ * cbc[8 * qstride];
+        const D4 Cq = jQ * cbc[2 * qstride] + aQ * cbc[6 * qstride] + rQ * cbc[9 * qstride];
+        sc += A.v + c2c * Bq.v + s2c * Cq.v;
+        T dq[4];
 #pragma unroll
-        for (int k = 0; k < 7; ++k) fl[k] += qd.d[k];
+        for (int k = 0; k < 4; ++k) dq[k] = A.d[k] + c2c * Bq.d[k] + s2c * Cq.d[k];
+        fl[0] += dq[0];   // ln Te
+        fl[1] += dq[1];   // ln B
+        // the frame's rows through nu_f = nu / g (d nu_f = -nu_f dg / g), cos theta_B and the rotation
+        const T dnuf_dg = -nufv / gv;
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            fl[2 + k] += dq[2] * dnuf_dg * lf.g.d[k] + dq[3] * lf.cosB.d[k] + Bq.v * lf.c2c.d[k] + Cq.v * lf.s2c.d[k];
         any = true;
     }
     if (!any) return false;

@@ -71,6 +71,18 @@ __device__ __forceinline__ void fsincos(float x, float& s, float& c) { __sincosf
 __device__ __forceinline__ float fcos(float x) { return __cosf(freduce(x)); }
 template <class T> __device__ __forceinline__ void fsincos(const T& x, T& s, T& c) { s = sin(x); c = cos(x); }
 template <class T> __device__ __forceinline__ T fcos(const T& x) { return cos(x); }
+// FP32 duals: the value by the reduced hardware pair, the partials by the chain rule
+template <int N> __device__ __forceinline__ void fsincos(const Dual<float, N>& x, Dual<float, N>& s, Dual<float, N>& c) {
+    float sv, cv;
+    fsincos(x.v, sv, cv);
+    s = dchain(x, sv, cv);
+    c = dchain(x, cv, -sv);
+}
+template <int N> __device__ __forceinline__ Dual<float, N> fcos(const Dual<float, N>& x) {
+    float sv, cv;
+    fsincos(x.v, sv, cv);
+    return dchain(x, cv, -sv);
+}
 // the same for dual numbers (the adjoint's forward-mode derivatives)
 template <class T, int N> __device__ __forceinline__ Dual<T, N> fexp(const Dual<T, N>& x) { T e = fexp(x.v); return dchain(x, e, e); }
 template <class T, int N> __device__ __forceinline__ Dual<T, N> flog(const Dual<T, N>& x) { return dchain(x, flog(x.v), T(1) / x.v); }
