@@ -468,6 +468,88 @@ def run_fit(args):
     cache.close()
 
 
+def run_dft(args):
+    """The visibility transform of configuration 5 (a 1024 x 1024 four-Stokes image onto 2000 baselines,
+    and the adjoint seed back), mixed precision: per step one ks_visibilities and one ks_vis_seed call
+    from host arrays (the e2e figure: host->device copies of the image and weights, device->host copies
+    of V and the seed, inside the timed region), with the L2 flushed between steps (a 256 MB write).
+    The two 3xTF32 GEMMs of a step (4096 x 4000 x 1024 and 1024 x 4096 x 4000) are timed with CUDA
+    events (ks_gemm_stats) on the tcgen05 kernel and on the mma.sync fallback; the FP64 direct sums
+    (the reference's algorithm) are timed once."""
+    import torch
+    import kerrsplat_b200 as ks
+    from kerrsplat_b200 import build, scenes
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    build.build(verbose=False)
+    c = scenes.config5(res=args.res, N=8, nsets=1)
+    cache = ks.GeodesicCache(c["camera"], 8, device=local)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    rng = np.random.Generator(np.random.PCG64(11 + rank))
+    npix = c["camera"].npix
+    img = np.abs(rng.standard_normal((npix, 4))) * np.array([1.0, 0.2, 0.2, 0.05])
+    nuv = len(c["u"])
+    w = rng.standard_normal((nuv, 4)) + 1j * rng.standard_normal((nuv, 4))
+    img_h = torch.from_numpy(img).pin_memory().numpy()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        V = ks.visibilities(cache, img_h, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_MIXED)
+        S = ks.vis_seed(cache, w, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_MIXED)
+        return V, S
+
+    res = {}
+    for path in ("mma.sync", "tcgen05"):
+        cache.set_tensor_path(path)
+        for _ in range(args.warmup):
+            step()
+        cache.gemm_stats(reset=True)
+        tot = 0.0
+        clocks = ClockSampler(local)
+        with clocks:
+            for _ in range(args.steps):
+                flush.fill_(1)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                V, S = step()
+                tot += time.perf_counter() - t0
+        gms, gl, gfl = cache.gemm_stats(reset=True)
+        res[path] = {"ms_per_step": tot * 1e3 / args.steps, "gemm_ms_per_step": gms / args.steps, "gemm_launches": gl,
+                     "gemm_tflops": gfl / (gms * 1e-3) / 1e12, "V": V, "S": S, "clocks": clocks.summary()}
+    cache.set_tensor_path("tcgen05")
+    t0 = time.perf_counter()
+    V64 = ks.visibilities(cache, img_h, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_FP64)
+    S64 = ks.vis_seed(cache, w, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_FP64)
+    ms64 = (time.perf_counter() - t0) * 1e3
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    tc, ms = res["tcgen05"], res["mma.sync"]
+    pk = peaks()
+    tf32_peak = pk["bf16_tflops"] / 2 if "bf16_tflops" in pk else 1590.0 / 2
+    h2d = img.nbytes + w.nbytes + 2 * 8 * nuv * 2
+    d2h = 8 * nuv * 8 + npix * 4 * 8
+    line = {"metric": "visibility transforms/s (forward + adjoint)", "value": 1e3 / tc["ms_per_step"], "unit": "transforms/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tc["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (3xTF32)", "data": "synthetic (seeded image, cfg 5 baselines)",
+            "config": {"workload": f"config-5 DFT: {args.res}x{args.res} x 4 Stokes image onto {nuv} baselines and the adjoint seed back",
+                       "gemms": f"T = A Tu^T ({4 * args.res} x {2 * nuv} x {args.res}), S = Tu C^T ({args.res} x {4 * args.res} x {2 * nuv})",
+                       "l2": "flushed between steps (256 MB write); each GEMM reads the operands its producer kernels just wrote",
+                       "timing": "wall clock around the host-array calls (e2e); CUDA events around each GEMM"},
+            "e2e": {"value": 1e3 / tc["ms_per_step"], "unit": "transforms/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "tensor", "achieved": tc["gemm_tflops"], "peak": tf32_peak, "unit": "TFLOP/s",
+                         "frac": tc["gemm_tflops"] / tf32_peak, "traffic": None, "kernel": "k_gemm_tc",
+                         "kernel_ms_per_step": tc["gemm_ms_per_step"],
+                         "peak_source": "TF32 dense = half the measured BF16 burst (MEASURED_PEAKS.json bf16_tflops)"
+                         if "bf16_tflops" in pk else "TF32 dense = half the fallback BF16 burst",
+                         "flops": "3 x 2 M N K per GEMM (the three TF32 products are issued)"},
+            "mma_sync": {"ms_per_step": ms["ms_per_step"], "gemm_ms_per_step": ms["gemm_ms_per_step"], "gemm_tflops": ms["gemm_tflops"],
+                         "V_rel_vs_tcgen05": rel(ms["V"], tc["V"]), "seed_rel_vs_tcgen05": rel(ms["S"], tc["S"])},
+            "fp64_direct": {"ms": ms64, "V_rel_mixed_vs_fp64": rel(tc["V"], V64), "seed_rel_mixed_vs_fp64": rel(tc["S"], S64),
+                            "speedup_mixed_over_fp64": ms64 / tc["ms_per_step"]},
+            "clocks": tc["clocks"]}
+    print(json.dumps(line), flush=True)
+    cache.close()
+
+
 def cpu_sample(c, nrays, seed=7):
     rng = np.random.Generator(np.random.PCG64(seed))
     idx = np.sort(rng.choice(c["camera"].npix, size=min(nrays, c["camera"].npix), replace=False))
@@ -532,13 +614,14 @@ def main():
                     help="time the consumer's launch shapes before the timed steps (ks_autotune)")
     ap.add_argument("--res", type=int, default=None, help="screen resolution (default: the workload's; smaller cases for profiling)")
     ap.add_argument("--nsamples", type=int, default=None, help="samples per ray (default: the workload's)")
-    ap.add_argument("--workload", default="polarized", choices=["polarized", "movie", "fit"],
-                    help="polarized: configurations 2 and 3 (the headline); movie: configuration 4; fit: configuration 5")
+    ap.add_argument("--workload", default="polarized", choices=["polarized", "movie", "fit", "dft"],
+                    help="polarized: configurations 2 and 3 (the headline); movie: configuration 4; fit: configuration 5; "
+                         "dft: configuration 5's visibility transform on both tensor-core kernels")
     ap.add_argument("--sets", type=int, default=16, help="fit: parameter sets")
     ap.add_argument("--frames", type=int, default=32, help="movie frames")
     args = ap.parse_args()
     # the sizes of each workload's configuration unless given
-    dres, dn = {"polarized": (256, 1024), "movie": (512, 2048), "fit": (1024, 512)}[args.workload]
+    dres, dn = {"polarized": (256, 1024), "movie": (512, 2048), "fit": (1024, 512), "dft": (1024, 8)}[args.workload]
     args.res = dres if args.res is None else args.res
     args.nsamples = dn if args.nsamples is None else args.nsamples
     if args.impl == "reference":
@@ -547,6 +630,8 @@ def main():
         run_movie(args)
     elif args.workload == "fit":
         run_fit(args)
+    elif args.workload == "dft":
+        run_dft(args)
     else:
         run_ours(args)
 

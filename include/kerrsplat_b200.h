@@ -214,6 +214,17 @@ int ks_spacetime_derivatives(ks_context* ctx, const ks_splat_set* sets, int32_t 
 
 /* normal_matrix(J) (src/Fit/gauss_newton.jl:486-494): A = J^T J of a row-major m x n Jacobian (FP64),
  * A n x n. KS_FP64: FP64 tiles; KS_MIXED: the 3xTF32 tensor-core GEMM with FP32 accumulation. */
+#define KS_TENSOR_TCGEN05 0   /* tcgen05 UMMA, TMA-fed operand tiles, TMEM accumulator (the default) */
+#define KS_TENSOR_MMA_SYNC 1  /* mma.sync m16n8k8 (the checked fallback) */
+
+/* Which kernel runs the 3xTF32 GEMMs of the KS_MIXED DFT, its adjoint and ks_normal_matrix (no
+ * reference counterpart: the reference's transforms are direct sums). Both read the same split
+ * operands and give the same products up to FP32 accumulation order. */
+int ks_set_tensor_path(ks_context* ctx, int32_t path);
+
+/* Device time (CUDA events on the context stream) of the 3xTF32 GEMMs since the last reset, their
+ * launches and their tensor-core flops (3 x 2 M N K each: the three TF32 products are issued). */
+int ks_gemm_stats(ks_context* ctx, double* ms, long long* launches, double* flops, int reset);
 int ks_normal_matrix(ks_context* ctx, const double* J, int64_t m, int64_t n, int32_t precision, double* A);
 
 /* sample_adjoint (src/Transfer/transport.jl:221-245) of n independent samples in FP64: for the summed
@@ -254,8 +265,10 @@ int ks_graph_destroy(ks_context* ctx);
 
 /* Test hook for the bounded waits (no reference counterpart): while on != 0, the mixed kernels arm
  * the shared-memory barrier of their splat-table staging without issuing the copy and poll it only
- * 4096 times, so every block's wait runs out; the kernels record it and return (no fault, no hang) and
- * the call fails with KS_ERR_TIMEOUT. The context stays usable; turn the hook off to render again. */
+ * 4096 times, and the tcgen05 GEMM arms its operand barriers without issuing the tile copies and gives
+ * each wait ~10 ms, so every block's wait runs out; the kernels record it, free what they hold and
+ * return (no fault, no hang) and the call fails with KS_ERR_TIMEOUT. The context stays usable; turn
+ * the hook off to render again. */
 int ks_set_stage_test(ks_context* ctx, int32_t on);
 
 /* Device time (CUDA events on the context stream) of the persistent consumer k_consume alone in the

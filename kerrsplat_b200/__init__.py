@@ -227,6 +227,19 @@ class GeodesicCache:
         """Test hook: while on, mixed calls fail with a timeout of the table-staging wait (no fault)."""
         self._check(self._lib.ks_set_stage_test(self._ctx, int(bool(on))))
 
+    def set_tensor_path(self, path):
+        """Kernel of the 3xTF32 GEMMs: "tcgen05" (UMMA, the default) or "mma.sync" (the fallback)."""
+        code = {"tcgen05": 0, "mma.sync": 1}[path]
+        self._check(self._lib.ks_set_tensor_path(self._ctx, code))
+
+    def gemm_stats(self, reset=False):
+        """(ms, launches, flops) of the 3xTF32 GEMMs since the last reset (CUDA events, device time)."""
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        fl = ctypes.c_double()
+        self._check(self._lib.ks_gemm_stats(self._ctx, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(fl), int(reset)))
+        return ms.value, n.value, fl.value
+
     def consume_stats(self, reset=False):
         """(ms, launches) of k_consume alone in the mixed renders since the last reset."""
         ms = ctypes.c_double()

@@ -92,6 +92,8 @@ EXTRA_SIGNATURES = [
     ("ks_adjoint_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     ("ks_consume_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
     ("ks_set_stage_test", ctypes.c_int, [_VP, ctypes.c_int32]),
+    ("ks_set_tensor_path", ctypes.c_int, [_VP, ctypes.c_int32]),
+    ("ks_gemm_stats", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_longlong), _D, ctypes.c_int]),
     ("ks_render_graph_capture", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
                                                ctypes.c_double, ctypes.c_int32, ctypes.c_double, _VP, ctypes.c_int32]),
     ("ks_graph_launch", ctypes.c_int, [_VP, ctypes.c_int32]),

@@ -1323,12 +1323,9 @@ __global__ void k_normal_fp64(long long m, int n, const double* __restrict__ J, 
     }
 }
 
-__global__ void k_to_f32(long long n, const double* __restrict__ x, float* __restrict__ y) {
-    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (q < n) y[q] = float(x[q]);
-}
-// row-major m x n (double) -> row-major n x m (float)
-__global__ void k_transpose_f32(long long m, int n, const double* __restrict__ x, float* __restrict__ y) {
+// row-major m x n (double) -> the split GEMM operand y[n][ld] (row c holds column c of x)
+__global__ void k_transpose_split(long long m, int n, const double* __restrict__ x, float* __restrict__ hi, float* __restrict__ lo,
+                                  long long ld) {
     __shared__ float t[32][33];
     const long long r0 = (long long)blockIdx.y * 32;
     const int c0 = blockIdx.x * 32;
@@ -1341,7 +1338,7 @@ __global__ void k_transpose_f32(long long m, int n, const double* __restrict__ x
     for (int q = threadIdx.y; q < 32; q += blockDim.y) {
         const int cc = c0 + q;
         const long long r = r0 + threadIdx.x;
-        if (cc < n && r < m) y[(long long)cc * m + r] = t[threadIdx.x][q];
+        if (cc < n && r < m) ksdft::split_store(hi, lo, (long long)cc * ld + r, t[threadIdx.x][q]);
     }
 }
 __global__ void k_to_f64(long long n, const float* __restrict__ x, double* __restrict__ y) {

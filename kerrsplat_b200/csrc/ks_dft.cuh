@@ -8,32 +8,75 @@
 //     T[(s, j), (k, c|s)] = sum_i I_s[i, j] (cos | sin)(2 pi u_k l_i)          (a GEMM, K = na)
 //     V_k,s = tap_k scale sum_j exp(2 pi i v_k m_j) (T_c + i T_s)[(s, j), k]    (a reduction over j)
 // and the adjoint seed[i, (s, j)] = sum_k [cos . C_r + sin . C_i][i, k]         (a GEMM, K = 2 nuv)
-// with C[k, (s, j)] = conj(exp(2 pi i v_k m_j)) w_k,s tap_k scale. The GEMMs run on the tensor cores in
-// 3xTF32 (a = a_hi + a_lo, a_hi b_hi + a_hi b_lo + a_lo b_hi with FP32 accumulation; mma.sync m16n8k8).
-// Twiddles are evaluated with the phase reduced in FP64 (sincospi of the fractional cycle).
+// with C[k, (s, j)] = conj(exp(2 pi i v_k m_j)) w_k,s tap_k scale.
+//
+// The GEMMs run on the tensor cores in 3xTF32. Every operand x is stored split, x_hi = tf32(x) and
+// x_lo = tf32(x - x_hi) (round to nearest), by the kernel that produces it, and C = A_lo B_hi^T +
+// A_hi B_lo^T + A_hi B_hi^T accumulates in FP32. Both operands are K-major: C[M][N] = A[M][K] B[N][K]^T,
+// row strides a multiple of 4 floats. k_gemm_tc (tcgen05: TMA tiles with the 128-byte swizzle, UMMA
+// 128 x 128 x 8 into a TMEM accumulator) is the default; k_gemm_3xtf32 (mma.sync m16n8k8) reads the same
+// split operands and is the checked fallback. Twiddles are evaluated with the phase reduced in FP64
+// (sincospi of the fractional cycle).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 namespace ksdft {
 
 constexpr double kPi = 3.141592653589793238462643383279502884;
 
-// out[x][2k + c] = (cos | sin)(2 pi f_k x), rows x = 0..nx-1 with offset(x) = sign * (x + 1 - (nx + 1)/2) * psize
+// Row stride (floats) of a split operand: a multiple of 4 floats (16 bytes, the tensor-map stride rule).
+inline long long pad4(long long n) { return (n + 3) & ~3LL; }
+
+__device__ __forceinline__ unsigned tf32(float x) {
+    unsigned y;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(x));
+    return y;
+}
+
+// x = hi + lo up to 2^-22 |x|, both exactly representable in TF32
+__device__ __forceinline__ void split_store(float* __restrict__ hi, float* __restrict__ lo, long long at, float x) {
+    const float h = __uint_as_float(tf32(x));
+    hi[at] = h;
+    lo[at] = __uint_as_float(tf32(x - h));
+}
+
+// (cos, sin)(2 pi f x) at row x, offset(x) = sign * (x + 1 - (nx + 1)/2) * psize
+__device__ __forceinline__ void twiddle(long long x, int nx, double sign, double psize, double fk, float* c, float* s) {
+    const double off = sign * (double(x + 1) - double(nx + 1) / 2.0) * psize;
+    const double cyc = fk * off;   // phase in cycles
+    const double fr = cyc - rint(cyc);
+    double sd, cd;
+    sincospi(2.0 * fr, &sd, &cd);
+    *c = float(cd);
+    *s = float(sd);
+}
+
+// out[x][2k + c] = (cos | sin)(2 pi f_k offset(x)), rows x = 0..nx-1
 __global__ void k_twiddle(int nx, double sign, double psize, long long nf, const double* __restrict__ f, float* __restrict__ out, long long ld) {
     long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= (long long)nx * nf) return;
     long long x = q / nf, k = q % nf;
-    double off = sign * (double(x + 1) - double(nx + 1) / 2.0) * psize;
-    double cyc = f[k] * off;                 // phase in cycles
-    double fr = cyc - rint(cyc);
-    double s, c;
-    sincospi(2.0 * fr, &s, &c);
-    out[x * ld + 2 * k] = float(c);
-    out[x * ld + 2 * k + 1] = float(s);
+    twiddle(x, nx, sign, psize, f[k], &out[x * ld + 2 * k], &out[x * ld + 2 * k + 1]);
 }
 
-// image (npix x 4 doubles, screen order p = i + j na, or sorted with perm) -> A[(s nb + j) na + i] FP32
-__global__ void k_pack_image(const double* __restrict__ img, const long long* __restrict__ inv_perm, int na, int nb, float* __restrict__ A) {
+// The same table as a split GEMM operand, [x][2k + c] (transposed = 0) or [2k + c][x] (transposed = 1);
+// consecutive threads write consecutive addresses in either layout.
+__global__ void k_twiddle_split(int nx, double sign, double psize, long long nf, const double* __restrict__ f, int transposed,
+                                float* __restrict__ hi, float* __restrict__ lo, long long ld) {
+    long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= (long long)nx * nf) return;
+    const long long x = transposed ? q % nx : q / nf, k = transposed ? q / nx : q % nf;
+    float c, s;
+    twiddle(x, nx, sign, psize, f[k], &c, &s);
+    split_store(hi, lo, transposed ? (2 * k) * ld + x : x * ld + 2 * k, c);
+    split_store(hi, lo, transposed ? (2 * k + 1) * ld + x : x * ld + 2 * k + 1, s);
+}
+
+// image (npix x 4 doubles, screen order p = i + j na, or sorted with perm) -> split A[(s nb + j) lda + i]
+__global__ void k_pack_image(const double* __restrict__ img, const long long* __restrict__ inv_perm, int na, int nb,
+                             float* __restrict__ hi, float* __restrict__ lo, long long lda) {
     long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     long long npix = (long long)na * nb;
     if (q >= npix * 4) return;
@@ -41,14 +84,10 @@ __global__ void k_pack_image(const double* __restrict__ img, const long long* __
     int s = int(q / npix);
     long long src = inv_perm ? inv_perm[p] : p;
     long long i = p % na, j = p / na;
-    A[((long long)s * nb + j) * na + i] = float(img[src * 4 + s]);
+    split_store(hi, lo, ((long long)s * nb + j) * lda + i, float(img[src * 4 + s]));
 }
 
-__device__ __forceinline__ unsigned tf32(float x) {
-    unsigned y;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(y) : "f"(x));
-    return y;
-}
+// ---- the mma.sync fallback ------------------------------------------------------------------------
 
 __device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, const unsigned* b) {
     asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
@@ -58,12 +97,13 @@ __device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, const unsi
 
 constexpr int BM = 128, BN = 128, BK = 16, NTHREADS = 256;
 
-// C[M x N] = A[M x K] B[K x N], all row-major FP32, 3xTF32 on the tensor cores. 8 warps in a 2 x 4
-// grid, each owning a 64 x 32 tile of C (4 x 4 m16n8 fragments). Edges are zero-filled in shared memory.
-__global__ void __launch_bounds__(NTHREADS) k_gemm_3xtf32(int M, int N, int K, const float* __restrict__ A, long long lda,
-                                                          const float* __restrict__ B, long long ldb, float* __restrict__ C, long long ldc) {
-    __shared__ float As[BK][BM + 4];   // transposed: As[k][m]
-    __shared__ float Bs[BK][BN + 4];
+// C[M x N] = A[M x K] B[N x K]^T from split operands, 3xTF32 with mma.sync. 8 warps in a 2 x 4 grid,
+// each owning a 64 x 32 tile of C (4 x 4 m16n8 fragments). Edges are zero-filled in shared memory.
+__global__ void __launch_bounds__(NTHREADS) k_gemm_3xtf32(int M, int N, int K, const float* __restrict__ Ah, const float* __restrict__ Al,
+                                                          long long lda, const float* __restrict__ Bh, const float* __restrict__ Bl,
+                                                          long long ldb, float* __restrict__ C, long long ldc) {
+    __shared__ float Ash[BK][BM + 4], Asl[BK][BM + 4];   // transposed: As[k][m]
+    __shared__ float Bsh[BK][BN + 4], Bsl[BK][BN + 4];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp >> 2, wn = warp & 3;   // 2 x 4 warps
     const long long m0 = (long long)blockIdx.y * BM, n0 = (long long)blockIdx.x * BN;
@@ -76,20 +116,17 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_3xtf32(int M, int N, int K, c
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
     for (int k0 = 0; k0 < K; k0 += BK) {
-        // A tile: 128 rows x 16 k -> 2048 values, 8 per thread
+        // 128 rows x 16 k of each operand: 2048 values, 8 per thread
 #pragma unroll
         for (int q = 0; q < (BM * BK) / NTHREADS; ++q) {
-            int e = tid + q * NTHREADS;
-            int r = e / BK, kk = e % BK;
-            long long gm = m0 + r, gk = k0 + kk;
-            As[kk][r] = (gm < M && gk < K) ? A[gm * lda + gk] : 0.f;
-        }
-#pragma unroll
-        for (int q = 0; q < (BK * BN) / NTHREADS; ++q) {
-            int e = tid + q * NTHREADS;
-            int kk = e / BN, c = e % BN;
-            long long gk = k0 + kk, gn = n0 + c;
-            Bs[kk][c] = (gk < K && gn < N) ? B[gk * ldb + gn] : 0.f;
+            const int e = tid + q * NTHREADS;
+            const int r = e / BK, kk = e % BK;
+            const long long gk = k0 + kk, gm = m0 + r, gn = n0 + r;
+            const bool am = gm < M && gk < K, bn = gn < N && gk < K;
+            Ash[kk][r] = am ? Ah[gm * lda + gk] : 0.f;
+            Asl[kk][r] = am ? Al[gm * lda + gk] : 0.f;
+            Bsh[kk][r] = bn ? Bh[gn * ldb + gk] : 0.f;
+            Bsl[kk][r] = bn ? Bl[gn * ldb + gk] : 0.f;
         }
         __syncthreads();
 #pragma unroll
@@ -98,22 +135,20 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_3xtf32(int M, int N, int K, c
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi) {
                 const int rm = wm * 64 + mi * 16;
-                float v[4] = {As[ks + t][rm + g], As[ks + t][rm + g + 8], As[ks + t + 4][rm + g], As[ks + t + 4][rm + g + 8]};
+                const int rr[4] = {rm + g, rm + g + 8, rm + g, rm + g + 8}, kq[4] = {ks + t, ks + t, ks + t + 4, ks + t + 4};
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    ah[mi][q] = tf32(v[q]);
-                    al[mi][q] = tf32(v[q] - __uint_as_float(ah[mi][q]));
+                    ah[mi][q] = __float_as_uint(Ash[kq[q]][rr[q]]);
+                    al[mi][q] = __float_as_uint(Asl[kq[q]][rr[q]]);
                 }
             }
 #pragma unroll
             for (int ni = 0; ni < 4; ++ni) {
                 const int cn = wn * 32 + ni * 8;
-                float v[2] = {Bs[ks + t][cn + g], Bs[ks + t + 4][cn + g]};
-#pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    bh[ni][q] = tf32(v[q]);
-                    bl[ni][q] = tf32(v[q] - __uint_as_float(bh[ni][q]));
-                }
+                bh[ni][0] = __float_as_uint(Bsh[ks + t][cn + g]);
+                bh[ni][1] = __float_as_uint(Bsh[ks + t + 4][cn + g]);
+                bl[ni][0] = __float_as_uint(Bsl[ks + t][cn + g]);
+                bl[ni][1] = __float_as_uint(Bsl[ks + t + 4][cn + g]);
             }
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi)
@@ -138,6 +173,189 @@ __global__ void __launch_bounds__(NTHREADS) k_gemm_3xtf32(int M, int N, int K, c
         }
 }
 
+// ---- the tcgen05 kernel -----------------------------------------------------------------------------
+//
+// One CTA of 128 threads per 128 x 128 tile of C. Shared memory holds TC_STAGES stages of four operand
+// tiles (A_hi, A_lo, B_hi, B_lo), each 128 rows x 32 floats (128 bytes: one 128-byte swizzle atom per
+// 8 rows), filled by TMA from this GPU's memory (no multicast) with zero fill past the edges of the
+// matrices. Thread 0 issues the copies, thread 32 issues the MMAs (three UMMA 128 x 128 x 8 per 8 k:
+// lo.hi, hi.lo, hi.hi) and commits each stage back to the copier; the accumulator lives in 128 TMEM
+// columns and all four warps read it back (tcgen05.ld 32x32b, warp w owns lanes 32w..32w+31 = rows).
+// Every wait is bounded by `wait_limit` SM clock cycles: a wait that gives up sets bit 2 of `errflag`,
+// the block skips the epilogue, waits (bounded) for the copies it issued, frees its TMEM and returns.
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_STAGES = 3, TC_THREADS = 128;
+constexpr int TC_TILE = TC_BM * TC_BK * 4;                      // bytes of one operand tile
+constexpr int TC_STAGE = 4 * TC_TILE;
+constexpr int TC_BARS = 2 * TC_STAGES + 1;                      // full[S], empty[S], done
+constexpr int TC_SMEM = 1024 + TC_STAGES * TC_STAGE + 8 * TC_BARS + 16;
+constexpr int TC_TMEM_COLS = 128;
+// instruction descriptor of kind::tf32: F32 accumulator (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12
+// = 2), both K-major (bits 15, 16 = 0), N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(TC_BN >> 3) << 17) | (uint32_t(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > limit) return false;
+    }
+}
+
+// Shared-memory matrix descriptor of a K-major tile with the 128-byte swizzle: start address >> 4
+// (bits 0-13), leading offset 1 (unused by swizzled K-major layouts, bits 16-29), stride between 8-row
+// groups 1024 B >> 4 (bits 32-45), descriptor version 1 (bits 46-47), layout SWIZZLE_128B = 2 (bits 61-63).
+// The k-th 8-column slice of the atom starts 32 k bytes further (the swizzle is applied to the address).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return uint64_t((addr & 0x3FFFFu) >> 4) | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) | (uint64_t(1) << 46) | (uint64_t(2) << 61);
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 :
+                 : "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+                 :
+                 : "r"(tmem), "l"(a), "l"(b), "r"(TC_IDESC), "r"(accumulate)
+                 : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+#define KS_R8(b) "=r"(r[b]), "=r"(r[b + 1]), "=r"(r[b + 2]), "=r"(r[b + 3]), "=r"(r[b + 4]), "=r"(r[b + 5]), "=r"(r[b + 6]), "=r"(r[b + 7])
+// 32 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : KS_R8(0), KS_R8(8), KS_R8(16), KS_R8(24)
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+#undef KS_R8
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_gemm_tc(int M, int N, int K, const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
+              const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, float* __restrict__ C, long long ldc,
+              long long wait_limit, int skip_copies, unsigned* __restrict__ errflag) {
+    extern __shared__ unsigned char tc_smem[];
+    const uint32_t raw = smem_u32(tc_smem);
+    const uint32_t base = (raw + 1023u) & ~1023u;   // the swizzle atoms need 1024-byte alignment
+    const uint32_t bars = base + TC_STAGES * TC_STAGE;
+    volatile uint32_t* slots = reinterpret_cast<volatile uint32_t*>(tc_smem + (bars + 8 * TC_BARS - raw));   // [0] TMEM base, [1] stop
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * TC_BN;
+    const int nkb = (K + TC_BK - 1) / TC_BK;
+    const uint32_t done = bars + 8u * (2 * TC_STAGES);
+
+    if (tid == 0) {
+        for (int q = 0; q < TC_BARS; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bars + 8u * q) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        slots[1] = 0;
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(bars + 8u * TC_BARS), "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = slots[0];
+
+    bool gave_up = false;
+    int issued = 0;   // thread 0: k-blocks whose copies are in flight or landed
+    if (tid == 0) {
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % TC_STAGES;
+            if (kb >= TC_STAGES && !mbar_wait(bars + 8u * (TC_STAGES + s), uint32_t((kb / TC_STAGES - 1) & 1), wait_limit)) {
+                gave_up = true;
+                break;
+            }
+            if (slots[1]) break;   // the MMA thread gave up
+            const uint32_t full = bars + 8u * s, st = base + s * TC_STAGE;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full), "r"(TC_STAGE) : "memory");
+            if (skip_copies) continue;   // error-path test hook: the stage never fills
+            const int kx = kb * TC_BK;
+            tma_load_2d(st, &tAh, kx, m0, full);
+            tma_load_2d(st + TC_TILE, &tAl, kx, m0, full);
+            tma_load_2d(st + 2 * TC_TILE, &tBh, kx, n0, full);
+            tma_load_2d(st + 3 * TC_TILE, &tBl, kx, n0, full);
+            issued = kb + 1;
+        }
+    } else if (tid == 32) {
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % TC_STAGES;
+            if (!mbar_wait(bars + 8u * s, uint32_t((kb / TC_STAGES) & 1), wait_limit)) {
+                gave_up = true;
+                slots[1] = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + s * TC_STAGE;
+#pragma unroll
+            for (int k = 0; k < TC_BK / 8; ++k) {
+                const uint64_t ah = sw128_desc(st + 32 * k), al = sw128_desc(st + TC_TILE + 32 * k);
+                const uint64_t bh = sw128_desc(st + 2 * TC_TILE + 32 * k), bl = sw128_desc(st + 3 * TC_TILE + 32 * k);
+                umma_tf32(tmem, al, bh, (kb | k) != 0);   // small terms first
+                umma_tf32(tmem, ah, bl, 1);
+                umma_tf32(tmem, ah, bh, 1);
+            }
+            umma_commit(bars + 8u * (TC_STAGES + s));   // the stage is free once these MMAs complete
+        }
+        umma_commit(done);   // every MMA this thread issued
+    }
+    if (!mbar_wait(done, 0, wait_limit)) gave_up = true;
+    if (gave_up) atomicOr(errflag, 2u);
+    const int bad = __syncthreads_or(gave_up ? 1 : 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncwarp();
+    if (!bad) {
+        const int row = m0 + warp * 32 + (tid & 31);
+        const bool vec = (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+#pragma unroll 1
+        for (int ch = 0; ch < TC_BN / 32 && n0 + ch * 32 < N; ++ch) {
+            uint32_t r[32];
+            tmem_ld32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(ch * 32), r);
+            const int col = n0 + ch * 32;
+            if (row < M) {
+                float* out = C + (long long)row * ldc + col;
+                if (vec && col + 32 <= N) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        reinterpret_cast<float4*>(out)[q] =
+                            make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]), __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 32; ++q)
+                        if (col + q < N) out[q] = __uint_as_float(r[q]);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        // copies still in flight into this block's shared memory land before it exits
+        for (int kb = issued > TC_STAGES ? issued - TC_STAGES : 0; kb < issued; ++kb)
+            mbar_wait(bars + 8u * (kb % TC_STAGES), uint32_t((kb / TC_STAGES) & 1), wait_limit);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    __syncwarp();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+}
+
 // V[k][s] = tap_k scale sum_j (Bc + i Bs)[j][k] (Tc + i Ts)[(s, j)][k]  (complex, written as re, im doubles)
 __global__ void k_vis_combine(int nb, long long nuv, const float* __restrict__ Tm, long long ldt, const float* __restrict__ Bv, long long ldb,
                               const double* __restrict__ tap, double scale, double* __restrict__ V) {
@@ -158,21 +376,19 @@ __global__ void k_vis_combine(int nb, long long nuv, const float* __restrict__ T
     V[(k * 4 + s) * 2 + 1] = im * f;
 }
 
-// The adjoint right-hand side: Cm[(2k + c) ld + s nb + j] = (C_r | C_i)[k][(s, j)],
+// The adjoint right-hand side, split and K-major: CT[(s nb + j) ld + 2k + c] = (C_r | C_i)[k][(s, j)],
 // C = conj(exp(2 pi i v_k m_j)) w_k,s tap_k scale.
 __global__ void k_seed_rhs(int nb, long long nuv, const float* __restrict__ Bv, long long ldb, const double* __restrict__ w,
-                           const double* __restrict__ tap, double scale, float* __restrict__ Cm, long long ldc) {
+                           const double* __restrict__ tap, double scale, float* __restrict__ hi, float* __restrict__ lo, long long ldc) {
     long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= nuv * 4 * nb) return;
-    int j = int(q % nb);
-    long long r = q / nb;
-    int s = int(r % 4);
-    long long k = r / 4;
+    const long long k = q % nuv, sj = q / nuv;
+    const int s = int(sj / nb), j = int(sj % nb);
     double f = (tap ? tap[k] : 1.0) * scale;
     double wr = w[(k * 4 + s) * 2] * f, wi = w[(k * 4 + s) * 2 + 1] * f;
     double bc = Bv[(long long)j * ldb + 2 * k], bs = Bv[(long long)j * ldb + 2 * k + 1];
-    Cm[(2 * k) * ldc + (long long)s * nb + j] = float(bc * wr + bs * wi);
-    Cm[(2 * k + 1) * ldc + (long long)s * nb + j] = float(bc * wi - bs * wr);
+    split_store(hi, lo, sj * ldc + 2 * k, float(bc * wr + bs * wi));
+    split_store(hi, lo, sj * ldc + 2 * k + 1, float(bc * wi - bs * wr));
 }
 
 // seed[(i, (s, j))] -> out (npix x 4, screen order or sorted through perm)

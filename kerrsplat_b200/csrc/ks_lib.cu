@@ -10,6 +10,7 @@
 //   ks_thin_image / ks_render: k_splat_table (per-splat FP64 constants) -> k_thin / k_polarized
 //     (one thread per ray, the fused march with the consumer folded over the samples) -> k_unsort.
 #include <cub/cub.cuh>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -870,6 +871,7 @@ struct ks_context {
     double adjoint_ms = 0.0;
     long long adjoint_launches = 0;
     bool count_events = false;
+    int tensor_path = 0;  // 3xTF32 GEMMs: 0 tcgen05 (k_gemm_tc), 1 mma.sync (k_gemm_3xtf32); ks_set_tensor_path
     bool geo64 = true;    // mixed path: FP64 march feeding the FP32 transport (false: KS_MIXED_FP32 march)
     long long total_anchors = 0;
     int max_nanch = 0;
@@ -877,6 +879,9 @@ struct ks_context {
     // timing of the render kernels (CUDA events on the context stream)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t evc0 = nullptr, evc1 = nullptr;   // around k_consume (the mixed path's dominant kernel)
+    cudaEvent_t evg0 = nullptr, evg1 = nullptr;   // around each 3xTF32 GEMM (outside graph captures)
+    double gemm_ms = 0.0, gemm_flops = 0.0;       // ks_gemm_stats: device time and tensor-core flops (3 x 2 M N K)
+    long long gemm_launches = 0;
     bool consume_timed = false;
     double consume_ms = 0.0;
     long long consume_launches = 0;
@@ -1059,13 +1064,15 @@ int build_tables(ks_context* c, const ks_splat_set* sets, int nsets, int* ntot_o
     return KS_OK;
 }
 
-// A kernel's bounded wait that gave up (the device flag, cleared): KS_ERR_TIMEOUT.
+// A kernel's bounded wait that gave up (the device flag, cleared): KS_ERR_TIMEOUT. Bit 1: a mixed
+// kernel's table-staging copy; bit 2: a wait of the tcgen05 GEMM.
 int check_device_flag(ks_context* c, const char* what) {
     unsigned f = 0;
     KS_CUDA(c, cudaMemcpy(&f, c->errflag.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
     if (f) {
         KS_CUDA(c, cudaMemset(c->errflag.p, 0, sizeof(unsigned)));
-        return fail(c, KS_ERR_TIMEOUT, "%s: a shared-memory staging copy did not complete", what);
+        return fail(c, KS_ERR_TIMEOUT, "%s: %s", what,
+                    (f & 2u) ? "a wait of the tensor-core GEMM gave up" : "a shared-memory staging copy did not complete");
     }
     return KS_OK;
 }
@@ -1239,6 +1246,8 @@ int ks_context_create(int device, int flags, ks_context** out) {
     cudaEventCreate(&c->ev1);
     cudaEventCreate(&c->evc0);
     cudaEventCreate(&c->evc1);
+    cudaEventCreate(&c->evg0);
+    cudaEventCreate(&c->evg1);
     if (c->errflag.ensure(sizeof(unsigned)) != cudaSuccess || cudaMemset(c->errflag.p, 0, sizeof(unsigned)) != cudaSuccess) {
         delete c;
         return KS_ERR_DEVICE;
@@ -1260,6 +1269,8 @@ int ks_context_destroy(ks_context* c) {
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->evc0) cudaEventDestroy(c->evc0);
     if (c->evc1) cudaEventDestroy(c->evc1);
+    if (c->evg0) cudaEventDestroy(c->evg0);
+    if (c->evg1) cudaEventDestroy(c->evg1);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->graph) cudaGraphDestroy(c->graph);
@@ -1292,6 +1303,22 @@ int ks_kernel_stats(ks_context* c, double* render_ms, long long* render_launches
 int ks_set_stage_test(ks_context* c, int32_t on) {
     if (!c) return KS_ERR_ARGUMENT;
     c->stage_test = on ? 1 : 0;
+    return KS_OK;
+}
+
+int ks_gemm_stats(ks_context* c, double* ms, long long* launches, double* flops, int reset) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (ms) *ms = c->gemm_ms;
+    if (launches) *launches = c->gemm_launches;
+    if (flops) *flops = c->gemm_flops;
+    if (reset) { c->gemm_ms = 0.0; c->gemm_launches = 0; c->gemm_flops = 0.0; }
+    return KS_OK;
+}
+
+int ks_set_tensor_path(ks_context* c, int32_t path) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (path != KS_TENSOR_TCGEN05 && path != KS_TENSOR_MMA_SYNC) return fail(c, KS_ERR_ARGUMENT, "unknown tensor path %d", path);
+    c->tensor_path = path;
     return KS_OK;
 }
 
@@ -1793,7 +1820,8 @@ int ks_graph_destroy(ks_context* c) {
 // ---- the adjoint (src/Splats/dual_gradient.jl, src/Fit/Fit.jl:451-577) --------------------------------
 
 namespace {
-void gemm(ks_context* c, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb, float* C, long long ldc);
+int gemm(ks_context* c, int M, int N, int K, const float* Ah, const float* Al, long long lda, const float* Bh, const float* Bl, long long ldb,
+         float* C, long long ldc);
 int dft_stage(ks_context* c, int slot, const double* src, size_t count, const double** dev);
 int dft_checks(ks_context* c, int64_t nuv, double psize, double scale, int32_t precision);
 int dft_forward(ks_context* c, const double* dimg, int32_t order, int64_t nuv, const double* du, const double* dv, const double* dtap,
@@ -2406,16 +2434,18 @@ int ks_normal_matrix(ks_context* c, const double* J, int64_t m, int64_t n, int32
         c->launches++;
         KS_CUDA(c, cudaGetLastError());
     } else {
-        // 3xTF32 tensor-core GEMM: A = J^T J from a transposed FP32 copy
-        KS_CUDA(c, c->dft_a.ensure(size_t(m) * n * 2 * sizeof(float) + size_t(n) * n * sizeof(float)));
-        float* Jt = c->dft_a.as<float>();
-        float* Jf = Jt + size_t(m) * n;
-        float* Af = Jf + size_t(m) * n;
-        k_transpose_f32<<<dim3(nb, unsigned((m + 31) / 32)), dim3(32, 8), 0, c->stream>>>(m, int(n), dJ, Jt);
-        k_to_f32<<<nblocks(m * n, 256), 256, 0, c->stream>>>(m * n, dJ, Jf);
-        gemm(c, int(n), int(n), int(m), Jt, m, Jf, n, Af, n);
+        // 3xTF32 tensor-core GEMM: A = J^T J = Jt Jt^T from a split, transposed FP32 copy Jt[n][m]
+        const long long ldj = ksdft::pad4(m);
+        KS_CUDA(c, c->dft_a.ensure(size_t(n) * ldj * 2 * sizeof(float) + size_t(n) * n * sizeof(float)));
+        float* jt_h = c->dft_a.as<float>();
+        float* jt_l = jt_h + n * ldj;
+        float* Af = jt_l + n * ldj;
+        k_transpose_split<<<dim3(nb, unsigned((m + 31) / 32)), dim3(32, 8), 0, c->stream>>>(m, int(n), dJ, jt_h, jt_l, ldj);
+        c->launches++;
+        int s = gemm(c, int(n), int(n), int(m), jt_h, jt_l, ldj, jt_h, jt_l, ldj, Af, n);
+        if (s) return s;
         k_to_f64<<<nblocks(n * n, 256), 256, 0, c->stream>>>(n * n, Af, dA);
-        c->launches += 3;
+        c->launches++;
         KS_CUDA(c, cudaGetLastError());
     }
     if (!dev) KS_CUDA(c, cudaMemcpyAsync(A, dA, size_t(n) * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -2517,23 +2547,117 @@ int dft_checks(ks_context* c, int64_t nuv, double psize, double scale, int32_t p
     return KS_OK;
 }
 
-// The twiddle tables of the separable transform: Tu[i][2k + c] (l_i, u_k) and Tv[j][2k + c] (m_j, v_k).
+// The twiddle tables of the separable transform: Tv[j][2k + c] (m_j, v_k, plain FP32, read by the
+// combine and seed kernels) and the split GEMM operands Tu[i][2k + c] (the adjoint's A, K = 2 nuv) and
+// TuT[2k + c][i] (the forward's B, K = na), both from (l_i, u_k).
+struct Twiddles {
+    float *tu_h, *tu_l, *tut_h, *tut_l;
+    long long ldu, ldut;
+};
+
+Twiddles twiddle_layout(ks_context* c, int64_t nuv) {
+    Twiddles t;
+    const int na = c->nalpha;
+    t.ldu = ksdft::pad4(2 * nuv);
+    t.ldut = ksdft::pad4(na);
+    t.tu_h = c->dft_tu.as<float>();
+    t.tu_l = t.tu_h + na * t.ldu;
+    t.tut_h = t.tu_l + na * t.ldu;
+    t.tut_l = t.tut_h + 2 * nuv * t.ldut;
+    return t;
+}
+
 int dft_twiddles(ks_context* c, int64_t nuv, const double* du, const double* dv, double psize) {
     const int na = c->nalpha, nb = c->nbeta;
-    KS_CUDA(c, c->dft_tu.ensure(size_t(na) * 2 * nuv * sizeof(float)));
+    KS_CUDA(c, c->dft_tu.ensure((size_t(na) * ksdft::pad4(2 * nuv) * 2 + size_t(2 * nuv) * ksdft::pad4(na) * 2) * sizeof(float)));
     KS_CUDA(c, c->dft_tv.ensure(size_t(nb) * 2 * nuv * sizeof(float)));
-    ksdft::k_twiddle<<<nblocks((long long)na * nuv, 256), 256, 0, c->stream>>>(na, -1.0, psize, nuv, du, c->dft_tu.as<float>(), 2 * nuv);
+    const Twiddles t = twiddle_layout(c, nuv);
+    const long long nu = (long long)na * nuv;
+    ksdft::k_twiddle_split<<<nblocks(nu, 256), 256, 0, c->stream>>>(na, -1.0, psize, nuv, du, 0, t.tu_h, t.tu_l, t.ldu);
+    ksdft::k_twiddle_split<<<nblocks(nu, 256), 256, 0, c->stream>>>(na, -1.0, psize, nuv, du, 1, t.tut_h, t.tut_l, t.ldut);
     ksdft::k_twiddle<<<nblocks((long long)nb * nuv, 256), 256, 0, c->stream>>>(nb, 1.0, psize, nuv, dv, c->dft_tv.as<float>(), 2 * nuv);
-    c->launches += 2;
+    c->launches += 3;
     KS_CUDA(c, cudaGetLastError());
     return KS_OK;
 }
 
-void gemm(ks_context* c, int M, int N, int K, const float* A, long long lda, const float* B, long long ldb, float* C, long long ldc) {
-    dim3 grid(unsigned((N + ksdft::BN - 1) / ksdft::BN), unsigned((M + ksdft::BM - 1) / ksdft::BM));
-    ksdft::k_gemm_3xtf32<<<grid, ksdft::NTHREADS, 0, c->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link against libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// A split operand (rows x K floats, row stride ld) as 128-row x 32-float boxes with the 128-byte
+// swizzle; reads past K or past the last row are zero-filled.
+bool operand_map(CUtensorMap* m, const float* p, long long rows, long long K, long long ld) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || (reinterpret_cast<uintptr_t>(p) & 15) || (ld & 3)) return false;
+    cuuint64_t dims[2] = {cuuint64_t(K), cuuint64_t(rows)};
+    cuuint64_t strides[1] = {cuuint64_t(ld) * sizeof(float)};
+    cuuint32_t box[2] = {cuuint32_t(ksdft::TC_BK), cuuint32_t(ksdft::TC_BM)};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(p), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// C[M][N] = A[M][K] B[N][K]^T in 3xTF32 from split operands (ksdft): the tcgen05 kernel unless the
+// context selects the mma.sync fallback. Outside a graph capture, the tcgen05 path reads the device
+// flag after the launch, so a wait that gave up fails the call with KS_ERR_TIMEOUT.
+int gemm(ks_context* c, int M, int N, int K, const float* Ah, const float* Al, long long lda, const float* Bh, const float* Bl, long long ldb,
+         float* C, long long ldc) {
+    if (M < 1 || N < 1) return KS_OK;
+    if (K < 1) {
+        KS_CUDA(c, cudaMemset2DAsync(C, size_t(ldc) * sizeof(float), 0, size_t(N) * sizeof(float), size_t(M), c->stream));
+        return KS_OK;
+    }
     c->launches++;
     c->kernel_launches++;
+    const bool timed = !c->capturing;
+    if (c->tensor_path == 1) {
+        dim3 grid(unsigned((N + ksdft::BN - 1) / ksdft::BN), unsigned((M + ksdft::BM - 1) / ksdft::BM));
+        if (timed) cudaEventRecord(c->evg0, c->stream);
+        ksdft::k_gemm_3xtf32<<<grid, ksdft::NTHREADS, 0, c->stream>>>(M, N, K, Ah, Al, lda, Bh, Bl, ldb, C, ldc);
+        KS_CUDA(c, cudaGetLastError());
+    } else {
+        CUtensorMap tah, tal, tbh, tbl;
+        if (!operand_map(&tah, Ah, M, K, lda) || !operand_map(&tal, Al, M, K, lda) || !operand_map(&tbh, Bh, N, K, ldb) ||
+            !operand_map(&tbl, Bl, N, K, ldb))
+            return fail(c, KS_ERR_DEVICE, "tensor-core GEMM: cannot describe the operands as TMA tensor maps (M %d, N %d, K %d)", M, N, K);
+        {
+            static std::mutex mu;
+            static unsigned long long done_devices = 0;   // one bit per device: the shared-memory opt-in is per device
+            std::lock_guard<std::mutex> lock(mu);
+            if (!(done_devices >> (c->device & 63) & 1)) {
+                KS_CUDA(c, cudaFuncSetAttribute(ksdft::k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, ksdft::TC_SMEM));
+                done_devices |= 1ull << (c->device & 63);
+            }
+        }
+        // a wait gives up after ~1 s at the maximum SM clock (10 ms under the staging test hook)
+        const long long limit = c->stage_test ? 20000000LL : 2000000000LL;
+        dim3 grid(unsigned((N + ksdft::TC_BN - 1) / ksdft::TC_BN), unsigned((M + ksdft::TC_BM - 1) / ksdft::TC_BM));
+        if (timed) cudaEventRecord(c->evg0, c->stream);
+        ksdft::k_gemm_tc<<<grid, ksdft::TC_THREADS, ksdft::TC_SMEM, c->stream>>>(M, N, K, tah, tal, tbh, tbl, C, ldc, limit, c->stage_test,
+                                                                              c->errflag.as<unsigned>());
+        KS_CUDA(c, cudaGetLastError());
+    }
+    if (!timed) return KS_OK;
+    cudaEventRecord(c->evg1, c->stream);
+    KS_CUDA(c, cudaEventSynchronize(c->evg1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->evg0, c->evg1);
+    c->gemm_ms += ms;
+    c->gemm_flops += 6.0 * M * double(N) * K;
+    c->gemm_launches++;
+    return c->tensor_path == 1 ? KS_OK : check_device_flag(c, "tensor-core GEMM");
 }
 
 // V (nuv x 4 complex) of a device image
@@ -2550,13 +2674,17 @@ int dft_forward(ks_context* c, const double* dimg, int32_t order, int64_t nuv, c
     }
     int s = dft_twiddles(c, nuv, du, dv, psize);
     if (s) return s;
-    KS_CUDA(c, c->dft_a.ensure(size_t(4) * nb * na * sizeof(float)));
-    KS_CUDA(c, c->dft_t.ensure(size_t(4) * nb * 2 * nuv * sizeof(float)));
-    ksdft::k_pack_image<<<nblocks((long long)na * nb * 4, 256), 256, 0, c->stream>>>(dimg, inv, na, nb, c->dft_a.as<float>());
+    const Twiddles t = twiddle_layout(c, nuv);
+    const long long lda = ksdft::pad4(na), ldt = ksdft::pad4(2 * nuv);
+    KS_CUDA(c, c->dft_a.ensure(size_t(2) * 4 * nb * lda * sizeof(float)));
+    KS_CUDA(c, c->dft_t.ensure(size_t(4) * nb * ldt * sizeof(float)));
+    float* a_h = c->dft_a.as<float>();
+    float* a_l = a_h + 4LL * nb * lda;
+    ksdft::k_pack_image<<<nblocks((long long)na * nb * 4, 256), 256, 0, c->stream>>>(dimg, inv, na, nb, a_h, a_l, lda);
     c->launches++;
-    gemm(c, 4 * nb, int(2 * nuv), na, c->dft_a.as<float>(), na, c->dft_tu.as<float>(), 2 * nuv, c->dft_t.as<float>(), 2 * nuv);
-    ksdft::k_vis_combine<<<nblocks(nuv * 4, 128), 128, 0, c->stream>>>(nb, nuv, c->dft_t.as<float>(), 2 * nuv, c->dft_tv.as<float>(),
-                                                                       2 * nuv, dtap, scale, dV);
+    if ((s = gemm(c, 4 * nb, int(2 * nuv), na, a_h, a_l, lda, t.tut_h, t.tut_l, t.ldut, c->dft_t.as<float>(), ldt))) return s;
+    ksdft::k_vis_combine<<<nblocks(nuv * 4, 128), 128, 0, c->stream>>>(nb, nuv, c->dft_t.as<float>(), ldt, c->dft_tv.as<float>(), 2 * nuv,
+                                                                       dtap, scale, dV);
     c->launches++;
     KS_CUDA(c, cudaGetLastError());
     return KS_OK;
@@ -2578,12 +2706,16 @@ int dft_adjoint(ks_context* c, const double* dw, int64_t nuv, const double* du, 
         int s = dft_twiddles(c, nuv, du, dv, psize);
         if (s) return s;
     }
-    KS_CUDA(c, c->dft_c.ensure(size_t(2) * nuv * 4 * nb * sizeof(float)));
+    const Twiddles t = twiddle_layout(c, nuv);
+    const long long ldc = ksdft::pad4(2 * nuv);
+    KS_CUDA(c, c->dft_c.ensure(size_t(2) * 4 * nb * ldc * sizeof(float)));
     KS_CUDA(c, c->dft_s.ensure(size_t(na) * 4 * nb * sizeof(float)));
-    ksdft::k_seed_rhs<<<nblocks(nuv * 4 * nb, 256), 256, 0, c->stream>>>(nb, nuv, c->dft_tv.as<float>(), 2 * nuv, dw, dtap, scale,
-                                                                        c->dft_c.as<float>(), 4 * nb);
+    float* c_h = c->dft_c.as<float>();
+    float* c_l = c_h + 4LL * nb * ldc;
+    ksdft::k_seed_rhs<<<nblocks(nuv * 4 * nb, 256), 256, 0, c->stream>>>(nb, nuv, c->dft_tv.as<float>(), 2 * nuv, dw, dtap, scale, c_h, c_l, ldc);
     c->launches++;
-    gemm(c, na, 4 * nb, int(2 * nuv), c->dft_tu.as<float>(), 2 * nuv, c->dft_c.as<float>(), 4 * nb, c->dft_s.as<float>(), 4 * nb);
+    int s = gemm(c, na, 4 * nb, int(2 * nuv), t.tu_h, t.tu_l, t.ldu, c_h, c_l, ldc, c->dft_s.as<float>(), 4 * nb);
+    if (s) return s;
     ksdft::k_unpack_seed<<<nblocks((long long)na * nb * 4, 256), 256, 0, c->stream>>>(c->dft_s.as<float>(), 4 * nb, na, nb, inv, dseed);
     c->launches++;
     KS_CUDA(c, cudaGetLastError());

@@ -89,3 +89,78 @@ def test_transform_of_ehtim_source_image_matches_its_observation(prec, tol):
     print("GPU transform of the source image vs the noiseless observation", prec, err)
     assert err < tol
     cache.close()
+
+
+def _ragged_case(na, nb, nuv, seed):
+    cam = ks.Camera((-16.0, 16.0), (-14.0, 14.0), (na, nb))
+    cache = ks.GeodesicCache(cam, 8)
+    ks.regenerate(cache, 0.7, np.deg2rad(30.0))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    img = np.abs(rng.standard_normal((na * nb, 4))) * np.array([1.0, 0.2, 0.2, 0.05])
+    rad = 10e9 * np.sqrt(rng.uniform(0, 1, nuv))
+    ang = rng.uniform(0, 2 * np.pi, nuv)
+    L, D = ks.gravitational_radius(6.5e9), 16.8e6 * 3.085678e18
+    psize = (32.0 / max(na - 1, 1)) * L / D
+    w = rng.standard_normal((nuv, 4)) + 1j * rng.standard_normal((nuv, 4))
+    return cache, img, rad * np.cos(ang), rad * np.sin(ang), psize, psize ** 2 / 1e-23, np.exp(-rng.uniform(0, 0.3, nuv)), w
+
+
+@pytest.mark.parametrize("na,nb,nuv", [(48, 40, 300), (37, 29, 131), (130, 3, 1), (8, 200, 257), (300, 33, 70)])
+def test_tensor_paths_agree_on_ragged_shapes(oracle, na, nb, nuv):
+    """The tcgen05 GEMM (TMA tiles, UMMA into TMEM) and the mma.sync fallback on the same split
+    operands, at shapes with partial tiles in M, N and K (K = na < 32, na not a multiple of 4, one
+    baseline): both within 1e-5 of the FP64 oracle (forward and adjoint) and within 1e-6 of each other
+    (they differ only in the FP32 accumulation order)."""
+    cache, img, u, v, psize, scale, tap, w = _ragged_case(na, nb, nuv, 7 + na)
+    ref_v = oracle.visibilities(img, na, nb, u, v, tap, psize, scale)
+    ref_s = oracle.vis_seed(w, na, nb, u, v, tap, psize, scale)
+    got = {}
+    for path in ("tcgen05", "mma.sync"):
+        cache.set_tensor_path(path)
+        got[path] = (ks.visibilities(cache, img, u, v, psize, scale, tap=tap, precision=ks.KS_MIXED),
+                     ks.vis_seed(cache, w, u, v, psize, scale, tap=tap, precision=ks.KS_MIXED))
+        assert rel(got[path][0], ref_v) < 1e-5, (path, rel(got[path][0], ref_v))
+        assert rel(got[path][1], ref_s) < 1e-5, (path, rel(got[path][1], ref_s))
+    cache.set_tensor_path("tcgen05")
+    assert rel(got["tcgen05"][0], got["mma.sync"][0]) < 1e-6
+    assert rel(got["tcgen05"][1], got["mma.sync"][1]) < 1e-6
+    # repeated calls are bitwise reproducible (fixed tiles, fixed accumulation order)
+    again = ks.visibilities(cache, img, u, v, psize, scale, tap=tap, precision=ks.KS_MIXED)
+    assert np.array_equal(again, got["tcgen05"][0])
+    cache.close()
+
+
+@pytest.mark.parametrize("m,n", [(1000, 77), (131, 300), (5, 3)])
+def test_normal_matrix_tensor_paths(m, n):
+    """J^T J through both GEMM kernels (Jt Jt^T from one split transposed copy) against numpy. The
+    bound is 5e-5 of the largest entry: the products are 3xTF32-exact to ~5e-7, and what remains is the
+    FP32 accumulation of K = m terms in the tensor cores (up to m 2^-23 relative for same-sign terms,
+    1.1e-5 measured at m = 1000); both kernels accumulate in the same order and agree to 1e-6."""
+    cam = ks.Camera((-1.0, 1.0), (-1.0, 1.0), 2)
+    cache = ks.GeodesicCache(cam, 8)
+    rng = np.random.Generator(np.random.PCG64(m + n))
+    J = rng.standard_normal((m, n)) * np.exp(rng.uniform(-2, 2, n))[None]
+    ref = J.T @ J
+    out = {}
+    for path in ("tcgen05", "mma.sync"):
+        cache.set_tensor_path(path)
+        out[path] = ks.normal_matrix(cache, J, precision=ks.KS_MIXED)
+        assert np.max(np.abs(out[path] - ref)) <= 5e-5 * np.abs(ref).max(), path
+    assert np.max(np.abs(out["tcgen05"] - out["mma.sync"])) <= 1e-6 * np.abs(ref).max()
+    cache.close()
+
+
+def test_tensor_core_gemm_wait_gives_up_cleanly():
+    """The tcgen05 GEMM's bounded waits: under the test hook its operand barriers are armed but no
+    tile copy is issued, every wait gives up after ~10 ms, the blocks free their TMEM and return, and
+    the call fails with KS_ERR_TIMEOUT; the context then computes the same visibilities as before."""
+    cache, img, u, v, psize, scale, tap, w = _ragged_case(40, 36, 200, 3)
+    ref = ks.visibilities(cache, img, u, v, psize, scale, tap=tap, precision=ks.KS_MIXED)
+    cache.set_stage_test(True)
+    with pytest.raises(ks.KsError) as err:
+        ks.visibilities(cache, img, u, v, psize, scale, tap=tap, precision=ks.KS_MIXED)
+    assert err.value.status == ks._lib.KS_ERR_TIMEOUT
+    cache.set_stage_test(False)
+    again = ks.visibilities(cache, img, u, v, psize, scale, tap=tap, precision=ks.KS_MIXED)
+    assert np.array_equal(again, ref)
+    cache.close()
