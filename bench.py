@@ -490,12 +490,14 @@ def run_dft(args):
     img = np.abs(rng.standard_normal((npix, 4))) * np.array([1.0, 0.2, 0.2, 0.05])
     nuv = len(c["u"])
     w = rng.standard_normal((nuv, 4)) + 1j * rng.standard_normal((nuv, 4))
+    # pinned host buffers for the image and the seed (the two large copies of a step)
     img_h = torch.from_numpy(img).pin_memory().numpy()
+    seed_h = torch.empty((npix, 4), dtype=torch.float64).pin_memory().numpy()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
     def step():
         V = ks.visibilities(cache, img_h, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_MIXED)
-        S = ks.vis_seed(cache, w, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_MIXED)
+        S = ks.vis_seed(cache, w, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_MIXED, out=seed_h)
         return V, S
 
     res = {}
@@ -515,7 +517,7 @@ def run_dft(args):
                 tot += time.perf_counter() - t0
         gms, gl, gfl = cache.gemm_stats(reset=True)
         res[path] = {"ms_per_step": tot * 1e3 / args.steps, "gemm_ms_per_step": gms / args.steps, "gemm_launches": gl,
-                     "gemm_tflops": gfl / (gms * 1e-3) / 1e12, "V": V, "S": S, "clocks": clocks.summary()}
+                     "gemm_tflops": gfl / (gms * 1e-3) / 1e12, "V": V, "S": S.copy(), "clocks": clocks.summary()}
     cache.set_tensor_path("tcgen05")
     t0 = time.perf_counter()
     V64 = ks.visibilities(cache, img_h, c["u"], c["v"], c["psize"], c["scale"], precision=ks.KS_FP64)

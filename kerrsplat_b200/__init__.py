@@ -733,27 +733,36 @@ def _complex_pairs(z):
     return z.view(np.float64)
 
 
-def visibilities(cache, image, u, v, psize, scale, tap=None, precision=KS_MIXED, order="screen"):
+def _out_array(out, shape, dtype):
+    if out is None:
+        return np.empty(shape, dtype=dtype)
+    if out.shape != shape or out.dtype != dtype or not out.flags.c_contiguous:
+        raise ValueError(f"out must be a C-contiguous {dtype.__name__} array of shape {shape}")
+    return out
+
+
+def visibilities(cache, image, u, v, psize, scale, tap=None, precision=KS_MIXED, order="screen", out=None):
     """Stokes visibilities V (nuv, 4) complex of an (npix, 4) image (device_visibilities.jl:61-73):
     V_k = tap_k scale sum_j I_j exp(2 pi i (u_k l_j + v_k m_j)), l toward the east (-alpha). The mixed
-    path runs the separable transform as 3xTF32 tensor-core GEMMs; KS_FP64 is the direct transform."""
+    path runs the separable transform as 3xTF32 tensor-core GEMMs; KS_FP64 is the direct transform.
+    `out` (optional): a (nuv, 4) complex128 array to write into (pinned host memory copies faster)."""
     img = np.ascontiguousarray(image, dtype=np.float64).reshape(cache.npix, 4)
     u = np.ascontiguousarray(u, dtype=np.float64); v = np.ascontiguousarray(v, dtype=np.float64)
     tp = None if tap is None else np.ascontiguousarray(tap, dtype=np.float64)
-    out = np.empty((u.size, 4), dtype=np.complex128)
+    out = _out_array(out, (u.size, 4), np.complex128)
     o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
     cache._check(cache._lib.ks_visibilities(cache._ctx, _ptr(img), o, u.size, _ptr(u), _ptr(v), None if tp is None else _ptr(tp),
                                             float(psize), float(scale), _precision(precision), _ptr(out.view(np.float64))))
     return out
 
 
-def vis_seed(cache, w, u, v, psize, scale, tap=None, precision=KS_MIXED, order="screen"):
+def vis_seed(cache, w, u, v, psize, scale, tap=None, precision=KS_MIXED, order="screen", out=None):
     """The adjoint of `visibilities` applied to weights w (nuv, 4) complex: seed (npix, 4)
-    (seed_kernel!, device_visibilities.jl:76-88)."""
+    (seed_kernel!, device_visibilities.jl:76-88). `out` (optional): an (npix, 4) float64 array."""
     wp = _complex_pairs(w)
     u = np.ascontiguousarray(u, dtype=np.float64); v = np.ascontiguousarray(v, dtype=np.float64)
     tp = None if tap is None else np.ascontiguousarray(tap, dtype=np.float64)
-    out = np.empty((cache.npix, 4))
+    out = _out_array(out, (cache.npix, 4), np.float64)
     o = _lib.KS_ORDER_SCREEN if order == "screen" else _lib.KS_ORDER_SORTED
     cache._check(cache._lib.ks_vis_seed(cache._ctx, _ptr(wp), u.size, _ptr(u), _ptr(v), None if tp is None else _ptr(tp), float(psize),
                                         float(scale), _precision(precision), _ptr(out), o))

@@ -7,7 +7,7 @@
 // the plain FP64 path here does the same. The mixed path uses the separable form
 //     T[(s, j), (k, c|s)] = sum_i I_s[i, j] (cos | sin)(2 pi u_k l_i)          (a GEMM, K = na)
 //     V_k,s = tap_k scale sum_j exp(2 pi i v_k m_j) (T_c + i T_s)[(s, j), k]    (a reduction over j)
-// and the adjoint seed[i, (s, j)] = sum_k [cos . C_r + sin . C_i][i, k]         (a GEMM, K = 2 nuv)
+// and the adjoint seed[(s, j), i] = sum_k [C_r . cos + C_i . sin][(s, j), k]   (a GEMM, K = 2 nuv)
 // with C[k, (s, j)] = conj(exp(2 pi i v_k m_j)) w_k,s tap_k scale.
 //
 // The GEMMs run on the tensor cores in 3xTF32. Every operand x is stored split, x_hi = tf32(x) and
@@ -74,17 +74,23 @@ __global__ void k_twiddle_split(int nx, double sign, double psize, long long nf,
     split_store(hi, lo, transposed ? (2 * k + 1) * ld + x : x * ld + 2 * k + 1, s);
 }
 
-// image (npix x 4 doubles, screen order p = i + j na, or sorted with perm) -> split A[(s nb + j) lda + i]
+// image (npix x 4 doubles, screen order p = i + j na, or sorted with perm) -> split A[(s nb + j) lda + i];
+// one thread per pixel (its four Stokes values are one 32-byte read)
 __global__ void k_pack_image(const double* __restrict__ img, const long long* __restrict__ inv_perm, int na, int nb,
                              float* __restrict__ hi, float* __restrict__ lo, long long lda) {
-    long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    long long npix = (long long)na * nb;
-    if (q >= npix * 4) return;
-    long long p = q % npix;   // screen index
-    int s = int(q / npix);
-    long long src = inv_perm ? inv_perm[p] : p;
-    long long i = p % na, j = p / na;
-    split_store(hi, lo, ((long long)s * nb + j) * lda + i, float(img[src * 4 + s]));
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;   // screen index
+    if (p >= (long long)na * nb) return;
+    const long long src = inv_perm ? inv_perm[p] : p;
+    double v[4];
+    if ((reinterpret_cast<uintptr_t>(img) & 31) == 0) {
+        const double4 I = *reinterpret_cast<const double4*>(img + src * 4);
+        v[0] = I.x, v[1] = I.y, v[2] = I.z, v[3] = I.w;
+    } else {
+        for (int s = 0; s < 4; ++s) v[s] = img[src * 4 + s];
+    }
+    const long long i = p % na, j = p / na;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) split_store(hi, lo, ((long long)s * nb + j) * lda + i, float(v[s]));
 }
 
 // ---- the mma.sync fallback ------------------------------------------------------------------------
@@ -356,24 +362,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
 }
 
-// V[k][s] = tap_k scale sum_j (Bc + i Bs)[j][k] (Tc + i Ts)[(s, j)][k]  (complex, written as re, im doubles)
-__global__ void k_vis_combine(int nb, long long nuv, const float* __restrict__ Tm, long long ldt, const float* __restrict__ Bv, long long ldb,
-                              const double* __restrict__ tap, double scale, double* __restrict__ V) {
-    long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (q >= nuv * 4) return;
-    long long k = q % nuv;
-    int s = int(q / nuv);
+// V[k][s] = tap_k scale sum_j (Bc + i Bs)[j][k] (Tc + i Ts)[(s, j)][k]  (complex, written as re, im doubles).
+// A block of 32 baselines x 8 row groups for one Stokes parameter (grid.y): each thread sums the rows
+// j = g, g + 8, ... of its baseline in FP64, and the 8 partial sums are added in a fixed order.
+constexpr int VC_K = 32, VC_G = 8;
+__global__ void __launch_bounds__(VC_K* VC_G) k_vis_combine(int nb, long long nuv, const float* __restrict__ Tm, long long ldt,
+                                                             const float* __restrict__ Bv, long long ldb, const double* __restrict__ tap,
+                                                             double scale, double* __restrict__ V) {
+    __shared__ double red[2][VC_G][VC_K];
+    const int kl = threadIdx.x % VC_K, g = threadIdx.x / VC_K, s = blockIdx.y;
+    const long long k = (long long)blockIdx.x * VC_K + kl;
     double re = 0.0, im = 0.0;
-    for (int j = 0; j < nb; ++j) {
-        double bc = Bv[(long long)j * ldb + 2 * k], bs = Bv[(long long)j * ldb + 2 * k + 1];
-        const float* tr = Tm + ((long long)s * nb + j) * ldt + 2 * k;
-        double tc = tr[0], ts = tr[1];
-        re += bc * tc - bs * ts;
-        im += bc * ts + bs * tc;
+    if (k < nuv) {
+        for (int j = g; j < nb; j += VC_G) {
+            const float2 b = *reinterpret_cast<const float2*>(Bv + (long long)j * ldb + 2 * k);
+            const float2 t = *reinterpret_cast<const float2*>(Tm + ((long long)s * nb + j) * ldt + 2 * k);
+            re += double(b.x) * t.x - double(b.y) * t.y;
+            im += double(b.x) * t.y + double(b.y) * t.x;
+        }
     }
-    double f = (tap ? tap[k] : 1.0) * scale;
-    V[(k * 4 + s) * 2] = re * f;
-    V[(k * 4 + s) * 2 + 1] = im * f;
+    red[0][g][kl] = re;
+    red[1][g][kl] = im;
+    __syncthreads();
+    if (g == 0 && k < nuv) {
+        for (int q = 1; q < VC_G; ++q) { re += red[0][q][kl]; im += red[1][q][kl]; }
+        const double f = (tap ? tap[k] : 1.0) * scale;
+        V[(k * 4 + s) * 2] = re * f;
+        V[(k * 4 + s) * 2 + 1] = im * f;
+    }
 }
 
 // The adjoint right-hand side, split and K-major: CT[(s nb + j) ld + 2k + c] = (C_r | C_i)[k][(s, j)],
@@ -391,17 +407,23 @@ __global__ void k_seed_rhs(int nb, long long nuv, const float* __restrict__ Bv, 
     split_store(hi, lo, sj * ldc + 2 * k + 1, float(bc * wi - bs * wr));
 }
 
-// seed[(i, (s, j))] -> out (npix x 4, screen order or sorted through perm)
+// seed S[(s nb + j) lds + i] -> out (npix x 4, screen order or sorted through perm); one thread per pixel
 __global__ void k_unpack_seed(const float* __restrict__ S, long long lds, int na, int nb, const long long* __restrict__ inv_perm,
                               double* __restrict__ out) {
-    long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    long long npix = (long long)na * nb;
-    if (q >= npix * 4) return;
-    long long p = q % npix;
-    int s = int(q / npix);
-    long long i = p % na, j = p / na;
-    long long dst = inv_perm ? inv_perm[p] : p;
-    out[dst * 4 + s] = double(S[i * lds + (long long)s * nb + j]);
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= (long long)na * nb) return;
+    const long long i = p % na, j = p / na;
+    const long long dst = inv_perm ? inv_perm[p] : p;
+    double4 o;
+    o.x = S[j * lds + i];
+    o.y = S[((long long)nb + j) * lds + i];
+    o.z = S[(2LL * nb + j) * lds + i];
+    o.w = S[(3LL * nb + j) * lds + i];
+    if ((reinterpret_cast<uintptr_t>(out) & 31) == 0) {
+        *reinterpret_cast<double4*>(out + dst * 4) = o;
+    } else {
+        out[dst * 4] = o.x, out[dst * 4 + 1] = o.y, out[dst * 4 + 2] = o.z, out[dst * 4 + 3] = o.w;
+    }
 }
 
 // The plain FP64 port of vis_kernel! (one thread per baseline, a sincos per pixel).

@@ -2548,7 +2548,7 @@ int dft_checks(ks_context* c, int64_t nuv, double psize, double scale, int32_t p
 }
 
 // The twiddle tables of the separable transform: Tv[j][2k + c] (m_j, v_k, plain FP32, read by the
-// combine and seed kernels) and the split GEMM operands Tu[i][2k + c] (the adjoint's A, K = 2 nuv) and
+// combine and seed kernels) and the split GEMM operands Tu[i][2k + c] (the adjoint's B, K = 2 nuv) and
 // TuT[2k + c][i] (the forward's B, K = na), both from (l_i, u_k).
 struct Twiddles {
     float *tu_h, *tu_l, *tut_h, *tut_l;
@@ -2680,11 +2680,11 @@ int dft_forward(ks_context* c, const double* dimg, int32_t order, int64_t nuv, c
     KS_CUDA(c, c->dft_t.ensure(size_t(4) * nb * ldt * sizeof(float)));
     float* a_h = c->dft_a.as<float>();
     float* a_l = a_h + 4LL * nb * lda;
-    ksdft::k_pack_image<<<nblocks((long long)na * nb * 4, 256), 256, 0, c->stream>>>(dimg, inv, na, nb, a_h, a_l, lda);
+    ksdft::k_pack_image<<<nblocks((long long)na * nb, 256), 256, 0, c->stream>>>(dimg, inv, na, nb, a_h, a_l, lda);
     c->launches++;
     if ((s = gemm(c, 4 * nb, int(2 * nuv), na, a_h, a_l, lda, t.tut_h, t.tut_l, t.ldut, c->dft_t.as<float>(), ldt))) return s;
-    ksdft::k_vis_combine<<<nblocks(nuv * 4, 128), 128, 0, c->stream>>>(nb, nuv, c->dft_t.as<float>(), ldt, c->dft_tv.as<float>(), 2 * nuv,
-                                                                       dtap, scale, dV);
+    ksdft::k_vis_combine<<<dim3(unsigned((nuv + ksdft::VC_K - 1) / ksdft::VC_K), 4), ksdft::VC_K * ksdft::VC_G, 0, c->stream>>>(
+        nb, nuv, c->dft_t.as<float>(), ldt, c->dft_tv.as<float>(), 2 * nuv, dtap, scale, dV);
     c->launches++;
     KS_CUDA(c, cudaGetLastError());
     return KS_OK;
@@ -2709,14 +2709,16 @@ int dft_adjoint(ks_context* c, const double* dw, int64_t nuv, const double* du, 
     const Twiddles t = twiddle_layout(c, nuv);
     const long long ldc = ksdft::pad4(2 * nuv);
     KS_CUDA(c, c->dft_c.ensure(size_t(2) * 4 * nb * ldc * sizeof(float)));
-    KS_CUDA(c, c->dft_s.ensure(size_t(na) * 4 * nb * sizeof(float)));
+    const long long lds = ksdft::pad4(na);
+    KS_CUDA(c, c->dft_s.ensure(size_t(4) * nb * lds * sizeof(float)));
     float* c_h = c->dft_c.as<float>();
     float* c_l = c_h + 4LL * nb * ldc;
     ksdft::k_seed_rhs<<<nblocks(nuv * 4 * nb, 256), 256, 0, c->stream>>>(nb, nuv, c->dft_tv.as<float>(), 2 * nuv, dw, dtap, scale, c_h, c_l, ldc);
     c->launches++;
-    int s = gemm(c, na, 4 * nb, int(2 * nuv), t.tu_h, t.tu_l, t.ldu, c_h, c_l, ldc, c->dft_s.as<float>(), 4 * nb);
+    // S[(s, j)][i] = CT Tu^T: rows of the seed image, so that the unpacking reads along i
+    int s = gemm(c, 4 * nb, na, int(2 * nuv), c_h, c_l, ldc, t.tu_h, t.tu_l, t.ldu, c->dft_s.as<float>(), lds);
     if (s) return s;
-    ksdft::k_unpack_seed<<<nblocks((long long)na * nb * 4, 256), 256, 0, c->stream>>>(c->dft_s.as<float>(), 4 * nb, na, nb, inv, dseed);
+    ksdft::k_unpack_seed<<<nblocks((long long)na * nb, 256), 256, 0, c->stream>>>(c->dft_s.as<float>(), lds, na, nb, inv, dseed);
     c->launches++;
     KS_CUDA(c, cudaGetLastError());
     return KS_OK;
