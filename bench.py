@@ -129,7 +129,7 @@ def run_ours(args):
     torch.cuda.set_device(local)
     build.build(verbose=False)
     c = workload(seed_offset=rank, res=args.res, nsamples=args.nsamples)
-    prec = {"mixed": ks.KS_MIXED, "mixed_fp32": ks.KS_MIXED_FP32, "fp64": ks.KS_FP64}[args.precision]
+    prec = {"mixed": ks.KS_MIXED, "mixed_geo64": ks.KS_MIXED_GEO64, "fp64": ks.KS_FP64}[args.precision]
     cache = ks.GeodesicCache(c["camera"], c["N"], device=local)
     ks.regenerate(cache, c["a"], c["theta_o"], marcher=ks.Fused(c["M"]))
     dev = torch.device("cuda", local)
@@ -607,7 +607,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed_fp32", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed_geo64", "fp64"])
     ap.add_argument("--cpu-rays", type=int, default=1024)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -37,11 +37,12 @@ extern "C" {
 
 /* precision of a render */
 #define KS_FP64 0   /* the plain FP64 path: one re-march per (frame, frequency), like the reference */
-#define KS_MIXED 1  /* FP64 geodesics (constants, anchors and the march, once per render) feeding the
-                       FP32 transport (coefficients, frames, the exact step): the reference's
-                       precision(cache, Float32) arrangement, cache.jl:212-232 */
-#define KS_MIXED_FP32 2  /* ks_render only: the march in FP32 as well, re-anchored to the FP64 anchors
-                            (about 9% faster; 5e-4 relative on axis-grazing and near-critical rays) */
+#define KS_MIXED 1  /* FP64 ray constants and anchors; the march once per render in FP32 (the radial
+                       recurrence and the quadrature, re-anchored to the FP64 anchors every M samples;
+                       the polar state, cos theta and krang_visible in FP64); the FP32 transport
+                       (coefficients, frames, the exact step) */
+#define KS_MIXED_GEO64 2  /* ks_render, the adjoint and J v: the FP64 march feeding the same FP32 transport
+                             (the reference's precision(cache, Float32) arrangement, cache.jl:212-232) */
 
 /* output order */
 #define KS_ORDER_SORTED 0   /* root-case-sorted slots (the reference's fused_march! output) */

@@ -19,13 +19,13 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import KS_FP64, KS_MIXED, KS_MIXED_FP32, KsError
+from ._lib import KS_FP64, KS_MIXED, KS_MIXED_GEO64, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
     "polarized_image", "polarized_cube", "render", "capture_render", "RenderGraph", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "RIAFModel", "riaf_image", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
-    "KS_FP64", "KS_MIXED", "KS_MIXED_FP32", "KsError", "NU0",
+    "KS_FP64", "KS_MIXED", "KS_MIXED_GEO64", "KsError", "NU0",
 ]
 
 # constants.jl:3-12 and coefficients.jl:299
@@ -289,8 +289,8 @@ def _precision(p):
         return KS_FP64
     if p in (KS_MIXED, "mixed", "fp32"):
         return KS_MIXED
-    if p in (KS_MIXED_FP32, "mixed_fp32"):
-        return KS_MIXED_FP32
+    if p in (KS_MIXED_GEO64, "mixed_geo64"):
+        return KS_MIXED_GEO64
     raise ValueError(f"unknown precision {p!r}")
 
 

@@ -19,7 +19,7 @@ KS_ERR_TIMEOUT = 6
 
 KS_FP64 = 0
 KS_MIXED = 1
-KS_MIXED_FP32 = 2
+KS_MIXED_GEO64 = 2
 KS_ORDER_SORTED = 0
 KS_ORDER_SCREEN = 1
 

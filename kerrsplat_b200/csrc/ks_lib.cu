@@ -56,6 +56,7 @@ __device__ __forceinline__ MarchRay<T> march_ray_of(const RayCT<T>& R, const Spa
     M.Qt = R.Qt; M.Qtm = R.Qtm; M.Qphi = R.Qphi; M.Qphim = R.Qphim; M.r4 = R.r4; M.qC = R.qC; M.qn = R.qn;
     M.sqrt_eps = R.sqrt_eps; M.gc = R.gc; M.mp = R.mp; M.K2 = R.K2;
     M.vabsalpha = R.vabsalpha; M.valpha2 = R.valpha2; M.vabsbeta = R.vabsbeta; M.vabscos = st.abscos; M.vcos2 = st.cos2;
+    M.pa = st.a;
     return M;
 }
 
@@ -872,7 +873,7 @@ struct ks_context {
     long long adjoint_launches = 0;
     bool count_events = false;
     int tensor_path = 0;  // 3xTF32 GEMMs: 0 tcgen05 (k_gemm_tc), 1 mma.sync (k_gemm_3xtf32); ks_set_tensor_path
-    bool geo64 = true;    // mixed path: FP64 march feeding the FP32 transport (false: KS_MIXED_FP32 march)
+    bool geo64 = false;   // mixed path: the FP64 march feeds the FP32 transport (KS_MIXED_GEO64) instead of the FP32 march
     long long total_anchors = 0;
     int max_nanch = 0;
     long long ranges[6] = {0, 0, 0, 0, 0, 0};
@@ -1077,7 +1078,8 @@ int check_device_flag(ks_context* c, const char* what) {
     return KS_OK;
 }
 
-// The FP32 sample stream of every ray (k_stream; FP64 march unless c->geo64 is off), [k][field][npad].
+// The FP32 sample stream of every ray (k_stream: the FP32 march, or the FP64 march under
+// KS_MIXED_GEO64), [k][field][npad].
 int launch_stream(ks_context* c) {
     const int M = c->st.M, N = c->st.N;
     const int sseg = std::max(M, (N / 4 + M - 1) / M * M);
@@ -1589,12 +1591,12 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
     if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
     if (nsets < 0 || (nsets > 0 && !sets)) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
     if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
-    if (precision != KS_FP64 && precision != KS_MIXED && precision != KS_MIXED_FP32)
+    if (precision != KS_FP64 && precision != KS_MIXED && precision != KS_MIXED_GEO64)
         return fail(c, KS_ERR_ARGUMENT, "unknown precision %d", precision);
     if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
     if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
-    c->geo64 = precision != KS_MIXED_FP32;
-    if (precision == KS_MIXED_FP32) precision = KS_MIXED;
+    c->geo64 = precision == KS_MIXED_GEO64;
+    if (precision == KS_MIXED_GEO64) precision = KS_MIXED;
     if (!std::isfinite(slab)) return fail(c, KS_ERR_NONFINITE, "non-finite slab");
     KS_CUDA(c, cudaSetDevice(c->device));
     std::vector<double> ht(nframes), hnu(nfreq);
@@ -1973,6 +1975,8 @@ int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double
     if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
     if (nsets < 0 || (nsets > 0 && !sets)) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
     if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    const bool geo = precision == KS_MIXED_GEO64;   // the FP64 march under the mixed transport
+    if (geo) precision = KS_MIXED;
     if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d for the adjoint", precision);
     if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
     if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
@@ -2021,7 +2025,7 @@ int adjoint_run(ks_context* c, const ks_splat_set* sets, int nsets, const double
     const int* kst = nullptr;
     const size_t tab_smem = size_t(ntot) * ST_COUNT * sizeof(double);
     if (mixed) {
-        c->geo64 = true;
+        c->geo64 = geo;
         const size_t rows = size_t(ncombo) * N * c->npad;
         KS_CUDA(c, c->adj_state.ensure(rows * 27 * sizeof(float)));
         KS_CUDA(c, c->adj_act.ensure(rows));
@@ -2246,6 +2250,8 @@ int jvp_impl(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doubl
     if (!c->regenerated) return fail(c, KS_ERR_NOT_REGENERATED, "regenerate the context first");
     if (nsets < 1 || !sets) return fail(c, KS_ERR_ARGUMENT, "bad splat sets");
     if (nframes < 1 || nfreq < 1 || !times || !nus) return fail(c, KS_ERR_ARGUMENT, "need at least one frame and one frequency");
+    const bool geo = precision == KS_MIXED_GEO64;
+    if (geo) precision = KS_MIXED;
     if (precision != KS_FP64 && precision != KS_MIXED) return fail(c, KS_ERR_ARGUMENT, "unknown precision %d for the JVP", precision);
     if (order != KS_ORDER_SORTED && order != KS_ORDER_SCREEN) return fail(c, KS_ERR_ARGUMENT, "unknown order %d", order);
     if (!(std::isfinite(L) && L > 0)) return fail(c, KS_ERR_NONFINITE, "length unit must be finite and positive");
@@ -2297,8 +2303,8 @@ int jvp_impl(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doubl
     KS_CUDA(c, c->jvp_out.ensure(size_t(K) * nrc * 4 * sizeof(double)));
     cudaEventRecord(c->ev0, c->stream);
     if (precision == KS_MIXED) {
-        // the mixed J v reads the samples of the FP32 stream (the FP64 march, once for every chunk)
-        c->geo64 = true;
+        // the mixed J v reads the samples of the FP32 stream (the march once for every chunk)
+        c->geo64 = geo;
         int s = launch_stream(c);
         if (s) return s;
     }

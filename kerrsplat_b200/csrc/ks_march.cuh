@@ -2,9 +2,14 @@
 // reading the FP64 plan and anchor table built by regenerate.
 //
 // T = double is the plain FP64 port of the reference's march_ray, sample for sample. T = float is
-// the mixed path: the recurrence and the quadrature run in FP32 and are reset to the FP64 anchors
-// every M samples; the smooth t-integrand uses the cancellation-free large-r form there (its
-// r^2 terms would otherwise lose everything in FP32 at r ~ 1e4).
+// the mixed path: the radial recurrence and the quadrature run in FP32 and are reset to the FP64
+// anchors every M samples; the smooth t-integrand uses the cancellation-free large-r form there (its
+// r^2 terms would otherwise lose everything in FP32 at r ~ 1e4). The polar recurrence, cos theta and
+// the visibility test stay in FP64 (PolarT): the test is krang_visible (recurrence.jl:299-308), whose
+// boundary |beta| = beta_boundary(theta_s) is the polar turning point itself, so the samples next to a
+// turning point flip validity under an FP32 cos theta (2.5e-4 of the configuration-2 image, all of
+// it from those flags); with the polar state in FP64 the flags are the FP64 march's, operation for
+// operation.
 #pragma once
 #include "ks_plan.cuh"
 
@@ -22,16 +27,25 @@ template <class T> struct TimeOf { using type = double; };
 template <class S, int N> struct TimeOf<Dual<S, N>> { using type = Dual<S, N>; };
 template <class T> using TimeT = typename TimeOf<T>::type;
 
+// The precision of the polar state (Jacobi amplitude of theta, cos theta, the visibility test): FP64
+// under the FP32 march, the march's own type otherwise.
+template <class T> struct PolarOf { using type = T; };
+template <> struct PolarOf<float> { using type = double; };
+template <class T> using PolarT = typename PolarOf<T>::type;
+
 template <class T>
 struct MarchRay {
+    using PT = PolarT<T>;
     int rcase;
     T k, c, fo, m0, m1, m2, m3;
     TimeT<T> tau_valid, dtau, fo_d;  // compared against sample times in FP64
-    T pmu, pscale, tempfac, poffset, sqrt_up, um, up_m_um, psign;
+    PT pmu, pscale, sqrt_up, um, up_m_um, psign;
+    T tempfac, poffset;
     bool vortical, scattering;
     T a, lam, eta, rp, rmn, sp, sm, Qt, Qtm, Qphi, Qphim, r4, qC, qn, sqrt_eps, gc, mp, K2;
-    T vabsalpha, valpha2, vabsbeta, vabscos, vcos2;
-    JS<T> dr, dth;
+    PT vabsalpha, valpha2, vabsbeta, vabscos, vcos2, pa;   // krang_visible's constants (pa: the spin)
+    JS<T> dr;
+    JS<PT> dth;
     int turn_k, Manchor, nanch, nsamp;
     long long anchor_off;
 };
@@ -51,19 +65,20 @@ __device__ __forceinline__ MarchRay<T> load_ray(const PlanView& P, const Spaceti
     R.k = T(P.get(PF_K, j)); R.c = T(P.get(PF_C, j)); R.fo = T(P.get(PF_FO, j));
     R.m0 = T(P.get(PF_MAP0, j)); R.m1 = T(P.get(PF_MAP1, j)); R.m2 = T(P.get(PF_MAP2, j)); R.m3 = T(P.get(PF_MAP3, j));
     R.tau_valid = P.get(PF_TAU_VALID, j); R.dtau = P.get(PF_DTAU, j); R.fo_d = P.get(PF_FO, j);
-    R.pmu = T(P.get(PF_PMU, j)); R.pscale = T(P.get(PF_PSCALE, j)); R.tempfac = T(P.get(PF_TEMPFAC, j));
-    R.poffset = T(P.get(PF_POFFSET, j)); R.sqrt_up = T(P.get(PF_SQRTUP, j)); R.um = T(P.get(PF_UM, j));
-    R.up_m_um = T(P.get(PF_UPMUM, j)); R.psign = T(P.get(PF_PSIGN, j));
+    using PT = PolarT<T>;
+    R.pmu = PT(P.get(PF_PMU, j)); R.pscale = PT(P.get(PF_PSCALE, j)); R.tempfac = T(P.get(PF_TEMPFAC, j));
+    R.poffset = T(P.get(PF_POFFSET, j)); R.sqrt_up = PT(P.get(PF_SQRTUP, j)); R.um = PT(P.get(PF_UM, j));
+    R.up_m_um = PT(P.get(PF_UPMUM, j)); R.psign = PT(P.get(PF_PSIGN, j));
     R.vortical = P.get(PF_VORTICAL, j) != 0.0; R.scattering = P.get(PF_SCATTER, j) != 0.0;
     R.a = T(st.a); R.lam = T(P.get(PF_LAM, j)); R.eta = T(P.get(PF_ETA, j)); R.rp = T(st.rp); R.rmn = T(st.rmn);
     R.sp = T(P.get(PF_SP, j)); R.sm = T(P.get(PF_SM, j)); R.Qt = T(P.get(PF_QT, j)); R.Qtm = T(P.get(PF_QTM, j));
     R.Qphi = T(P.get(PF_QPHI, j)); R.Qphim = T(P.get(PF_QPHIM, j)); R.r4 = T(P.get(PF_R4, j));
     R.qC = T(P.get(PF_QC, j)); R.qn = T(P.get(PF_QN, j)); R.sqrt_eps = T(P.get(PF_SQRTEPS, j));
     R.gc = T(P.get(PF_GC, j)); R.mp = T(P.get(PF_MP, j)); R.K2 = T(P.get(PF_K2, j));
-    R.vabsalpha = T(P.get(PF_VABSALPHA, j)); R.valpha2 = T(P.get(PF_VALPHA2, j)); R.vabsbeta = T(P.get(PF_VABSBETA, j));
-    R.vabscos = T(st.abscos); R.vcos2 = T(st.cos2);
+    R.vabsalpha = PT(P.get(PF_VABSALPHA, j)); R.valpha2 = PT(P.get(PF_VALPHA2, j)); R.vabsbeta = PT(P.get(PF_VABSBETA, j));
+    R.vabscos = PT(st.abscos); R.vcos2 = PT(st.cos2); R.pa = PT(st.a);
     R.dr = {T(P.get(PF_DR_SN, j)), T(P.get(PF_DR_CN, j)), T(P.get(PF_DR_DN, j))};
-    R.dth = {T(P.get(PF_DTH_SN, j)), T(P.get(PF_DTH_CN, j)), T(P.get(PF_DTH_DN, j))};
+    R.dth = {PT(P.get(PF_DTH_SN, j)), PT(P.get(PF_DTH_CN, j)), PT(P.get(PF_DTH_DN, j))};
     R.turn_k = int(P.get(PF_TURN_K, j));
     R.Manchor = int(P.get(PF_MANCHOR, j));
     R.nanch = int(P.get(PF_NANCH, j));
@@ -93,39 +108,58 @@ __device__ __forceinline__ T radius(const MarchRay<T>& R, const JS<T>& x) {
     return -(R.m0 * (R.m2 - sc) / (T(1) + R.m2 * sc) + R.m1);
 }
 
+// cos theta in the polar precision (and theta in the march's, from the rounded cos theta)
 template <class T>
-__device__ __forceinline__ void polar_cos(const MarchRay<T>& R, const JS<T>& x, T& theta, T& cth, bool& nu) {
-    T snX = x.sn / (R.pscale * x.dn);
-    T c;
+__device__ __forceinline__ void polar_cos(const MarchRay<T>& R, const JS<PolarT<T>>& x, T& theta, PolarT<T>& cth, bool& nu) {
+    using PT = PolarT<T>;
+    PT snX = x.sn / (R.pscale * x.dn);
+    PT c;
     if (R.vortical) {
-        c = R.psign * sqrt(fmax(R.um + R.up_m_um * snX * snX, T(0)));
-        nu = R.psign * x.sn * x.cn > T(0);
+        c = R.psign * sqrt(fmax(R.um + R.up_m_um * snX * snX, PT(0)));
+        nu = R.psign * x.sn * x.cn > PT(0);
     } else {
         c = R.psign * R.sqrt_up * snX;
-        nu = R.psign * x.cn > T(0);
+        nu = R.psign * x.cn > PT(0);
     }
-    c = fmin(T(1), fmax(T(-1), c));
+    c = fmin(PT(1), fmax(PT(-1), c));
     cth = c;
-    theta = acos(c);
+    theta = acos(T(c));
 }
 
 template <class T>
-__device__ __forceinline__ bool visible(const MarchRay<T>& R, T cths) {
+__device__ __forceinline__ bool visible(const MarchRay<T>& R, PolarT<T> cths) {
+    using PT = PolarT<T>;
     if (!(cths > R.vabscos)) return true;
-    T c2 = cths * cths;
-    T s2 = T(1) - c2;
-    T amin = R.a * sqrt(s2);
-    if (!(R.vabsalpha >= amin + keps<T>())) return true;
-    T temp = (R.vcos2 - c2) * (R.valpha2 - R.a * R.a * s2) / (c2 - T(1));
-    T bb = sqrt(fmax(temp, T(0)));
+    PT c2 = cths * cths;
+    PT s2 = PT(1) - c2;
+    PT amin = R.pa * sqrt(s2);
+    if (!(R.vabsalpha >= amin + keps<PT>())) return true;
+    PT temp = (R.vcos2 - c2) * (R.valpha2 - R.pa * R.pa * s2) / (c2 - PT(1));
+    PT bb = sqrt(fmax(temp, PT(0)));
     return !(R.vabsbeta < bb);
 }
 
 template <class T>
 struct Point {
     T r, theta, cth, s, sn, cn, gt, gphi;
+    PolarT<T> cthp;   // cos theta in the polar precision (the visibility test)
     bool nur, nuth;
 };
+
+// sn, cn of the polar map and 1/dn (the smooth integrand's inputs) in the march's precision
+template <class T>
+__device__ __forceinline__ void polar_map(const MarchRay<T>& R, const JS<PolarT<T>>& xt, Point<T>& p, T& dn_inv) {
+    if constexpr (std::is_same<T, PolarT<T>>::value) {
+        p.sn = xt.sn / (R.pscale * xt.dn);
+        p.cn = xt.cn / xt.dn;
+        dn_inv = T(1) / xt.dn;
+    } else {
+        const T sn = T(xt.sn), cn = T(xt.cn), dn = T(xt.dn);
+        dn_inv = T(1) / dn;
+        p.sn = sn * dn_inv / T(R.pscale);
+        p.cn = cn * dn_inv;
+    }
+}
 
 template <class T>
 __device__ __forceinline__ void smooth(const MarchRay<T>& R, Point<T>& p, T dn) {
@@ -163,28 +197,30 @@ __device__ __forceinline__ T r_pot(const MarchRay<T>& R, T r) {
 }
 
 template <class T>
-__device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<T>& xr, const JS<T>& xt, TimeT<T> tau) {
+__device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<T>& xr, const JS<PolarT<T>>& xt, TimeT<T> tau) {
     Point<T> p;
     p.r = radius(R, xr);
-    polar_cos(R, xt, p.theta, p.cth, p.nuth);
+    polar_cos(R, xt, p.theta, p.cthp, p.nuth);
+    p.cth = T(p.cthp);
     p.nur = tau < R.fo_d;
     p.s = (p.nur ? T(-1) : T(1)) * sqrt(fmax(r_pot(R, p.r), T(0)));
-    p.sn = xt.sn / (R.pscale * xt.dn);
-    p.cn = xt.cn / xt.dn;
-    smooth(R, p, T(1) / xt.dn);
+    T dn_inv;
+    polar_map(R, xt, p, dn_inv);
+    smooth(R, p, dn_inv);
     return p;
 }
 
 template <class T>
-__device__ __forceinline__ Point<T> turning_point(const MarchRay<T>& R, const JS<T>& xt) {
+__device__ __forceinline__ Point<T> turning_point(const MarchRay<T>& R, const JS<PolarT<T>>& xt) {
     Point<T> p;
     p.r = R.r4;
-    polar_cos(R, xt, p.theta, p.cth, p.nuth);
+    polar_cos(R, xt, p.theta, p.cthp, p.nuth);
+    p.cth = T(p.cthp);
     p.nur = true;
     p.s = T(0);
-    p.sn = xt.sn / (R.pscale * xt.dn);
-    p.cn = xt.cn / xt.dn;
-    smooth(R, p, T(1) / xt.dn);
+    T dn_inv;
+    polar_map(R, xt, p, dn_inv);
+    smooth(R, p, dn_inv);
     return p;
 }
 
@@ -234,12 +270,14 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
         if (m > R.nanch - 1) m = R.nanch - 1;
         const int ka = 1 + m * R.Manchor;
         const double* A0 = P.anchors + (R.anchor_off + m) * AF_COUNT;
-        JS<T> xr = load_js<T>(A0, AF_XR_SN), xt = load_js<T>(A0, AF_XT_SN);
+        using PT = PolarT<T>;
+        JS<T> xr = load_js<T>(A0, AF_XR_SN);
+        JS<PT> xt = load_js<PT>(A0, AF_XT_SN);
         Point<T> pa = ray_point(R, xr, xt, ka * dtau);
         T pca = polar_closed(R, ka * dtau, pa.sn, pa.cn);
         T t = T(A0[AF_T]), phi = T(A0[AF_PHI]);
         if (ka >= k_begin) {
-            Sample<T> s{t, pa.r, pa.theta, pa.cth, phi, pa.nur, pa.nuth, (ka * dtau <= R.tau_valid) && visible(R, pa.cth)};
+            Sample<T> s{t, pa.r, pa.theta, pa.cth, phi, pa.nur, pa.nuth, (ka * dtau <= R.tau_valid) && visible(R, pa.cthp)};
             f(ka, s);
         }
         int next_anchor = ka + R.Manchor;
@@ -252,7 +290,7 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
             const bool anchor = (k == next_anchor);
             const double* Am = P.anchors + (R.anchor_off + m) * AF_COUNT;
             if (anchor) {
-                xr = load_js<T>(Am, AF_XR_SN); xt = load_js<T>(Am, AF_XT_SN);
+                xr = load_js<T>(Am, AF_XR_SN); xt = load_js<PT>(Am, AF_XT_SN);
             } else {
                 xr = jstep(xr, R.dr, R.k);
                 xt = jstep(xt, R.dth, R.pmu);
@@ -263,10 +301,10 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
                 const double* pf = P.f;
                 const long long np = P.npad;
                 JS<T> p1r = {T(pf[PF_P1R_SN * np + j]), T(pf[PF_P1R_CN * np + j]), T(pf[PF_P1R_DN * np + j])};
-                JS<T> p1t = {T(pf[PF_P1T_SN * np + j]), T(pf[PF_P1T_CN * np + j]), T(pf[PF_P1T_DN * np + j])};
+                JS<PT> p1t = {PT(pf[PF_P1T_SN * np + j]), PT(pf[PF_P1T_CN * np + j]), PT(pf[PF_P1T_DN * np + j])};
                 JS<T> p2r = {T(pf[PF_P2R_SN * np + j]), T(pf[PF_P2R_CN * np + j]), T(pf[PF_P2R_DN * np + j])};
-                JS<T> p2t = {T(pf[PF_P2T_SN * np + j]), T(pf[PF_P2T_CN * np + j]), T(pf[PF_P2T_DN * np + j])};
-                JS<T> ptt = {T(pf[PF_PTT_SN * np + j]), T(pf[PF_PTT_CN * np + j]), T(pf[PF_PTT_DN * np + j])};
+                JS<PT> p2t = {PT(pf[PF_P2T_SN * np + j]), PT(pf[PF_P2T_CN * np + j]), PT(pf[PF_P2T_DN * np + j])};
+                JS<PT> ptt = {PT(pf[PF_PTT_SN * np + j]), PT(pf[PF_PTT_CN * np + j]), PT(pf[PF_PTT_DN * np + j])};
                 double fo = R.fo_d;
                 Point<T> pt = turning_point(R, ptt);
                 Point<T> p1 = ray_point(R, p1r, p1t, (ta + fo) / 2.0);
@@ -294,7 +332,7 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
                 next_anchor += R.Manchor;
             }
             if (k >= k_begin) {
-                Sample<T> s{t, pb.r, pb.theta, pb.cth, phi, pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cth)};
+                Sample<T> s{t, pb.r, pb.theta, pb.cth, phi, pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cthp)};
                 f(k, s);
             }
             pa = pb;
