@@ -2,14 +2,17 @@
 // reading the FP64 plan and anchor table built by regenerate.
 //
 // T = double is the plain FP64 port of the reference's march_ray, sample for sample. T = float is
-// the mixed path: the radial recurrence and the quadrature run in FP32 and are reset to the FP64
-// anchors every M samples; the smooth t-integrand uses the cancellation-free large-r form there (its
-// r^2 terms would otherwise lose everything in FP32 at r ~ 1e4). The polar recurrence, cos theta and
-// the visibility test stay in FP64 (PolarT): the test is krang_visible (recurrence.jl:299-308), whose
-// boundary |beta| = beta_boundary(theta_s) is the polar turning point itself, so the samples next to a
-// turning point flip validity under an FP32 cos theta (2.5e-4 of the configuration-2 image, all of
-// it from those flags); with the polar state in FP64 the flags are the FP64 march's, operation for
-// operation.
+// the mixed path: the smooth integrands, the interval increments (their logarithms and the polar
+// closed form) and the sample positions run in FP32, reset to the FP64 anchors every M samples; the
+// smooth t-integrand uses the cancellation-free large-r form there (its r^2 terms would otherwise lose
+// everything in FP32 at r ~ 1e4). The Jacobi states of both recurrences, r, cos theta, the visibility
+// test and the t~/phi running sums stay in FP64 (GeoT), a few multiplications and one division per
+// half step:
+// - the visibility test is krang_visible (recurrence.jl:299-308), whose boundary |beta| =
+//   beta_boundary(theta_s) is the polar turning point itself, so the samples next to a turning point
+//   flip validity under an FP32 cos theta (2.5e-4 of the configuration-2 image came from those flags);
+// - FP32 recurrences drift between anchors (6e-4 on a 16^2, N = 128 scene at M = 64, falling as the
+//   anchor spacing shrinks).
 #pragma once
 #include "ks_plan.cuh"
 
@@ -27,25 +30,25 @@ template <class T> struct TimeOf { using type = double; };
 template <class S, int N> struct TimeOf<Dual<S, N>> { using type = Dual<S, N>; };
 template <class T> using TimeT = typename TimeOf<T>::type;
 
-// The precision of the polar state (Jacobi amplitude of theta, cos theta, the visibility test): FP64
-// under the FP32 march, the march's own type otherwise.
-template <class T> struct PolarOf { using type = T; };
-template <> struct PolarOf<float> { using type = double; };
-template <class T> using PolarT = typename PolarOf<T>::type;
+// The precision of the geometry state (the Jacobi states, r, cos theta, the visibility test and the
+// running sums): FP64 under the FP32 march, the march's own type otherwise.
+template <class T> struct GeoOf { using type = T; };
+template <> struct GeoOf<float> { using type = double; };
+template <class T> using GeoT = typename GeoOf<T>::type;
 
 template <class T>
 struct MarchRay {
-    using PT = PolarT<T>;
+    using PT = GeoT<T>;
     int rcase;
-    T k, c, fo, m0, m1, m2, m3;
+    PT k, m0, m1, m2, m3;
+    T c, fo;
     TimeT<T> tau_valid, dtau, fo_d;  // compared against sample times in FP64
     PT pmu, pscale, sqrt_up, um, up_m_um, psign;
     T tempfac, poffset;
     bool vortical, scattering;
     T a, lam, eta, rp, rmn, sp, sm, Qt, Qtm, Qphi, Qphim, r4, qC, qn, sqrt_eps, gc, mp, K2;
     PT vabsalpha, valpha2, vabsbeta, vabscos, vcos2, pa;   // krang_visible's constants (pa: the spin)
-    JS<T> dr;
-    JS<PT> dth;
+    JS<PT> dr, dth;
     int turn_k, Manchor, nanch, nsamp;
     long long anchor_off;
 };
@@ -62,10 +65,10 @@ template <class T>
 __device__ __forceinline__ MarchRay<T> load_ray(const PlanView& P, const Spacetime& st, long long j) {
     MarchRay<T> R;
     R.rcase = int(P.get(PF_CASE, j));
-    R.k = T(P.get(PF_K, j)); R.c = T(P.get(PF_C, j)); R.fo = T(P.get(PF_FO, j));
-    R.m0 = T(P.get(PF_MAP0, j)); R.m1 = T(P.get(PF_MAP1, j)); R.m2 = T(P.get(PF_MAP2, j)); R.m3 = T(P.get(PF_MAP3, j));
+    using PT = GeoT<T>;
+    R.k = PT(P.get(PF_K, j)); R.c = T(P.get(PF_C, j)); R.fo = T(P.get(PF_FO, j));
+    R.m0 = PT(P.get(PF_MAP0, j)); R.m1 = PT(P.get(PF_MAP1, j)); R.m2 = PT(P.get(PF_MAP2, j)); R.m3 = PT(P.get(PF_MAP3, j));
     R.tau_valid = P.get(PF_TAU_VALID, j); R.dtau = P.get(PF_DTAU, j); R.fo_d = P.get(PF_FO, j);
-    using PT = PolarT<T>;
     R.pmu = PT(P.get(PF_PMU, j)); R.pscale = PT(P.get(PF_PSCALE, j)); R.tempfac = T(P.get(PF_TEMPFAC, j));
     R.poffset = T(P.get(PF_POFFSET, j)); R.sqrt_up = PT(P.get(PF_SQRTUP, j)); R.um = PT(P.get(PF_UM, j));
     R.up_m_um = PT(P.get(PF_UPMUM, j)); R.psign = PT(P.get(PF_PSIGN, j));
@@ -77,7 +80,7 @@ __device__ __forceinline__ MarchRay<T> load_ray(const PlanView& P, const Spaceti
     R.gc = T(P.get(PF_GC, j)); R.mp = T(P.get(PF_MP, j)); R.K2 = T(P.get(PF_K2, j));
     R.vabsalpha = PT(P.get(PF_VABSALPHA, j)); R.valpha2 = PT(P.get(PF_VALPHA2, j)); R.vabsbeta = PT(P.get(PF_VABSBETA, j));
     R.vabscos = PT(st.abscos); R.vcos2 = PT(st.cos2); R.pa = PT(st.a);
-    R.dr = {T(P.get(PF_DR_SN, j)), T(P.get(PF_DR_CN, j)), T(P.get(PF_DR_DN, j))};
+    R.dr = {PT(P.get(PF_DR_SN, j)), PT(P.get(PF_DR_CN, j)), PT(P.get(PF_DR_DN, j))};
     R.dth = {PT(P.get(PF_DTH_SN, j)), PT(P.get(PF_DTH_CN, j)), PT(P.get(PF_DTH_DN, j))};
     R.turn_k = int(P.get(PF_TURN_K, j));
     R.Manchor = int(P.get(PF_MANCHOR, j));
@@ -97,21 +100,22 @@ template <> __device__ __forceinline__ double keps<double>() { return kEps; }
 template <> __device__ __forceinline__ float keps<float>() { return 1.1920929e-7f; }
 
 template <class T>
-__device__ __forceinline__ T radius(const MarchRay<T>& R, const JS<T>& x) {
+__device__ __forceinline__ GeoT<T> radius(const MarchRay<T>& R, const JS<GeoT<T>>& x) {
+    using PT = GeoT<T>;
     if (R.rcase == 2) {
-        T cn2 = R.m2 * x.cn * x.cn;
+        PT cn2 = R.m2 * x.cn * x.cn;
         return (R.m1 * cn2 - R.m0 * R.m3) / (cn2 - R.m3);
     } else if (R.rcase == 3) {
         return (R.m0 + R.m1 * x.cn) / (R.m2 + R.m3 * x.cn);
     }
-    T sc = x.sn / x.cn;
-    return -(R.m0 * (R.m2 - sc) / (T(1) + R.m2 * sc) + R.m1);
+    PT sc = x.sn / x.cn;
+    return -(R.m0 * (R.m2 - sc) / (PT(1) + R.m2 * sc) + R.m1);
 }
 
 // cos theta in the polar precision (and theta in the march's, from the rounded cos theta)
 template <class T>
-__device__ __forceinline__ void polar_cos(const MarchRay<T>& R, const JS<PolarT<T>>& x, T& theta, PolarT<T>& cth, bool& nu) {
-    using PT = PolarT<T>;
+__device__ __forceinline__ void polar_cos(const MarchRay<T>& R, const JS<GeoT<T>>& x, T& theta, GeoT<T>& cth, bool& nu) {
+    using PT = GeoT<T>;
     PT snX = x.sn / (R.pscale * x.dn);
     PT c;
     if (R.vortical) {
@@ -127,8 +131,8 @@ __device__ __forceinline__ void polar_cos(const MarchRay<T>& R, const JS<PolarT<
 }
 
 template <class T>
-__device__ __forceinline__ bool visible(const MarchRay<T>& R, PolarT<T> cths) {
-    using PT = PolarT<T>;
+__device__ __forceinline__ bool visible(const MarchRay<T>& R, GeoT<T> cths) {
+    using PT = GeoT<T>;
     if (!(cths > R.vabscos)) return true;
     PT c2 = cths * cths;
     PT s2 = PT(1) - c2;
@@ -142,14 +146,14 @@ __device__ __forceinline__ bool visible(const MarchRay<T>& R, PolarT<T> cths) {
 template <class T>
 struct Point {
     T r, theta, cth, s, sn, cn, gt, gphi;
-    PolarT<T> cthp;   // cos theta in the polar precision (the visibility test)
+    GeoT<T> cthp;   // cos theta in the polar precision (the visibility test)
     bool nur, nuth;
 };
 
 // sn, cn of the polar map and 1/dn (the smooth integrand's inputs) in the march's precision
 template <class T>
-__device__ __forceinline__ void polar_map(const MarchRay<T>& R, const JS<PolarT<T>>& xt, Point<T>& p, T& dn_inv) {
-    if constexpr (std::is_same<T, PolarT<T>>::value) {
+__device__ __forceinline__ void polar_map(const MarchRay<T>& R, const JS<GeoT<T>>& xt, Point<T>& p, T& dn_inv) {
+    if constexpr (std::is_same<T, GeoT<T>>::value) {
         p.sn = xt.sn / (R.pscale * xt.dn);
         p.cn = xt.cn / xt.dn;
         dn_inv = T(1) / xt.dn;
@@ -197,9 +201,9 @@ __device__ __forceinline__ T r_pot(const MarchRay<T>& R, T r) {
 }
 
 template <class T>
-__device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<T>& xr, const JS<PolarT<T>>& xt, TimeT<T> tau) {
+__device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<GeoT<T>>& xr, const JS<GeoT<T>>& xt, TimeT<T> tau) {
     Point<T> p;
-    p.r = radius(R, xr);
+    p.r = T(radius(R, xr));
     polar_cos(R, xt, p.theta, p.cthp, p.nuth);
     p.cth = T(p.cthp);
     p.nur = tau < R.fo_d;
@@ -211,7 +215,7 @@ __device__ __forceinline__ Point<T> ray_point(const MarchRay<T>& R, const JS<T>&
 }
 
 template <class T>
-__device__ __forceinline__ Point<T> turning_point(const MarchRay<T>& R, const JS<PolarT<T>>& xt) {
+__device__ __forceinline__ Point<T> turning_point(const MarchRay<T>& R, const JS<GeoT<T>>& xt) {
     Point<T> p;
     p.r = R.r4;
     polar_cos(R, xt, p.theta, p.cthp, p.nuth);
@@ -270,14 +274,14 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
         if (m > R.nanch - 1) m = R.nanch - 1;
         const int ka = 1 + m * R.Manchor;
         const double* A0 = P.anchors + (R.anchor_off + m) * AF_COUNT;
-        using PT = PolarT<T>;
-        JS<T> xr = load_js<T>(A0, AF_XR_SN);
+        using PT = GeoT<T>;
+        JS<PT> xr = load_js<PT>(A0, AF_XR_SN);
         JS<PT> xt = load_js<PT>(A0, AF_XT_SN);
         Point<T> pa = ray_point(R, xr, xt, ka * dtau);
         T pca = polar_closed(R, ka * dtau, pa.sn, pa.cn);
-        T t = T(A0[AF_T]), phi = T(A0[AF_PHI]);
+        PT t = PT(A0[AF_T]), phi = PT(A0[AF_PHI]);
         if (ka >= k_begin) {
-            Sample<T> s{t, pa.r, pa.theta, pa.cth, phi, pa.nur, pa.nuth, (ka * dtau <= R.tau_valid) && visible(R, pa.cthp)};
+            Sample<T> s{T(t), pa.r, pa.theta, pa.cth, T(phi), pa.nur, pa.nuth, (ka * dtau <= R.tau_valid) && visible(R, pa.cthp)};
             f(ka, s);
         }
         int next_anchor = ka + R.Manchor;
@@ -290,7 +294,7 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
             const bool anchor = (k == next_anchor);
             const double* Am = P.anchors + (R.anchor_off + m) * AF_COUNT;
             if (anchor) {
-                xr = load_js<T>(Am, AF_XR_SN); xt = load_js<PT>(Am, AF_XT_SN);
+                xr = load_js<PT>(Am, AF_XR_SN); xt = load_js<PT>(Am, AF_XT_SN);
             } else {
                 xr = jstep(xr, R.dr, R.k);
                 xt = jstep(xt, R.dth, R.pmu);
@@ -300,9 +304,9 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
             if (k == R.turn_k) {
                 const double* pf = P.f;
                 const long long np = P.npad;
-                JS<T> p1r = {T(pf[PF_P1R_SN * np + j]), T(pf[PF_P1R_CN * np + j]), T(pf[PF_P1R_DN * np + j])};
+                JS<PT> p1r = {PT(pf[PF_P1R_SN * np + j]), PT(pf[PF_P1R_CN * np + j]), PT(pf[PF_P1R_DN * np + j])};
                 JS<PT> p1t = {PT(pf[PF_P1T_SN * np + j]), PT(pf[PF_P1T_CN * np + j]), PT(pf[PF_P1T_DN * np + j])};
-                JS<T> p2r = {T(pf[PF_P2R_SN * np + j]), T(pf[PF_P2R_CN * np + j]), T(pf[PF_P2R_DN * np + j])};
+                JS<PT> p2r = {PT(pf[PF_P2R_SN * np + j]), PT(pf[PF_P2R_CN * np + j]), PT(pf[PF_P2R_DN * np + j])};
                 JS<PT> p2t = {PT(pf[PF_P2T_SN * np + j]), PT(pf[PF_P2T_CN * np + j]), PT(pf[PF_P2T_DN * np + j])};
                 JS<PT> ptt = {PT(pf[PF_PTT_SN * np + j]), PT(pf[PF_PTT_CN * np + j]), PT(pf[PF_PTT_DN * np + j])};
                 double fo = R.fo_d;
@@ -313,11 +317,11 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
                 T It1, Ip1, It2, Ip2;
                 increment(R, pa, p1, pt, ta, fo, pca, pct, It1, Ip1);
                 increment(R, pt, p2, pb, fo, tb, pct, pcb, It2, Ip2);
-                t += It1 + It2; phi += Ip1 + Ip2;
+                t += PT(It1) + PT(It2); phi += PT(Ip1) + PT(Ip2);
             } else {
                 T It, Ip;
                 increment(R, pa, pm, pb, ta, tb, pca, pcb, It, Ip);
-                t += It; phi += Ip;
+                t += PT(It); phi += PT(Ip);
             }
             if (anchor) {
                 if (Am[AF_OK] != 0.0) {
@@ -326,13 +330,13 @@ __device__ __forceinline__ void march_impl(const PlanView& P, long long j, const
                         rt = fmax(rt, fabs(double(t) - at));
                         rphi = fmax(rphi, fabs(double(phi) - ap));
                     }
-                    t = T(at); phi = T(ap);
+                    t = PT(at); phi = PT(ap);
                 }
                 ++m;
                 next_anchor += R.Manchor;
             }
             if (k >= k_begin) {
-                Sample<T> s{t, pb.r, pb.theta, pb.cth, phi, pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cthp)};
+                Sample<T> s{T(t), pb.r, pb.theta, pb.cth, T(phi), pb.nur, pb.nuth, (tb <= R.tau_valid) && visible(R, pb.cthp)};
                 f(k, s);
             }
             pa = pb;
