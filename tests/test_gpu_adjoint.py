@@ -228,9 +228,12 @@ def test_jvp_matches_finite_differences_and_adjoint(scene, oracle, prec, tol):
         print("jvp", prec, d, "rel L2 vs FD", e, "duality", dual, ref)
         assert e < tol, (d, e)
         assert abs(dual - ref) <= tol * abs(ref) + 1e-30, (d, dual, ref)
-    # one direction (the one-partial pass the fit's Gauss-Newton curvature uses) equals the 8-wide pass
+    # one direction (the one-partial pass the fit's Gauss-Newton curvature uses) equals the 8-wide pass:
+    # the same arithmetic on Dual<S, 1> and Dual<S, 8>, which the compiler contracts into FMAs
+    # differently, so they agree to the rounding of S (FP64 1e-9, FP32 duals 1e-5)
     jv1 = ks.jvp(s["cache"], m, s["times"], s["nus"], c["L"], dirs[:1], precision=prec)
-    assert rel_l2(jv1[0], jv[0]) < 1e-6, rel_l2(jv1[0], jv[0])
+    bound = 1e-9 if prec == ks.KS_FP64 else 1e-5
+    assert rel_l2(jv1[0], jv[0]) < bound, rel_l2(jv1[0], jv[0])
 
 
 @pytest.mark.parametrize("prec,tol", [(ks.KS_FP64, 1e-12), (ks.KS_MIXED, 1e-5)])
