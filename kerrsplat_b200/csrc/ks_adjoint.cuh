@@ -900,6 +900,8 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
         const unsigned long long u = s_unit;
         if (u >= (unsigned long long)btotal) break;
         const AdjUnit U = adj_block_unit<CH>(job, btotal, u, warp, W, lane, N);
+        // the live warps (dead ones, past the last ray, are the trailing warps) evaluate and accumulate
+        const int ntl = 32 * __syncthreads_count(lane == 0 && !U.dead);
         const float t_obs = float(ct[U.f]);
         if (tid < CH) nu[tid] = float(cnu[min(U.v0 + tid, job.nfreq - 1)]);   // read after the next barrier
         const float dtau = float(plan_f[(long long)PF_DTAU * npad + U.j]);
@@ -991,8 +993,6 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
                 int total;
                 const int off = block_exscan<NT>(n, total, wsum, scan_par);
                 if (!single && total > item_cap) { single_end = g1; continue; }
-                // this warp's pairs: [wlo, whi) of the list (its threads' ranges are consecutive)
-                const int wlo = __shfl_sync(full, off, 0), whi = __shfl_sync(full, off + n, 31);
                 for (int wb = 0; wb < total; wb += item_cap) {
                     if (n > 0 && off + n > wb && off < wb + item_cap) {
                         int kk = off;
@@ -1007,26 +1007,47 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
                         }
                     }
                     __syncthreads();
+                    // Rounds of ntl pairs over the live warps' threads; each warp then adds the 32 pairs its
+                    // own lanes evaluated to its accumulator, in list order (a fixed partition of the list,
+                    // so the sums are deterministic), with no block barrier inside the window.
                     const int wt = min(item_cap, total - wb);
-                    for (int base = 0; base < wt; base += NT) {
+                    for (int base = 0; base < wt; base += ntl) {
                         const int kk0 = base + tid;
-                        if (kk0 < wt) {
+                        if (tid < ntl && kk0 < wt) {
                             const unsigned it = items[kk0];
                             const int o = int(it >> 9), i = int(it & 511u);
                             element_adjoint_ool<CH, NT>(tab + i * ST_COUNT, gtab + (long long)i * GT_COUNT, sf + o, t_obs, a, a_sin_tho, nu, U.nc,
                                                         meta_bits[o], cbs + o, gitem + tid * GR_COUNT);
                         }
-                        __syncthreads();
-                        // this warp's pairs of the round, per splat in list order
-                        const int lo = max(wlo, wb + base), hi = min(whi, wb + base + NT);
-                        if (lane < GR_COUNT) {
-                            for (int q = lo; q < hi; ++q) {
-                                const int i = int(items[q - wb] & 511u);
-                                gacc[i * GR_COUNT + lane] += gitem[(q - wb - base) * GR_COUNT + lane];
+                        __syncwarp();
+                        // four pairs at a time: their rows are read before any sum is written back; four
+                        // pairs of which two share a splat go one by one (each splat's sum in list order)
+                        const int lo = base + warp * 32, hi = min(wt, lo + 32);
+                        if (tid < ntl && lane < GR_COUNT) {
+                            int q = lo;
+                            for (; q + 4 <= hi; q += 4) {
+                                const int i0 = int(items[q] & 511u), i1 = int(items[q + 1] & 511u);
+                                const int i2 = int(items[q + 2] & 511u), i3 = int(items[q + 3] & 511u);
+                                const float* gi = gitem + (q - base) * GR_COUNT + lane;
+                                const float v0 = gi[0], v1 = gi[GR_COUNT], v2 = gi[2 * GR_COUNT], v3 = gi[3 * GR_COUNT];
+                                float* a0 = gacc + i0 * GR_COUNT + lane;
+                                float* a1 = gacc + i1 * GR_COUNT + lane;
+                                float* a2 = gacc + i2 * GR_COUNT + lane;
+                                float* a3 = gacc + i3 * GR_COUNT + lane;
+                                if (i0 != i1 && i0 != i2 && i0 != i3 && i1 != i2 && i1 != i3 && i2 != i3) {
+                                    const float s0 = *a0 + v0, s1 = *a1 + v1, s2 = *a2 + v2, s3 = *a3 + v3;
+                                    *a0 = s0; *a1 = s1; *a2 = s2; *a3 = s3;
+                                } else {
+                                    *a0 += v0; *a1 += v1; *a2 += v2; *a3 += v3;
+                                }
                             }
+                            for (; q < hi; ++q)
+                                gacc[int(items[q] & 511u) * GR_COUNT + lane] += gitem[(q - base) * GR_COUNT + lane];
                         }
-                        __syncthreads();
+                        __syncwarp();
                     }
+                    // the next window's items and the next group's pass masks (in gitem) are written after this
+                    __syncthreads();
                 }
                 g0 = g1;
             }
