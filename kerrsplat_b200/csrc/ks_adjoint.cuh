@@ -882,7 +882,8 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
     float* gacc_smem = reinterpret_cast<float*>(bb + W * AS::kFixed + size_t(warp) * AS::acc_bytes(ntot));   // [splat][21]
     const int item_cap = W * AS::kItemBytes / 4;
     __syncthreads();
-    const unsigned full = 0xffffffffu;
+    __shared__ float s_reach;
+    const float reach2 = table_reach2(tab, ntot, &s_reach);   // samples farther out weigh no splat
     const int N = st.N;
     const long long npad = job.npad;
     const float a = float(st.a), a_sin_tho = float(st.a * sin(st.thetao));
@@ -918,7 +919,9 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
             for (int k = U.k0; k < U.k1; ++k) {
                 const float* bp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
                 if (!U.live || k > nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
-                unit_box_add(b, bp[SM_X * npad], bp[SM_Y * npad], bp[SM_Z * npad], t_obs - bp[SM_T * npad]);
+                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
+                if (x * x + y * y + z * z > reach2) continue;
+                unit_box_add(b, x, y, z, t_obs - bp[SM_T * npad]);
             }
             unit_box_reduce(b);
             unit_candidates(tab, ntot, b, lane, cand);
@@ -1142,6 +1145,7 @@ struct JvpSink {
     S t_obs, nu, Lnu, a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
     int nmax;
     int lnL_dir;      // >= 0: the direction that carries d/d(ln L) (the step length scales with L)
+    S reach2 = S(3e38f);   // table_reach2: farther samples weigh no splat
     D P[16], Sv[4];
     S zprev; int wn; bool inside, crossed, zset;
 
@@ -1185,6 +1189,7 @@ struct JvpSink {
         emit(x, y, z, ts, r, sth, cth, nur, nuth);
     }
     __device__ void emit(S x, S y, S z, S ts, S r, S sth, S cth, bool nur, bool nuth) {
+        if (x * x + y * y + z * z > reach2) return;   // no splat reaches the sample: no element, no step
         const S t = t_obs - ts;
         D in[11];
         for (int q = 0; q < 11; ++q) in[q] = D(S(0));
@@ -1281,13 +1286,15 @@ __global__ void __launch_bounds__(64, 8) k_jvp_stream(PlanView P, Spacetime st, 
                                                    const double* __restrict__ ct, const double* __restrict__ cnu, int ncombo, double L, int nmax,
                                                    double slab, const float* __restrict__ stream, double* __restrict__ img, double* __restrict__ out,
                                                    int lnL_dir) {
+    __shared__ float s_reach;
+    const float reach2 = table_reach2(dtab, ntot, &s_reach);   // before any thread leaves: it has block barriers
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (idx >= npix * ncombo) return;
     const long long j = idx % npix;
     const int c = int(idx / npix);
     const long long npad = P.npad;
     JvpSink<float, K> sink;
-    sink.tab = dtab; sink.ntot = ntot;
+    sink.tab = dtab; sink.ntot = ntot; sink.reach2 = reach2;
     sink.t_obs = float(ct[c]); sink.nu = float(cnu[c]);
     const double nh = cnu[c] / kNU0;
     sink.Lnu = float(L / nh);

@@ -87,6 +87,29 @@ __device__ __forceinline__ bool arc_box(const float* p, float lo, float hi, floa
     return true;
 }
 
+// The squared radius (about the origin of the quasi-Cartesian frame) beyond which no splat of the
+// table can weigh a sample: the pattern rotation keeps a centre's distance from the origin, so a
+// pattern-rotating splat reaches |c| + sqrt(support); a knot splat reaches its bounding sphere. Padded
+// by 1e-3 relative for the FP32 rounding of the positions. Every thread of the block calls it (the
+// table in shared or global memory, values or duals); `slot` is a block-shared float.
+template <class TAB>
+__device__ __forceinline__ float table_reach2(const TAB* tab, int ntot, float* slot) {
+    if (threadIdx.x == 0) *slot = 0.f;
+    __syncthreads();
+    float m = 0.f;
+    for (int i = threadIdx.x; i < ntot; i += blockDim.x) {
+        const TAB* p = tab + (long long)i * ST_COUNT;
+        const float cx = float(value_of(p[ST_CX])), cy = float(value_of(p[ST_CY])), cz = float(value_of(p[ST_CZ]));
+        const bool knot = int(value_of(p[ST_KIND])) == KS_KNOT21;
+        const float c = sqrtf(cx * cx + cy * cy + cz * cz);
+        m = fmaxf(m, c + sqrtf(float(value_of(knot ? p[ST_RHO] : p[ST_SUPP]))));
+    }
+    atomicMax(reinterpret_cast<int*>(slot), __float_as_int(m));   // non-negative floats order as ints
+    __syncthreads();
+    const float r = *slot * 1.001f + 1e-3f;
+    return r * r;
+}
+
 // the candidate mask words of a unit (all lanes call it; cand gets ceil(ntot / 32) words)
 __device__ __forceinline__ void unit_candidates(const float* tab, int ntot, const UnitBox& b, int lane, unsigned* cand) {
     for (int s0 = 0; s0 < ntot; s0 += 32) {
@@ -290,6 +313,7 @@ struct MixedSink {
     float nu[CH], Lnu[CH];
     int nc;
     float a, rh_lo, dtau, alpha, beta, eta, lam, a_sin_tho, slab;
+    float reach2;     // table_reach2: samples farther out test no splat
     int nmax;
     int tid;
     bool live;        // false for the padding threads past the last ray
@@ -421,6 +445,8 @@ struct MixedSink {
         bool valid = live && inrange && usable;
         if (valid) ev[1]++;
         if (valid && nmax >= 0) valid = wind_ok(r * cth);
+        // beyond every splat's reach a sample has no pair: its tests are skipped (they would all fail)
+        const bool testable = valid && x * x + y * y + z * z <= reach2;
         float* mys = sf + tid;
         float t = 0.f, rho = 0.f;
         if (valid) {
@@ -450,7 +476,7 @@ struct MixedSink {
             for (int wd = g0; wd < g1; ++wd) {
                 const unsigned cm = cand[wd];
                 unsigned mask = 0u;
-                if (valid && cm) {
+                if (testable && cm) {
                     unsigned cbits = cm;
                     while (cbits) {
                         const int b = __ffs(cbits) - 1;
@@ -728,6 +754,8 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const float* __restrict__ tab3
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned* cand = cand_b + warp * kMaxSplatWords;
     __syncthreads();
+    __shared__ float s_reach;
+    const float reach2 = table_reach2(tab, ntot, &s_reach);
     unsigned int ev[7] = {0, 0, 0, 0, 0, 0, 0};
     unsigned int samples_c = 0;
     const int N = st.N;
@@ -778,6 +806,7 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const float* __restrict__ tab3
         sink.alpha = float(P.get(PF_ALPHA, j)); sink.beta = float(P.get(PF_BETA, j));
         sink.eta = float(P.get(PF_ETA, j)); sink.lam = float(P.get(PF_LAM, j));
         sink.a_sin_tho = float(st.a * sin(st.thetao)); sink.slab = job.slab; sink.nmax = job.nmax;
+        sink.reach2 = reach2;
         sink.tid = threadIdx.x; sink.live = live;
         sink.nsamp = int(P.get(PF_NSAMP, j));
         sink.gstate = job.gstate; sink.gact = job.gact; sink.gnpad = npad; sink.jbase = (ur / per_chunk) * NT;
@@ -802,7 +831,9 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const float* __restrict__ tab3
             const float* bp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
             for (int k = k0; k < k1; ++k, bp += SM_COUNT * npad) {
                 if (!live || k > sink.nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
-                unit_box_add(b, bp[SM_X * npad], bp[SM_Y * npad], bp[SM_Z * npad], sink.t_obs - bp[SM_T * npad]);
+                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
+                if (x * x + y * y + z * z > reach2) continue;   // beyond every splat: no candidate needed
+                unit_box_add(b, x, y, z, sink.t_obs - bp[SM_T * npad]);
             }
             unit_box_reduce(b);
             unit_candidates(tab, ntot, b, lane, cand);
