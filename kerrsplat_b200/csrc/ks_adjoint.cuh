@@ -912,21 +912,23 @@ k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, cons
         float* gacc = global_acc ? gunit + (U.dead ? 0 : U.ur) * gsz : gacc_smem;
         if (!U.dead)
             for (long long q = lane; q < gsz; q += 32) gacc[q] = 0.f;
-        {
-            // the unit's bounds and candidate splats (as the forward pass)
-            UnitBox b = unit_box_empty();
-            const int nsamp = int(plan_f[(long long)PF_NSAMP * npad + U.j]);
-            for (int k = U.k0; k < U.k1; ++k) {
-                const float* bp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
-                if (!U.live || k > nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
-                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
-                if (x * x + y * y + z * z > reach2) continue;
-                unit_box_add(b, x, y, z, t_obs - bp[SM_T * npad]);
-            }
-            unit_box_reduce(b);
-            unit_candidates(tab, ntot, b, lane, cand);
-        }
+        const int nsamp = int(plan_f[(long long)PF_NSAMP * npad + U.j]);
+        const int cl = job.cand_len > 0 ? job.cand_len : job.seg_len;   // the forward pass's candidate runs
         for (int k = U.k0; k < U.k1; ++k) {
+            if ((k - U.k0) % cl == 0) {
+                // the candidate splats of samples [k, k + cl) (as the forward pass)
+                UnitBox b = unit_box_empty();
+                const int ke = min(U.k1, k + cl);
+                for (int kk = k; kk < ke; ++kk) {
+                    const float* bp = stream + (long long)(kk - 1) * SM_COUNT * npad + U.j;
+                    if (!U.live || kk > nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
+                    const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
+                    if (x * x + y * y + z * z > reach2) continue;
+                    unit_box_add(b, x, y, z, t_obs - bp[SM_T * npad]);
+                }
+                unit_box_reduce(b);
+                unit_candidates(tab, ntot, b, lane, cand);
+            }
             const float* sp = stream + (long long)(k - 1) * SM_COUNT * npad + U.j;
             const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
             unsigned actbits = 0u;

@@ -721,6 +721,7 @@ struct MixedJob {
     unsigned char* gact = nullptr;
     int nkv = 0;                      // knot values after the splat table
     int ch = 1;                       // frequencies per work unit
+    int cand_len = 0;                 // samples per candidate mask (0: the whole segment)
     int stage_test = 0;               // test hook: arm the table-staging barrier without the copy
 };
 
@@ -825,25 +826,30 @@ k_consume(PlanView P, Spacetime st, MixedJob job, const float* __restrict__ tab3
         sink.cand = cand;
         sink.state = state_b + threadIdx.x;
         sink.init();
-        {
-            // the unit's bounds and candidate splats
-            UnitBox b = unit_box_empty();
-            const float* bp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
-            for (int k = k0; k < k1; ++k, bp += SM_COUNT * npad) {
-                if (!live || k > sink.nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
-                const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
-                if (x * x + y * y + z * z > reach2) continue;   // beyond every splat: no candidate needed
-                unit_box_add(b, x, y, z, sink.t_obs - bp[SM_T * npad]);
-            }
-            unit_box_reduce(b);
-            unit_candidates(tab, ntot, b, lane, cand);
-        }
+        // the unit's samples in runs of cand_len, each with the candidate splats of its own box (a
+        // segment's box spans the emission region in depth and keeps most of a large table)
+        const int cl = job.cand_len > 0 ? job.cand_len : job.seg_len;
         const float* sp = stream + (long long)(k0 - 1) * SM_COUNT * npad + j;
-        for (int k = k0; k < k1; ++k, sp += SM_COUNT * npad) {
-            sink.kcur = k;
-            const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
-            sink.consume((flags & 8u) != 0u, sp[SM_X * npad], sp[SM_Y * npad], sp[SM_Z * npad], sp[SM_T * npad], sp[SM_R * npad],
-                         sp[SM_STH * npad], sp[SM_CTH * npad], (flags & 2u) != 0u, (flags & 4u) != 0u);
+        for (int kb = k0; kb < k1; kb += cl) {
+            const int ke = min(k1, kb + cl);
+            {
+                UnitBox b = unit_box_empty();
+                const float* bp = sp;
+                for (int k = kb; k < ke; ++k, bp += SM_COUNT * npad) {
+                    if (!live || k > sink.nsamp || !(__float_as_uint(bp[SM_FLAGS * npad]) & 8u)) continue;
+                    const float x = bp[SM_X * npad], y = bp[SM_Y * npad], z = bp[SM_Z * npad];
+                    if (x * x + y * y + z * z > reach2) continue;   // beyond every splat: no candidate needed
+                    unit_box_add(b, x, y, z, sink.t_obs - bp[SM_T * npad]);
+                }
+                unit_box_reduce(b);
+                unit_candidates(tab, ntot, b, lane, cand);
+            }
+            for (int k = kb; k < ke; ++k, sp += SM_COUNT * npad) {
+                sink.kcur = k;
+                const unsigned flags = __float_as_uint(sp[SM_FLAGS * npad]);
+                sink.consume((flags & 8u) != 0u, sp[SM_X * npad], sp[SM_Y * npad], sp[SM_Z * npad], sp[SM_T * npad], sp[SM_R * npad],
+                             sp[SM_STH * npad], sp[SM_CTH * npad], (flags & 2u) != 0u, (flags & 4u) != 0u);
+            }
         }
         if (live) {
             for (int c = 0; c < sink.nc; ++c) {
