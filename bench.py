@@ -37,9 +37,10 @@ FLOPS = {"samples": 330, "valid_samples": 95, "splat_tests": 22, "weights": 32, 
          "frames": 115, "steps": 1150}
 SFU = {"samples": 12, "valid_samples": 9, "splat_tests": 2, "weights": 1, "coefficients": 22, "frames": 4, "steps": 12}
 # k_consume's DRAM traffic per ray-sample: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch
-# of this workload at full size (256x256, N = 1024, 3 frequencies: 2.9926e9 + 0.1260e9 B over 65536 x 1024
-# ray-samples; reads = the FP32 sample stream, 32 B per ray-sample, + the plan; writes = segment states)
-CONSUME_TRAFFIC_PER_RAY_SAMPLE = (2.992645e9 + 0.126026e9) / (65536 * 1024)
+# of this workload at full size (256x256, N = 1024, 3 frequencies: 2.1709e9 + 0.1235e9 B over 65536 x 1024
+# ray-samples; reads = the FP32 sample stream, 32 B per ray-sample, partly still in L2 after k_stream
+# writes it, + the plan; writes = segment states)
+CONSUME_TRAFFIC_PER_RAY_SAMPLE = (2.170923e9 + 0.123528e9) / (65536 * 1024)
 
 
 def rank_info():
