@@ -847,10 +847,10 @@ k_adj_steps(Spacetime st, MixedJob job, const double* __restrict__ cnu, const do
 // The element phase: every block work unit visits its samples (in order, all threads together); the
 // threads with an active sample test the splats against the support, the passing (thread, splat)
 // pairs of up to kGroupWords candidate words go into one block list and are evaluated NT at a time
-// with the sample's c-bar (read back from gstate), and every warp sums the 21 rows of its own
-// threads' pairs per splat, in list order, into its accumulator (the same pairs in the same order as
-// a warp-private list: the per-unit partial sums do not depend on the pooling); each warp unit writes
-// its partial sums to gunit.
+// with the sample's c-bar (read back from gstate); every warp then sums the 21 rows of the 32 pairs
+// its own lanes evaluated, per splat in list order, into its accumulator (a fixed partition of the
+// list: deterministic sums, no block barrier inside a round); each warp unit writes its partial sums
+// to gunit, and the units are added in a fixed order.
 template <int CH, int NT>
 __global__ void __launch_bounds__(NT, 1)
 k_adj_elements(Spacetime st, MixedJob job, const float* __restrict__ tab32, const double* __restrict__ gtab, int ntot,
