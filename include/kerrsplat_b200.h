@@ -261,7 +261,26 @@ int ks_render_graph_capture(ks_context* ctx, const ks_splat_set* sets, int32_t n
  * bounded wait gave up, KS_ERR_TIMEOUT). */
 int ks_graph_launch(ks_context* ctx, int32_t wait);
 
-/* Release the captured graph. */
+/* CUDA graph of one mixed chi^2 + gradient evaluation (chi2_gradient!, Fit.jl:502-534, with chi^2 and
+ * its seeds kept on the device as Fit.jl:515-519 would need; no counterpart for the capture itself):
+ * records the device work of ks_chi2_gradient(..., KS_MIXED, ...) for device-resident thermal sets and
+ * device-resident data, sigma (or the scalar sigma), mask, chi2 (one double) and dparams. That work is
+ * the splat and gradient tables from the parameters, the sample stream, the forward pass with the
+ * reverse pass's state, chi^2 and its seeds, the reverse pass, the fixed-order reduction into dparams
+ * (added when accumulate != 0) and chi^2 into `chi2`. The call first evaluates once the ordinary way,
+ * which writes chi2 and dparams. Frames, frequencies, L, nmax, slab, the splat counts and all pointers
+ * are fixed at capture; every replay re-reads the parameters and the data. One such graph per context;
+ * a new capture releases the previous one, and so do ks_graph_destroy and a new ks_regenerate. */
+int ks_chi2_gradient_graph_capture(ks_context* ctx, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes,
+                                   const double* nus, int32_t nfreq, double L, int32_t nmax, double slab, const double* data,
+                                   const double* sigma, double sigma_scalar, const uint8_t* mask, double* chi2, double* dparams,
+                                   int32_t accumulate);
+
+/* Replay the captured chi^2 + gradient evaluation on the context stream; wait != 0 synchronises (and
+ * reports a kernel whose bounded wait gave up, KS_ERR_TIMEOUT). */
+int ks_chi2_gradient_graph_launch(ks_context* ctx, int32_t wait);
+
+/* Release the captured graphs (the render's and the chi^2 + gradient evaluation's). */
 int ks_graph_destroy(ks_context* ctx);
 
 /* Test hook for the bounded waits (no reference counterpart): while on != 0, the mixed kernels arm

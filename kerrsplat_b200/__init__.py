@@ -23,7 +23,7 @@ from ._lib import KS_FP64, KS_MIXED, KS_MIXED_GEO64, KsError
 
 __all__ = [
     "Camera", "GeodesicCache", "Fused", "Recurrence", "regenerate", "thin_image", "thin_image_sorted",
-    "polarized_image", "polarized_cube", "render", "capture_render", "RenderGraph", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "RIAFModel", "riaf_image", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
+    "polarized_image", "polarized_cube", "render", "capture_render", "RenderGraph", "capture_chi2_gradient", "Chi2GradientGraph", "KnotSplats", "adjoint", "chi2_gradient", "sweep_passes", "sample_adjoint", "jvp", "normal_matrix", "spacetime_derivatives", "vis_chi2_gradient", "autotune", "thin_image_noalloc", "RIAFModel", "riaf_image", "visibilities", "vis_seed", "frame_chi2_seed", "PolarizedSplats", "PowerLawSplats", "KappaSplats",
     "CompositeModel", "to_screen", "unsort", "gravitational_radius", "flux_density", "pixel_solid_angle",
     "KS_FP64", "KS_MIXED", "KS_MIXED_GEO64", "KsError", "NU0",
 ]
@@ -476,6 +476,46 @@ def capture_render(cache, model, times, nus, L, out=None, nmax=-1, slab=0.0, ord
     if out is None:
         out = _out_like(model.sets()[0].params, (nf, nt, cache.npix, 4))
     return RenderGraph(cache, model, times, nus, L, out, nmax, slab, order)
+
+
+class Chi2GradientGraph:
+    """One mixed chi^2 + gradient evaluation captured as a CUDA graph (ks_chi2_gradient_graph_capture):
+    replay() recomputes chi2 (a one-element device tensor) and dparams (a device tensor laid out as
+    chi2_gradient's dparams) from the current values of the model's device parameter buffers,
+    model.sets()[i].params, and of the data. The fit loop's evaluation with no host work: update the
+    parameters in place on the device, replay, read chi2 and dparams on the device."""
+
+    def __init__(self, cache, model, times, nus, L, data, sigma, mask, chi2, dparams, nmax, slab, accumulate):
+        self.cache, self.model, self.chi2, self.dparams = cache, model, chi2, dparams
+        times = _as_f64(np.atleast_1d(times) if not hasattr(times, "data_ptr") else times)
+        nus = _as_f64(np.atleast_1d(nus) if not hasattr(nus, "data_ptr") else nus)
+        self._keep = [data, sigma, mask]
+        arr, nsets, self._keep_sets = _set_array(model)
+        sg, ss = (None, float(sigma)) if np.isscalar(sigma) else (sigma, 0.0)
+        cache._check(cache._lib.ks_chi2_gradient_graph_capture(
+            cache._ctx, arr, nsets, _ptr(times), int(times.shape[0]), _ptr(nus), int(nus.shape[0]), float(L), int(nmax), float(slab),
+            _ptr(data), _ptr(sg) if sg is not None else None, ss, _ptr(mask) if mask is not None else None, _ptr(chi2), _ptr(dparams),
+            int(bool(accumulate))))
+
+    def replay(self, wait=True):
+        self.cache._check(self.cache._lib.ks_chi2_gradient_graph_launch(self.cache._ctx, int(bool(wait))))
+        return self.chi2, self.dparams
+
+    def close(self):
+        self.cache._check(self.cache._lib.ks_graph_destroy(self.cache._ctx))
+
+
+def capture_chi2_gradient(cache, model, times, nus, L, data, sigma, mask=None, nmax=-1, slab=0.0, accumulate=False):
+    """Capture one mixed chi^2 + gradient evaluation of a device-resident thermal model against
+    device-resident data (torch CUDA tensors; sigma a tensor of data's shape or a scalar, mask uint8
+    (nfreq, nframes, npix)). Returns a Chi2GradientGraph whose replay() fills its `chi2` (one float64)
+    and `dparams` (sum of 21 x nsplat per set, float64) tensors on the device."""
+    import torch
+    dev = data.device
+    ntot = sum(s.nsplat for s in model.sets())
+    chi2 = torch.zeros(1, dtype=torch.float64, device=dev)
+    dparams = torch.zeros(21 * ntot, dtype=torch.float64, device=dev)
+    return Chi2GradientGraph(cache, model, times, nus, L, data, sigma, mask, chi2, dparams, nmax, slab, accumulate)
 
 
 def _grad_like(model):

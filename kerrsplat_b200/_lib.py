@@ -97,6 +97,10 @@ EXTRA_SIGNATURES = [
     ("ks_render_graph_capture", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32,
                                                ctypes.c_double, ctypes.c_int32, ctypes.c_double, _VP, ctypes.c_int32]),
     ("ks_graph_launch", ctypes.c_int, [_VP, ctypes.c_int32]),
+    ("ks_chi2_gradient_graph_capture", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP,
+                                                      ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_double, _VP, _VP,
+                                                      ctypes.c_double, _VP, _VP, _VP, ctypes.c_int32]),
+    ("ks_chi2_gradient_graph_launch", ctypes.c_int, [_VP, ctypes.c_int32]),
     ("ks_graph_destroy", ctypes.c_int, [_VP]),
     ("ks_autotune", ctypes.c_int, [_VP, ctypes.POINTER(SplatSetC), ctypes.c_int32, _VP, ctypes.c_int32, _VP, ctypes.c_int32, ctypes.c_double,
                                    ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),

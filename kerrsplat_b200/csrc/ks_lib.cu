@@ -860,6 +860,9 @@ struct ks_context {
     DevBuf errflag;   // set by a kernel whose bounded wait gave up
     cudaGraph_t graph = nullptr;          // ks_render_graph_capture: one mixed render of device-resident sets
     cudaGraphExec_t graph_exec = nullptr;
+    cudaGraph_t cgraph = nullptr;         // ks_chi2_gradient_graph_capture: one mixed chi^2 + gradient evaluation
+    cudaGraphExec_t cgraph_exec = nullptr;
+    std::vector<void*> cgraph_bufs;
     bool capturing = false;               // inside that capture: no timing events
     int stage_test = 0;                   // ks_set_stage_test
     std::vector<void*> graph_bufs;        // the buffers the graph uses, as captured (a replay checks them)
@@ -1121,7 +1124,7 @@ int launch_consume(ks_context* c, const MixedJob& job0, int ntot, int nsm, int p
     c->last_job = job;
     const size_t seg_bytes = size_t(job.nframes) * job.nfreq * job.nseg * c->npix * 20 * sizeof(float);
     KS_CUDA(c, c->seg_out.ensure(seg_bytes));
-    KS_CUDA(c, c->work.ensure(sizeof(unsigned long long)));
+    KS_CUDA(c, c->work.ensure(2 * sizeof(unsigned long long)));   // the adjoint's two counters: no move under a captured render
     KS_CUDA(c, cudaMemsetAsync(c->work.p, 0, sizeof(unsigned long long), c->stream));
     const long long grid = std::min<long long>(job.total / W + 1, (long long)nsm * per_sm);
     if (!c->capturing) cudaEventRecord(c->evc0, c->stream);
@@ -1626,7 +1629,9 @@ int ks_render(ks_context* c, const ks_splat_set* sets, int32_t nsets, const doub
         hc.assign(ht.begin(), ht.end());
         hc.insert(hc.end(), hnu.begin(), hnu.end());
     }
-    KS_CUDA(c, c->combos.ensure(hc.size() * sizeof(double)));
+    // sized for the adjoint's layout too (times, frequencies, then per combination), so that an
+    // adjoint call does not move the buffer under a captured render
+    KS_CUDA(c, c->combos.ensure((size_t(nframes) + nfreq + 2 * size_t(ncombo)) * sizeof(double)));
     KS_CUDA(c, cudaMemcpyAsync(c->combos.p, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     KS_CUDA(c, c->out_sorted.ensure(size_t(n) * 4 * ncombo * sizeof(double)));
     const double* dct = c->combos.as<double>();
@@ -1726,6 +1731,49 @@ std::vector<void*> graph_buffers(const ks_context* c) {
             c->perm.p, c->plan.p, c->anchors.p, c->aoff.p};
 }
 
+void release_graph(cudaGraph_t& g, cudaGraphExec_t& ex) {
+    if (ex) cudaGraphExecDestroy(ex);
+    if (g) cudaGraphDestroy(g);
+    ex = nullptr;
+    g = nullptr;
+}
+
+// ... and those of a captured chi^2 + gradient evaluation
+std::vector<void*> chi2_graph_buffers(const ks_context* c) {
+    std::vector<void*> b = graph_buffers(c);
+    for (const DevBuf* d : {&c->gtab, &c->adj_state, &c->adj_act, &c->adj_bnd, &c->adj_unit, &c->adj_part, &c->seeds, &c->chi_part,
+                            &c->chi_val, &c->dgrad})
+        b.push_back(d->p);
+    return b;
+}
+
+// The splat tables of device-resident sets rebuilt on the device inside a capture (the knot array
+// stays as the ordinary call before the capture wrote it): k_splat_table per set, with grad the
+// gradient table (k_grad_table), and the FP32 copy.
+int capture_tables(ks_context* c, const ks_splat_set* sets, int nsets, int ntot, bool grad) {
+    int first = 0, koff = 0;
+    for (int s = 0; s < nsets; ++s) {
+        const ks_splat_set& S = sets[s];
+        if (S.nsplat == 0) continue;
+        const int nk = S.kind == KS_KNOT21 ? S.nknots : 0;
+        SetDesc d{S.kind, nrows_of(S.kind), S.nsplat, first, static_cast<const double*>(S.params),
+                  S.kind == KS_KAPPA22 ? static_cast<const double*>(S.hyp) : nullptr, S.gamma_max > 0 ? S.gamma_max : 1e5,
+                  S.kind == KS_KNOT21 ? koff : 0, nk,
+                  c->tab.as<const double>() + size_t(ntot) * ST_COUNT};
+        k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
+        if (grad) k_grad_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(S.nsplat, first, static_cast<const double*>(S.params),
+                                                                           c->gtab.as<double>());
+        if (cudaGetLastError() != cudaSuccess) return fail(c, KS_ERR_DEVICE, "graph capture: splat table of set %d", s);
+        first += S.nsplat;
+        koff += S.nsplat * 4 * nk;   // per knot splat: its nk times and 3 nk centres
+    }
+    const long long nv = (long long)ntot * ST_COUNT + c->nkv;
+    const long long np4 = std::max<long long>(4, (nv + 3) / 4 * 4);
+    k_tab_f32<<<nblocks(np4, 256), 256, 0, c->stream>>>(nv, np4, c->tab.as<double>(), c->tab32.as<float>());
+    if (cudaGetLastError() != cudaSuccess) return fail(c, KS_ERR_DEVICE, "graph capture: FP32 table");
+    return KS_OK;
+}
+
 // One mixed render of device-resident splat sets recorded into a CUDA graph: the splat tables built
 // from the parameters (in place on the device), their FP32 copy, the sample stream, the consumer, the
 // segment composition and the output in `order`. Frames, frequencies, L, the knot array, the splat
@@ -1740,7 +1788,7 @@ int ks_render_graph_capture(ks_context* c, const ks_splat_set* sets, int32_t nse
         if (sets[s].kind == KS_KAPPA22 && sets[s].nsplat > 0 && !is_device_ptr(sets[s].hyp))
             return fail(c, KS_ERR_ARGUMENT, "set %d: a graph reads device-resident hyp", s);
     }
-    ks_graph_destroy(c);
+    release_graph(c->graph, c->graph_exec);
     const bool counting = c->count_events;
     c->count_events = false;
     // one ordinary render: validation, tables and knots, buffers, the launch shape
@@ -1755,26 +1803,7 @@ int ks_render_graph_capture(ks_context* c, const ks_splat_set* sets, int32_t nse
     }
     KS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
     c->capturing = true;
-    int first = 0, koff = 0;
-    for (int s = 0; s < nsets && status == KS_OK; ++s) {
-        const ks_splat_set& S = sets[s];
-        if (S.nsplat == 0) continue;
-        const int nk = S.kind == KS_KNOT21 ? S.nknots : 0;
-        SetDesc d{S.kind, nrows_of(S.kind), S.nsplat, first, static_cast<const double*>(S.params),
-                  S.kind == KS_KAPPA22 ? static_cast<const double*>(S.hyp) : nullptr, S.gamma_max > 0 ? S.gamma_max : 1e5,
-                  S.kind == KS_KNOT21 ? koff : 0, nk,
-                  c->tab.as<const double>() + size_t(ntot) * ST_COUNT};
-        k_splat_table<<<nblocks(S.nsplat, 64), 64, 0, c->stream>>>(d, c->tab.as<double>());
-        if (cudaGetLastError() != cudaSuccess) status = fail(c, KS_ERR_DEVICE, "graph capture: splat table of set %d", s);
-        first += S.nsplat;
-        koff += S.nsplat * 4 * nk;   // per knot splat: its nk times and 3 nk centres
-    }
-    if (status == KS_OK) {
-        const long long nv = (long long)ntot * ST_COUNT + c->nkv;
-        const long long np4 = std::max<long long>(4, (nv + 3) / 4 * 4);
-        k_tab_f32<<<nblocks(np4, 256), 256, 0, c->stream>>>(nv, np4, c->tab.as<double>(), c->tab32.as<float>());
-        if (cudaGetLastError() != cudaSuccess) status = fail(c, KS_ERR_DEVICE, "graph capture: FP32 table");
-    }
+    status = capture_tables(c, sets, nsets, ntot, false);
     if (status == KS_OK) status = launch_mixed(c, ntot, nullptr, nframes, nfreq, L, nmax, slab, thermal_only);
     if (status == KS_OK) status = emit(c, c->out_sorted.as<double>(), 4, nframes * nfreq, order, out);
     cudaGraph_t g = nullptr;
@@ -1814,10 +1843,8 @@ int ks_graph_launch(ks_context* c, int32_t wait) {
 
 int ks_graph_destroy(ks_context* c) {
     if (!c) return KS_ERR_ARGUMENT;
-    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    if (c->graph) cudaGraphDestroy(c->graph);
-    c->graph_exec = nullptr;
-    c->graph = nullptr;
+    release_graph(c->graph, c->graph_exec);
+    release_graph(c->cgraph, c->cgraph_exec);
     return KS_OK;
 }
 
@@ -2207,6 +2234,104 @@ int ks_chi2_gradient(ks_context* c, const ks_splat_set* sets, int32_t nsets, con
     if (!c || !data) return KS_ERR_ARGUMENT;
     return adjoint_run(c, sets, nsets, times, nframes, nus, nfreq, L, precision, nmax, slab, nullptr, KS_ORDER_SCREEN, data, sigma,
                        sigma_scalar, mask, chi2, dparams, accumulate, image);
+}
+
+// One mixed chi^2 + gradient evaluation of device-resident thermal sets against device-resident
+// image-domain data, recorded into a CUDA graph: the splat and gradient tables from the parameters,
+// the sample stream, the forward pass with the reverse pass's state, chi^2 and its seeds, the reverse
+// pass, the fixed-order reduction into dparams, chi^2 into `chi2`. It runs one ordinary evaluation
+// first (validation, buffers, launch shapes), which writes chi2 and dparams as ks_chi2_gradient does.
+int ks_chi2_gradient_graph_capture(ks_context* c, const ks_splat_set* sets, int32_t nsets, const double* times, int32_t nframes,
+                                   const double* nus, int32_t nfreq, double L, int32_t nmax, double slab, const double* data,
+                                   const double* sigma, double sigma_scalar, const uint8_t* mask, double* chi2, double* dparams,
+                                   int32_t accumulate) {
+    if (!c || !sets || nsets < 1 || !data || !chi2 || !dparams) return KS_ERR_ARGUMENT;
+    if (!is_device_ptr(data) || (sigma && !is_device_ptr(sigma)) || (mask && !is_device_ptr(mask)) || !is_device_ptr(chi2) ||
+        !is_device_ptr(dparams))
+        return fail(c, KS_ERR_ARGUMENT, "a captured chi^2 + gradient reads and writes device memory only (data, sigma, mask, chi2, dparams)");
+    for (int s = 0; s < nsets; ++s)
+        if (sets[s].nsplat > 0 && !is_device_ptr(sets[s].params))
+            return fail(c, KS_ERR_ARGUMENT, "set %d: a graph reads device-resident parameters", s);
+    release_graph(c->cgraph, c->cgraph_exec);
+    const bool counting = c->count_events;
+    c->count_events = false;
+    int status = adjoint_run(c, sets, nsets, times, nframes, nus, nfreq, L, KS_MIXED, nmax, slab, nullptr, KS_ORDER_SCREEN, data, sigma,
+                             sigma_scalar, mask, chi2, dparams, accumulate, nullptr);
+    c->count_events = counting;
+    if (status) return status;
+    int ntot = 0;
+    for (int s = 0; s < nsets; ++s) ntot += sets[s].nsplat;
+    const long long n = c->npix;
+    const int ncombo = nframes * nfreq;
+    const long long nrc = n * ncombo;
+    const long long nblk = (nrc + 255) / 256;
+    const size_t rows = size_t(ncombo) * c->st.N * c->npad;
+    const double* dtimes = c->combos.as<double>();   // as the ordinary evaluation wrote them
+    const double* dfreqs = dtimes + nframes;
+    const int ch = c->last_job.ch;
+    KS_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    c->capturing = true;
+    status = capture_tables(c, sets, nsets, ntot, true);
+    if (status == KS_OK && ntot > 0) {
+        // the forward pass with the reverse pass's state
+        c->geo64 = false;
+        if (cudaMemsetAsync(c->adj_act.p, 0, rows, c->stream) != cudaSuccess) status = fail(c, KS_ERR_DEVICE, "graph capture: activity reset");
+        c->fwd_gstate = c->adj_state.as<float>();
+        c->fwd_gact = c->adj_act.as<unsigned char>();
+        if (status == KS_OK) status = launch_mixed(c, ntot, nullptr, nframes, nfreq, L, nmax, slab, true);
+        c->fwd_gstate = nullptr;
+        c->fwd_gact = nullptr;
+    }
+    if (status == KS_OK) {
+        k_chi2_seed<<<unsigned(nblk), 256, 0, c->stream>>>(c->out_sorted.as<double>(), c->perm.as<long long>(), n, ncombo, data, sigma,
+                                                           sigma_scalar, mask, c->seeds.as<double>(), c->chi_part.as<double>());
+        k_sum_partials<<<1, 256, 0, c->stream>>>(c->chi_part.as<double>(), nblk, c->chi_val.as<double>());
+        if (cudaGetLastError() != cudaSuccess) status = fail(c, KS_ERR_DEVICE, "graph capture: chi^2 seeds");
+    }
+    if (status == KS_OK && ntot > 0)
+        status = ch == 4 ? launch_adjoint_mixed_ch<4>(c, ntot, dtimes, dfreqs)
+                         : (ch == 3 ? launch_adjoint_mixed_ch<3>(c, ntot, dtimes, dfreqs)
+                                    : (ch == 2 ? launch_adjoint_mixed_ch<2>(c, ntot, dtimes, dfreqs) : launch_adjoint_mixed_ch<1>(c, ntot, dtimes, dfreqs)));
+    const long long ng = (long long)ntot * GR_COUNT;
+    if (status == KS_OK && ng > 0) {
+        k_accumulate<<<nblocks(ng, 256), 256, 0, c->stream>>>(dparams, c->dgrad.as<double>(), ng, accumulate);
+        if (cudaGetLastError() != cudaSuccess) status = fail(c, KS_ERR_DEVICE, "graph capture: gradient");
+    }
+    if (status == KS_OK && cudaMemcpyAsync(chi2, c->chi_val.p, sizeof(double), cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+        status = fail(c, KS_ERR_DEVICE, "graph capture: chi^2");
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    c->capturing = false;
+    if (status != KS_OK || ec != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return status != KS_OK ? status : fail(c, KS_ERR_DEVICE, "graph capture: %s", cudaGetErrorString(ec));
+    }
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ex, g, 0);
+    if (ei != cudaSuccess) {
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        return fail(c, KS_ERR_DEVICE, "graph instantiation: %s", cudaGetErrorString(ei));
+    }
+    c->cgraph = g;
+    c->cgraph_exec = ex;
+    c->cgraph_bufs = chi2_graph_buffers(c);
+    return KS_OK;
+}
+
+// Replay the captured chi^2 + gradient evaluation on the context stream; with wait, synchronise and
+// report a kernel whose bounded wait gave up.
+int ks_chi2_gradient_graph_launch(ks_context* c, int32_t wait) {
+    if (!c) return KS_ERR_ARGUMENT;
+    if (!c->cgraph_exec) return fail(c, KS_ERR_ARGUMENT, "no captured chi^2 + gradient graph");
+    if (chi2_graph_buffers(c) != c->cgraph_bufs)
+        return fail(c, KS_ERR_ARGUMENT, "a later call reallocated buffers the graph uses: capture again");
+    KS_CUDA(c, cudaGraphLaunch(c->cgraph_exec, c->stream));
+    c->launches++;
+    if (!wait) return KS_OK;
+    KS_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_device_flag(c, "chi^2 + gradient graph replay");
 }
 
 }  // extern "C"

@@ -421,3 +421,46 @@ def test_crowded_pair_lists():
     assert e < 1e-4
     assert abs(chi32 - chi64) <= 1e-3 * chi64
     assert rel_l2(g32, g64) < 1e-3
+
+
+def test_chi2_gradient_graph_replays_and_follows_parameters():
+    """ks_chi2_gradient_graph_capture / ks_chi2_gradient_graph_launch: a mixed chi^2 + gradient of a
+    device-resident thermal set against device-resident data, captured as a CUDA graph, replays to
+    ks_chi2_gradient's chi^2 and gradient bit for bit. After an in-place change of the model's
+    parameter buffer it replays to the new evaluation. A captured render survives the chi^2 capture,
+    and a regenerate drops both graphs."""
+    import torch
+    c = scenes.config2(res=24, N=96)
+    rng = np.random.Generator(np.random.PCG64(41))
+    p = scenes.thermal_params(rng, 6, c["a"])
+    cache = ks.GeodesicCache(c["camera"], c["N"])
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    nus, times = [230e9, 345e9], [0.0]
+    target = np.asarray(ks.render(cache, ks.PolarizedSplats(p * 1.02), times, nus, c["L"], precision=ks.KS_MIXED))
+    sigma = 0.01 * float(np.abs(target[..., 0]).max())
+    data = torch.tensor(target + sigma * rng.standard_normal(target.shape), device="cuda")
+    model = ks.PolarizedSplats(torch.tensor(p, device="cuda"))
+    rg = ks.capture_render(cache, model, times, nus, c["L"])
+
+    def direct():
+        buf = torch.zeros(21 * p.shape[1], dtype=torch.float64, device="cuda")
+        chi2, _ = ks.chi2_gradient(cache, model, times, nus, c["L"], data, sigma, precision=ks.KS_MIXED, dparams=buf)
+        return chi2, buf.cpu().numpy()
+
+    g = ks.capture_chi2_gradient(cache, model, times, nus, c["L"], data, sigma)
+    chi_ref, g_ref = direct()
+    assert np.abs(g_ref).max() > 0
+    chi2, dp = g.replay()
+    assert float(chi2.item()) == chi_ref and np.array_equal(dp.cpu().numpy(), g_ref)
+    model.sets()[0].params[:, 12] += np.log(1.2)   # the log densities, in place
+    chi_ref2, g_ref2 = direct()
+    assert chi_ref2 != chi_ref
+    chi2, dp = g.replay()
+    assert float(chi2.item()) == chi_ref2 and np.array_equal(dp.cpu().numpy(), g_ref2)
+    rg.replay()   # the render graph is still there
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    with pytest.raises(ValueError, match="no captured chi"):
+        g.replay()
+    with pytest.raises(ValueError, match="no captured graph"):
+        rg.replay()
+    cache.close()
