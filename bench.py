@@ -321,6 +321,22 @@ def chi2_grad_bench(args, cache, c, dev, stream, world):
            "parameters": int(c["params"].size), "chi2": float(chi2_h),
            "e2e": {"value": world * 1e3 / e2e_ms, "ms_per_eval": e2e_ms, "h2d_bytes_per_step": int(data.nbytes + c["params"].nbytes),
                    "d2h_bytes_per_step": int(c["params"].nbytes + 8)}}
+    # the same evaluation captured as a CUDA graph (device-resident model and data) and replayed
+    try:
+        cg = ks.capture_chi2_gradient(cache, model, times, nus, c["L"], data_dev, sigma)
+        cg.replay()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(steps):
+            cg.replay(wait=False)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        cg.replay(wait=True)
+        gms = max_over_ranks(e0.elapsed_time(e1) / steps, dev)
+        out["graph"] = {"value": world * 1e3 / gms, "ms_per_eval": gms, "chi2": float(cg.chi2.item())}
+        cg.close()
+    except Exception as exc:   # reported, not fatal
+        out["graph"] = {"error": str(exc)}
     if args.fp64_steps > 0:
         step(ks.KS_FP64)   # stored samples are built on the first FP64 call after a regenerate
         torch.cuda.synchronize(dev)
