@@ -17,11 +17,11 @@ frame's baselines in order, 8 values per baseline: Re and Im of the gained, nois
 """
 import numpy as np
 
-from . import (KS_FP64, KS_MIXED, PolarizedSplats, adjoint, chi2_gradient, jvp as image_jvp, render, vis_chi2_gradient, vis_seed,
-               visibilities)
+from . import (KS_FP64, KS_MIXED, PolarizedSplats, adjoint, capture_chi2_gradient, chi2_gradient, jvp as image_jvp, render,
+               vis_chi2_gradient, vis_seed, visibilities)
 
 __all__ = ["FrameScans", "BandScans", "timeresolved_gradient", "residuals", "jvp", "jtvp", "normal_diagonal", "lsqr", "lsqr_step",
-           "polish_timeresolved", "dual_valgrad", "Adam", "fit"]
+           "polish_timeresolved", "dual_valgrad", "GraphValgrad", "Adam", "fit"]
 
 
 class FrameScans:
@@ -289,6 +289,35 @@ def dual_valgrad(cache, params, times, nus, L, data, sigma, mask=None, precision
     _frame_seed! round trip). Returns (chi2, grad (21, nsplat))."""
     chi, g = chi2_gradient(cache, PolarizedSplats(params), times, nus, L, data, sigma, mask=mask, nmax=nmax, slab=slab, precision=precision)
     return chi, np.asarray(g)
+
+
+class GraphValgrad:
+    """dual_valgrad with the mixed evaluation captured once as a CUDA graph (capture_chi2_gradient):
+    each call writes the parameters into the model's device buffer, replays the graph, and reads
+    chi^2 and the gradient back. That is one host-to-device copy of the parameters, one replay and
+    one device-to-host copy of the gradient per evaluation, with no validation, table staging or
+    launch setup on the host. Same values as dual_valgrad(..., precision=KS_MIXED) bit for bit. The
+    data, sigma and mask are copied to the device once."""
+
+    def __init__(self, cache, params, times, nus, L, data, sigma, mask=None, nmax=-1, slab=0.0):
+        import torch
+        params = np.asarray(params, dtype=np.float64)
+        self.nsplat = params.shape[1]
+        self.model = PolarizedSplats(torch.tensor(params, device="cuda"))
+        self.data = torch.as_tensor(np.asarray(data, dtype=np.float64), device="cuda")
+        self.sigma = sigma if np.isscalar(sigma) else torch.as_tensor(np.asarray(sigma, dtype=np.float64), device="cuda")
+        self.mask = None if mask is None else torch.as_tensor(np.ascontiguousarray(mask, dtype=np.uint8), device="cuda")
+        self.graph = capture_chi2_gradient(cache, self.model, times, nus, L, self.data, self.sigma, mask=self.mask, nmax=nmax, slab=slab)
+
+    def __call__(self, params):
+        import torch
+        # the model's device buffer is the column-major copy: (nsplat, 21) row-major
+        self.model.sets()[0].params.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(params, dtype=np.float64).T)))
+        chi2, dp = self.graph.replay()
+        return float(chi2.item()), dp.cpu().numpy().reshape(self.nsplat, 21).T.copy()
+
+    def close(self):
+        self.graph.close()
 
 
 class Adam:

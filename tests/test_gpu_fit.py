@@ -124,3 +124,27 @@ def test_polish_and_adam_lower_chi2(problem):
     q, hist2 = fit.fit(vg, p, iterations=40, lr=0.02, scale=sc)
     print("adam chi2", hist2[0], hist2[-1])
     assert hist2[-1] < 0.2 * hist2[0]
+
+
+def test_graph_valgrad_matches_dual_valgrad(problem):
+    """fit.GraphValgrad (the evaluation captured once, replayed per call) against fit.dual_valgrad with
+    the mixed path: the same chi^2 and gradient bit for bit at the starting parameters. Ten Adam steps
+    on each follow the same trajectory."""
+    s = problem
+    p, L, cache = s["p"], s["L"], s["cache"]
+    truth = p.copy()
+    truth[12] += 0.2
+    data = np.asarray(ks.render(cache, ks.PolarizedSplats(truth), [0.0], [230e9], L, precision=ks.KS_FP64))
+    sigma = 0.01 * np.abs(data[..., 0]).max()
+    direct = lambda q: fit.dual_valgrad(cache, q, [0.0], [230e9], L, data, sigma, precision=ks.KS_MIXED)
+    graph = fit.GraphValgrad(cache, p, [0.0], [230e9], L, data, sigma)
+    c0, g0 = direct(p)
+    c1, g1 = graph(p)
+    assert c1 == c0 and g1.shape == g0.shape and np.array_equal(g1, g0)
+    sc = np.zeros_like(p)
+    sc[12] = 1.0
+    qa, ha = fit.fit(direct, p, iterations=10, lr=0.02, scale=sc)
+    qb, hb = fit.fit(graph, p, iterations=10, lr=0.02, scale=sc)
+    assert np.array_equal(np.asarray(ha), np.asarray(hb)) and np.array_equal(qa, qb)
+    assert hb[-1] < hb[0]
+    graph.close()
