@@ -569,6 +569,128 @@ def run_dft(args):
     cache.close()
 
 
+def run_shards(args):
+    """Configuration 3's chi^2 + gradient with the rays sharded over ranks (kerrsplat_b200.shard): each
+    rank regenerates and evaluates its own rays, then one all-reduce of [chi^2, dparams] (1345 FP64).
+    Under torchrun every rank evaluates its shard and the step time (evaluation + all-reduce) is the
+    max over ranks. On one process the shards of 2, 4 and 8 ranks run one after another on this GPU:
+    each shard's evaluation is timed with CUDA events (data already on the device), and the largest
+    one against the whole screen's time / ranks is the load balance of that partition; the sums of
+    the shards' chi^2 and gradients are checked against the whole screen's."""
+    import torch
+    import kerrsplat_b200 as ks
+    from kerrsplat_b200 import build, scenes
+    from kerrsplat_b200.shard import RayShard, allreduce_sum
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    build.build(verbose=False)
+    c = scenes.config2(res=args.res, N=args.nsamples)
+    cache = ks.GeodesicCache(c["camera"], c["N"], device=local)
+    ks.regenerate(cache, c["a"], c["theta_o"])
+    pt, rng = scenes.config3_target(c["params"])
+    target = np.asarray(ks.render(cache, ks.PolarizedSplats(pt), [c["t_obs"]], c["nus"], c["L"], precision=ks.KS_MIXED))
+    sigma = 0.01 * float(np.abs(target[..., 0]).max())
+    data = torch.tensor(target + sigma * rng.standard_normal(target.shape), device=dev)
+    model = ks.PolarizedSplats(torch.tensor(c["params"], device=dev))
+    times, nus = [c["t_obs"]], c["nus"]
+    steps = max(1, min(args.steps, 10))
+    nparam = c["params"].size
+
+    def timed(sh_cache, d):
+        # the timed calls add into one buffer; the checked gradient comes from a call on a zeroed one
+        # (buffers written on torch's stream are waited for before the library's stream reads them)
+        acc = torch.zeros(nparam, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        for _ in range(max(1, args.warmup)):
+            ks.chi2_gradient(sh_cache, model, times, nus, c["L"], d, sigma, precision=ks.KS_MIXED, dparams=acc)
+        stream = torch.cuda.ExternalStream(sh_cache.stream(), device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(steps):
+            ks.chi2_gradient(sh_cache, model, times, nus, c["L"], d, sigma, precision=ks.KS_MIXED, dparams=acc)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        grad = torch.zeros(nparam, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        chi2, _ = ks.chi2_gradient(sh_cache, model, times, nus, c["L"], d, sigma, precision=ks.KS_MIXED, dparams=grad)
+        return e0.elapsed_time(e1) / steps, chi2, grad.cpu().numpy()
+
+    full_ms, full_chi2, full_g = timed(cache, data)
+    line = {"metric": "chi^2+grad evals/s (rays sharded over ranks)", "unit": "evals/s", "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded PCG64 scene, cfg 3 target)",
+            "config": {"workload": f"config 3: {args.res}x{args.res}, N={args.nsamples}, 64 thermal splats, 86/230/345 GHz, 1344 parameters",
+                       "l2": "no flush: the per-ray plan + anchor table exceeds the 126 MB L2 at 256x256"}}
+    if world > 1:
+        import torch.distributed as dist
+        sh = RayShard(c["camera"], c["N"], c["a"], c["theta_o"], rank=rank, world=world, device=local)
+        d = sh.take(data, 2)
+        if sh.cache is None:
+            raise RuntimeError("empty shard")
+        g = torch.zeros(1 + nparam, dtype=torch.float64, device=dev)
+
+        def step():
+            # [chi^2, dparams] of this rank's rays, then the sum over ranks (the library's call returns
+            # after its stream finishes; the all-reduce follows on torch's stream)
+            g.zero_()
+            torch.cuda.current_stream(dev).synchronize()
+            chi2, _ = ks.chi2_gradient(sh.cache, model, times, nus, c["L"], d, sigma, precision=ks.KS_MIXED, dparams=g[1:])
+            g[0] = chi2
+            dist.all_reduce(g, op=dist.ReduceOp.SUM)
+        for _ in range(max(1, args.warmup)):
+            step()
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        stream = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        dist.barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, dev)
+        gv = g.cpu().numpy()
+        line.update({"value": 1e3 / ms, "ms_per_step": ms, "whole_screen_one_gpu_ms": full_ms,
+                     "chi2_rel_vs_one_gpu": abs(gv[0] - full_chi2) / full_chi2,
+                     "grad_rel_vs_one_gpu": float(np.linalg.norm(gv[1:] - full_g) / np.linalg.norm(full_g))})
+        sh.close()
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        dist.barrier()
+        dist.destroy_process_group()
+        cache.close()
+        return
+    emulated = {}
+    for w in (2, 4, 8):
+        for layout in ("contiguous", "strided"):
+            per, chi2s, gsum = [], 0.0, np.zeros_like(full_g)
+            for r in range(w):
+                sh = RayShard(c["camera"], c["N"], c["a"], c["theta_o"], rank=r, world=w, layout=layout, device=local)
+                ms_r, chi2_r, g_r = timed(sh.cache, sh.take(data, 2))
+                per.append(ms_r)
+                chi2s += chi2_r
+                gsum += g_r
+                sh.close()
+            vec = allreduce_sum(np.concatenate([[chi2s], gsum]))   # one process: the identity
+            emulated[f"{w}/{layout}"] = {"shard_ms": [round(x, 3) for x in per], "max_shard_ms": max(per),
+                                         "balance": max(per) / (full_ms / w), "sum_shard_ms": sum(per),
+                                         "chi2_rel": abs(vec[0] - full_chi2) / full_chi2,
+                                         "grad_rel": float(np.linalg.norm(vec[1:] - full_g) / np.linalg.norm(full_g))}
+    line.update({"value": 1e3 / full_ms, "ms_per_step": full_ms,
+                 "emulated_ranks": emulated,
+                 "note": "one GPU: each rank's shard timed alone, one after another; balance = the largest shard's time / "
+                         "(whole screen's time / ranks); a rank's step adds one all-reduce of 1345 FP64 values"})
+    print(json.dumps(line), flush=True)
+    cache.close()
+
+
 def cpu_sample(c, nrays, seed=7):
     rng = np.random.Generator(np.random.PCG64(seed))
     idx = np.sort(rng.choice(c["camera"].npix, size=min(nrays, c["camera"].npix), replace=False))
@@ -633,14 +755,16 @@ def main():
                     help="time the consumer's launch shapes before the timed steps (ks_autotune)")
     ap.add_argument("--res", type=int, default=None, help="screen resolution (default: the workload's; smaller cases for profiling)")
     ap.add_argument("--nsamples", type=int, default=None, help="samples per ray (default: the workload's)")
-    ap.add_argument("--workload", default="polarized", choices=["polarized", "movie", "fit", "dft"],
+    ap.add_argument("--workload", default="polarized", choices=["polarized", "movie", "fit", "dft", "shards"],
                     help="polarized: configurations 2 and 3 (the headline); movie: configuration 4; fit: configuration 5; "
-                         "dft: configuration 5's visibility transform on both tensor-core kernels")
+                         "dft: configuration 5's visibility transform on both tensor-core kernels; "
+                         "shards: configuration 3's chi^2 + gradient with the rays sharded over ranks")
     ap.add_argument("--sets", type=int, default=16, help="fit: parameter sets")
     ap.add_argument("--frames", type=int, default=32, help="movie frames")
     args = ap.parse_args()
     # the sizes of each workload's configuration unless given
-    dres, dn = {"polarized": (256, 1024), "movie": (512, 2048), "fit": (1024, 512), "dft": (1024, 8)}[args.workload]
+    dres, dn = {"polarized": (256, 1024), "movie": (512, 2048), "fit": (1024, 512), "dft": (1024, 8),
+                "shards": (256, 1024)}[args.workload]
     args.res = dres if args.res is None else args.res
     args.nsamples = dn if args.nsamples is None else args.nsamples
     if args.impl == "reference":
@@ -651,6 +775,8 @@ def main():
         run_fit(args)
     elif args.workload == "dft":
         run_dft(args)
+    elif args.workload == "shards":
+        run_shards(args)
     else:
         run_ours(args)
 
