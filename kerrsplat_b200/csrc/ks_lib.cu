@@ -1082,10 +1082,12 @@ int check_device_flag(ks_context* c, const char* what) {
 }
 
 // The FP32 sample stream of every ray (k_stream: the FP32 march, or the FP64 march under
-// KS_MIXED_GEO64), [k][field][npad].
+// KS_MIXED_GEO64), [k][field][npad]. Each ray is marched as up to eight segments, each starting
+// at an anchor (a multiple of M samples). At 256 x 256, N = 1024 that is 6.9 waves of 16 warps per
+// SM instead of 3.5 with four segments (the render 22.04 against 22.34 ms).
 int launch_stream(ks_context* c) {
     const int M = c->st.M, N = c->st.N;
-    const int sseg = std::max(M, (N / 4 + M - 1) / M * M);
+    const int sseg = std::max(M, (N / 8 + M - 1) / M * M);
     const int nsseg = (N + sseg - 1) / sseg;
     KS_CUDA(c, c->stream_buf.ensure(size_t(N) * SM_COUNT * c->npad * sizeof(float)));
     if (c->geo64)
